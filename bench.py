@@ -1,0 +1,362 @@
+"""Benchmark: THC-GW iteration time (and RPA E_c time) on one B200, mixed vs FP64.
+
+One step = one THC-GW iteration of the G0W0 workload
+``g0w0_k4_nb64_np512`` (4x4x4 k-grid = 64 k, 64 orbitals / 24 occupied, N_mu = 512,
+beta = 1000, IR Lambda = 1e4 "low" -> 48 tau points): Pi(tau) -> Pi(iW) -> Dyson W(iW) ->
+W(tau) -> Sigma(tau), i.e. scr_coulomb_t::update_w + gw_t::evaluate.
+
+* ``value``: device time per iteration with G resident in HBM (CUDA events on the
+  library's stream), mixed precision; ``e2e``: the same through the public C ABI with the
+  host G copied in and Sigma copied out every step (pinned host buffers).
+* ``--impl reference``: the FP64 oracle (numpy/OpenBLAS restatement of the reference
+  algorithm) on the host cores, bounded samples extrapolated to one iteration.
+* Multi-GPU (torchrun): the path does not shard; ranks run independent replicas.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "g0w0_k4_nb64_np512"
+METRIC = "THC-GW iteration time (mixed precision, 1 B200)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default=WORKLOAD)
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.rows, self.stop = device, [], threading.Event()
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_case(name):
+    from coqui_b200.iaft import IAFT
+    from coqui_b200.synthetic import WORKLOADS, make_system
+    w = WORKLOADS[name]
+    s = make_system(w["n"], w["nb"], w["nocc"], w["Np"], beta=w["beta"], seed=2024)
+    ft = IAFT(w["beta"], w["lam"] / w["beta"], w["prec"])
+    return w, s, ft
+
+
+def make_ctx(s, ft, mode):
+    from coqui_b200 import capi
+    c = capi.Context(s.nk, s.nb, s.Np, ft.nt_f, ft.nw_b, s.kp_grid, mode=mode)
+    c.set_ir(ft)
+    c.set_kmesh(s.kpts, s.lattv, s.chi_bar)
+    c.set_thc(s.X, s.V)
+    return c
+
+
+def total_ms(ctx):
+    return sum(ms for _, ms in ctx.timings())
+
+
+def gemm_flops_c(M, N, K):
+    return 8.0 * M * N * K  # complex MAC = 8 real flops (FP64-equivalent count)
+
+
+def algorithmic_work(w, s, ft):
+    """Per-iteration algorithmic flops/bytes per kernel group (FP64-equivalent count)."""
+    nk, nb, Np, nth, nwh = s.nk, s.nb, s.Np, ft.nt_half, ft.nw_half
+    ncol = Np * Np
+    return {
+        # per launch group
+        "proj_p2a": dict(flops=nk * (gemm_flops_c(Np, nb, nb) + gemm_flops_c(Np, Np, nb)),
+                         bytes=nk * ncol * 8),
+        "proj_a2p": dict(flops=nk * (gemm_flops_c(nb, Np, Np) + gemm_flops_c(nb, nb, Np)),
+                         bytes=nk * ncol * 8),
+        "pi_fused": dict(bytes=3 * nk * ncol * 8),
+        "sigma_fused": dict(bytes=5 * nk * ncol * 8),
+        "ir_transform": dict(bytes=(nth + nwh) * nk * ncol * 8),
+        "dyson_M_gemm": dict(flops=2 * gemm_flops_c(Np, Np, Np) * nk),
+        "dyson_W_gemm": dict(flops=gemm_flops_c(Np, Np, Np) * nk),
+        "dyson_trsm": dict(flops=4.0 * Np ** 3 * nk),
+        "dyson_potrf": dict(flops=8.0 / 3.0 * Np ** 3 * nk),
+    }
+
+
+def cpu_sample(s, ft, threads):
+    """Time the FP64 oracle on bounded samples and extrapolate one GW iteration (ms)."""
+    from oracle import thc_oracle as O
+    nk, Np, nt, nth, nwh = s.nk, s.Np, ft.nt_f, ft.nt_half, ft.nw_half
+    G = s.G0(ft)
+    f_Rk = O.k_to_R_coefficients(s.kpts, s.lattv, s.kp_grid)
+    f_qR = O.R_to_k_coefficients(s.kpts, s.lattv, s.kp_grid)
+    parts = {}
+    # Pi: one tau slice (rpa_pi.icc:102-176)
+    t0 = time.perf_counter()
+    Gp = O.primary_to_aux(G[0], s.X)[0]
+    Gn = O.primary_to_aux(G[nt - 1], s.X)[0]
+    GpR = f_Rk @ Gp.reshape(nk, -1)
+    GnR = f_Rk @ Gn.reshape(nk, -1)
+    Pi1 = (f_qR @ (-2.0 * GpR * np.conj(GnR))).reshape(nk, Np, Np)
+    parts["Pi"] = (time.perf_counter() - t0) * nth
+    # tau <-> w: 1/8 of the columns of one full transform
+    cols = nk * Np * Np // 8
+    X = np.repeat(Pi1.reshape(1, -1)[:, :cols], nth, axis=0)
+    t0 = time.perf_counter()
+    Xw = ft.Twt_pos() @ X
+    parts["IR"] = (time.perf_counter() - t0) * 8 * 2
+    # Dyson: two (q, w) problems in the reference's LU form (scr_coulomb_t.cpp:171-199)
+    t0 = time.perf_counter()
+    O.dyson_W_in_place(Pi1[None, :2] * 0.1, s.V[:2])
+    parts["Dyson"] = (time.perf_counter() - t0) / 2 * nk * nwh
+    # Sigma: one tau, both halves (thc_gw.icc:70-213)
+    t0 = time.perf_counter()
+    for Gx in (Gp, Gn):
+        GR = f_Rk @ Gx.reshape(nk, -1)
+        Sk = (f_qR @ (-GR * GpR)).reshape(1, nk, Np, Np)
+        O.aux_to_primary(Sk, s.X)
+    GR = O.primary_to_aux(G[1], s.X)  # the G projections of the sigma step
+    GR = O.primary_to_aux(G[nt - 2], s.X)
+    parts["Sigma"] = (time.perf_counter() - t0) * nth
+    del Xw, GR
+    total = sum(parts.values()) * 1e3
+    return total, parts
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    w, s, ft = make_case(args.workload)
+    threads = os.cpu_count()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        t, parts = cpu_sample(s, ft, threads)
+        if i >= args.warmup:
+            vals.append(t)
+    v = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "ms",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic", "config": {"workload": args.workload, "nk": s.nk, "nb": s.nb,
+                                        "Np": s.Np, "nt": ft.nt_f, "prec": w["prec"]},
+        "cpu_baseline": {"value": v, "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": "FP64 numpy/OpenBLAS oracle: 1 tau of Pi and Sigma, 1/8 of one "
+                                   "IR transform, 2 (q,W) LU Dyson solves; extrapolated to one "
+                                   "iteration"},
+        "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    from coqui_b200 import capi
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    w, s, ft = make_case(args.workload)
+    G = s.G0(ft)
+    ctx = make_ctx(s, ft, capi.MIXED)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # warm-up (resident G)
+    ctx.gw_iteration(G, want_sigma=False)
+    for _ in range(max(args.warmup - 1, 0)):
+        ctx.gw_iteration(None, want_sigma=False)
+    barrier()
+    launches0 = ctx.kernel_launches()
+    ctx.set_profiling(True)
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            ctx.gw_iteration(None, want_sigma=False)
+            times.append(total_ms(ctx))
+    barrier()
+    launches = (ctx.kernel_launches() - launches0) // max(args.steps, 1)
+    stats = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    t_step = float(np.sum(times)) / args.steps
+    phases = dict(ctx.timings())
+
+    # e2e through the public API with pinned host buffers
+    Gh = torch.empty(G.shape, dtype=torch.complex128, pin_memory=True).numpy()
+    Gh[...] = G
+    Sh = torch.empty(G.shape, dtype=torch.complex128, pin_memory=True).numpy()
+    ctx.gw_iteration(Gh, sigma_out=Sh)
+    e2e = []
+    for _ in range(args.steps):
+        ctx.gw_iteration(Gh, sigma_out=Sh)
+        e2e.append(total_ms(ctx))
+    t_e2e = float(np.mean(e2e))
+
+    # RPA energy time (resident G) and E_c
+    ctx.rpa_energy(Gh)
+    rpa = []
+    for _ in range(max(1, args.steps // 2)):
+        e_c = ctx.rpa_energy(None)
+        rpa.append(total_ms(ctx))
+    t_rpa = float(np.mean(rpa))
+
+    fp64 = None
+    if not args.no_fp64:
+        c64 = make_ctx(s, ft, capi.FP64)
+        S64, _ = c64.gw_iteration(Gh)
+        t64 = []
+        for _ in range(2):
+            c64.gw_iteration(None, want_sigma=False)
+            t64.append(total_ms(c64))
+        e64 = c64.rpa_energy(None)
+        r64 = total_ms(c64)
+        dS = float(np.abs(Sh - S64).max())
+        fp64 = {"gw_iteration_ms": float(np.mean(t64)), "rpa_energy_ms": r64, "E_c": e64,
+                "max_abs_dSigma_mixed_vs_fp64": dS, "abs_dE_c_mixed_vs_fp64": abs(e_c - e64),
+                "speedup_gw_iteration": float(np.mean(t64)) / t_step,
+                "speedup_rpa": r64 / t_rpa}
+        c64.close()
+
+    # max over ranks
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t_step, t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step, t_e2e = float(tt[0]), float(tt[1])
+
+    # dominant kernel group and its roofline
+    work = algorithmic_work(w, s, ft)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    bf16 = peaks.get("bf16_tflops", 1590.0)
+    top = max(stats.items(), key=lambda kv: kv[1][0]) if stats else None
+    roof = None
+    if top:
+        name, (ms, n) = top
+        per = ms / max(n, 1) / 1e3
+        wk = work.get(name, {})
+        if "flops" in wk:
+            ach = wk["flops"] / per / 1e12
+            roof = {"kernel": name, "bound": "tensor", "achieved": ach, "peak": bf16,
+                    "unit": "TFLOP/s", "frac": ach / bf16, "traffic": None,
+                    "peak_source": "measured bf16 dense (MEASURED_PEAKS.json)"}
+        elif "bytes" in wk:
+            ach = wk["bytes"] / per / 1e9
+            roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                    "frac": ach / hbm, "traffic": None,
+                    "peak_source": "measured HBM copy (MEASURED_PEAKS.json)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, parts = cpu_sample(s, ft, os.cpu_count())
+        cpu = {"value": v, "unit": "ms", "cores": os.cpu_count(), "kind": "port",
+               "sample": "FP64 numpy/OpenBLAS oracle: 1 tau of Pi and Sigma, 1/8 of one IR "
+                         "transform, 2 (q,W) LU Dyson solves; extrapolated to one iteration",
+               "parts_ms": {k: v * 1e3 for k, v in parts.items()}}
+
+    gbytes = G.nbytes
+    line = {
+        "metric": METRIC, "value": t_step / world, "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c64/f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "nk": s.nk, "nb": s.nb, "Np": s.Np,
+                   "nt": ft.nt_f, "nw_b": ft.nw_b, "prec": w["prec"], "parallelism": "replicas",
+                   "l2": "working set (Pi/W 3.2 GB) far above L2; no flush"},
+        "e2e": {"value": t_e2e / world, "unit": "ms", "h2d_bytes_per_step": gbytes,
+                "d2h_bytes_per_step": gbytes},
+        "gpu_launches": int(launches),
+        "rpa_energy_ms": t_rpa, "E_c": e_c,
+        "fp64_form": fp64,
+        "phases_ms": phases,
+        "kernel_ms_per_step": {k: v[0] / args.steps for k, v in stats.items()},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

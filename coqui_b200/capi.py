@@ -1,0 +1,269 @@
+"""ctypes binding of the C ABI declared in include/coqui_b200.h.
+
+Loading fails loudly (ImportError) when the in-tree library has not been built: there is
+no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libcoqui_b200.so")
+
+OK = 0
+ERRORS = {
+    -1: "EINVAL", -2: "EUNSUPPORTED", -3: "ECUDA", -4: "ENOMEM", -5: "ENOTHPD", -6: "EPHSYM",
+    -7: "ETIMEDOUT",
+}
+FP64, MIXED = 0, 1
+
+# Every exported entry point of include/coqui_b200.h.
+SYMBOLS = [
+    "coqui_b200_create", "coqui_b200_destroy", "coqui_b200_last_error", "coqui_b200_version",
+    "coqui_b200_set_ir", "coqui_b200_set_kmesh", "coqui_b200_set_thc", "coqui_b200_eval_pi",
+    "coqui_b200_update_w", "coqui_b200_eval_sigma", "coqui_b200_set_w", "coqui_b200_rpa_energy",
+    "coqui_b200_primary_to_aux", "coqui_b200_aux_to_primary", "coqui_b200_tau_to_w",
+    "coqui_b200_w_to_tau", "coqui_b200_dyson_w", "coqui_b200_last_timings",
+    "coqui_b200_kernel_launches", "coqui_b200_gw_iteration", "coqui_b200_set_profiling",
+    "coqui_b200_kernel_stats",
+]
+
+
+class Dims(ctypes.Structure):
+    _fields_ = [("ns", ctypes.c_int64), ("nk", ctypes.c_int64), ("nb", ctypes.c_int64),
+                ("Np", ctypes.c_int64), ("nt_f", ctypes.c_int64), ("nw_b", ctypes.c_int64),
+                ("kp_grid", ctypes.c_int64 * 3), ("precision_mode", ctypes.c_int32),
+                ("device", ctypes.c_int32)]
+
+
+class CoquiB200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m coqui_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    lib.coqui_b200_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(Dims)]
+    lib.coqui_b200_destroy.argtypes = [P]
+    lib.coqui_b200_destroy.restype = None
+    lib.coqui_b200_last_error.argtypes = [P]
+    lib.coqui_b200_last_error.restype = ctypes.c_char_p
+    lib.coqui_b200_version.restype = ctypes.c_char_p
+    lib.coqui_b200_set_ir.argtypes = [P, P, P, P, P]
+    lib.coqui_b200_set_kmesh.argtypes = [P, P, P, P]
+    lib.coqui_b200_set_thc.argtypes = [P, P, P]
+    lib.coqui_b200_eval_pi.argtypes = [P, P, P]
+    lib.coqui_b200_update_w.argtypes = [P, P, P, P]
+    lib.coqui_b200_eval_sigma.argtypes = [P, P, P]
+    lib.coqui_b200_set_w.argtypes = [P, P]
+    lib.coqui_b200_rpa_energy.argtypes = [P, P, ctypes.POINTER(ctypes.c_double)]
+    lib.coqui_b200_primary_to_aux.argtypes = [P, ctypes.c_int64, P, P]
+    lib.coqui_b200_aux_to_primary.argtypes = [P, ctypes.c_int64, P, P]
+    lib.coqui_b200_tau_to_w.argtypes = [P, P, P]
+    lib.coqui_b200_w_to_tau.argtypes = [P, P, P]
+    lib.coqui_b200_dyson_w.argtypes = [P, P, P]
+    lib.coqui_b200_last_timings.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, ctypes.c_int]
+    lib.coqui_b200_gw_iteration.argtypes = [P, P, P, P]
+    lib.coqui_b200_set_profiling.argtypes = [P, ctypes.c_int]
+    lib.coqui_b200_kernel_stats.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, P, ctypes.c_int]
+    lib.coqui_b200_kernel_launches.argtypes = [P]
+    lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
+    _lib = lib
+    return lib
+
+
+def _ptr(a, name):
+    if a is None:
+        return None
+    if not isinstance(a, np.ndarray) or not a.flags.c_contiguous:
+        raise ValueError(f"{name} must be a C-contiguous numpy array")
+    return a.ctypes.data
+
+
+def _c128(a, shape, name):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    if tuple(a.shape) != tuple(shape):
+        raise ValueError(f"{name} has shape {a.shape}, expected {tuple(shape)}")
+    return a
+
+
+class Context:
+    """One device context: THC data, IR grid, k-mesh and device buffers of one system."""
+
+    def __init__(self, nk, nb, Np, nt_f, nw_b, kp_grid, mode=MIXED, device=0, ns=1):
+        self.lib = load()
+        d = Dims(ns=ns, nk=nk, nb=nb, Np=Np, nt_f=nt_f, nw_b=nw_b,
+                 kp_grid=(ctypes.c_int64 * 3)(*kp_grid), precision_mode=mode, device=device)
+        self.h = ctypes.c_void_p()
+        rc = self.lib.coqui_b200_create(ctypes.byref(self.h), ctypes.byref(d))
+        if rc != OK:
+            raise CoquiB200Error(rc, "coqui_b200_create failed")
+        self.nk, self.nb, self.Np, self.nt, self.nw_b = nk, nb, Np, nt_f, nw_b
+        self.nt_half, self.nw_half = (nt_f + 1) // 2, (nw_b + 1) // 2
+        self.mode = mode
+
+    def close(self):
+        if self.h:
+            self.lib.coqui_b200_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != OK:
+            raise CoquiB200Error(rc, self.lib.coqui_b200_last_error(self.h).decode())
+
+    # -- set-up ------------------------------------------------------------------------
+    def set_ir(self, ft):
+        nt, nw = self.nt, self.nw_b
+        Twt = _c128(ft.Twt_bb, (nw, nt), "Twt_bb")
+        Ttw = _c128(ft.Ttw_bb, (nt, nw), "Ttw_bb")
+        Tb = _c128(ft.T_beta_t_ff, (nt,), "T_beta_t_ff")
+        x = np.ascontiguousarray(ft.tau_mesh_x, np.float64)
+        self._check(self.lib.coqui_b200_set_ir(self.h, _ptr(Twt, "Twt"), _ptr(Ttw, "Ttw"),
+                                               _ptr(Tb, "Tb"), _ptr(x, "tau")))
+
+    def set_kmesh(self, kpts, lattv, chi_bar=None):
+        k = np.ascontiguousarray(kpts, np.float64).reshape(self.nk, 3)
+        L = np.ascontiguousarray(lattv, np.float64).reshape(3, 3)
+        c = None if chi_bar is None else _c128(chi_bar, (self.nk, self.Np), "chi_bar")
+        self._check(self.lib.coqui_b200_set_kmesh(self.h, _ptr(k, "kpts"), _ptr(L, "lattv"),
+                                                  _ptr(c, "chi")))
+
+    def set_thc(self, X, V):
+        X = _c128(X, (1, self.nk, self.Np, self.nb), "X")
+        V = _c128(V, (self.nk, self.Np, self.Np), "V")
+        self._check(self.lib.coqui_b200_set_thc(self.h, _ptr(X, "X"), _ptr(V, "V")))
+
+    # -- solvers -----------------------------------------------------------------------
+    def _G(self, G):
+        return _c128(G, (self.nt, 1, self.nk, self.nb, self.nb), "G_tskij")
+
+    def eval_pi(self, G, out=None):
+        G = self._G(G)
+        if out is None:
+            out = np.empty((self.nt_half, self.nk, self.Np, self.Np), np.complex128)
+        self._check(self.lib.coqui_b200_eval_pi(self.h, _ptr(G, "G"), _ptr(out, "Pi")))
+        return out
+
+    def update_w(self, G, want_w=True, want_head=True, out=None):
+        G = self._G(G)
+        W = None
+        if want_w:
+            W = out if out is not None else np.empty((self.nk, self.nt_half, self.Np, self.Np),
+                                                     np.complex128)
+        head = np.empty(self.nt_half, np.complex128) if want_head else None
+        self._check(self.lib.coqui_b200_update_w(self.h, _ptr(G, "G"), _ptr(W, "W"),
+                                                 _ptr(head, "head")))
+        return W, head
+
+    def set_w(self, dW_qtPQ):
+        W = _c128(dW_qtPQ, (self.nk, self.nt_half, self.Np, self.Np), "dW_qtPQ")
+        self._check(self.lib.coqui_b200_set_w(self.h, _ptr(W, "W")))
+
+    def eval_sigma(self, G, out=None):
+        G = self._G(G)
+        if out is None:
+            out = np.empty_like(G)
+        self._check(self.lib.coqui_b200_eval_sigma(self.h, _ptr(G, "G"), _ptr(out, "Sigma")))
+        return out
+
+    def rpa_energy(self, G):
+        """G = None reuses the device-resident G of the previous call."""
+        G = None if G is None else self._G(G)
+        e = ctypes.c_double(0.0)
+        self._check(self.lib.coqui_b200_rpa_energy(self.h, _ptr(G, "G"), ctypes.byref(e)))
+        return e.value
+
+    def gw_iteration(self, G, sigma_out=None, want_sigma=True, want_head=False):
+        """update_w + evaluate.  G = None reuses the device-resident G; with want_sigma False
+        Sigma stays on the device.  Returns (Sigma or None, eps_inv_head or None)."""
+        G = None if G is None else self._G(G)
+        S = None
+        if want_sigma:
+            S = sigma_out if sigma_out is not None else np.empty(
+                (self.nt, 1, self.nk, self.nb, self.nb), np.complex128)
+        head = np.empty(self.nt_half, np.complex128) if want_head else None
+        self._check(self.lib.coqui_b200_gw_iteration(self.h, _ptr(G, "G"), _ptr(S, "Sigma"),
+                                                     _ptr(head, "head")))
+        return S, head
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.coqui_b200_set_profiling(self.h, 1 if on else 0))
+
+    def kernel_stats(self):
+        """{name: (total_ms, launch_groups)} accumulated while profiling was on."""
+        n, L = 64, 48
+        names = ctypes.create_string_buffer(n * L)
+        ms = np.zeros(n)
+        cnt = np.zeros(n, np.int64)
+        k = self.lib.coqui_b200_kernel_stats(self.h, names, L, ms.ctypes.data, cnt.ctypes.data, n)
+        raw = names.raw
+        return {raw[i * L:(i + 1) * L].split(b"\0")[0].decode(): (float(ms[i]), int(cnt[i]))
+                for i in range(k)}
+
+    def primary_to_aux(self, O_tskab):
+        O = np.ascontiguousarray(O_tskab, np.complex128)
+        nt = O.size // (self.nk * self.nb * self.nb)
+        O = O.reshape(nt, 1, self.nk, self.nb, self.nb)
+        out = np.empty((nt, 1, self.nk, self.Np, self.Np), np.complex128)
+        self._check(self.lib.coqui_b200_primary_to_aux(self.h, nt, _ptr(O, "O"), _ptr(out, "out")))
+        return out
+
+    def aux_to_primary(self, O_tskPQ):
+        O = np.ascontiguousarray(O_tskPQ, np.complex128)
+        nt = O.size // (self.nk * self.Np * self.Np)
+        O = O.reshape(nt, 1, self.nk, self.Np, self.Np)
+        out = np.empty((nt, 1, self.nk, self.nb, self.nb), np.complex128)
+        self._check(self.lib.coqui_b200_aux_to_primary(self.h, nt, _ptr(O, "O"), _ptr(out, "out")))
+        return out
+
+    def tau_to_w(self, X_tqPQ):
+        X = _c128(X_tqPQ, (self.nt_half, self.nk, self.Np, self.Np), "X_tqPQ")
+        out = np.empty((self.nw_half, self.nk, self.Np, self.Np), np.complex128)
+        self._check(self.lib.coqui_b200_tau_to_w(self.h, _ptr(X, "X"), _ptr(out, "out")))
+        return out
+
+    def w_to_tau(self, X_wqPQ):
+        X = _c128(X_wqPQ, (self.nw_half, self.nk, self.Np, self.Np), "X_wqPQ")
+        out = np.empty((self.nt_half, self.nk, self.Np, self.Np), np.complex128)
+        self._check(self.lib.coqui_b200_w_to_tau(self.h, _ptr(X, "X"), _ptr(out, "out")))
+        return out
+
+    def dyson_w(self, Pi_wqPQ):
+        P = _c128(Pi_wqPQ, (self.nw_half, self.nk, self.Np, self.Np), "Pi_wqPQ")
+        out = np.empty_like(P)
+        self._check(self.lib.coqui_b200_dyson_w(self.h, _ptr(P, "Pi"), _ptr(out, "W")))
+        return out
+
+    # -- introspection -----------------------------------------------------------------
+    def timings(self):
+        n, L = 32, 48
+        names = ctypes.create_string_buffer(n * L)
+        ms = np.zeros(n)
+        k = self.lib.coqui_b200_last_timings(self.h, names, L, ms.ctypes.data, n)
+        raw = names.raw
+        return [(raw[i * L:(i + 1) * L].split(b"\0")[0].decode(), float(ms[i])) for i in range(k)]
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.coqui_b200_kernel_launches(self.h))
+
+
+def version() -> str:
+    return load().coqui_b200_version().decode()

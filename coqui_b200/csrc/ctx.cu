@@ -1,0 +1,896 @@
+// C ABI of the THC-RPA/GW hot path: context, data upload and the solver entry points.
+//
+// Pipeline of one screened-interaction update (scr_coulomb_t::update_w,
+// src/methods/scr_coulomb/scr_coulomb_t.cpp:37-95), all on one stream:
+//   for tau in [0, nt_half): G^k_PQ(tau), G^k_PQ(beta - tau)  (projection GEMMs)
+//                            -> fused k->R DFT, -2 Gp o conj(Gn), R->q DFT -> Pi(tau)
+//   Pi(tau) -> Pi(iW)  (in-place IR transform)
+//   per (q, iW): V = L L^H, M = L^H Pi L, I - M = C C^H (FP64), W = Y^H Y - V, Y = C^{-1} L^H
+//   W(iW) -> W(tau)    (in-place IR transform), eps^-1 head.
+// The self-energy and the RPA energy reuse the same stages.
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <complex>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dyson.cuh"
+#include "kernels.cuh"
+#include "tc_gemm.cuh"
+
+using cq::Error;
+using cq::KGrid;
+
+namespace {
+
+const char* kVersion = "coqui_b200 0.1.0 (sm_100a)";
+
+#define CQ_CHECK_BLAS(expr)                                                              \
+  do {                                                                                   \
+    cublasStatus_t _s = (expr);                                                          \
+    if (_s != CUBLAS_STATUS_SUCCESS)                                                     \
+      throw Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
+  } while (0)
+#define CQ_CHECK_SOLVER(expr)                                                            \
+  do {                                                                                   \
+    cusolverStatus_t _s = (expr);                                                        \
+    if (_s != CUSOLVER_STATUS_SUCCESS)                                                   \
+      throw Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
+  } while (0)
+
+using cq::DevBuf;
+
+cublasOperation_t blas_op(char c) {
+  return c == 'N' ? CUBLAS_OP_N : (c == 'T' ? CUBLAS_OP_T : CUBLAS_OP_C);
+}
+
+}  // namespace
+
+struct coqui_b200_ctx {
+  coqui_b200_dims d{};
+  int64_t ns = 1, nk = 0, nq = 0, nb = 0, Np = 0, nt = 0, nth = 0, nwb = 0, nwh = 0, nmax = 0;
+  KGrid g{1, 1, 1};
+  int mode = COQUI_B200_MIXED;
+  int dev = 0;
+  std::string err;
+  cudaStream_t st = nullptr;
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t sol = nullptr;
+  int64_t launch_base = 0;
+  bool have_ir = false, have_k = false, have_thc = false, w_valid = false, w_in_R = false;
+  bool g_resident = false;
+  cq::Prof prof;
+
+  // host-side IR data
+  std::vector<double2> Twt_pos, Ttw_pos, Ttw_bb, T_beta;
+  // host-side head factors
+  std::vector<double> head_fac;
+  int64_t q_smallest = 0;
+
+  // device data
+  DevBuf<double2> X, V, L, LH, chi, G, Sig, Tproj, stage, dTwt, dTtw;
+  DevBuf<double> fac;
+  DevBuf<double2> eps;
+  DevBuf<unsigned char> Gp, Gn, PW;  // storage precision, bytes
+  DevBuf<unsigned char> dyn;         // Dyson scratch
+  cq::TcOperand Xtc;                 // packed X for the tensor-core projections
+
+  // phase timing of the last call
+  std::vector<std::pair<std::string, cudaEvent_t>> marks;
+  std::vector<std::pair<std::string, double>> last_ms;
+
+  size_t elem() const { return mode == COQUI_B200_FP64 ? sizeof(double2) : sizeof(float2); }
+
+  void mark(const char* name) {
+    cudaEvent_t e;
+    CQ_CHECK_CUDA(cudaEventCreate(&e));
+    CQ_CHECK_CUDA(cudaEventRecord(e, st));
+    marks.emplace_back(name, e);
+  }
+  void begin_timing() {
+    for (auto& m : marks) cudaEventDestroy(m.second);
+    marks.clear();
+    mark("start");
+  }
+  void end_timing() {
+    CQ_CHECK_CUDA(cudaStreamSynchronize(st));
+    prof.resolve();
+    last_ms.clear();
+    for (size_t i = 1; i < marks.size(); ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, marks[i - 1].second, marks[i].second);
+      last_ms.emplace_back(marks[i].first, ms);
+    }
+    for (auto& m : marks) cudaEventDestroy(m.second);
+    marks.clear();
+  }
+};
+
+namespace {
+
+using Ctx = coqui_b200_ctx;
+
+template <typename F> int guarded(Ctx* c, F&& f) {
+  if (!c) return COQUI_B200_EINVAL;
+  try {
+    CQ_CHECK_CUDA(cudaSetDevice(c->dev));
+    f();
+    c->err.clear();
+    return COQUI_B200_OK;
+  } catch (const Error& e) {
+    c->err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    c->err = "host allocation failed";
+    return COQUI_B200_ENOMEM;
+  } catch (const std::exception& e) {
+    c->err = e.what();
+    return COQUI_B200_EINVAL;
+  }
+}
+
+// Row-major complex128 GEMM through cuBLAS (column-major): C = alpha op(A) op(B) + beta C,
+// batched with constant strides.
+void zgemm_rm(Ctx* c, char opA, char opB, int64_t M, int64_t N, int64_t K, double2 alpha,
+              const double2* A, int64_t lda, int64_t sA, const double2* B, int64_t ldb,
+              int64_t sB, double2 beta, double2* C, int64_t ldc, int64_t sC, int64_t batch) {
+  CQ_CHECK_BLAS(cublasZgemmStridedBatched(
+      c->blas, blas_op(opB), blas_op(opA), (int)N, (int)M, (int)K,
+      reinterpret_cast<const cuDoubleComplex*>(&alpha), reinterpret_cast<const cuDoubleComplex*>(B),
+      (int)ldb, sB, reinterpret_cast<const cuDoubleComplex*>(A), (int)lda, sA,
+      reinterpret_cast<const cuDoubleComplex*>(&beta), reinterpret_cast<cuDoubleComplex*>(C),
+      (int)ldc, sC, (int)batch));
+}
+
+void upload(Ctx* c, void* dst, const void* src, size_t bytes) {
+  CQ_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->st));
+}
+void download(Ctx* c, void* dst, const void* src, size_t bytes) {
+  CQ_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->st));
+}
+
+void require_ready(Ctx* c, bool thc, bool ir, bool k) {
+  CQ_REQUIRE(!thc || c->have_thc, COQUI_B200_EINVAL, "set_thc not called");
+  CQ_REQUIRE(!ir || c->have_ir, COQUI_B200_EINVAL, "set_ir not called");
+  CQ_REQUIRE(!k || c->have_k, COQUI_B200_EINVAL, "set_kmesh not called");
+}
+
+// ---------------------------------------------------------------------------------------
+// projections: O_PQ = X G X^H (primary -> aux) and O_ab = X^H O X (aux -> primary)
+// ---------------------------------------------------------------------------------------
+
+// G_k (nk, nb, nb) complex128 on device -> out (nk, Np, Np) in storage precision.
+void project_p2a(Ctx* c, const double2* Gk, void* out) {
+  cq::Prof::Scope sc(&c->prof, "proj_p2a");
+  const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
+  if (c->mode == COQUI_B200_FP64) {
+    c->Tproj.ensure((size_t)nk * Np * nb);
+    // T = X G  (Np x nb)
+    zgemm_rm(c, 'N', 'N', Np, nb, nb, make_double2(1, 0), c->X.p, nb, Np * nb, Gk, nb, nb * nb,
+             make_double2(0, 0), c->Tproj.p, nb, Np * nb, nk);
+    // O = T X^H  (Np x Np)
+    zgemm_rm(c, 'N', 'C', Np, Np, nb, make_double2(1, 0), c->Tproj.p, nb, Np * nb, c->X.p, nb,
+             Np * nb, make_double2(0, 0), (double2*)out, Np, Np * Np, nk);
+  } else {
+    cq::tc_project_p2a(c->Xtc, Gk, (float2*)out, nk, Np, nb, c->st);
+  }
+}
+
+// S_k (nk, Np, Np) storage -> out (nk, nb, nb) complex128 (device).
+void project_a2p(Ctx* c, const void* Sk, double2* out) {
+  cq::Prof::Scope sc(&c->prof, "proj_a2p");
+  const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
+  if (c->mode == COQUI_B200_FP64) {
+    c->Tproj.ensure((size_t)nk * Np * nb);
+    // T = X^H S  (nb x Np)
+    zgemm_rm(c, 'C', 'N', nb, Np, Np, make_double2(1, 0), c->X.p, nb, Np * nb,
+             (const double2*)Sk, Np, Np * Np, make_double2(0, 0), c->Tproj.p, Np, Np * nb, nk);
+    // O = T X  (nb x nb)
+    zgemm_rm(c, 'N', 'N', nb, nb, Np, make_double2(1, 0), c->Tproj.p, Np, Np * nb, c->X.p, nb,
+             Np * nb, make_double2(0, 0), out, nb, nb * nb, nk);
+  } else {
+    cq::tc_project_a2p(c->Xtc, (const float2*)Sk, out, nk, Np, nb, c->st);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Pi(tau) for all tau in [0, nt_half) into the PW buffer (rpa_pi.icc:102-176)
+// ---------------------------------------------------------------------------------------
+void eval_pi_device(Ctx* c) {
+  const int64_t nk = c->nk, Np = c->Np, ncol = Np * Np, nt = c->nt;
+  const size_t slab = (size_t)nk * ncol * c->elem();
+  c->Gp.ensure(slab);
+  c->Gn.ensure(slab);
+  c->PW.ensure((size_t)c->nmax * c->nq * ncol * c->elem());
+  const double sp = (c->ns == 2) ? -1.0 : -2.0;
+  for (int64_t it = 0; it < c->nth; ++it) {
+    project_p2a(c, c->G.p + it * nk * c->nb * c->nb, c->Gp.p);
+    project_p2a(c, c->G.p + (nt - it - 1) * nk * c->nb * c->nb, c->Gn.p);
+    unsigned char* dst = c->PW.p + (size_t)it * c->nq * ncol * c->elem();
+    cq::Prof::Scope sc(&c->prof, "pi_fused");
+    if (c->mode == COQUI_B200_FP64)
+      cq::launch_pi_fused<double>((double2*)c->Gp.p, (double2*)c->Gn.p, (double2*)dst, ncol, c->g,
+                                  sp, c->st);
+    else
+      cq::launch_pi_fused<float>((float2*)c->Gp.p, (float2*)c->Gn.p, (float2*)dst, ncol, c->g, sp,
+                                 c->st);
+  }
+  c->w_valid = false;
+}
+
+void ir_inplace(Ctx* c, int n_in, int n_out, const double2* M) {
+  cq::Prof::Scope sc(&c->prof, "ir_transform");
+  const int64_t ncol = c->nq * c->Np * c->Np;
+  if (c->mode == COQUI_B200_FP64)
+    cq::launch_ir_transform<double>((double2*)c->PW.p, ncol, n_in, n_out, M, c->st);
+  else
+    cq::launch_ir_transform<float>((float2*)c->PW.p, ncol, n_in, n_out, M, c->st);
+}
+
+// G_tskij == NULL reuses the G already resident on the device.
+void upload_G(Ctx* c, const double* G_tskij) {
+  const size_t n = (size_t)c->nt * c->nk * c->nb * c->nb;
+  if (!G_tskij) {
+    CQ_REQUIRE(c->g_resident, COQUI_B200_EINVAL, "G_tskij is null and no G is resident");
+    return;
+  }
+  c->G.ensure(n);
+  upload(c, c->G.p, G_tskij, n * sizeof(double2));
+  c->g_resident = true;
+}
+
+// E_c accumulation (thc_rpa.icc:130-173) from per-(w, q) log det and traces.
+double rpa_energy_from(Ctx* c, const std::vector<double>& logdet, const std::vector<double2>& tr) {
+  const int64_t nwb = c->nwb, nwh = c->nwh, nq = c->nq;
+  std::vector<std::complex<double>> e_w(nwb, 0.0);
+  for (int64_t n = 0; n < nwh; ++n)
+    for (int64_t q = 0; q < nq; ++q) {
+      const int64_t p = n * nq + q;
+      const std::complex<double> v(tr[p].x + logdet[p], tr[p].y);  // q_weight = 1
+      const int64_t wn = nwb / 2 + n, mwn = nwb / 2 - n;
+      e_w[wn] += v;
+      if (mwn != wn) e_w[mwn] += v;
+    }
+  // e(tau) = Ttw_bb e(w) on the nt_f-point mesh, then tau -> beta^- with T_beta_t_ff
+  std::complex<double> e = 0;
+  for (int64_t t = 0; t < c->nt; ++t) {
+    std::complex<double> et = 0;
+    for (int64_t w = 0; w < nwb; ++w) {
+      const double2 T = c->Ttw_bb[t * nwb + w];
+      et += std::complex<double>(T.x, T.y) * e_w[w];
+    }
+    e += std::complex<double>(c->T_beta[t].x, c->T_beta[t].y) * et;
+  }
+  e /= (2.0 * (double)c->nk);
+  return e.real();
+}
+
+}  // namespace
+
+// =======================================================================================
+// ABI
+// =======================================================================================
+extern "C" {
+
+const char* coqui_b200_version(void) { return kVersion; }
+
+int coqui_b200_create(coqui_b200_ctx** out, const coqui_b200_dims* dims) {
+  if (!out || !dims) return COQUI_B200_EINVAL;
+  *out = nullptr;
+  std::unique_ptr<Ctx> c(new (std::nothrow) Ctx());
+  if (!c) return COQUI_B200_ENOMEM;
+  const coqui_b200_dims& d = *dims;
+  if (d.ns != 1 || d.nk < 1 || d.nb < 1 || d.Np < 1 || d.nt_f < 2 || d.nw_b < 1 ||
+      d.kp_grid[0] * d.kp_grid[1] * d.kp_grid[2] != d.nk ||
+      (d.precision_mode != COQUI_B200_FP64 && d.precision_mode != COQUI_B200_MIXED))
+    return COQUI_B200_EINVAL;
+  c->d = d;
+  c->dev = d.device;
+  int rc = guarded(c.get(), [&] {
+    c->ns = d.ns;
+    c->nk = c->nq = d.nk;
+    c->nb = d.nb;
+    c->Np = d.Np;
+    c->nt = d.nt_f;
+    c->nth = (d.nt_f + 1) / 2;
+    c->nwb = d.nw_b;
+    c->nwh = (d.nw_b + 1) / 2;
+    c->nmax = std::max(c->nth, c->nwh);
+    c->g = KGrid{(int)d.kp_grid[0], (int)d.kp_grid[1], (int)d.kp_grid[2]};
+    CQ_REQUIRE(c->g.n0 <= 8 && c->g.n1 <= 8 && c->g.n2 <= 8, COQUI_B200_EUNSUPPORTED,
+               "k-grid edges above 8 are not supported");
+    c->mode = d.precision_mode;
+    CQ_CHECK_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CQ_CHECK_BLAS(cublasCreate(&c->blas));
+    CQ_CHECK_BLAS(cublasSetStream(c->blas, c->st));
+    CQ_CHECK_BLAS(cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
+    CQ_CHECK_SOLVER(cusolverDnCreate(&c->sol));
+    CQ_CHECK_SOLVER(cusolverDnSetStream(c->sol, c->st));
+    c->prof.st = c->st;
+    cq::upload_twiddles();
+    c->launch_base = cq::launches_total();
+  });
+  if (rc != COQUI_B200_OK) {
+    coqui_b200_destroy(c.release());
+    return rc;
+  }
+  *out = c.release();
+  return COQUI_B200_OK;
+}
+
+void coqui_b200_destroy(coqui_b200_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->dev);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (auto* b : {&c->X, &c->V, &c->L, &c->LH, &c->chi, &c->G, &c->Sig, &c->Tproj, &c->stage,
+                  &c->dTwt, &c->dTtw, &c->eps})
+    b->release();
+  c->fac.release();
+  c->Gp.release();
+  c->Gn.release();
+  c->PW.release();
+  c->dyn.release();
+  c->Xtc.release();
+  for (auto& m : c->marks) cudaEventDestroy(m.second);
+  if (c->sol) cusolverDnDestroy(c->sol);
+  if (c->blas) cublasDestroy(c->blas);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+const char* coqui_b200_last_error(const coqui_b200_ctx* c) {
+  return c ? c->err.c_str() : "null context";
+}
+
+int64_t coqui_b200_kernel_launches(const coqui_b200_ctx* c) {
+  return c ? cq::launches_total() - c->launch_base : 0;
+}
+
+int coqui_b200_last_timings(const coqui_b200_ctx* c, char* names, int name_len, double* ms, int n) {
+  if (!c) return COQUI_B200_EINVAL;
+  int k = 0;
+  for (const auto& p : c->last_ms) {
+    if (k >= n) break;
+    if (names && name_len > 0) {
+      std::strncpy(names + (size_t)k * name_len, p.first.c_str(), name_len - 1);
+      names[(size_t)k * name_len + name_len - 1] = 0;
+    }
+    if (ms) ms[k] = p.second;
+    ++k;
+  }
+  return k;
+}
+
+int coqui_b200_set_ir(coqui_b200_ctx* c, const double* Twt_bb, const double* Ttw_bb,
+                      const double* T_beta_t_ff, const double* tau_mesh_x) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(Twt_bb && Ttw_bb && T_beta_t_ff && tau_mesh_x, COQUI_B200_EINVAL, "null IR table");
+    const int64_t nt = c->nt, nwb = c->nwb, nth = c->nth, nwh = c->nwh;
+    // thc_gw.cpp:56-66 particle-hole symmetry of the tau mesh
+    for (int64_t it = 0; it < nt; ++it) {
+      const double diff = std::abs(tau_mesh_x[it]) - std::abs(tau_mesh_x[nt - it - 1]);
+      CQ_REQUIRE(diff <= 1e-6, COQUI_B200_EPHSYM,
+                 "IAFT grid is not compatible with particle-hole symmetry");
+    }
+    auto at = [](const double* p, int64_t i) { return make_double2(p[2 * i], p[2 * i + 1]); };
+    // IAFT.icc:61-70 (tau -> w) and :116-125 (w -> tau); nt_b() == nt_f (IAFT.hpp:167-169)
+    c->Twt_pos.assign(nwh * nth, make_double2(0, 0));
+    for (int64_t n = 0; n < nwh; ++n)
+      for (int64_t it = 0; it < nth; ++it) {
+        const int64_t iw = nwb / 2 + n, imt = nt - it - 1;
+        double2 v = at(Twt_bb, iw * nt + it);
+        if (it != imt) {
+          const double2 u = at(Twt_bb, iw * nt + imt);
+          v.x += u.x;
+          v.y += u.y;
+        }
+        c->Twt_pos[n * nth + it] = v;
+      }
+    c->Ttw_pos.assign(nth * nwh, make_double2(0, 0));
+    for (int64_t it = 0; it < nth; ++it)
+      for (int64_t n = 0; n < nwh; ++n) {
+        const int64_t iw = nwb / 2 + n, imw = nwb / 2 - n;
+        double2 v = at(Ttw_bb, it * nwb + iw);
+        if (iw != imw) {
+          const double2 u = at(Ttw_bb, it * nwb + imw);
+          v.x += u.x;
+          v.y += u.y;
+        }
+        c->Ttw_pos[it * nwh + n] = v;
+      }
+    c->Ttw_bb.resize(nt * nwb);
+    for (int64_t i = 0; i < nt * nwb; ++i) c->Ttw_bb[i] = at(Ttw_bb, i);
+    c->T_beta.resize(nt);
+    for (int64_t i = 0; i < nt; ++i) c->T_beta[i] = at(T_beta_t_ff, i);
+    c->dTwt.ensure(c->Twt_pos.size());
+    c->dTtw.ensure(c->Ttw_pos.size());
+    upload(c, c->dTwt.p, c->Twt_pos.data(), c->Twt_pos.size() * sizeof(double2));
+    upload(c, c->dTtw.p, c->Ttw_pos.data(), c->Ttw_pos.size() * sizeof(double2));
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->have_ir = true;
+  });
+}
+
+int coqui_b200_set_kmesh(coqui_b200_ctx* c, const double* kpts, const double* lattv,
+                         const double* chi_bar_qP) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(kpts && lattv, COQUI_B200_EINVAL, "null k-mesh");
+    const int64_t nk = c->nk;
+    const int n[3] = {c->g.n0, c->g.n1, c->g.n2};
+    // The device DFT equals the reference's dense f_Rk / f_kR (kpoint_utils.hpp:461-705)
+    // when k_i = (i0 b0/n0 + i1 b1/n1 + i2 b2/n2) in lexicographic order, b = 2 pi lattv^-T.
+    for (int64_t k = 0; k < nk; ++k) {
+      const int64_t idx[3] = {k / (n[1] * n[2]), (k / n[2]) % n[1], k % n[2]};
+      for (int j = 0; j < 3; ++j) {
+        // fractional coordinate along lattice vector j: k . a_j / (2 pi)
+        double f = 0;
+        for (int x = 0; x < 3; ++x) f += kpts[k * 3 + x] * lattv[j * 3 + x];
+        f /= 2.0 * 3.14159265358979323846;
+        const double want = (double)idx[j] / n[j];
+        const double dlt = f - want;
+        CQ_REQUIRE(std::abs(dlt - std::round(dlt)) < 1e-8, COQUI_B200_EUNSUPPORTED,
+                   "k-points are not a Gamma-centred grid in lexicographic order");
+      }
+    }
+    // dielectric-head prefactors (g0_div_utils.hpp:196-207) and smallest |q|
+    const double* a = lattv;
+    const double vol = std::abs(a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                                a[2] * (a[3] * a[7] - a[4] * a[6]));
+    const double fpi = 4.0 * 3.14159265358979323846;
+    c->head_fac.resize(nk);
+    double best = 1e300;
+    for (int64_t q = 0; q < nk; ++q) {
+      const double q2 = kpts[3 * q] * kpts[3 * q] + kpts[3 * q + 1] * kpts[3 * q + 1] +
+                        kpts[3 * q + 2] * kpts[3 * q + 2];
+      c->head_fac[q] = q2 / fpi * vol;
+      if (q2 < best) {
+        best = q2;
+        c->q_smallest = q;
+      }
+    }
+    c->fac.ensure(nk);
+    upload(c, c->fac.p, c->head_fac.data(), nk * sizeof(double));
+    c->chi.ensure((size_t)nk * c->Np);
+    if (chi_bar_qP)
+      upload(c, c->chi.p, chi_bar_qP, (size_t)nk * c->Np * sizeof(double2));
+    else
+      CQ_CHECK_CUDA(cudaMemsetAsync(c->chi.p, 0, (size_t)nk * c->Np * sizeof(double2), c->st));
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->have_k = true;
+  });
+}
+
+int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_qPQ) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(X_skPa && V_qPQ, COQUI_B200_EINVAL, "null THC data");
+    const int64_t nk = c->nk, Np = c->Np, nb = c->nb;
+    c->X.ensure((size_t)nk * Np * nb);
+    c->V.ensure((size_t)nk * Np * Np);
+    upload(c, c->X.p, X_skPa, (size_t)nk * Np * nb * sizeof(double2));
+    upload(c, c->V.p, V_qPQ, (size_t)nk * Np * Np * sizeof(double2));
+    // V^q = L L^H once per q (FP64)
+    c->L.ensure((size_t)nk * Np * Np);
+    c->LH.ensure((size_t)nk * Np * Np);
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->L.p, c->V.p, (size_t)nk * Np * Np * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, c->st));
+    int info = cq::cholesky_lower_batched(c->sol, c->L.p, Np, nk, c->st);
+    CQ_REQUIRE(info == 0, COQUI_B200_ENOTHPD, "Coulomb matrix V^q is not positive definite");
+    cq::launch_zero_upper_and_adjoint(c->L.p, c->LH.p, Np, nk, c->st);
+    if (c->mode == COQUI_B200_MIXED) cq::tc_pack_X(c->Xtc, c->X.p, nk, Np, nb, c->st);
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->have_thc = true;
+    c->w_valid = false;
+  });
+}
+
+int coqui_b200_primary_to_aux(coqui_b200_ctx* c, int64_t n_tau, const double* O_tskab,
+                              double* O_tskPQ) {
+  return guarded(c, [&] {
+    require_ready(c, true, false, false);
+    CQ_REQUIRE(n_tau >= 1 && O_tskab && O_tskPQ, COQUI_B200_EINVAL, "bad arguments");
+    const int64_t nk = c->nk, nb = c->nb, Np = c->Np, ncol = Np * Np;
+    const size_t gsz = (size_t)nk * nb * nb;
+    c->G.ensure(gsz);
+    c->Gp.ensure((size_t)nk * ncol * c->elem());
+    c->stage.ensure((size_t)nk * ncol);
+    for (int64_t t = 0; t < n_tau; ++t) {
+      upload(c, c->G.p, O_tskab + 2 * t * gsz, gsz * sizeof(double2));
+      project_p2a(c, c->G.p, c->Gp.p);
+      const double2* src = (const double2*)c->Gp.p;
+      if (c->mode == COQUI_B200_MIXED) {
+        cq::launch_to_c128<float>((float2*)c->Gp.p, c->stage.p, nk * ncol, c->st);
+        src = c->stage.p;
+      }
+      download(c, O_tskPQ + 2 * t * nk * ncol, src, (size_t)nk * ncol * sizeof(double2));
+      CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    }
+  });
+}
+
+int coqui_b200_aux_to_primary(coqui_b200_ctx* c, int64_t n_tau, const double* O_tskPQ,
+                              double* O_tskab) {
+  return guarded(c, [&] {
+    require_ready(c, true, false, false);
+    CQ_REQUIRE(n_tau >= 1 && O_tskab && O_tskPQ, COQUI_B200_EINVAL, "bad arguments");
+    const int64_t nk = c->nk, nb = c->nb, Np = c->Np, ncol = Np * Np;
+    const size_t gsz = (size_t)nk * nb * nb;
+    c->Sig.ensure(gsz);
+    c->Gp.ensure((size_t)nk * ncol * c->elem());
+    c->stage.ensure((size_t)nk * ncol);
+    for (int64_t t = 0; t < n_tau; ++t) {
+      if (c->mode == COQUI_B200_FP64) {
+        upload(c, c->Gp.p, O_tskPQ + 2 * t * nk * ncol, (size_t)nk * ncol * sizeof(double2));
+      } else {
+        upload(c, c->stage.p, O_tskPQ + 2 * t * nk * ncol, (size_t)nk * ncol * sizeof(double2));
+        cq::launch_from_c128<float>(c->stage.p, (float2*)c->Gp.p, nk * ncol, c->st);
+      }
+      project_a2p(c, c->Gp.p, c->Sig.p);
+      download(c, O_tskab + 2 * t * gsz, c->Sig.p, gsz * sizeof(double2));
+      CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    }
+  });
+}
+
+int coqui_b200_eval_pi(coqui_b200_ctx* c, const double* G_tskij, double* Pi_tqPQ) {
+  return guarded(c, [&] {
+    require_ready(c, true, true, true);
+    c->begin_timing();
+    upload_G(c, G_tskij);
+    c->mark("h2d_G");
+    eval_pi_device(c);
+    c->mark("EVALUATE_PI_R");
+    if (Pi_tqPQ) {
+      const int64_t n = c->nth * c->nq * c->Np * c->Np;
+      if (c->mode == COQUI_B200_FP64) {
+        download(c, Pi_tqPQ, c->PW.p, n * sizeof(double2));
+      } else {
+        // stream out in slabs of one tau through the staging buffer
+        const int64_t slab = c->nq * c->Np * c->Np;
+        c->stage.ensure(slab);
+        for (int64_t t = 0; t < c->nth; ++t) {
+          cq::launch_to_c128<float>((float2*)c->PW.p + t * slab, c->stage.p, slab, c->st);
+          download(c, Pi_tqPQ + 2 * t * slab, c->stage.p, slab * sizeof(double2));
+        }
+      }
+    }
+    c->mark("d2h");
+    c->end_timing();
+  });
+}
+
+namespace {
+
+// Pi(iW) in the PW buffer -> W(iW) (want_w) and/or per-problem log det / trace (want_e).
+void dyson_all(Ctx* c, bool want_w, bool want_e, std::vector<double>* logdet,
+               std::vector<double2>* tr) {
+  cq::DysonArgs a;
+  a.Np = c->Np;
+  a.nq = c->nq;
+  a.nw = c->nwh;
+  a.L = c->L.p;
+  a.LH = c->LH.p;
+  a.V = c->V.p;
+  a.want_w = want_w;
+  a.want_e = want_e;
+  a.mixed = (c->mode == COQUI_B200_MIXED);
+  a.PW = c->PW.p;
+  a.prof = &c->prof;
+  std::vector<double> ld;
+  std::vector<double2> t;
+  cq::dyson_run(a, c->blas, c->sol, c->dyn, c->st, want_e ? &ld : nullptr, want_e ? &t : nullptr);
+  if (logdet) *logdet = std::move(ld);
+  if (tr) *tr = std::move(t);
+}
+
+void update_w_device(Ctx* c) {
+  eval_pi_device(c);
+  c->mark("EVALUATE_PI_R");
+  ir_inplace(c, (int)c->nth, (int)c->nwh, c->dTwt.p);
+  c->mark("IMAG_FT_TtoW");
+  dyson_all(c, true, false, nullptr, nullptr);
+  c->mark("EVALUATE_W");
+  ir_inplace(c, (int)c->nwh, (int)c->nth, c->dTtw.p);
+  c->mark("IMAG_FT_WtoT");
+  c->w_valid = true;
+  c->w_in_R = false;
+}
+
+void eps_head(Ctx* c, double* out) {
+  cq::Prof::Scope sc(&c->prof, "eps_head");
+  c->eps.ensure((size_t)c->nth * c->nq);
+  if (c->mode == COQUI_B200_FP64)
+    cq::launch_eps_head<double>((double2*)c->PW.p, c->chi.p, c->fac.p, c->eps.p, c->nth, c->nq,
+                                c->Np, c->st);
+  else
+    cq::launch_eps_head<float>((float2*)c->PW.p, c->chi.p, c->fac.p, c->eps.p, c->nth, c->nq,
+                               c->Np, c->st);
+  std::vector<double2> h((size_t)c->nth * c->nq);
+  download(c, h.data(), c->eps.p, h.size() * sizeof(double2));
+  CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+  for (int64_t t = 0; t < c->nth; ++t) {
+    out[2 * t] = h[t * c->nq + c->q_smallest].x;
+    out[2 * t + 1] = h[t * c->nq + c->q_smallest].y;
+  }
+}
+
+void download_w_qt(Ctx* c, double* dW_qtPQ) {
+  const int64_t ncol = c->Np * c->Np;
+  const int64_t per_q = c->nth * ncol;
+  // one q at a time through the staging buffer (transposes (t, q) -> (q, t))
+  c->stage.ensure(per_q);
+  for (int64_t q = 0; q < c->nq; ++q) {
+    if (c->mode == COQUI_B200_FP64)
+      cq::launch_tq_to_qt_c128<double>((double2*)c->PW.p, c->stage.p, c->nth, c->nq, ncol, q, 1,
+                                       c->st);
+    else
+      cq::launch_tq_to_qt_c128<float>((float2*)c->PW.p, c->stage.p, c->nth, c->nq, ncol, q, 1,
+                                      c->st);
+    download(c, dW_qtPQ + 2 * q * per_q, c->stage.p, per_q * sizeof(double2));
+  }
+}
+
+// Sigma(tau) for all tau into c->Sig (device, complex128), thc_gw.icc:70-213 twice.
+void sigma_device(Ctx* c) {
+  CQ_REQUIRE(c->w_valid, COQUI_B200_EINVAL, "no screened interaction: call update_w or set_w");
+  const int64_t nk = c->nk, nb = c->nb, Np = c->Np, ncol = Np * Np, nt = c->nt;
+  const size_t slab = (size_t)nk * ncol * c->elem();
+  const size_t gsz = (size_t)nk * nb * nb;
+  c->Gp.ensure(slab);
+  c->Gn.ensure(slab);
+  c->Sig.ensure((size_t)nt * gsz);
+  // W q -> R once (thc_gw.icc:148-153); stays in R until the next update
+  if (!c->w_in_R) {
+    cq::Prof::Scope sc(&c->prof, "dft_w");
+    const double s = 1.0 / (double)nk;
+    if (c->mode == COQUI_B200_FP64)
+      cq::launch_dft_plain<double>((double2*)c->PW.p, ncol, c->g, -1, s, c->nth, c->nq * ncol,
+                                   c->st);
+    else
+      cq::launch_dft_plain<float>((float2*)c->PW.p, ncol, c->g, -1, s, c->nth, c->nq * ncol,
+                                  c->st);
+    c->w_in_R = true;
+  }
+  c->mark("SIGMA_FT_W");
+  for (int64_t it = 0; it < c->nth; ++it) {
+    const bool minus = it < nt / 2;  // thc_gw.icc:59-61 writes Sigma(nt-1-it) for it < nt/2
+    project_p2a(c, c->G.p + it * gsz, c->Gp.p);
+    if (minus) project_p2a(c, c->G.p + (nt - it - 1) * gsz, c->Gn.p);
+    unsigned char* WR = c->PW.p + (size_t)it * c->nq * ncol * c->elem();
+    {
+      cq::Prof::Scope sc(&c->prof, "sigma_fused");
+      if (c->mode == COQUI_B200_FP64)
+        cq::launch_sigma_fused<double>((double2*)c->Gp.p, minus ? (double2*)c->Gn.p : nullptr,
+                                       (double2*)WR, (double2*)c->Gp.p,
+                                       minus ? (double2*)c->Gn.p : nullptr, ncol, c->g, c->st);
+      else
+        cq::launch_sigma_fused<float>((float2*)c->Gp.p, minus ? (float2*)c->Gn.p : nullptr,
+                                      (float2*)WR, (float2*)c->Gp.p,
+                                      minus ? (float2*)c->Gn.p : nullptr, ncol, c->g, c->st);
+    }
+    project_a2p(c, c->Gp.p, c->Sig.p + it * gsz);
+    if (minus) project_a2p(c, c->Gn.p, c->Sig.p + (nt - it - 1) * gsz);
+  }
+  c->mark("EVALUATE_SIGMA_R");
+}
+
+[[maybe_unused]] void w_to_q_space(Ctx* c) {
+  if (!c->w_in_R) return;
+  const int64_t ncol = c->Np * c->Np;
+  if (c->mode == COQUI_B200_FP64)
+    cq::launch_dft_plain<double>((double2*)c->PW.p, ncol, c->g, +1, 1.0, c->nth, c->nq * ncol,
+                                 c->st);
+  else
+    cq::launch_dft_plain<float>((float2*)c->PW.p, ncol, c->g, +1, 1.0, c->nth, c->nq * ncol,
+                                c->st);
+  c->w_in_R = false;
+}
+
+}  // namespace
+
+int coqui_b200_update_w(coqui_b200_ctx* c, const double* G_tskij, double* dW_qtPQ,
+                        double* eps_inv_head) {
+  return guarded(c, [&] {
+    require_ready(c, true, true, true);
+    c->begin_timing();
+    upload_G(c, G_tskij);
+    c->mark("h2d_G");
+    update_w_device(c);
+    if (eps_inv_head) {
+      eps_head(c, eps_inv_head);
+      c->mark("EPS_INV_HEAD");
+    }
+    if (dW_qtPQ) {
+      download_w_qt(c, dW_qtPQ);
+      c->mark("d2h_W");
+    }
+    c->end_timing();
+  });
+}
+
+int coqui_b200_set_w(coqui_b200_ctx* c, const double* dW_qtPQ) {
+  return guarded(c, [&] {
+    require_ready(c, true, true, true);
+    CQ_REQUIRE(dW_qtPQ, COQUI_B200_EINVAL, "null W");
+    const int64_t ncol = c->Np * c->Np, n = c->nq * c->nth * ncol;
+    c->PW.ensure((size_t)c->nmax * c->nq * ncol * c->elem());
+    c->stage.ensure(n);
+    upload(c, c->stage.p, dW_qtPQ, n * sizeof(double2));
+    if (c->mode == COQUI_B200_FP64)
+      cq::launch_qt_to_tq<double>(c->stage.p, (double2*)c->PW.p, c->nth, c->nq, ncol, c->st);
+    else
+      cq::launch_qt_to_tq<float>(c->stage.p, (float2*)c->PW.p, c->nth, c->nq, ncol, c->st);
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->stage.release();
+    c->w_valid = true;
+    c->w_in_R = false;
+  });
+}
+
+int coqui_b200_eval_sigma(coqui_b200_ctx* c, const double* G_tskij, double* Sigma_tskij) {
+  return guarded(c, [&] {
+    require_ready(c, true, true, true);
+    CQ_REQUIRE(c->w_valid, COQUI_B200_EINVAL, "no screened interaction: call update_w or set_w");
+    c->begin_timing();
+    upload_G(c, G_tskij);
+    c->mark("h2d_G");
+    sigma_device(c);
+    if (Sigma_tskij) {
+      download(c, Sigma_tskij, c->Sig.p, (size_t)c->nt * c->nk * c->nb * c->nb * sizeof(double2));
+      c->mark("d2h_Sigma");
+    }
+    c->end_timing();
+  });
+}
+
+int coqui_b200_gw_iteration(coqui_b200_ctx* c, const double* G_tskij, double* Sigma_tskij,
+                            double* eps_inv_head) {
+  return guarded(c, [&] {
+    require_ready(c, true, true, true);
+    c->begin_timing();
+    upload_G(c, G_tskij);
+    c->mark("h2d_G");
+    update_w_device(c);
+    if (eps_inv_head) {
+      eps_head(c, eps_inv_head);
+      c->mark("EPS_INV_HEAD");
+    }
+    sigma_device(c);
+    if (Sigma_tskij) {
+      download(c, Sigma_tskij, c->Sig.p, (size_t)c->nt * c->nk * c->nb * c->nb * sizeof(double2));
+      c->mark("d2h_Sigma");
+    }
+    c->end_timing();
+  });
+}
+
+int coqui_b200_set_profiling(coqui_b200_ctx* c, int on) {
+  return guarded(c, [&] {
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->prof.resolve();
+    c->prof.acc.clear();
+    c->prof.on = (on != 0);
+  });
+}
+
+int coqui_b200_kernel_stats(const coqui_b200_ctx* c, char* names, int name_len, double* ms,
+                            int64_t* launches, int n) {
+  if (!c) return COQUI_B200_EINVAL;
+  int k = 0;
+  for (const auto& p : c->prof.acc) {
+    if (k >= n) break;
+    if (names && name_len > 0) {
+      std::strncpy(names + (size_t)k * name_len, p.first.c_str(), name_len - 1);
+      names[(size_t)k * name_len + name_len - 1] = 0;
+    }
+    if (ms) ms[k] = p.second.first;
+    if (launches) launches[k] = p.second.second;
+    ++k;
+  }
+  return k;
+}
+
+int coqui_b200_rpa_energy(coqui_b200_ctx* c, const double* G_tskij, double* e_rpa) {
+  return guarded(c, [&] {
+    require_ready(c, true, true, true);
+    CQ_REQUIRE(e_rpa, COQUI_B200_EINVAL, "null e_rpa");
+    CQ_REQUIRE(c->Ttw_bb.size() == (size_t)(c->nt * c->nwb), COQUI_B200_EINVAL, "IR tables");
+    c->begin_timing();
+    upload_G(c, G_tskij);
+    c->mark("h2d_G");
+    eval_pi_device(c);
+    c->mark("EVALUATE_PI_R");
+    ir_inplace(c, (int)c->nth, (int)c->nwh, c->dTwt.p);
+    c->mark("IMAG_FT_TtoW");
+    std::vector<double> ld;
+    std::vector<double2> tr;
+    dyson_all(c, false, true, &ld, &tr);
+    c->mark("EVALUATE_RPA");
+    for (double v : ld)
+      CQ_REQUIRE(std::isfinite(v), COQUI_B200_ENOTHPD, "I - Pi V is not positive definite");
+    *e_rpa = rpa_energy_from(c, ld, tr);
+    c->end_timing();
+  });
+}
+
+int coqui_b200_tau_to_w(coqui_b200_ctx* c, const double* X_tqPQ, double* X_wqPQ) {
+  return guarded(c, [&] {
+    require_ready(c, false, true, false);
+    CQ_REQUIRE(X_tqPQ && X_wqPQ, COQUI_B200_EINVAL, "null arguments");
+    const int64_t ncol = c->nq * c->Np * c->Np;
+    c->PW.ensure((size_t)c->nmax * ncol * c->elem());
+    c->stage.ensure((size_t)c->nmax * ncol);
+    upload(c, c->stage.p, X_tqPQ, (size_t)c->nth * ncol * sizeof(double2));
+    if (c->mode == COQUI_B200_FP64)
+      CQ_CHECK_CUDA(cudaMemcpyAsync(c->PW.p, c->stage.p, (size_t)c->nth * ncol * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, c->st));
+    else
+      cq::launch_from_c128<float>(c->stage.p, (float2*)c->PW.p, c->nth * ncol, c->st);
+    ir_inplace(c, (int)c->nth, (int)c->nwh, c->dTwt.p);
+    if (c->mode == COQUI_B200_FP64)
+      download(c, X_wqPQ, c->PW.p, (size_t)c->nwh * ncol * sizeof(double2));
+    else {
+      cq::launch_to_c128<float>((float2*)c->PW.p, c->stage.p, c->nwh * ncol, c->st);
+      download(c, X_wqPQ, c->stage.p, (size_t)c->nwh * ncol * sizeof(double2));
+    }
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->w_valid = false;
+  });
+}
+
+int coqui_b200_w_to_tau(coqui_b200_ctx* c, const double* X_wqPQ, double* X_tqPQ) {
+  return guarded(c, [&] {
+    require_ready(c, false, true, false);
+    CQ_REQUIRE(X_tqPQ && X_wqPQ, COQUI_B200_EINVAL, "null arguments");
+    const int64_t ncol = c->nq * c->Np * c->Np;
+    c->PW.ensure((size_t)c->nmax * ncol * c->elem());
+    c->stage.ensure((size_t)c->nmax * ncol);
+    upload(c, c->stage.p, X_wqPQ, (size_t)c->nwh * ncol * sizeof(double2));
+    if (c->mode == COQUI_B200_FP64)
+      CQ_CHECK_CUDA(cudaMemcpyAsync(c->PW.p, c->stage.p, (size_t)c->nwh * ncol * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, c->st));
+    else
+      cq::launch_from_c128<float>(c->stage.p, (float2*)c->PW.p, c->nwh * ncol, c->st);
+    ir_inplace(c, (int)c->nwh, (int)c->nth, c->dTtw.p);
+    if (c->mode == COQUI_B200_FP64)
+      download(c, X_tqPQ, c->PW.p, (size_t)c->nth * ncol * sizeof(double2));
+    else {
+      cq::launch_to_c128<float>((float2*)c->PW.p, c->stage.p, c->nth * ncol, c->st);
+      download(c, X_tqPQ, c->stage.p, (size_t)c->nth * ncol * sizeof(double2));
+    }
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->w_valid = false;
+  });
+}
+
+int coqui_b200_dyson_w(coqui_b200_ctx* c, const double* Pi_wqPQ, double* W_wqPQ) {
+  return guarded(c, [&] {
+    require_ready(c, true, false, false);
+    CQ_REQUIRE(Pi_wqPQ && W_wqPQ, COQUI_B200_EINVAL, "null arguments");
+    // one frequency at a time: reuse the PW buffer with nw = 1 slabs
+    const int64_t ncol = c->nq * c->Np * c->Np;
+    const int64_t nw = c->nwh;
+    c->PW.ensure((size_t)c->nmax * ncol * c->elem());
+    c->stage.ensure((size_t)nw * ncol);
+    upload(c, c->stage.p, Pi_wqPQ, (size_t)nw * ncol * sizeof(double2));
+    if (c->mode == COQUI_B200_FP64)
+      CQ_CHECK_CUDA(cudaMemcpyAsync(c->PW.p, c->stage.p, (size_t)nw * ncol * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, c->st));
+    else
+      cq::launch_from_c128<float>(c->stage.p, (float2*)c->PW.p, nw * ncol, c->st);
+    dyson_all(c, true, false, nullptr, nullptr);
+    if (c->mode == COQUI_B200_FP64)
+      download(c, W_wqPQ, c->PW.p, (size_t)nw * ncol * sizeof(double2));
+    else {
+      cq::launch_to_c128<float>((float2*)c->PW.p, c->stage.p, nw * ncol, c->st);
+      download(c, W_wqPQ, c->stage.p, (size_t)nw * ncol * sizeof(double2));
+    }
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->w_valid = false;
+  });
+}
+
+}  // extern "C"

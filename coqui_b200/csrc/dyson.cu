@@ -1,0 +1,208 @@
+// Batched Dyson solve per (q, iW): products, FP64 Cholesky, log-determinant, W.
+#include <algorithm>
+#include <string>
+
+#include "dyson.cuh"
+#include "kernels.cuh"
+#include "tc_gemm.cuh"
+
+namespace cq {
+
+#define CQ_BLAS(expr)                                                                     \
+  do {                                                                                    \
+    cublasStatus_t _s = (expr);                                                           \
+    if (_s != CUBLAS_STATUS_SUCCESS)                                                      \
+      throw Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
+  } while (0)
+#define CQ_SOLVER(expr)                                                                   \
+  do {                                                                                    \
+    cusolverStatus_t _s = (expr);                                                         \
+    if (_s != CUSOLVER_STATUS_SUCCESS)                                                    \
+      throw Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
+  } while (0)
+
+__global__ void k_zero_upper_adjoint(double2* __restrict__ L, double2* __restrict__ LH, int64_t Np,
+                                     int64_t total) {
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = idx / (Np * Np), e = idx % (Np * Np);
+    const int64_t i = e / Np, j = e % Np;
+    double2* Lb = L + b * Np * Np;
+    // LH[i][j] = conj(L[j][i]) for j >= i (lower element of L), 0 otherwise
+    double2 v = make_double2(0, 0);
+    if (j >= i) {
+      const double2 l = Lb[j * Np + i];
+      v = make_double2(l.x, -l.y);
+    }
+    LH[idx] = v;
+    if (j > i) Lb[i * Np + j] = make_double2(0, 0);
+  }
+}
+
+void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t nbatch,
+                                   cudaStream_t s) {
+  const int64_t total = Np * Np * nbatch;
+  k_zero_upper_adjoint<<<grid_for(total, 256), 256, 0, s>>>(L, LH, Np, total);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+// cuSOLVER is column-major: the row-major buffer of a Hermitian A reads as conj(A); its
+// upper factor U (conj(A) = U^H U) reads back row-major as the lower C with A = C C^H.
+static void potrf_ptrs(cusolverDnHandle_t sol, double2** dptrs, int64_t Np, int* dinfo,
+                       int64_t nb) {
+  CQ_SOLVER(cusolverDnZpotrfBatched(sol, CUBLAS_FILL_MODE_UPPER, (int)Np,
+                                    reinterpret_cast<cuDoubleComplex**>(dptrs), (int)Np, dinfo,
+                                    (int)nb));
+}
+
+int cholesky_lower_batched(cusolverDnHandle_t sol, double2* A, int64_t Np, int64_t nbatch,
+                           cudaStream_t s) {
+  std::vector<double2*> h(nbatch);
+  for (int64_t b = 0; b < nbatch; ++b) h[b] = A + b * Np * Np;
+  DevBuf<unsigned char> buf;
+  buf.ensure(nbatch * (sizeof(double2*) + sizeof(int)));
+  double2** dp = (double2**)buf.p;
+  int* dinfo = (int*)(buf.p + nbatch * sizeof(double2*));
+  CQ_CHECK_CUDA(cudaMemcpyAsync(dp, h.data(), nbatch * sizeof(double2*), cudaMemcpyHostToDevice, s));
+  potrf_ptrs(sol, dp, Np, dinfo, nbatch);
+  std::vector<int> info(nbatch);
+  CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), dinfo, nbatch * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CQ_CHECK_CUDA(cudaStreamSynchronize(s));
+  buf.release();
+  for (int v : info)
+    if (v != 0) return v;
+  return 0;
+}
+
+void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
+               DevBuf<unsigned char>& scratch, cudaStream_t s, std::vector<double>* logdet,
+               std::vector<double2>* trace) {
+  const int64_t Np = a.Np, NN = Np * Np, nq = a.nq, nw = a.nw;
+  const size_t es = a.mixed ? sizeof(float2) : sizeof(double2);
+  // per problem: T1 (es), M (es), A (c128, own region in mixed mode), Y (c128 if want_w)
+  const size_t per = NN * (es + es + (a.mixed ? sizeof(double2) : 0) +
+                           (a.want_w ? sizeof(double2) : 0)) +
+                     4 * sizeof(void*) + sizeof(int) + sizeof(double) + sizeof(double2) + 64;
+  const size_t budget = (size_t)4 << 30;
+  const int64_t nbq = std::max<int64_t>(1, std::min<int64_t>(nq, (int64_t)(budget / per)));
+  scratch.ensure(per * nbq + 1024);
+  unsigned char* base = scratch.p;
+  auto carve = [&](size_t bytes) {
+    unsigned char* p = base;
+    base += (bytes + 255) & ~(size_t)255;
+    return p;
+  };
+  unsigned char* T1 = carve(nbq * NN * es);
+  unsigned char* Mb = carve(nbq * NN * es);
+  double2* A = a.mixed ? (double2*)carve(nbq * NN * sizeof(double2)) : (double2*)T1;
+  double2* Y = a.want_w ? (double2*)carve(nbq * NN * sizeof(double2)) : nullptr;
+  double2** dptrA = (double2**)carve(nbq * sizeof(void*));
+  double2** dptrY = (double2**)carve(nbq * sizeof(void*));
+  int* dinfo = (int*)carve(nbq * sizeof(int));
+  double* dld = (double*)carve(nbq * sizeof(double));
+  double2* dtr = (double2*)carve(nbq * sizeof(double2));
+
+  std::vector<double2*> hA(nbq), hY(nbq);
+  for (int64_t i = 0; i < nbq; ++i) {
+    hA[i] = A + i * NN;
+    hY[i] = Y ? Y + i * NN : nullptr;
+  }
+  CQ_CHECK_CUDA(cudaMemcpyAsync(dptrA, hA.data(), nbq * sizeof(void*), cudaMemcpyHostToDevice, s));
+  CQ_CHECK_CUDA(cudaMemcpyAsync(dptrY, hY.data(), nbq * sizeof(void*), cudaMemcpyHostToDevice, s));
+
+  if (a.want_e) {
+    logdet->assign(nw * nq, 0.0);
+    trace->assign(nw * nq, make_double2(0, 0));
+  }
+  std::vector<int> info_all;
+  std::vector<double> ld_h(nbq);
+  std::vector<double2> tr_h(nbq);
+  std::vector<int> info_h(nbq);
+
+  const double2 one = make_double2(1, 0), zero = make_double2(0, 0), mone = make_double2(-1, 0);
+  for (int64_t n = 0; n < nw; ++n) {
+    for (int64_t q0 = 0; q0 < nq; q0 += nbq) {
+      const int64_t nb = std::min(nbq, nq - q0);
+      const int64_t p0 = n * nq + q0;
+      unsigned char* Pi = a.PW + (size_t)p0 * NN * es;
+      const double2* L = a.L + q0 * NN;
+      const double2* LH = a.LH + q0 * NN;
+      const double2* V = a.V + q0 * NN;
+      // M = L^H (Pi L)
+      {
+      Prof::Scope sc(a.prof, "dyson_M_gemm");
+      if (a.mixed) {
+        tc_gemm_c(TcOp::N, (const float2*)Pi, TcOp::N, L, (float2*)T1, Np, Np, Np, nb, s);
+        tc_gemm_c(TcOp::N, LH, TcOp::N, (const float2*)T1, (float2*)Mb, Np, Np, Np, nb, s);
+        launch_eye_minus<float>((const float2*)Mb, A, Np, nb, s);
+      } else {
+        // row-major C = A B  ->  column-major C^T = B^T A^T
+        CQ_BLAS(cublasZgemmStridedBatched(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)Np, (int)Np, (int)Np,
+                                          (const cuDoubleComplex*)&one, (const cuDoubleComplex*)L,
+                                          (int)Np, NN, (const cuDoubleComplex*)Pi, (int)Np, NN,
+                                          (const cuDoubleComplex*)&zero, (cuDoubleComplex*)T1,
+                                          (int)Np, NN, (int)nb));
+        CQ_BLAS(cublasZgemmStridedBatched(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)Np, (int)Np, (int)Np,
+                                          (const cuDoubleComplex*)&one, (const cuDoubleComplex*)T1,
+                                          (int)Np, NN, (const cuDoubleComplex*)LH, (int)Np, NN,
+                                          (const cuDoubleComplex*)&zero, (cuDoubleComplex*)Mb,
+                                          (int)Np, NN, (int)nb));
+        launch_eye_minus<double>((const double2*)Mb, A, Np, nb, s);
+      }
+      }
+      // I - M = C C^H (FP64)
+      {
+        Prof::Scope sc(a.prof, "dyson_potrf");
+        potrf_ptrs(sol, dptrA, Np, dinfo, nb);
+      }
+      CQ_CHECK_CUDA(cudaMemcpyAsync(info_h.data(), dinfo, nb * sizeof(int), cudaMemcpyDeviceToHost, s));
+      if (a.want_e) {
+        Prof::Scope sc(a.prof, "rpa_logdet");
+        if (a.mixed)
+          launch_logdet_trace<float>(A, (const float2*)Mb, dld, dtr, Np, nb, s);
+        else
+          launch_logdet_trace<double>(A, (const double2*)Mb, dld, dtr, Np, nb, s);
+        CQ_CHECK_CUDA(cudaMemcpyAsync(ld_h.data(), dld, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CQ_CHECK_CUDA(cudaMemcpyAsync(tr_h.data(), dtr, nb * sizeof(double2), cudaMemcpyDeviceToHost, s));
+      }
+      if (a.want_w) {
+        // Y = C^{-1} L^H: column-major Y^T C^T = (L^H)^T  (right, upper)
+        CQ_CHECK_CUDA(cudaMemcpyAsync(Y, LH, nb * NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        {
+        Prof::Scope sc(a.prof, "dyson_trsm");
+        CQ_BLAS(cublasZtrsmBatched(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                                   CUBLAS_DIAG_NON_UNIT, (int)Np, (int)Np,
+                                   (const cuDoubleComplex*)&one,
+                                   (const cuDoubleComplex* const*)dptrA, (int)Np,
+                                   (cuDoubleComplex* const*)dptrY, (int)Np, (int)nb));
+        }
+        Prof::Scope sc(a.prof, "dyson_W_gemm");
+        // W = Y^H Y - V, written over Pi
+        if (a.mixed) {
+          launch_from_c128<float>(V, (float2*)Pi, nb * NN, s);
+          tc_gemm_c(TcOp::C, Y, TcOp::N, Y, (float2*)Pi, Np, Np, Np, nb, s, /*beta_minus_one=*/true);
+        } else {
+          CQ_CHECK_CUDA(cudaMemcpyAsync(Pi, V, nb * NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+          CQ_BLAS(cublasZgemmStridedBatched(blas, CUBLAS_OP_N, CUBLAS_OP_C, (int)Np, (int)Np, (int)Np,
+                                            (const cuDoubleComplex*)&one, (const cuDoubleComplex*)Y,
+                                            (int)Np, NN, (const cuDoubleComplex*)Y, (int)Np, NN,
+                                            (const cuDoubleComplex*)&mone, (cuDoubleComplex*)Pi,
+                                            (int)Np, NN, (int)nb));
+        }
+      }
+      CQ_CHECK_CUDA(cudaStreamSynchronize(s));
+      for (int64_t i = 0; i < nb; ++i) {
+        if (info_h[i] != 0)
+          throw Error(COQUI_B200_ENOTHPD, "I - L^H Pi L is not positive definite at (w=" +
+                                              std::to_string(n) + ", q=" + std::to_string(q0 + i) + ")");
+        if (a.want_e) {
+          (*logdet)[p0 + i] = ld_h[i];
+          (*trace)[p0 + i] = tr_h[i];
+        }
+      }
+    }
+  }
+}
+
+}  // namespace cq

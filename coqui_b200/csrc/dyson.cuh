@@ -1,0 +1,45 @@
+// Batched per-(q, iW) Dyson solve for the screened interaction and the RPA log-determinant.
+//
+// Reference (scr_coulomb_t.cpp:171-199, thc_rpa.icc:130-165) forms A = V Pi, inverts
+// I - A by LU and returns W = ([I - V Pi]^{-1} - I) V, and ln det(I - Pi V) by LU.
+// Here the Hermitian form of the same quantities is used:
+//   V = L L^H (once per q),  M = L^H Pi L,  I - M = C C^H  (FP64 Cholesky),
+//   Tr(Pi V) = Tr M,  ln det(I - Pi V) = 2 sum_i ln C_ii,
+//   W = L (I - M)^{-1} L^H - V = Y^H Y - V  with  Y = C^{-1} L^H.
+#pragma once
+
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace cq {
+
+// In-place lower Cholesky factor (row-major, A = L L^H) of nbatch Np x Np matrices.
+// Returns the first nonzero LAPACK info (0 = success).  The strict upper triangle is left
+// undefined.
+int cholesky_lower_batched(cusolverDnHandle_t sol, double2* A, int64_t Np, int64_t nbatch,
+                           cudaStream_t s);
+
+// Zero the strict upper triangle of L and write LH = L^H (row-major), batched.
+void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t nbatch,
+                                   cudaStream_t s);
+
+struct DysonArgs {
+  int64_t Np = 0, nq = 0, nw = 0;
+  const double2* L = nullptr;   // (nq, Np, Np) lower Cholesky factors of V
+  const double2* LH = nullptr;  // (nq, Np, Np) L^H
+  const double2* V = nullptr;   // (nq, Np, Np)
+  bool want_w = true, want_e = false, mixed = true;
+  unsigned char* PW = nullptr;  // (nw, nq, Np, Np): Pi(iW) in, W(iW) out (if want_w)
+  Prof* prof = nullptr;
+};
+
+// Runs every (iW, q) problem; fills logdet / trace (indexed n * nq + q) if want_e.
+void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
+               DevBuf<unsigned char>& scratch, cudaStream_t s, std::vector<double>* logdet,
+               std::vector<double2>* trace);
+
+}  // namespace cq

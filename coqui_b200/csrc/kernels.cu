@@ -1,0 +1,702 @@
+// SIMT kernels of the THC-RPA/GW path: fused k<->R DFT + Hadamard products, in-place IR
+// transforms, layout conversions, determinants and the dielectric head.
+//
+// All large arrays are (leading index, ncol) row-major with ncol = Np * Np consecutive
+// auxiliary-basis elements, so every kernel reads and writes whole 32-column runs per warp.
+#include <atomic>
+#include <mutex>
+
+#include "kernels.cuh"
+
+namespace cq {
+
+static std::atomic<int64_t> g_launches{0};
+int64_t launches_total() { return g_launches.load(); }
+void count_launch(int64_t n) { g_launches += n; }
+
+#define CQ_LAUNCHED() \
+  do {                \
+    count_launch();   \
+    CQ_CHECK_CUDA(cudaGetLastError()); \
+  } while (0)
+
+// ---------------------------------------------------------------------------------------
+// small DFTs
+// ---------------------------------------------------------------------------------------
+constexpr int kMaxDftN = 8;
+// c_tw[n][r] = exp(-2 pi i r / n)
+__constant__ double2 c_tw[kMaxDftN + 1][kMaxDftN];
+
+void upload_twiddles() {
+  static std::mutex mu;
+  static int done_mask = 0;  // one bit per device ordinal (< 32)
+  int dev = 0;
+  CQ_CHECK_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 32 && (done_mask >> dev) & 1) return;
+  double2 h[kMaxDftN + 1][kMaxDftN] = {};
+  const double pi = 3.14159265358979323846;
+  for (int n = 1; n <= kMaxDftN; ++n)
+    for (int r = 0; r < n; ++r) {
+      h[n][r].x = std::cos(2.0 * pi * r / n);
+      h[n][r].y = -std::sin(2.0 * pi * r / n);
+    }
+  // exact values for the quarter turns
+  for (int n = 1; n <= kMaxDftN; ++n)
+    for (int r = 0; r < n; ++r) {
+      if ((4 * r) % n == 0) {
+        int q = (4 * r) / n;  // r/n = q/4
+        const double cs[4] = {1, 0, -1, 0}, sn[4] = {0, -1, 0, 1};
+        h[n][r].x = cs[q & 3];
+        h[n][r].y = sn[q & 3];
+      }
+    }
+  CQ_CHECK_CUDA(cudaMemcpyToSymbol(c_tw, h, sizeof(h)));
+  if (dev < 32) done_mask |= 1 << dev;
+}
+
+template <typename C, int N>
+__device__ __forceinline__ void dft_line(C (&x)[N], int sign) {
+  if constexpr (N == 1) {
+    return;
+  } else if constexpr (N == 2) {
+    C a = x[0], b = x[1];
+    x[0] = cadd(a, b);
+    x[1] = csub(a, b);
+  } else if constexpr (N == 4) {
+    C a0 = cadd(x[0], x[2]), a1 = csub(x[0], x[2]);
+    C b0 = cadd(x[1], x[3]), b1 = csub(x[1], x[3]);
+    C b1w;  // b1 * exp(sign i pi / 2)
+    if (sign > 0) { b1w.x = -b1.y; b1w.y = b1.x; }
+    else { b1w.x = b1.y; b1w.y = -b1.x; }
+    x[0] = cadd(a0, b0);
+    x[2] = csub(a0, b0);
+    x[1] = cadd(a1, b1w);
+    x[3] = csub(a1, b1w);
+  } else {
+    C y[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      C acc = x[0];
+#pragma unroll
+      for (int m = 1; m < N; ++m) {
+        const double2 t = c_tw[N][(j * m) % N];
+        C w;
+        w.x = t.x;
+        w.y = sign > 0 ? -t.y : t.y;
+        acc = cadd(acc, cmul(x[m], w));
+      }
+      y[j] = acc;
+    }
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = y[j];
+  }
+}
+
+// One dimension (length N, stride `stride` in k units) of the DFT of a smem tile A[k][TILE].
+template <typename C, int TILE, int N>
+__device__ __forceinline__ void dft_dim_n(C* A, int stride, int nk, int sign) {
+  const int lines = nk / N;
+  const int items = lines * TILE;
+  for (int i = threadIdx.x; i < items; i += blockDim.x) {
+    const int c = i % TILE;
+    const int line = i / TILE;
+    const int inner = line % stride, outer = line / stride;
+    const int k0 = outer * N * stride + inner;
+    C x[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) x[m] = A[(k0 + m * stride) * TILE + c];
+    dft_line<C, N>(x, sign);
+#pragma unroll
+    for (int m = 0; m < N; ++m) A[(k0 + m * stride) * TILE + c] = x[m];
+  }
+}
+
+template <typename C, int TILE>
+__device__ void dft_dim(C* A, int n, int stride, int nk, int sign) {
+  switch (n) {
+    case 1: break;
+    case 2: dft_dim_n<C, TILE, 2>(A, stride, nk, sign); break;
+    case 3: dft_dim_n<C, TILE, 3>(A, stride, nk, sign); break;
+    case 4: dft_dim_n<C, TILE, 4>(A, stride, nk, sign); break;
+    case 5: dft_dim_n<C, TILE, 5>(A, stride, nk, sign); break;
+    case 6: dft_dim_n<C, TILE, 6>(A, stride, nk, sign); break;
+    case 7: dft_dim_n<C, TILE, 7>(A, stride, nk, sign); break;
+    case 8: dft_dim_n<C, TILE, 8>(A, stride, nk, sign); break;
+    default: break;  // rejected on the host
+  }
+}
+
+// 3D DFT of up to three tiles at once (fewer barriers).
+template <typename C, int TILE>
+__device__ void dft3(C* A, C* B, int n0, int n1, int n2, int sign) {
+  const int nk = n0 * n1 * n2;
+  dft_dim<C, TILE>(A, n2, 1, nk, sign);
+  if (B) dft_dim<C, TILE>(B, n2, 1, nk, sign);
+  __syncthreads();
+  dft_dim<C, TILE>(A, n1, n2, nk, sign);
+  if (B) dft_dim<C, TILE>(B, n1, n2, nk, sign);
+  __syncthreads();
+  dft_dim<C, TILE>(A, n0, n1 * n2, nk, sign);
+  if (B) dft_dim<C, TILE>(B, n0, n1 * n2, nk, sign);
+  __syncthreads();
+}
+
+template <typename C, int TILE>
+__device__ __forceinline__ void load_tile(C* A, const C* __restrict__ src, int nk, int64_t ncol,
+                                          int64_t col0) {
+  for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) {
+    const int k = i / TILE, c = i % TILE;
+    const int64_t col = col0 + c;
+    C v;
+    v.x = 0;
+    v.y = 0;
+    if (col < ncol) v = src[(int64_t)k * ncol + col];
+    A[i] = v;
+  }
+}
+
+template <typename C, int TILE>
+__device__ __forceinline__ void store_tile(const C* A, C* dst, int nk, int64_t ncol,
+                                           int64_t col0) {
+  for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) {
+    const int k = i / TILE, c = i % TILE;
+    const int64_t col = col0 + c;
+    if (col < ncol) dst[(int64_t)k * ncol + col] = A[i];
+  }
+}
+
+template <typename R, int TILE>
+__global__ void __launch_bounds__(256) k_pi_fused(const cplx_t<R>* __restrict__ Gp,
+                                                  const cplx_t<R>* __restrict__ Gn,
+                                                  cplx_t<R>* __restrict__ Pi, int64_t ncol,
+                                                  int n0, int n1, int n2, R scale) {
+  using C = cplx_t<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nk = n0 * n1 * n2;
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + nk * TILE;
+  const int64_t ntiles = (ncol + TILE - 1) / TILE;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t col0 = t * TILE;
+    load_tile<C, TILE>(A, Gp, nk, ncol, col0);
+    load_tile<C, TILE>(B, Gn, nk, ncol, col0);
+    __syncthreads();
+    dft3<C, TILE>(A, B, n0, n1, n2, -1);
+    for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) A[i] = cscale(cmulc(A[i], B[i]), scale);
+    __syncthreads();
+    dft3<C, TILE>(A, (C*)nullptr, n0, n1, n2, +1);
+    store_tile<C, TILE>(A, Pi, nk, ncol, col0);
+    __syncthreads();
+  }
+}
+
+template <typename R, int TILE>
+__global__ void __launch_bounds__(256) k_sigma_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gm,
+                                                     const cplx_t<R>* __restrict__ WR,
+                                                     cplx_t<R>* Sp, cplx_t<R>* Sm, int64_t ncol,
+                                                     int n0, int n1, int n2, R scale) {
+  using C = cplx_t<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nk = n0 * n1 * n2;
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + nk * TILE;
+  C* Wt = B + nk * TILE;
+  const bool has_m = (Gm != nullptr);
+  const int64_t ntiles = (ncol + TILE - 1) / TILE;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t col0 = t * TILE;
+    load_tile<C, TILE>(A, Gp, nk, ncol, col0);
+    if (has_m) load_tile<C, TILE>(B, Gm, nk, ncol, col0);
+    load_tile<C, TILE>(Wt, WR, nk, ncol, col0);
+    __syncthreads();
+    dft3<C, TILE>(A, has_m ? B : (C*)nullptr, n0, n1, n2, -1);
+    for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) {
+      const C w = cscale(Wt[i], scale);
+      A[i] = cmul(A[i], w);
+      if (has_m) B[i] = cmul(B[i], w);
+    }
+    __syncthreads();
+    dft3<C, TILE>(A, has_m ? B : (C*)nullptr, n0, n1, n2, +1);
+    store_tile<C, TILE>(A, Sp, nk, ncol, col0);
+    if (has_m) store_tile<C, TILE>(B, Sm, nk, ncol, col0);
+    __syncthreads();
+  }
+}
+
+template <typename R, int TILE>
+__global__ void __launch_bounds__(256) k_dft_plain(cplx_t<R>* __restrict__ buf, int64_t ncol,
+                                                   int n0, int n1, int n2, int sign, R scale,
+                                                   int64_t nbatch, int64_t bstride) {
+  using C = cplx_t<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nk = n0 * n1 * n2;
+  C* A = reinterpret_cast<C*>(smem_raw);
+  const int64_t ntiles = (ncol + TILE - 1) / TILE;
+  for (int64_t t = blockIdx.x; t < ntiles * nbatch; t += gridDim.x) {
+    const int64_t b = t / ntiles;
+    const int64_t col0 = (t % ntiles) * TILE;
+    C* base = buf + b * bstride;
+    load_tile<C, TILE>(A, base, nk, ncol, col0);
+    __syncthreads();
+    dft3<C, TILE>(A, (C*)nullptr, n0, n1, n2, sign);
+    for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) A[i] = cscale(A[i], scale);
+    __syncthreads();
+    store_tile<C, TILE>(A, base, nk, ncol, col0);
+    __syncthreads();
+  }
+}
+
+template <typename R>
+static int pick_tile(int nk) {
+  // keep at most ~96 KB of tiles per block (three tiles in the sigma kernel)
+  const int64_t per32 = (int64_t)nk * 32 * sizeof(cplx_t<R>) * 3;
+  return per32 <= 96 * 1024 ? 32 : 16;
+}
+
+static void check_grid(KGrid g) {
+  CQ_REQUIRE(g.n0 >= 1 && g.n1 >= 1 && g.n2 >= 1 && g.n0 <= kMaxDftN && g.n1 <= kMaxDftN &&
+                 g.n2 <= kMaxDftN,
+             COQUI_B200_EUNSUPPORTED, "k-grid edges must be in [1, 8]");
+}
+
+static void set_smem(const void* fn, size_t bytes) {
+  if (bytes > 48 * 1024)
+    CQ_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+template <typename R>
+void launch_pi_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gn, cplx_t<R>* Pi, int64_t ncol,
+                     KGrid g, double sp, cudaStream_t s) {
+  check_grid(g);
+  const int nk = g.nk();
+  const R scale = (R)(sp / ((double)nk * (double)nk));
+  const int tile = pick_tile<R>(nk);
+  const size_t smem = (size_t)2 * nk * tile * sizeof(cplx_t<R>);
+  const int64_t ntiles = (ncol + tile - 1) / tile;
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, 148 * 16);
+  if (tile == 32) {
+    set_smem((const void*)k_pi_fused<R, 32>, smem);
+    k_pi_fused<R, 32><<<grid, 256, smem, s>>>(Gp, Gn, Pi, ncol, g.n0, g.n1, g.n2, scale);
+  } else {
+    set_smem((const void*)k_pi_fused<R, 16>, smem);
+    k_pi_fused<R, 16><<<grid, 256, smem, s>>>(Gp, Gn, Pi, ncol, g.n0, g.n1, g.n2, scale);
+  }
+  CQ_LAUNCHED();
+}
+
+template <typename R>
+void launch_sigma_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gm, const cplx_t<R>* WR,
+                        cplx_t<R>* Sp, cplx_t<R>* Sm, int64_t ncol, KGrid g, cudaStream_t s) {
+  check_grid(g);
+  const int nk = g.nk();
+  // Sigma = f_kR [ -(f_Rk G) * W_R ]; f_Rk carries 1/nk
+  const R scale = (R)(-1.0 / (double)nk);
+  const int tile = pick_tile<R>(nk);
+  const size_t smem = (size_t)3 * nk * tile * sizeof(cplx_t<R>);
+  const int64_t ntiles = (ncol + tile - 1) / tile;
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, 148 * 16);
+  if (tile == 32) {
+    set_smem((const void*)k_sigma_fused<R, 32>, smem);
+    k_sigma_fused<R, 32><<<grid, 256, smem, s>>>(Gp, Gm, WR, Sp, Sm, ncol, g.n0, g.n1, g.n2, scale);
+  } else {
+    set_smem((const void*)k_sigma_fused<R, 16>, smem);
+    k_sigma_fused<R, 16><<<grid, 256, smem, s>>>(Gp, Gm, WR, Sp, Sm, ncol, g.n0, g.n1, g.n2, scale);
+  }
+  CQ_LAUNCHED();
+}
+
+template <typename R>
+void launch_dft_plain(cplx_t<R>* buf, int64_t ncol, KGrid g, int sign, double scale,
+                      int64_t nbatch, int64_t bstride, cudaStream_t s) {
+  check_grid(g);
+  const int nk = g.nk();
+  const int tile = pick_tile<R>(nk);
+  const size_t smem = (size_t)nk * tile * sizeof(cplx_t<R>);
+  const int64_t ntiles = (ncol + tile - 1) / tile * nbatch;
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, 148 * 16);
+  if (tile == 32) {
+    set_smem((const void*)k_dft_plain<R, 32>, smem);
+    k_dft_plain<R, 32><<<grid, 256, smem, s>>>(buf, ncol, g.n0, g.n1, g.n2, sign, (R)scale,
+                                               nbatch, bstride);
+  } else {
+    set_smem((const void*)k_dft_plain<R, 16>, smem);
+    k_dft_plain<R, 16><<<grid, 256, smem, s>>>(buf, ncol, g.n0, g.n1, g.n2, sign, (R)scale,
+                                               nbatch, bstride);
+  }
+  CQ_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------------------
+// IR transforms along the leading (tau or iw) index, in place, FP64 accumulation
+// ---------------------------------------------------------------------------------------
+template <typename R, int MAXT>
+__global__ void __launch_bounds__(128) k_ir_transform(cplx_t<R>* __restrict__ buf, int64_t ncol,
+                                                      int n_in, int n_out,
+                                                      const double2* __restrict__ M) {
+  extern __shared__ double2 sM[];
+  for (int i = threadIdx.x; i < n_in * n_out; i += blockDim.x) sM[i] = M[i];
+  __syncthreads();
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ncol;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    double2 x[MAXT];
+#pragma unroll
+    for (int t = 0; t < MAXT; ++t) {
+      if (t < n_in) {
+        const cplx_t<R> v = buf[(int64_t)t * ncol + e];
+        x[t].x = v.x;
+        x[t].y = v.y;
+      } else {
+        x[t].x = 0;
+        x[t].y = 0;
+      }
+    }
+    for (int n = 0; n < n_out; ++n) {
+      double ar = 0, ai = 0;
+      const double2* row = sM + n * n_in;
+#pragma unroll
+      for (int t = 0; t < MAXT; ++t) {
+        if (t < n_in) {
+          const double2 m = row[t];
+          ar = fma(m.x, x[t].x, ar);
+          ar = fma(-m.y, x[t].y, ar);
+          ai = fma(m.x, x[t].y, ai);
+          ai = fma(m.y, x[t].x, ai);
+        }
+      }
+      cplx_t<R> o;
+      o.x = (R)ar;
+      o.y = (R)ai;
+      buf[(int64_t)n * ncol + e] = o;
+    }
+  }
+}
+
+template <typename R>
+void launch_ir_transform(cplx_t<R>* buf, int64_t ncol, int n_in, int n_out, const double2* M,
+                         cudaStream_t s) {
+  CQ_REQUIRE(n_in >= 1 && n_in <= 96 && n_out >= 1, COQUI_B200_EUNSUPPORTED,
+             "IR transform supports at most 96 input points");
+  const size_t smem = (size_t)n_in * n_out * sizeof(double2);
+  const unsigned grid = grid_for(ncol, 128, 148 * 32);
+  if (n_in <= 32) {
+    set_smem((const void*)k_ir_transform<R, 32>, smem);
+    k_ir_transform<R, 32><<<grid, 128, smem, s>>>(buf, ncol, n_in, n_out, M);
+  } else {
+    set_smem((const void*)k_ir_transform<R, 96>, smem);
+    k_ir_transform<R, 96><<<grid, 128, smem, s>>>(buf, ncol, n_in, n_out, M);
+  }
+  CQ_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------------------
+// conversions, layout changes
+// ---------------------------------------------------------------------------------------
+template <typename R>
+__global__ void k_from_c128(const double2* __restrict__ in, cplx_t<R>* __restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = in[i];
+    cplx_t<R> o;
+    o.x = (R)v.x;
+    o.y = (R)v.y;
+    out[i] = o;
+  }
+}
+template <typename R>
+__global__ void k_to_c128(const cplx_t<R>* __restrict__ in, double2* __restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const cplx_t<R> v = in[i];
+    out[i] = make_double2(v.x, v.y);
+  }
+}
+template <typename R>
+void launch_from_c128(const double2* in, cplx_t<R>* out, int64_t n, cudaStream_t s) {
+  k_from_c128<R><<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
+  CQ_LAUNCHED();
+}
+template <typename R>
+void launch_to_c128(const cplx_t<R>* in, double2* out, int64_t n, cudaStream_t s) {
+  k_to_c128<R><<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
+  CQ_LAUNCHED();
+}
+
+template <typename R>
+__global__ void k_tq_to_qt(const cplx_t<R>* __restrict__ W, double2* __restrict__ out, int64_t nt,
+                           int64_t nq, int64_t ncol, int64_t q0, int64_t nqc) {
+  const int64_t total = nqc * nt * ncol;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = i % ncol;
+    const int64_t t = (i / ncol) % nt;
+    const int64_t q = i / (ncol * nt);
+    const cplx_t<R> v = W[(t * nq + q0 + q) * ncol + e];
+    out[i] = make_double2(v.x, v.y);
+  }
+}
+template <typename R>
+void launch_tq_to_qt_c128(const cplx_t<R>* W, double2* out, int64_t nt, int64_t nq, int64_t ncol,
+                          int64_t q0, int64_t nqc, cudaStream_t s) {
+  k_tq_to_qt<R><<<grid_for(nqc * nt * ncol, 256), 256, 0, s>>>(W, out, nt, nq, ncol, q0, nqc);
+  CQ_LAUNCHED();
+}
+
+template <typename R>
+__global__ void k_qt_to_tq(const double2* __restrict__ in, cplx_t<R>* __restrict__ W, int64_t nt,
+                           int64_t nq, int64_t ncol) {
+  const int64_t total = nq * nt * ncol;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = i % ncol;
+    const int64_t q = (i / ncol) % nq;
+    const int64_t t = i / (ncol * nq);
+    const double2 v = in[(q * nt + t) * ncol + e];
+    cplx_t<R> o;
+    o.x = (R)v.x;
+    o.y = (R)v.y;
+    W[i] = o;
+  }
+}
+template <typename R>
+void launch_qt_to_tq(const double2* in, cplx_t<R>* W, int64_t nt, int64_t nq, int64_t ncol,
+                     cudaStream_t s) {
+  k_qt_to_tq<R><<<grid_for(nq * nt * ncol, 256), 256, 0, s>>>(in, W, nt, nq, ncol);
+  CQ_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------------------
+// Dyson helpers
+// ---------------------------------------------------------------------------------------
+template <typename R>
+__global__ void k_eye_minus(const cplx_t<R>* __restrict__ M, double2* __restrict__ A, int64_t Np,
+                            int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = i % (Np * Np);
+    const cplx_t<R> m = M[i];
+    double2 a = make_double2(-(double)m.x, -(double)m.y);
+    if (e / Np == e % Np) a.x += 1.0;
+    A[i] = a;
+  }
+}
+template <typename R>
+void launch_eye_minus(const cplx_t<R>* M, double2* A, int64_t Np, int64_t nprob, cudaStream_t s) {
+  const int64_t n = Np * Np * nprob;
+  k_eye_minus<R><<<grid_for(n, 256), 256, 0, s>>>(M, A, Np, n);
+  CQ_LAUNCHED();
+}
+
+template <typename R>
+__global__ void k_logdet_trace(const double2* __restrict__ Cf, const cplx_t<R>* __restrict__ M,
+                               double* __restrict__ logdet, double2* __restrict__ trace,
+                               int64_t Np) {
+  const int64_t p = blockIdx.x;
+  const double2* c = Cf + p * Np * Np;
+  const cplx_t<R>* m = M + p * Np * Np;
+  double ld = 0, tr = 0, ti = 0;
+  for (int64_t i = threadIdx.x; i < Np; i += blockDim.x) {
+    ld += log(c[i * Np + i].x);
+    const cplx_t<R> v = m[i * Np + i];
+    tr += v.x;
+    ti += v.y;
+  }
+  __shared__ double s0[256], s1[256], s2[256];
+  s0[threadIdx.x] = ld;
+  s1[threadIdx.x] = tr;
+  s2[threadIdx.x] = ti;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s0[threadIdx.x] += s0[threadIdx.x + w];
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    logdet[p] = 2.0 * s0[0];
+    trace[p] = make_double2(s1[0], s2[0]);
+  }
+}
+template <typename R>
+void launch_logdet_trace(const double2* C, const cplx_t<R>* M, double* logdet, double2* trace,
+                         int64_t Np, int64_t nprob, cudaStream_t s) {
+  k_logdet_trace<R><<<(unsigned)nprob, 256, 0, s>>>(C, M, logdet, trace, Np);
+  CQ_LAUNCHED();
+}
+
+template <typename R>
+__global__ void k_eps_head(const cplx_t<R>* __restrict__ W, const double2* __restrict__ chi,
+                           const double* __restrict__ fac, double2* __restrict__ eps, int64_t nq,
+                           int64_t Np) {
+  const int64_t tq = blockIdx.x;  // t * nq + q
+  const int64_t q = tq % nq;
+  const cplx_t<R>* w = W + tq * Np * Np;
+  const double2* x = chi + q * Np;
+  double ar = 0, ai = 0;
+  for (int64_t i = threadIdx.x; i < Np * Np; i += blockDim.x) {
+    const int64_t P = i / Np, Q = i % Np;
+    const cplx_t<R> v = w[i];
+    // chi_P * W_PQ * conj(chi_Q)
+    const double2 a = x[P], b = x[Q];
+    const double pr = a.x * v.x - a.y * v.y, pi = a.x * v.y + a.y * v.x;
+    ar += pr * b.x + pi * b.y;
+    ai += pi * b.x - pr * b.y;
+  }
+  __shared__ double s0[256], s1[256];
+  s0[threadIdx.x] = ar;
+  s1[threadIdx.x] = ai;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) {
+      s0[threadIdx.x] += s0[threadIdx.x + k];
+      s1[threadIdx.x] += s1[threadIdx.x + k];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) eps[tq] = make_double2(fac[q] * s0[0], fac[q] * s1[0]);
+}
+template <typename R>
+void launch_eps_head(const cplx_t<R>* W, const double2* chi, const double* fac, double2* eps,
+                     int64_t nt, int64_t nq, int64_t Np, cudaStream_t s) {
+  k_eps_head<R><<<(unsigned)(nt * nq), 256, 0, s>>>(W, chi, fac, eps, nq, Np);
+  CQ_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------------------
+// generic strided batched complex GEMM on CUDA cores (64x64 tile, 4x4 per thread)
+// ---------------------------------------------------------------------------------------
+template <typename T> struct CReal;
+template <> struct CReal<float2> { using type = float; };
+template <> struct CReal<double2> { using type = double; };
+
+template <typename TA, typename TB, typename TC, typename Acc>
+__global__ void __launch_bounds__(256) k_gemm_simt(GemmDesc d, const TA* __restrict__ A,
+                                                   const TB* __restrict__ B, TC* __restrict__ C) {
+  constexpr int BM = 64, BN = 64, BK = 16;
+  __shared__ Acc sAr[BK][BM + 1], sAi[BK][BM + 1], sBr[BK][BN + 1], sBi[BK][BN + 1];
+  const int64_t b = blockIdx.z;
+  const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+  const TA* Ab = A + b * d.bsa;
+  const TB* Bb = B + b * d.bsb;
+  TC* Cb = C + b * d.bsc;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  Acc cr[4][4] = {}, ci[4][4] = {};
+  const Acc sa = d.conj_a ? -1 : 1, sb = d.conj_b ? -1 : 1;
+  for (int64_t k0 = 0; k0 < d.K; k0 += BK) {
+    for (int i = threadIdx.x; i < BM * BK; i += 256) {
+      const int mm = i % BM, kk = i / BM;
+      const int64_t m = m0 + mm, k = k0 + kk;
+      Acc vr = 0, vi = 0;
+      if (m < d.M && k < d.K) {
+        const TA v = Ab[m * d.sam + k * d.sak];
+        vr = (Acc)v.x;
+        vi = sa * (Acc)v.y;
+      }
+      sAr[kk][mm] = vr;
+      sAi[kk][mm] = vi;
+    }
+    for (int i = threadIdx.x; i < BN * BK; i += 256) {
+      const int nn = i % BN, kk = i / BN;
+      const int64_t n = n0 + nn, k = k0 + kk;
+      Acc vr = 0, vi = 0;
+      if (n < d.N && k < d.K) {
+        const TB v = Bb[k * d.sbk + n * d.sbn];
+        vr = (Acc)v.x;
+        vi = sb * (Acc)v.y;
+      }
+      sBr[kk][nn] = vr;
+      sBi[kk][nn] = vi;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      Acc ar[4], ai[4], br[4], bi[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        ar[i] = sAr[kk][ty + 16 * i];
+        ai[i] = sAi[kk][ty + 16 * i];
+        br[i] = sBr[kk][tx + 16 * i];
+        bi[i] = sBi[kk][tx + 16 * i];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          cr[i][j] += ar[i] * br[j] - ai[i] * bi[j];
+          ci[i][j] += ar[i] * bi[j] + ai[i] * br[j];
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
+      if (m < d.M && n < d.N) {
+        TC* c = Cb + m * d.scm + n * d.scn;
+        double re = d.alpha.x * (double)cr[i][j] - d.alpha.y * (double)ci[i][j];
+        double im = d.alpha.x * (double)ci[i][j] + d.alpha.y * (double)cr[i][j];
+        if (d.beta.x != 0.0 || d.beta.y != 0.0) {
+          const TC o = *c;
+          re += d.beta.x * (double)o.x - d.beta.y * (double)o.y;
+          im += d.beta.x * (double)o.y + d.beta.y * (double)o.x;
+        }
+        TC r;
+        r.x = re;
+        r.y = im;
+        *c = r;
+      }
+    }
+}
+
+template <typename TA, typename TB, typename TC, typename Acc>
+void launch_gemm_simt(const GemmDesc& d, const TA* A, const TB* B, TC* C, cudaStream_t s) {
+  CQ_REQUIRE(d.batch <= 65535, COQUI_B200_EINVAL, "gemm batch too large");
+  dim3 grid((unsigned)((d.N + 63) / 64), (unsigned)((d.M + 63) / 64), (unsigned)d.batch);
+  k_gemm_simt<TA, TB, TC, Acc><<<grid, 256, 0, s>>>(d, A, B, C);
+  CQ_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------------------
+// explicit instantiations
+// ---------------------------------------------------------------------------------------
+#define CQ_INST(R)                                                                                \
+  template void launch_pi_fused<R>(const cplx_t<R>*, const cplx_t<R>*, cplx_t<R>*, int64_t,     \
+                                   KGrid, double, cudaStream_t);                                \
+  template void launch_sigma_fused<R>(const cplx_t<R>*, const cplx_t<R>*, const cplx_t<R>*,    \
+                                      cplx_t<R>*, cplx_t<R>*, int64_t, KGrid, cudaStream_t);    \
+  template void launch_dft_plain<R>(cplx_t<R>*, int64_t, KGrid, int, double, int64_t, int64_t,  \
+                                    cudaStream_t);                                              \
+  template void launch_ir_transform<R>(cplx_t<R>*, int64_t, int, int, const double2*,           \
+                                       cudaStream_t);                                           \
+  template void launch_from_c128<R>(const double2*, cplx_t<R>*, int64_t, cudaStream_t);         \
+  template void launch_to_c128<R>(const cplx_t<R>*, double2*, int64_t, cudaStream_t);           \
+  template void launch_eye_minus<R>(const cplx_t<R>*, double2*, int64_t, int64_t, cudaStream_t); \
+  template void launch_logdet_trace<R>(const double2*, const cplx_t<R>*, double*, double2*,     \
+                                       int64_t, int64_t, cudaStream_t);                         \
+  template void launch_eps_head<R>(const cplx_t<R>*, const double2*, const double*, double2*,   \
+                                   int64_t, int64_t, int64_t, cudaStream_t);                    \
+  template void launch_tq_to_qt_c128<R>(const cplx_t<R>*, double2*, int64_t, int64_t, int64_t,  \
+                                        int64_t, int64_t, cudaStream_t);                        \
+  template void launch_qt_to_tq<R>(const double2*, cplx_t<R>*, int64_t, int64_t, int64_t,      \
+                                   cudaStream_t);
+
+CQ_INST(float)
+CQ_INST(double)
+
+#define CQ_GEMM_INST(TA, TB, TC, ACC)                                                   \
+  template void launch_gemm_simt<TA, TB, TC, ACC>(const GemmDesc&, const TA*, const TB*, TC*, \
+                                                  cudaStream_t);
+CQ_GEMM_INST(float2, float2, float2, float)
+CQ_GEMM_INST(float2, double2, float2, float)
+CQ_GEMM_INST(double2, float2, float2, float)
+CQ_GEMM_INST(double2, double2, float2, float)
+CQ_GEMM_INST(float2, float2, double2, double)
+CQ_GEMM_INST(float2, double2, double2, double)
+CQ_GEMM_INST(double2, float2, double2, double)
+CQ_GEMM_INST(double2, double2, double2, double)
+
+}  // namespace cq

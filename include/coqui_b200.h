@@ -1,0 +1,150 @@
+/*
+ * coqui_b200.h -- C ABI of the B200 THC-RPA/GW imaginary-time hot path.
+ *
+ * One context (coqui_b200_ctx) holds the THC data, the IR grids, the k-mesh and every
+ * device buffer of one system.  The entry points mirror CoQui's solver entry points
+ * on this path (paths relative to the CoQui tree):
+ *
+ *   coqui_b200_update_w     <- methods::solvers::scr_coulomb_t::update_w
+ *                              (src/methods/scr_coulomb/scr_coulomb_t.cpp:37-95)
+ *   coqui_b200_eval_sigma   <- methods::solvers::gw_t::evaluate(MBState&, THC_ERI const&)
+ *                              (src/methods/GW/thc_gw.cpp:26-89, thc_gw.icc:70-213)
+ *   coqui_b200_rpa_energy   <- methods::solvers::gw_t::rpa_energy / thc_rpa_Xqindep
+ *                              (src/methods/GW/thc_rpa.cpp:22, thc_rpa.icc:21-181)
+ *   coqui_b200_eval_pi      <- scr_coulomb_t::eval_Pi_qdep -> eval_Pi_rpa_Rspace
+ *                              (scr_coulomb_t.cpp:262-280, rpa_pi.icc:22-180)
+ *   coqui_b200_primary_to_aux / coqui_b200_aux_to_primary
+ *                           <- thc_solver_comm::primary_to_aux / aux_to_primary
+ *                              (src/methods/HF/thc_solver_comm.hpp:363-429, 516-569)
+ *   coqui_b200_tau_to_w / coqui_b200_w_to_tau
+ *                           <- scr_coulomb_t::tau_to_w / w_to_tau (PH-symmetric IR)
+ *                              (scr_coulomb_t.cpp:349-488, IAFT.icc:49-128)
+ *   coqui_b200_dyson_w      <- scr_coulomb_t::dyson_W_in_place (scr_coulomb_t.cpp:121-206)
+ *   coqui_b200_set_thc      <- thc_reader_t::X(is,ip,ik) / Z(iq,...) data
+ *                              (src/methods/ERI/thc_reader_t.hpp:590-604, 714-751)
+ *   coqui_b200_set_ir       <- imag_axes_ft::ir::IR tables (ir/ir_driver.hpp:23-76)
+ *   coqui_b200_set_kmesh    <- mf::MF kpts/lattv/kp_grid (src/mean_field/MF.hpp:152-247)
+ *
+ * Conventions (kept from the reference):
+ *   - host arrays are C-ordered and caller-owned; complex values are complex128 stored
+ *     as (re, im) double pairs;
+ *   - G_tskij and Sigma_tskij are (nt_f, ns, nk, nb, nb); X is (ns, nk, Np, nb);
+ *     V is (nq, Np, Np); W is returned as dW_qtPQ (nq, nt_half, Np, Np);
+ *   - Sigma is overwritten (thc_gw.cpp:136);
+ *   - no symmetry: nq == nk, k-points form a Gamma-centred kp_grid in lexicographic order
+ *     (kpts = 2 pi (i,j,l)/n in units where lattv rows are the lattice vectors).
+ * Errors: every entry point returns 0 or a negative COQUI_B200_E* code and never aborts;
+ * coqui_b200_last_error() gives the message.  One host thread per context; calls are
+ * synchronous (they return after the device work finished).
+ */
+#ifndef COQUI_B200_H
+#define COQUI_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define COQUI_B200_API __attribute__((visibility("default")))
+#else
+#define COQUI_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define COQUI_B200_OK 0
+#define COQUI_B200_EINVAL -1       /* bad argument, shape or order of calls */
+#define COQUI_B200_EUNSUPPORTED -2 /* input outside the supported domain (e.g. k-mesh order) */
+#define COQUI_B200_ECUDA -3        /* CUDA runtime / library error */
+#define COQUI_B200_ENOMEM -4       /* device allocation failed */
+#define COQUI_B200_ENOTHPD -5      /* a matrix that must be Hermitian positive definite is not */
+#define COQUI_B200_EPHSYM -6       /* tau mesh not particle-hole symmetric (thc_gw.cpp:56-66) */
+#define COQUI_B200_ETIMEDOUT -7    /* a bounded device-side wait gave up */
+
+/* precision_mode */
+#define COQUI_B200_FP64 0  /* complex128 everywhere: cuBLAS ZGEMM + FP64 factorizations */
+#define COQUI_B200_MIXED 1 /* split-TF32 tensor-core products, complex64 intermediates,
+                              FP64 Cholesky / log-det */
+
+typedef struct coqui_b200_ctx coqui_b200_ctx;
+
+typedef struct {
+  int64_t ns;          /* spin components (1 supported) */
+  int64_t nk;          /* k-points (= nq, no symmetry) */
+  int64_t nb;          /* orbitals */
+  int64_t Np;          /* THC interpolating points N_mu */
+  int64_t nt_f;        /* fermionic tau points */
+  int64_t nw_b;        /* bosonic Matsubara points */
+  int64_t kp_grid[3];  /* Monkhorst-Pack grid */
+  int32_t precision_mode;
+  int32_t device;      /* CUDA device ordinal */
+} coqui_b200_dims;
+
+COQUI_B200_API int coqui_b200_create(coqui_b200_ctx** ctx, const coqui_b200_dims* dims);
+COQUI_B200_API void coqui_b200_destroy(coqui_b200_ctx* ctx);
+COQUI_B200_API const char* coqui_b200_last_error(const coqui_b200_ctx* ctx);
+COQUI_B200_API const char* coqui_b200_version(void);
+
+/* IR tables, already rescaled by beta as in ir_driver.hpp:68-73; complex128 (re,im).
+   Twt_bb: (nw_b, nt_b), Ttw_bb: (nt_b, nw_b), T_beta_t_ff: (nt_f),
+   tau_mesh_x: (nt_f) in [-1, 1] (checked for particle-hole symmetry). */
+COQUI_B200_API int coqui_b200_set_ir(coqui_b200_ctx* ctx, const double* Twt_bb, const double* Ttw_bb,
+                      const double* T_beta_t_ff, const double* tau_mesh_x);
+
+/* kpts (nk,3) cartesian, lattv (3,3) rows = lattice vectors; chi_bar_qP (nq, Np) complex
+   (may be NULL: dielectric head is then zero). */
+COQUI_B200_API int coqui_b200_set_kmesh(coqui_b200_ctx* ctx, const double* kpts, const double* lattv,
+                         const double* chi_bar_qP);
+
+/* X_skPa complex128 (ns, nk, Np, nb); V_qPQ complex128 (nq, Np, Np), Hermitian PD. */
+COQUI_B200_API int coqui_b200_set_thc(coqui_b200_ctx* ctx, const double* X_skPa, const double* V_qPQ);
+
+/* Pi(tau) in the auxiliary basis: Pi_tqPQ (nt_half, nq, Np, Np) complex128. */
+COQUI_B200_API int coqui_b200_eval_pi(coqui_b200_ctx* ctx, const double* G_tskij, double* Pi_tqPQ);
+
+/* Screened interaction.  W kept on the device for coqui_b200_eval_sigma; copied out to
+   dW_qtPQ (nq, nt_half, Np, Np) if non-NULL; eps_inv_head (nt_half) complex if non-NULL. */
+COQUI_B200_API int coqui_b200_update_w(coqui_b200_ctx* ctx, const double* G_tskij, double* dW_qtPQ,
+                        double* eps_inv_head);
+
+/* Self-energy from G and the device-resident W of the last update_w (or set_w). */
+COQUI_B200_API int coqui_b200_eval_sigma(coqui_b200_ctx* ctx, const double* G_tskij, double* Sigma_tskij);
+
+/* Upload a screened interaction dW_qtPQ (nq, nt_half, Np, Np) for eval_sigma. */
+COQUI_B200_API int coqui_b200_set_w(coqui_b200_ctx* ctx, const double* dW_qtPQ);
+
+/* RPA correlation energy (Ha).  G_tskij == NULL reuses the device-resident G. */
+COQUI_B200_API int coqui_b200_rpa_energy(coqui_b200_ctx* ctx, const double* G_tskij, double* e_rpa);
+
+/* One GW iteration of scf_loop (src/methods/SCF/scf_driver.cpp:119-122): update_w then
+   gw_t::evaluate.  G_tskij == NULL reuses the device-resident G; Sigma_tskij == NULL keeps
+   Sigma on the device; eps_inv_head (nt_half complex) may be NULL.  W stays on the device. */
+COQUI_B200_API int coqui_b200_gw_iteration(coqui_b200_ctx* ctx, const double* G_tskij,
+                                           double* Sigma_tskij, double* eps_inv_head);
+
+/* Building blocks (same layouts as the reference's arguments). */
+COQUI_B200_API int coqui_b200_primary_to_aux(coqui_b200_ctx* ctx, int64_t n_tau, const double* O_tskab,
+                              double* O_tskPQ);
+COQUI_B200_API int coqui_b200_aux_to_primary(coqui_b200_ctx* ctx, int64_t n_tau, const double* O_tskPQ,
+                              double* O_tskab);
+COQUI_B200_API int coqui_b200_tau_to_w(coqui_b200_ctx* ctx, const double* X_tqPQ, double* X_wqPQ);
+COQUI_B200_API int coqui_b200_w_to_tau(coqui_b200_ctx* ctx, const double* X_wqPQ, double* X_tqPQ);
+COQUI_B200_API int coqui_b200_dyson_w(coqui_b200_ctx* ctx, const double* Pi_wqPQ, double* W_wqPQ);
+
+/* Device-timed breakdown of the last call: fills up to n (name, ms) pairs, returns count. */
+COQUI_B200_API int coqui_b200_last_timings(const coqui_b200_ctx* ctx, char* names, int name_len, double* ms,
+                            int n);
+
+/* Per-kernel CUDA-event timing (recorded on the context's stream around every launch
+   group) while profiling is on; set_profiling resets the accumulators. */
+COQUI_B200_API int coqui_b200_set_profiling(coqui_b200_ctx* ctx, int on);
+COQUI_B200_API int coqui_b200_kernel_stats(const coqui_b200_ctx* ctx, char* names, int name_len,
+                                           double* ms, int64_t* launches, int n);
+
+/* Number of kernels this library launched since the context was created. */
+COQUI_B200_API int64_t coqui_b200_kernel_launches(const coqui_b200_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COQUI_B200_H */

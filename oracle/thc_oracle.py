@@ -1,0 +1,420 @@
+"""FP64 CPU oracle for the THC-RPA/GW imaginary-time path -- TEST INFRASTRUCTURE ONLY.
+
+This module restates, in numpy complex128, the CoQui reference algorithm for the
+polarizability, the screened interaction, the GW self-energy, the RPA correlation energy
+and the scGW loop pieces.  It is the checker for the CUDA path: only tests, the smoke
+check and the benchmark's CPU-baseline leg may import it.  Nothing in the product path
+calls it.
+
+Every function names the reference lines it follows (paths relative to the CoQui tree).
+Conventions kept from the reference:
+
+* arrays are C-ordered; G_tskij is (nt, ns, nk, nb, nb); X is (ns, nk, Np, nb);
+  V is (nq, Np, Np); Pi/W are (n_tau_or_w_half, nq, Np, Np); dW_qtPQ is (nq, nt_half, Np, Np);
+* no symmetry: kp_to_ibz is the identity, kp_trev is all false, nq = nk, Qpts = kpts;
+* complex values are complex128.
+
+Parity pin: the IR transforms and G0 are checked against the reference's own fixtures
+(tests/golden); Pi, W, Sigma and E_c have no reference golden vectors on synthetic THC
+inputs (the reference cannot be built here), so they are pinned by this restatement and
+by internal identities (LU vs Cholesky Dyson forms, dense DFT vs FFT).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+_IR_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "coqui_b200", "ir_data")
+
+_PREC_EPS = {"high": "1e-15", "medium": "1e-10", "low": "1e-06"}
+
+
+# ----------------------------------------------------------------------------------------
+# IR grids and tau <-> iw transforms
+# ----------------------------------------------------------------------------------------
+def determine_lambda(lbda: float) -> float:
+    """ir_driver.hpp:143-157: round beta*wmax up to a decade in [1e2, 1e6]."""
+    for lam in (100.0, 1000.0, 10000.0, 100000.0, 1000000.0):
+        if lbda <= lam:
+            return lam
+    return -1.0
+
+
+class IAFT:
+    """Restatement of ``imag_axes_ft::ir::IR`` + ``IAFT`` (ir_driver.hpp:23-76, IAFT.icc)."""
+
+    def __init__(self, beta: float, wmax: float, prec: str = "high", ir_dir: str = _IR_DIR):
+        self.beta = float(beta)
+        self.lam = determine_lambda(beta * wmax)
+        if self.lam <= 0:
+            raise ValueError("invalid lambda")
+        self.wmax = self.lam / beta
+        self.prec = prec
+        name = {100.0: "1e2", 1000.0: "1e3", 10000.0: "1e4", 100000.0: "1e5",
+                1000000.0: "1e6"}[self.lam] + "." + _PREC_EPS[prec]
+        d = np.load(os.path.join(ir_dir, name + ".npz"))
+        self.nt_f = int(d["nt_f"])
+        self.nw_f = int(d["nw_f"])
+        self.nw_b = int(d["nw_b"])
+        self.tau_mesh_x = d["tau_mesh_f"].copy()
+        self.wn_mesh_f = d["wn_mesh_f"].copy()
+        self.wn_mesh_b = d["wn_mesh_b"].copy()
+        b = self.beta
+        # ir_driver.hpp:68-73 rescaling
+        self.Ttw_ff = d["Ttw_ff"] * (np.sqrt(2.0) / b)
+        self.Twt_ff = d["Twt_ff"] * (b / np.sqrt(2.0))
+        self.Ttw_bb = d["Ttw_bb"] * (np.sqrt(2.0) / b)
+        self.Twt_bb = d["Twt_bb"] * (b / np.sqrt(2.0))
+        self.T_beta_t_ff = d["T_beta_t_ff"].copy()
+        self.Tct_ff = d["Tct_ff"] * np.sqrt(2.0 / b)
+
+    @property
+    def nt_b(self) -> int:
+        """IAFT.hpp:167-169 returns nt_f for nt_b (kept as is)."""
+        return self.nt_f
+
+    @property
+    def nt_half(self) -> int:
+        return (self.nt_b + 1) // 2
+
+    @property
+    def nw_half(self) -> int:
+        return (self.nw_b + 1) // 2
+
+    def tau_mesh(self) -> np.ndarray:
+        """qp_scf_common.cpp:96-98: tau = (x+1) beta / 2."""
+        return (self.tau_mesh_x + 1.0) * self.beta / 2.0
+
+    def omega(self, n: int) -> complex:
+        """IAFT.hpp:55-57: i n pi / beta."""
+        return 1j * n * np.pi / self.beta
+
+    def tau_to_w(self, X_t, stats="fermi"):
+        """IAFT.icc:10-26."""
+        T = self.Twt_ff if stats == "fermi" else self.Twt_bb
+        sh = X_t.shape
+        return (T @ X_t.reshape(sh[0], -1)).reshape((T.shape[0],) + sh[1:])
+
+    def w_to_tau(self, X_w, stats="fermi"):
+        """IAFT.icc:82-98."""
+        T = self.Ttw_ff if stats == "fermi" else self.Ttw_bb
+        sh = X_w.shape
+        return (T @ X_w.reshape(sh[0], -1)).reshape((T.shape[0],) + sh[1:])
+
+    def tau_to_beta(self, A_t):
+        """IAFT.icc:226-238: A(beta^-) = sum_t T_beta_t_ff(t) A(t)."""
+        sh = A_t.shape
+        return (self.T_beta_t_ff @ A_t.reshape(sh[0], -1)).reshape(sh[1:])
+
+    def Twt_pos(self) -> np.ndarray:
+        """IAFT.icc:61-70: PH-symmetric tau->w matrix (nw_half, nt_half)."""
+        nt, nw = self.nt_half, self.nw_half
+        T = np.zeros((nw, nt), np.complex128)
+        for n in range(nw):
+            iw = self.nw_b // 2 + n
+            for it in range(nt):
+                imt = self.nt_b - it - 1
+                T[n, it] = self.Twt_bb[iw, it] if it == imt else self.Twt_bb[iw, it] + self.Twt_bb[iw, imt]
+        return T
+
+    def Ttw_pos(self) -> np.ndarray:
+        """IAFT.icc:116-125: PH-symmetric w->tau matrix (nt_half, nw_half)."""
+        nt, nw = self.nt_half, self.nw_half
+        T = np.zeros((nt, nw), np.complex128)
+        for it in range(nt):
+            for n in range(nw):
+                iw = self.nw_b // 2 + n
+                imw = self.nw_b // 2 - n
+                T[it, n] = self.Ttw_bb[it, iw] if iw == imw else self.Ttw_bb[it, iw] + self.Ttw_bb[it, imw]
+        return T
+
+    def tau_to_w_PHsym(self, X_t):
+        """IAFT.icc:49-73."""
+        sh = X_t.shape
+        T = self.Twt_pos()
+        return (T @ X_t.reshape(sh[0], -1)).reshape((T.shape[0],) + sh[1:])
+
+    def w_to_tau_PHsym(self, X_w):
+        """IAFT.icc:104-128."""
+        sh = X_w.shape
+        T = self.Ttw_pos()
+        return (T @ X_w.reshape(sh[0], -1)).reshape((T.shape[0],) + sh[1:])
+
+
+# ----------------------------------------------------------------------------------------
+# k <-> R coefficients
+# ----------------------------------------------------------------------------------------
+def R_points(kp_grid) -> np.ndarray:
+    """kpoint_utils.hpp:520-533: R index p -> (a, b, c) with wrap to (-n/2, n/2]."""
+    nx, ny, nz = (int(v) for v in kp_grid)
+    nnr = nx * ny * nz
+    R = np.zeros((nnr, 3), np.int64)
+    for p in range(nnr):
+        a, b, c = p // (ny * nz), (p // nz) % ny, p % nz
+        if a > nx // 2:
+            a -= nx
+        if b > ny // 2:
+            b -= ny
+        if c > nz // 2:
+            c -= nz
+        R[p] = (a, b, c)
+    return R
+
+
+def k_to_R_coefficients(kpts, lattv, kp_grid) -> np.ndarray:
+    """kpoint_utils.hpp:461-491 (+496-545): f_Rk(R, k) = exp(-i k.R) / nk."""
+    R = R_points(kp_grid)
+    Rc = R @ np.asarray(lattv, np.float64)  # a*a1 + b*a2 + c*a3
+    kR = Rc @ np.asarray(kpts, np.float64).T  # (nR, nk)
+    return np.exp(-1j * kR) / kpts.shape[0]
+
+
+def R_to_k_coefficients(kpts, lattv, kp_grid) -> np.ndarray:
+    """kpoint_utils.hpp:588-705: f_kR(k, R) = exp(+i k.R) / w_R with w_R = 1."""
+    R = R_points(kp_grid)
+    Rc = R @ np.asarray(lattv, np.float64)
+    kR = np.asarray(kpts, np.float64) @ Rc.T  # (nk, nR)
+    return np.exp(1j * kR)
+
+
+# ----------------------------------------------------------------------------------------
+# primary <-> auxiliary projections
+# ----------------------------------------------------------------------------------------
+def primary_to_aux(O_skab, X_skPa) -> np.ndarray:
+    """thc_solver_comm.hpp:405-428: O^k_PQ = X^k_Pa O^k_ab conj(X^k_Qb) (no symmetry).
+
+    O_skab: (..., ns, nk, nb, nb) -> (..., ns, nk, Np, Np).
+    """
+    A = np.matmul(X_skPa, O_skab)  # Ask_Pb = X_Pa O_ab
+    return np.matmul(A, np.conj(np.swapaxes(X_skPa, -1, -2)))  # A * X^dagger
+
+
+def aux_to_primary(O_skPQ, X_skPa) -> np.ndarray:
+    """thc_solver_comm.hpp:551-566: O^k_ab = conj(X^k_Pa) O^k_PQ X^k_Qb."""
+    A = np.matmul(np.conj(np.swapaxes(X_skPa, -1, -2)), O_skPQ)  # X^dagger O
+    return np.matmul(A, X_skPa)
+
+
+# ----------------------------------------------------------------------------------------
+# Polarizability, Dyson, W, head
+# ----------------------------------------------------------------------------------------
+def eval_Pi_rpa_Rspace(G_tskij, X_skPa, kpts, lattv, kp_grid, Qpts=None) -> np.ndarray:
+    """rpa_pi.icc:22-180 (single rank, no symmetry): Pi(nt_half, nq, Np, Np)."""
+    nt, ns, nk, nb, _ = G_tskij.shape
+    Np = X_skPa.shape[2]
+    nt_half = (nt + 1) // 2
+    sp = -1.0 if ns == 2 else -2.0  # rpa_pi.icc:46
+    Qpts = kpts if Qpts is None else Qpts
+    nq = Qpts.shape[0]
+    f_Rk = k_to_R_coefficients(kpts, lattv, kp_grid)
+    f_qR = R_to_k_coefficients(Qpts, lattv, kp_grid)
+    Pi = np.zeros((nt_half, nq, Np, Np), np.complex128)
+    for it in range(nt_half):
+        Gp = primary_to_aux(G_tskij[it], X_skPa)  # (ns, nk, Np, Np)
+        Gn = primary_to_aux(G_tskij[nt - it - 1], X_skPa)
+        if nk != 1:
+            Gp = np.einsum("Rk,skx->sRx", f_Rk, Gp.reshape(ns, nk, -1)).reshape(Gp.shape)
+            Gn = np.einsum("Rk,skx->sRx", f_Rk, Gn.reshape(ns, nk, -1)).reshape(Gn.shape)
+        GG = (Gp * np.conj(Gn)).sum(axis=0) * sp  # rpa_pi.icc:156-162
+        if nk != 1:
+            Pi[it] = (f_qR @ GG.reshape(nk, -1)).reshape(nq, Np, Np)
+        else:
+            Pi[it] = GG
+    return Pi
+
+
+def dyson_W_in_place(Pi_wqPQ, V_qPQ) -> np.ndarray:
+    """scr_coulomb_t.cpp:171-199: W = ([I - V Pi]^{-1} - I) V per (q, w)."""
+    nw, nq, Np, _ = Pi_wqPQ.shape
+    W = np.empty_like(Pi_wqPQ)
+    eye = np.eye(Np)
+    for iq in range(nq):
+        V = V_qPQ[iq]
+        A = eye - np.matmul(V, Pi_wqPQ[:, iq])  # (nw, Np, Np)
+        Ainv = np.linalg.inv(A) - eye
+        W[:, iq] = np.matmul(Ainv, V)
+    return W
+
+
+def dyson_W_cholesky(Pi_wqPQ, V_qPQ) -> np.ndarray:
+    """Hermitian form of the same Dyson solve: V = L L^H, M = L^H Pi L,
+    (I - M) = C C^H, W = K K^H - V with K = L C^{-H} (an internal identity check)."""
+    nw, nq, Np, _ = Pi_wqPQ.shape
+    W = np.empty_like(Pi_wqPQ)
+    for iq in range(nq):
+        L = np.linalg.cholesky(V_qPQ[iq])
+        for n in range(nw):
+            M = L.conj().T @ Pi_wqPQ[n, iq] @ L
+            C = np.linalg.cholesky(np.eye(Np) - M)
+            K = np.linalg.solve(C.conj(), L.T).T  # L C^{-H}
+            W[n, iq] = K @ K.conj().T - V_qPQ[iq]
+    return W
+
+
+def eval_eps_inv_q(W_tqPQ, chi_bar_qP, Qpts, lattv) -> np.ndarray:
+    """g0_div_utils.hpp:180-214: eps_inv(t, q) = |q|^2/(4 pi) * vol * chi_q^T W conj(chi_q)."""
+    vol = abs(np.linalg.det(np.asarray(lattv, np.float64)))
+    q2 = (np.asarray(Qpts) ** 2).sum(axis=1)
+    fpi = 4.0 * 3.14159265358979323846
+    buf = np.einsum("tqPQ,qQ->tqP", W_tqPQ, np.conj(chi_bar_qP))
+    return (q2 / fpi * vol)[None, :] * np.einsum("qP,tqP->tq", chi_bar_qP, buf)
+
+
+def eps_inv_head_ignore_g0(eps_inv_tq, Qpts) -> np.ndarray:
+    """g0_div_utils.hpp:102-107: head taken at the q with the smallest |q|."""
+    q2 = (np.asarray(Qpts) ** 2).sum(axis=1)
+    return eps_inv_tq[:, int(np.argmin(q2))]
+
+
+def update_w(G_tskij, X_skPa, V_qPQ, ft: IAFT, kpts, lattv, kp_grid, chi_bar_qP=None):
+    """scr_coulomb_t.cpp:37-95: Pi -> tau_to_w -> Dyson -> w_to_tau -> head -> dW_qtPQ."""
+    Pi_t = eval_Pi_rpa_Rspace(G_tskij, X_skPa, kpts, lattv, kp_grid)
+    Pi_w = ft.tau_to_w_PHsym(Pi_t)
+    W_w = dyson_W_in_place(Pi_w, V_qPQ)
+    W_t = ft.w_to_tau_PHsym(W_w)
+    nq, Np = V_qPQ.shape[0], V_qPQ.shape[1]
+    if chi_bar_qP is None:
+        chi_bar_qP = np.zeros((nq, Np), np.complex128)
+    eps_tq = eval_eps_inv_q(W_t, chi_bar_qP, kpts, lattv)
+    head = eps_inv_head_ignore_g0(eps_tq, kpts)
+    dW_qtPQ = np.ascontiguousarray(np.swapaxes(W_t, 0, 1))  # scr_coulomb_t.cpp:73-86
+    return dW_qtPQ, head, eps_tq
+
+
+# ----------------------------------------------------------------------------------------
+# Self-energy
+# ----------------------------------------------------------------------------------------
+def eval_Sigma_all_Rspace(G_tskij, dW_qtPQ, X_skPa, kpts, lattv, kp_grid) -> np.ndarray:
+    """thc_gw.cpp:152-166 + thc_gw.icc:70-213 + thc_gw.icc:37-65 (alg "R", no symmetry).
+
+    Returns Sigma_tskij (nt, ns, nk, nb, nb); the q->0 correction is a no-op for
+    ignore_g0 (thc_gw.icc:454-461).
+    """
+    nt, ns, nk, nb, _ = G_tskij.shape
+    nq, nt_half, Np, _ = dW_qtPQ.shape
+    f_Rk = k_to_R_coefficients(kpts, lattv, kp_grid)
+    f_kR = R_to_k_coefficients(kpts, lattv, kp_grid)
+    Sigma = np.zeros((nt, ns, nk, nb, nb), np.complex128)
+    W = dW_qtPQ.reshape(nq, -1)
+    if nk != 1:
+        W_R = f_Rk @ W  # W q->R with Qpts == kpts (thc_gw.icc:148-153)
+    else:
+        W_R = W
+    W_R = W_R.reshape(nk, nt_half, Np, Np)
+    for minus_t in (False, True):
+        # G_PQ(t) or G_PQ(beta - t), t in [0, nt_half)
+        idx = [nt - it - 1 if minus_t else it for it in range(nt_half)]
+        G_tsk = primary_to_aux(G_tskij[idx], X_skPa[None])  # (nt_half, ns, nk, Np, Np)
+        G_skt = np.transpose(G_tsk, (1, 2, 0, 3, 4))
+        if nk != 1:
+            G_skt = np.einsum("Rk,skx->sRx", f_Rk, G_skt.reshape(ns, nk, -1)).reshape(G_skt.shape)
+        S_skt = -(G_skt * W_R[None])  # thc_gw.icc:161-167
+        if nk != 1:
+            S_skt = np.einsum("kR,sRx->skx", f_kR, S_skt.reshape(ns, nk, -1)).reshape(S_skt.shape)
+        S_tsk = np.transpose(S_skt, (2, 0, 1, 3, 4))
+        S_ab = aux_to_primary(S_tsk, X_skPa[None])  # (nt_half, ns, nk, nb, nb)
+        if not minus_t:
+            Sigma[:nt_half] = S_ab
+        else:
+            for it in range(nt // 2):  # thc_gw.icc:59-61
+                Sigma[nt - it - 1] = S_ab[it]
+    return Sigma
+
+
+# ----------------------------------------------------------------------------------------
+# RPA correlation energy
+# ----------------------------------------------------------------------------------------
+def rpa_energy_from_Pi_w(Pi_wqPQ, V_qPQ, ft: IAFT, nk: int, q_weight=None) -> float:
+    """thc_rpa.icc:130-181."""
+    nw_half, nq, Np, _ = Pi_wqPQ.shape
+    if q_weight is None:
+        q_weight = np.ones(nq)
+    e_w = np.zeros(ft.nw_b, np.complex128)
+    eye = np.eye(Np)
+    for iq in range(nq):
+        for n in range(nw_half):
+            wn = ft.nw_b // 2 + n
+            mwn = ft.nw_b // 2 - n
+            A = Pi_wqPQ[n, iq] @ V_qPQ[iq]
+            tr = np.trace(A)
+            e_w[wn] += q_weight[iq] * tr
+            if mwn != wn:
+                e_w[mwn] += q_weight[iq] * tr
+            det = np.linalg.det(eye - A)
+            if det.real < 0:
+                det *= -1.0
+            e_w[wn] += q_weight[iq] * np.log(det.real)
+            if mwn != wn:
+                e_w[mwn] += q_weight[iq] * np.log(det.real)
+    e_t = ft.Ttw_bb @ e_w  # w_to_tau(boson), thc_rpa.icc:171
+    e = ft.T_beta_t_ff @ e_t  # tau_to_beta (fermionic T_beta_t), thc_rpa.icc:172
+    e /= 2.0 * nk
+    return float(e.real)
+
+
+def rpa_energy(G_tskij, X_skPa, V_qPQ, ft: IAFT, kpts, lattv, kp_grid) -> float:
+    """thc_rpa.icc:21-69: Pi(t) -> Pi(w) -> E_c."""
+    Pi_t = eval_Pi_rpa_Rspace(G_tskij, X_skPa, kpts, lattv, kp_grid)
+    Pi_w = ft.tau_to_w_PHsym(Pi_t)
+    return rpa_energy_from_Pi_w(Pi_w, V_qPQ, ft, kpts.shape[0])
+
+
+# ----------------------------------------------------------------------------------------
+# G0, Galitskii-Migdal energy, Dyson for G, damping
+# ----------------------------------------------------------------------------------------
+def g0_scalar(e, t, mu, beta):
+    """qp_scf_common.cpp:86-93."""
+    x = e - mu
+    if x > 0:
+        return -np.exp(-x * t) / (1 + np.exp(-x * beta))
+    return -np.exp(x * (beta - t)) / (1 + np.exp(x * beta))
+
+
+def update_G(MO_skia, E_ska, mu, ft: IAFT) -> np.ndarray:
+    """qp_scf_common.cpp:82-118: G_ij(t) = sum_a C_ia g(e_a, t) conj(C_ja)."""
+    ns, nk, nb, _ = MO_skia.shape
+    tau = ft.tau_mesh()
+    G = np.zeros((tau.size, ns, nk, nb, nb), np.complex128)
+    for it, t in enumerate(tau):
+        for s in range(ns):
+            for k in range(nk):
+                g = np.array([g0_scalar(E_ska[s, k, a].real, t, mu, ft.beta) for a in range(nb)])
+                C = MO_skia[s, k]
+                G[it, s, k] = C @ (g[:, None] * C.conj().T)
+    return G
+
+
+def eval_corr_energy(G_tskij, Sigma_tskij, ft: IAFT, k_weight) -> float:
+    """scf_common.cpp:87-136 (Galitskii-Migdal)."""
+    nts, ns, nk, nb, _ = G_tskij.shape
+    Sw = ft.tau_to_w(Sigma_tskij, "fermi")
+    Gw = ft.tau_to_w(G_tskij, "fermi")
+    SG_ws = np.einsum("k,wskij,wskji->ws", np.asarray(k_weight, np.complex128), Sw, Gw)
+    SG_ts = ft.w_to_tau(SG_ws, "fermi")
+    SG_beta = ft.tau_to_beta(SG_ts)
+    spin = 1.0 if ns == 2 else 2.0
+    return float((-0.5 * spin * SG_beta.sum()).real)
+
+
+def solve_dyson(H0_skij, S_skij, F_skij, Sigma_tskij, mu, ft: IAFT) -> np.ndarray:
+    """simple_dyson.cpp:11-115: G(iw) = [(iw+mu)S - H0 - F - Sigma(iw)]^{-1} -> G(tau)."""
+    Sw = ft.tau_to_w(Sigma_tskij, "fermi")
+    nw = Sw.shape[0]
+    Gw = np.empty_like(Sw)
+    for n in range(nw):
+        om = ft.omega(int(ft.wn_mesh_f[n])) + mu
+        Xm = om * S_skij - H0_skij - F_skij - Sw[n]
+        Gw[n] = np.linalg.inv(Xm)
+    return ft.w_to_tau(Gw, "fermi")
+
+
+def damp(H, H_prev, mixing=0.7):
+    """damp_t.hpp:34-48: H <- m H + (1-m) H_prev; returns (H, max|H_prev - H|)."""
+    Hn = mixing * H + (1.0 - mixing) * H_prev
+    return Hn, float(np.abs(H_prev - Hn).max())
+
+
+def hermitize(A):
+    """scf_driver.cpp:126-129: A <- (A + A^H)/2 over the last two axes."""
+    return 0.5 * (A + np.conj(np.swapaxes(A, -1, -2)))

@@ -1,0 +1,53 @@
+"""The C-ABI library loads and exports every entry point include/coqui_b200.h declares
+(no compute calls; the library is built by the driver's build step / conftest)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from coqui_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _header_symbols():
+    txt = open(os.path.join(ROOT, "include", "coqui_b200.h")).read()
+    return sorted(set(re.findall(r"\b(coqui_b200_[a-z0-9_]+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(capi.LIB_PATH):
+        from coqui_b200 import build
+        build.build(verbose=False)
+    return capi.load()
+
+
+def test_header_and_binding_agree():
+    assert _header_symbols() == sorted(capi.SYMBOLS)
+
+
+def test_library_exports_every_header_symbol(lib):
+    for name in _header_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_version(lib):
+    assert "sm_100a" in capi.version()
+
+
+def test_bad_dims_rejected_without_device(lib):
+    d = capi.Dims(ns=2, nk=8, nb=4, Np=4, nt_f=10, nw_b=11,
+                  kp_grid=(ctypes.c_int64 * 3)(2, 2, 2), precision_mode=1, device=0)
+    h = ctypes.c_void_p()
+    assert lib.coqui_b200_create(ctypes.byref(h), ctypes.byref(d)) == -1  # ns != 1
+    d.ns = 1
+    d.kp_grid = (ctypes.c_int64 * 3)(2, 2, 3)  # product != nk
+    assert lib.coqui_b200_create(ctypes.byref(h), ctypes.byref(d)) == -1
+    assert not h.value
+
+
+def test_null_context_is_an_error(lib):
+    assert lib.coqui_b200_set_thc(None, None, None) == -1
+    assert lib.coqui_b200_kernel_launches(None) == 0

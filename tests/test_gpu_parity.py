@@ -1,0 +1,171 @@
+"""GPU parity: every C-ABI entry point against the FP64 oracle on seeded inputs.
+
+Tolerances: the FP64 path agrees to 1e-10 max-abs; the mixed path (split-TF32 tensor-core
+products, complex64 intermediates, FP64 Cholesky) to the stated target of 1e-6 max-abs
+for Pi, W, Sigma and 1e-6 Ha for E_c.
+"""
+import numpy as np
+import pytest
+
+from coqui_b200 import capi, solvers
+from coqui_b200.iaft import IAFT as ProductIAFT
+from coqui_b200.synthetic import make_system
+from oracle import thc_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MODES = [(capi.FP64, 1e-10), (capi.MIXED, 1e-6)]
+MODE_IDS = ["fp64", "mixed"]
+
+
+def maxabs(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max())
+
+
+class Case:
+    def __init__(self, grid, nb, nocc, Np, lam=1e4, prec="low", seed=7):
+        self.s = make_system(grid, nb, nocc, Np, seed=seed)
+        self.ft = O.IAFT(1000.0, lam / 1000.0, prec)
+        self.pft = ProductIAFT(1000.0, lam / 1000.0, prec)
+        self.G = self.s.G0(self.ft)
+        s, ft = self.s, self.ft
+        self.Pi = O.eval_Pi_rpa_Rspace(self.G, s.X, s.kpts, s.lattv, s.kp_grid)
+        self.Pi_w = ft.tau_to_w_PHsym(self.Pi)
+        self.W_w = O.dyson_W_in_place(self.Pi_w, s.V)
+        self.dW, self.head, _ = O.update_w(self.G, s.X, s.V, ft, s.kpts, s.lattv, s.kp_grid,
+                                           s.chi_bar)
+        self.Sigma = O.eval_Sigma_all_Rspace(self.G, self.dW, s.X, s.kpts, s.lattv, s.kp_grid)
+        self.e_rpa = O.rpa_energy_from_Pi_w(self.Pi_w, s.V, ft, s.nk)
+
+    def ctx(self, mode):
+        s = self.s
+        c = capi.Context(s.nk, s.nb, s.Np, self.ft.nt_f, self.ft.nw_b, s.kp_grid, mode=mode)
+        c.set_ir(self.pft)
+        c.set_kmesh(s.kpts, s.lattv, s.chi_bar)
+        c.set_thc(s.X, s.V)
+        return c
+
+
+@pytest.fixture(scope="module")
+def base():
+    return Case(2, 16, 8, 64)
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_primary_to_aux(base, mode, tol):
+    c = base.ctx(mode)
+    out = c.primary_to_aux(base.G[:3])
+    ref = O.primary_to_aux(base.G[:3], base.s.X[None])
+    assert maxabs(out, ref) < tol
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_aux_to_primary(base, mode, tol):
+    c = base.ctx(mode)
+    S = base.Pi[:2, None] * 10.0  # any (nt, 1, nk, Np, Np) tensor
+    out = c.aux_to_primary(S)
+    ref = O.aux_to_primary(S, base.s.X[None])
+    assert maxabs(out, ref) < tol * max(1.0, float(np.abs(ref).max()))
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_eval_pi(base, mode, tol):
+    c = base.ctx(mode)
+    assert maxabs(c.eval_pi(base.G), base.Pi) < tol
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_tau_w_transforms(base, mode, tol):
+    c = base.ctx(mode)
+    assert maxabs(c.tau_to_w(base.Pi), base.Pi_w) < tol
+    Wt = base.ft.w_to_tau_PHsym(base.W_w)
+    assert maxabs(c.w_to_tau(base.W_w), Wt) < tol
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_dyson_w(base, mode, tol):
+    c = base.ctx(mode)
+    assert maxabs(c.dyson_w(base.Pi_w), base.W_w) < tol
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_update_w_and_sigma(base, mode, tol):
+    c = base.ctx(mode)
+    W, head = c.update_w(base.G)
+    assert maxabs(W, base.dW) < tol
+    assert maxabs(head, base.head) < tol
+    S = c.eval_sigma(base.G)
+    assert maxabs(S, base.Sigma) < tol
+    # Sigma from an uploaded W equals Sigma from the resident W
+    c.set_w(base.dW)
+    assert maxabs(c.eval_sigma(base.G), base.Sigma) < tol
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_gw_iteration_resident(base, mode, tol):
+    c = base.ctx(mode)
+    S, head = c.gw_iteration(base.G, want_head=True)
+    assert maxabs(S, base.Sigma) < tol and maxabs(head, base.head) < tol
+    S2, _ = c.gw_iteration(None)  # resident G
+    assert maxabs(S2, S) < 1e-12
+    n0 = c.kernel_launches()
+    c.gw_iteration(None, want_sigma=False)
+    assert c.kernel_launches() > n0
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_rpa_energy(base, mode, tol):
+    c = base.ctx(mode)
+    e = c.rpa_energy(base.G)
+    assert abs(e - base.e_rpa) < tol
+    assert abs(c.rpa_energy(None) - e) < 1e-12
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+@pytest.mark.parametrize("grid,nb,nocc,Np,lam", [
+    (1, 12, 6, 40, 1e4),          # Gamma only: no DFT
+    ((1, 2, 3), 10, 5, 50, 1e5),  # non-cubic grid, odd nt (61), Np not a multiple of 32
+    (3, 8, 4, 36, 1e4),           # 27 k-points (generic radix-3 DFT)
+])
+def test_edge_cases(mode, tol, grid, nb, nocc, Np, lam):
+    cs = Case(grid, nb, nocc, Np, lam=lam, seed=11)
+    c = cs.ctx(mode)
+    W, head = c.update_w(cs.G)
+    assert maxabs(W, cs.dW) < tol
+    assert maxabs(c.eval_sigma(cs.G), cs.Sigma) < tol
+    assert abs(c.rpa_energy(cs.G) - cs.e_rpa) < tol
+
+
+def test_solver_mirror_matches_oracle(base):
+    thc = solvers.THCData.from_synthetic(base.s)
+    scr = solvers.scr_coulomb_t(base.pft)
+    gw = solvers.gw_t(base.pft)
+    mb = solvers.MBState(sG_tskij=base.G)
+    scr.update_w(mb, thc)
+    gw.evaluate(mb, thc)
+    assert maxabs(mb.dW_qtPQ, base.dW) < 1e-6
+    assert maxabs(mb.sSigma_tskij, base.Sigma) < 1e-6
+    assert abs(gw.rpa_energy(base.G, thc) - base.e_rpa) < 1e-6
+    solvers.clear_contexts()
+
+
+def test_errors_are_codes_not_aborts(base):
+    s = base.s
+    c = capi.Context(s.nk, s.nb, s.Np, base.ft.nt_f, base.ft.nw_b, s.kp_grid)
+    with pytest.raises(capi.CoquiB200Error) as e:
+        c.update_w(base.G)  # nothing set yet
+    assert e.value.code == -1
+    c.set_ir(base.pft)
+    with pytest.raises(capi.CoquiB200Error) as e:
+        c.set_kmesh(s.kpts[::-1].copy(), s.lattv)  # not lexicographic
+    assert e.value.code == -2
+    bad = s.V.copy()
+    bad[0] = -np.eye(s.Np)
+    with pytest.raises(capi.CoquiB200Error) as e:
+        c.set_thc(s.X, bad)
+    assert e.value.code == -5
+    # the context stays usable after errors
+    c.set_kmesh(s.kpts, s.lattv, s.chi_bar)
+    c.set_thc(s.X, s.V)
+    W, _ = c.update_w(base.G)
+    assert maxabs(W, base.dW) < 1e-6

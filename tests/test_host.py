@@ -1,0 +1,56 @@
+"""Host-side logic that needs no GPU: synthetic inputs, argument validation."""
+import numpy as np
+import pytest
+
+from coqui_b200 import capi, solvers
+from coqui_b200.iaft import IAFT
+from coqui_b200.synthetic import WORKLOADS, kgrid, make_system
+
+
+def test_synthetic_distributions():
+    s = make_system(2, 16, 8, 64, seed=11)
+    assert s.X.shape == (1, 8, 64, 16) and s.V.shape == (8, 64, 64)
+    np.testing.assert_allclose(s.V, np.conj(np.swapaxes(s.V, -1, -2)), atol=1e-15)
+    assert np.linalg.eigvalsh(s.V).min() > 1e-3 - 1e-12
+    assert np.all(s.eps[0, :, :8] < -0.1 + 1e-15) and np.all(s.eps[0, :, 8:] > 0.1 - 1e-15)
+    # seeded
+    t = make_system(2, 16, 8, 64, seed=11)
+    np.testing.assert_array_equal(s.X, t.X)
+
+
+def test_kgrid_lexicographic():
+    k = kgrid((2, 3, 1))
+    assert k.shape == (6, 3)
+    np.testing.assert_allclose(k[4] / (2 * np.pi), [1 / 2, 1 / 3, 0])
+
+
+def test_g0_shape_and_sign():
+    ft = IAFT(1000.0, 10.0, "low")
+    s = make_system(1, 6, 3, 8, seed=2)
+    G = s.G0(ft)
+    assert G.shape == (ft.nt_f, 1, 1, 6, 6)
+    assert np.all(G.real[:, 0, 0, np.arange(6), np.arange(6)] <= 0)
+    # occupied: -G(beta^-) = 1; virtual: 0
+    Dm = -np.einsum("t,tskij->skij", ft.T_beta_t_ff, G)
+    np.testing.assert_allclose(np.diag(Dm[0, 0]).real, [1, 1, 1, 0, 0, 0], atol=1e-5)  # "low" IR: 1e-6
+
+
+def test_workloads_named():
+    assert WORKLOADS["g0w0_k4_nb64_np512"]["Np"] == 512
+
+
+def test_solver_argument_checks():
+    ft = IAFT(1000.0, 10.0, "low")
+    with pytest.raises(ValueError):
+        solvers.scr_coulomb_t(ft, screen_type="edmft")
+    with pytest.raises(NotImplementedError):
+        solvers.gw_t(ft, div_treatment="gygi")
+    with pytest.raises(capi.CoquiB200Error):
+        solvers.gw_t(ft).evaluate(solvers.MBState(), None)
+
+
+def test_shape_validation_before_device():
+    with pytest.raises(ValueError):
+        capi._c128(np.zeros((2, 3)), (3, 2), "x")
+    with pytest.raises(ValueError):
+        capi._ptr(np.zeros((4, 4))[:, ::2], "x")

@@ -1,0 +1,88 @@
+"""Internal identities of the FP64 oracle (Pi, W, Sigma, E_c have no reference golden
+vectors on synthetic THC inputs; these checks pin the restatement's conventions)."""
+import numpy as np
+import pytest
+
+from coqui_b200.synthetic import make_system
+from oracle import thc_oracle as O
+
+
+@pytest.fixture(scope="module")
+def small(ft_low):
+    s = make_system(2, 8, 4, 24, seed=3)
+    return s, s.G0(ft_low)
+
+
+def test_dense_dft_equals_fft(small):
+    s, _ = small
+    f_Rk = O.k_to_R_coefficients(s.kpts, s.lattv, s.kp_grid)
+    x = np.random.default_rng(0).standard_normal((s.nk, 5)) + 0j
+    ref = (np.fft.fftn(x.reshape(2, 2, 2, 5), axes=(0, 1, 2)) / s.nk).reshape(s.nk, 5)
+    np.testing.assert_allclose(f_Rk @ x, ref, atol=1e-14)
+    f_kR = O.R_to_k_coefficients(s.kpts, s.lattv, s.kp_grid)
+    np.testing.assert_allclose(f_kR @ f_Rk, np.eye(s.nk), atol=1e-14)
+
+
+def test_dft_non_cubic_grid():
+    s = make_system((1, 2, 3), 4, 2, 8, seed=1)
+    f_Rk = O.k_to_R_coefficients(s.kpts, s.lattv, s.kp_grid)
+    x = np.random.default_rng(1).standard_normal((6, 3)) + 0j
+    ref = (np.fft.fftn(x.reshape(1, 2, 3, 3), axes=(0, 1, 2)) / 6).reshape(6, 3)
+    np.testing.assert_allclose(f_Rk @ x, ref, atol=1e-14)
+
+
+def test_pi_hermitian_negative(small, ft_low):
+    s, G = small
+    Pi = O.eval_Pi_rpa_Rspace(G, s.X, s.kpts, s.lattv, s.kp_grid)
+    assert Pi.shape == (ft_low.nt_half, s.nk, 24, 24)
+    np.testing.assert_allclose(Pi, np.conj(np.swapaxes(Pi, -1, -2)), atol=1e-15)
+    Pw = ft_low.tau_to_w_PHsym(Pi)
+    assert np.linalg.eigvalsh(Pw).max() < 1e-12  # Pi(iW) is negative semidefinite
+
+
+def test_dyson_lu_equals_cholesky_form(small, ft_low):
+    s, G = small
+    Pw = ft_low.tau_to_w_PHsym(O.eval_Pi_rpa_Rspace(G, s.X, s.kpts, s.lattv, s.kp_grid))
+    W1 = O.dyson_W_in_place(Pw, s.V)
+    W2 = O.dyson_W_cholesky(Pw, s.V)
+    np.testing.assert_allclose(W1, W2, atol=1e-13)
+
+
+def test_rpa_logdet_equals_cholesky(small, ft_low):
+    s, G = small
+    Pw = ft_low.tau_to_w_PHsym(O.eval_Pi_rpa_Rspace(G, s.X, s.kpts, s.lattv, s.kp_grid))
+    A = Pw[3, 1] @ s.V[1]
+    L = np.linalg.cholesky(s.V[1])
+    C = np.linalg.cholesky(np.eye(24) - L.conj().T @ Pw[3, 1] @ L)
+    np.testing.assert_allclose(np.log(np.linalg.det(np.eye(24) - A).real),
+                               2 * np.log(np.diag(C).real).sum(), atol=1e-12)
+
+
+def test_gamma_only_path_skips_dft(ft_low):
+    s = make_system(1, 6, 3, 16, seed=5)
+    G = s.G0(ft_low)
+    Pi = O.eval_Pi_rpa_Rspace(G, s.X, s.kpts, s.lattv, s.kp_grid)
+    it = 2
+    Gp = O.primary_to_aux(G[it], s.X)
+    Gn = O.primary_to_aux(G[ft_low.nt_f - 1 - it], s.X)
+    np.testing.assert_allclose(Pi[it, 0], -2 * (Gp * np.conj(Gn))[0, 0], atol=1e-15)
+
+
+def test_sigma_hermitian_and_mirror(small, ft_low):
+    s, G = small
+    dW, head, _ = O.update_w(G, s.X, s.V, ft_low, s.kpts, s.lattv, s.kp_grid, s.chi_bar)
+    S = O.eval_Sigma_all_Rspace(G, dW, s.X, s.kpts, s.lattv, s.kp_grid)
+    np.testing.assert_allclose(S, np.conj(np.swapaxes(S, -1, -2)), atol=1e-14)
+    assert head.shape == (ft_low.nt_half,)
+    e = O.eval_corr_energy(G, S, ft_low, np.ones(s.nk) / s.nk)
+    assert e < 0
+
+
+def test_damp_and_hermitize():
+    a = np.array([[1 + 1j, 2], [0, 3]])
+    b = np.zeros_like(a)
+    h, diff = O.damp(a, b, 0.7)
+    np.testing.assert_allclose(h, 0.7 * a)
+    assert diff == pytest.approx(np.abs(0.7 * a).max())
+    hh = O.hermitize(a)
+    np.testing.assert_allclose(hh, hh.conj().T)
