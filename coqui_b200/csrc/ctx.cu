@@ -119,6 +119,9 @@ template <typename F> int guarded(Ctx* c, F&& f) {
   try {
     CQ_CHECK_CUDA(cudaSetDevice(c->dev));
     f();
+    if (c->st) CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    if (cq::tc_take_error())
+      throw Error(COQUI_B200_ETIMEDOUT, "a tensor-core kernel gave up a bounded wait");
     c->err.clear();
     return COQUI_B200_OK;
   } catch (const Error& e) {

@@ -39,6 +39,47 @@ __global__ void k_zero_upper_adjoint(double2* __restrict__ L, double2* __restric
   }
 }
 
+// Z[p] = I (complex128), nprob problems
+__global__ void k_set_identity(double2* __restrict__ Z, int64_t Np, int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = i % (Np * Np);
+    Z[i] = make_double2(e / Np == e % Np ? 1.0 : 0.0, 0.0);
+  }
+}
+// Z[p] -= I in place
+__global__ void k_sub_identity(double2* __restrict__ Z, int64_t Np, int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = i % (Np * Np);
+    if (e / Np == e % Np) Z[i].x -= 1.0;
+  }
+}
+// E = DH + DH^H + F  (32 x 32 tiles through shared memory for the transposed read)
+__global__ void k_herm_sum(const double2* __restrict__ DH, const float2* __restrict__ F,
+                           float2* __restrict__ E, int64_t Np) {
+  __shared__ double2 tile[32][33];
+  const int64_t p = blockIdx.z;
+  const double2* d = DH + p * Np * Np;
+  const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
+  // load DH[j0 + ty][i0 + tx] for the transposed term
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t r = j0 + ty, c = i0 + threadIdx.x;
+    tile[ty][threadIdx.x] = (r < Np && c < Np) ? d[r * Np + c] : make_double2(0, 0);
+  }
+  __syncthreads();
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t i = i0 + ty, j = j0 + threadIdx.x;
+    if (i < Np && j < Np) {
+      const double2 a = d[i * Np + j];
+      const double2 b = tile[threadIdx.x][ty];  // DH[j][i]
+      const float2 f = F[p * Np * Np + i * Np + j];
+      E[p * Np * Np + i * Np + j] =
+          make_float2((float)(a.x + b.x + (double)f.x), (float)(a.y - b.y + (double)f.y));
+    }
+  }
+}
+
 void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t nbatch,
                                    cudaStream_t s) {
   const int64_t total = Np * Np * nbatch;
@@ -133,8 +174,12 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       {
       Prof::Scope sc(a.prof, "dyson_M_gemm");
       if (a.mixed) {
-        tc_gemm_c(TcOp::N, (const float2*)Pi, TcOp::N, L, (float2*)T1, Np, Np, Np, nb, s);
-        tc_gemm_c(TcOp::N, LH, TcOp::N, (const float2*)T1, (float2*)Mb, Np, Np, Np, nb, s);
+        // P1 = L^H Pi  (Pi Hermitian: B(k, n) = Pi[k][n] = conj(Pi[n][k]))
+        tc_cgemm_nt(LH, true, false, Np, NN, Pi, false, true, Np, NN, (float2*)T1, Np, NN, Np,
+                    Np, Np, nb, s);
+        // M = P1 L  (B(k, n) = L[k][n] = conj(LH[n][k]))
+        tc_cgemm_nt(T1, false, false, Np, NN, LH, true, true, Np, NN, (float2*)Mb, Np, NN, Np, Np,
+                    Np, nb, s);
         launch_eye_minus<float>((const float2*)Mb, A, Np, nb, s);
       } else {
         // row-major C = A B  ->  column-major C^T = B^T A^T
@@ -166,7 +211,36 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         CQ_CHECK_CUDA(cudaMemcpyAsync(ld_h.data(), dld, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
         CQ_CHECK_CUDA(cudaMemcpyAsync(tr_h.data(), dtr, nb * sizeof(double2), cudaMemcpyDeviceToHost, s));
       }
-      if (a.want_w) {
+      if (a.want_w && a.mixed) {
+        // W = L E L^H with E = (I - M)^{-1} - I = D + D^H + D^H D, D = C^{-1} - I: no
+        // cancellation against V, so the split-TF32 products keep W to ~1e-8.
+        double2* Z = Y;  // Z = C^{-H}: column-major Z^T conj(C) = I  (right, upper, ^H)
+        {
+          Prof::Scope sc(a.prof, "dyson_trsm");
+          k_set_identity<<<grid_for(nb * NN, 256), 256, 0, s>>>(Z, Np, nb * NN);
+          count_launch();
+          CQ_BLAS(cublasZtrsmBatched(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C,
+                                     CUBLAS_DIAG_NON_UNIT, (int)Np, (int)Np,
+                                     (const cuDoubleComplex*)&one,
+                                     (const cuDoubleComplex* const*)dptrA, (int)Np,
+                                     (cuDoubleComplex* const*)dptrY, (int)Np, (int)nb));
+          k_sub_identity<<<grid_for(nb * NN, 256), 256, 0, s>>>(Z, Np, nb * NN);  // DH = D^H
+          count_launch();
+        }
+        Prof::Scope sc(a.prof, "dyson_W_gemm");
+        float2* F = (float2*)T1;
+        float2* E = (float2*)Mb;
+        // F = D^H D  (B(k, n) = D[k][n] = conj(DH[n][k]))
+        tc_cgemm_nt(Z, true, false, Np, NN, Z, true, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s);
+        dim3 hb(32, 8), hg((unsigned)((Np + 31) / 32), (unsigned)((Np + 31) / 32), (unsigned)nb);
+        k_herm_sum<<<hg, hb, 0, s>>>(Z, F, E, Np);
+        count_launch();
+        // T = L E  (E Hermitian: B(k, n) = conj(E[n][k]))
+        tc_cgemm_nt(L, true, false, Np, NN, E, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s);
+        // W = T L^H  (B(k, n) = conj(L[n][k])), written over Pi
+        tc_cgemm_nt(F, false, false, Np, NN, L, true, true, Np, NN, (float2*)Pi, Np, NN, Np, Np,
+                    Np, nb, s);
+      } else if (a.want_w) {
         // Y = C^{-1} L^H: column-major Y^T C^T = (L^H)^T  (right, upper)
         CQ_CHECK_CUDA(cudaMemcpyAsync(Y, LH, nb * NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
         {
@@ -178,11 +252,8 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
                                    (cuDoubleComplex* const*)dptrY, (int)Np, (int)nb));
         }
         Prof::Scope sc(a.prof, "dyson_W_gemm");
-        // W = Y^H Y - V, written over Pi
-        if (a.mixed) {
-          launch_from_c128<float>(V, (float2*)Pi, nb * NN, s);
-          tc_gemm_c(TcOp::C, Y, TcOp::N, Y, (float2*)Pi, Np, Np, Np, nb, s, /*beta_minus_one=*/true);
-        } else {
+        // W = Y^H Y - V, written over Pi (FP64 form)
+        {
           CQ_CHECK_CUDA(cudaMemcpyAsync(Pi, V, nb * NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
           CQ_BLAS(cublasZgemmStridedBatched(blas, CUBLAS_OP_N, CUBLAS_OP_C, (int)Np, (int)Np, (int)Np,
                                             (const cuDoubleComplex*)&one, (const cuDoubleComplex*)Y,

@@ -103,6 +103,8 @@ def make_system(n, nb: int, nocc: int, Np: int, beta: float = 1000.0, seed: int 
 WORKLOADS = {
     "rpa_k2_nb16_np128": dict(n=2, nb=16, nocc=8, Np=128, beta=1000.0, lam=1e4, prec="low"),
     "g0w0_k4_nb64_np512": dict(n=4, nb=64, nocc=24, Np=512, beta=1000.0, lam=1e4, prec="low"),
+    # same orbitals / N_mu on a 2x2x2 grid: the small case used for kernel profiles
+    "g0w0_k2_nb64_np512": dict(n=2, nb=64, nocc=24, Np=512, beta=1000.0, lam=1e4, prec="low"),
     "rpa_gw_k6_nb96_np1024": dict(n=6, nb=96, nocc=48, Np=1024, beta=1000.0, lam=1e5, prec="low"),
     "scgw_k3_nb48_np384": dict(n=3, nb=48, nocc=24, Np=384, beta=1000.0, lam=1e4, prec="low"),
 }
