@@ -1,0 +1,442 @@
+// Batched FP64 Cholesky factorisation, log-determinant and triangular inverse of
+// A = I - M (one CTA per Np x Np problem), the factorisation step of the Dyson solve.
+//
+//   A = C C^H (C lower, FP64), logdet = 2 sum_i ln C_ii, trace = sum_i M_ii,
+//   optional DH = C^{-H} - I (upper triangular, FP64) for W = L (D + D^H + D^H D) L^H.
+//
+// Right-looking blocked algorithm with 64 x 64 blocks: the diagonal block is factored and
+// inverted in shared memory, the panel below is L_ib = A_ib C_jj^{-H}, the trailing lower
+// triangle gets A_ik -= L_ij L_kj^H.  The inverse is formed block column by block column:
+// X_ij = -C_ii^{-1} sum_{k=j}^{i-1} C_ik X_kj.  Block products use 4 x 4 register tiles per
+// thread (256 threads per 64 x 64 output), operands staged in shared memory.
+#include <cstdint>
+
+#include "chol.cuh"
+
+namespace cq {
+
+namespace {
+
+constexpr int CB = 64;       // block size
+constexpr int CT = 256;      // threads per CTA
+constexpr int PITCH = CB + 1;  // smem row pitch (double2 elements)
+
+__device__ __forceinline__ double2 cmul_(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ double2 cmulc_(double2 a, double2 b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 conj_(double2 a) { return make_double2(a.x, -a.y); }
+
+// smem tile <- global block (rows r0.., cols c0..) of an ld x ld row-major matrix, rb x cb valid
+__device__ __forceinline__ void load_blk(double2* S, const double2* G, int64_t ld, int64_t r0,
+                                         int64_t c0, int rb, int cb) {
+  double2 v[CB * CB / CT];
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {  // all loads in flight before the smem stores
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;
+    v[u] = (r < rb && c < cb) ? G[(r0 + r) * ld + c0 + c] : make_double2(0, 0);
+  }
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    S[(i / CB) * PITCH + i % CB] = v[u];
+  }
+}
+// smem tile <- conj transpose of a global block: S[r][c] = conj(G[c0 + c][r0 + r])... given as
+// (the block stored at rows gr0, cols gc0 with gr x gc valid) -> S = G_blk^H
+__device__ __forceinline__ void load_blk_adj(double2* S, const double2* G, int64_t ld, int64_t gr0,
+                                             int64_t gc0, int gr, int gc) {
+  double2 v[CB * CB / CT];
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;  // S[c][r] = conj(G[gr0 + r][gc0 + c])
+    v[u] = (r < gr && c < gc) ? conj_(G[(gr0 + r) * ld + gc0 + c]) : make_double2(0, 0);
+  }
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    S[(i % CB) * PITCH + i / CB] = v[u];
+  }
+}
+// S (lower triangular part) <- adjoint of the upper triangle of a global diagonal block:
+// S[r][c] = conj(G[r0 + c][r0 + r]) for r >= c, 0 above
+__device__ __forceinline__ void load_blk_adjU(double2* S, const double2* G, int64_t ld, int64_t r0,
+                                              int nb) {
+  double2 v[CB * CB / CT];
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;  // v = conj(G[r0 + r][r0 + c]) feeds S[c][r], c >= r
+    v[u] = (r < nb && c < nb && c >= r) ? conj_(G[(r0 + r) * ld + r0 + c]) : make_double2(0, 0);
+  }
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    S[(i % CB) * PITCH + i / CB] = v[u];
+  }
+}
+// upper triangle of a global diagonal block <- adjoint of the lower-triangular S:
+// G[r0 + c][r0 + r] = conj(S[r][c]) for r >= c
+__device__ __forceinline__ void store_blk_adjU(const double2* S, double2* G, int64_t ld, int64_t r0,
+                                               int nb) {
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;
+    if (r < nb && c < nb && r >= c) G[(r0 + c) * ld + r0 + r] = conj_(S[r * PITCH + c]);
+  }
+}
+__device__ __forceinline__ void store_blk(const double2* S, double2* G, int64_t ld, int64_t r0,
+                                          int64_t c0, int rb, int cb) {
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;
+    if (r < rb && c < cb) G[(r0 + r) * ld + c0 + c] = S[r * PITCH + c];
+  }
+}
+
+// acc[i][j] (rows ty + 16 i, cols tx + 16 j) += sum_k X[r][k] * Y'[k][c] over k < K, where
+// Y'(k, c) = conj(Y[c][k]) if ADJ_Y (product with Y^H) else Y[k][c].
+template <bool ADJ_Y>
+__device__ __forceinline__ void mma_tile(const double2* X, const double2* Y, int K,
+                                         double2 (&acc)[4][4]) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int k = 0; k < K; ++k) {
+    double2 a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = X[(ty + 16 * i) * PITCH + k];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      b[j] = ADJ_Y ? conj_(Y[(tx + 16 * j) * PITCH + k]) : Y[k * PITCH + tx + 16 * j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        acc[i][j].x = fma(a[i].x, b[j].x, fma(-a[i].y, b[j].y, acc[i][j].x));
+        acc[i][j].y = fma(a[i].x, b[j].y, fma(a[i].y, b[j].x, acc[i][j].y));
+      }
+  }
+}
+
+// acc[i][j] -= sum_k X[r][k] conj(Y[c][k])  (A - X Y^H)
+__device__ __forceinline__ void mma_tile_sub(const double2* X, const double2* Y, int K,
+                                             double2 (&acc)[4][4]) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int k = 0; k < K; ++k) {
+    double2 a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = X[(ty + 16 * i) * PITCH + k];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = Y[(tx + 16 * j) * PITCH + k];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        // a * conj(b) = (ax bx + ay by) + i (ay bx - ax by)
+        acc[i][j].x = fma(-a[i].x, b[j].x, fma(-a[i].y, b[j].y, acc[i][j].x));
+        acc[i][j].y = fma(-a[i].y, b[j].x, fma(a[i].x, b[j].y, acc[i][j].y));
+      }
+  }
+}
+
+__device__ __forceinline__ void zero_acc(double2 (&acc)[4][4]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0, 0);
+}
+
+// In-place Cholesky of the lower triangle of S (n x n); adds sum ln C_ii to *ld_acc
+// (thread 0) and sets *bad if a pivot is not positive.  One barrier per column: column c is
+// used unscaled (times 1/d_c) in its rank-1 update and scaled during the next column's step.
+__device__ void factor_diag(double2* S, int n, double* ld_acc, int* bad) {
+  double prev_inv = 1.0, prev_d = 1.0;
+  for (int c = 0; c < n; ++c) {
+    __syncthreads();
+    double d = S[c * PITCH + c].x;
+    const bool good = d > 0.0;
+    d = good ? sqrt(d) : 1.0;
+    const double inv = 1.0 / d;
+    if (c > 0) {  // finish column c - 1: diagonal and scaled entries below it
+      if (threadIdx.x == 0) S[(c - 1) * PITCH + c - 1] = make_double2(prev_d, 0.0);
+      for (int r = c + threadIdx.x; r < n; r += CT) {
+        S[r * PITCH + c - 1].x *= prev_inv;
+        S[r * PITCH + c - 1].y *= prev_inv;
+      }
+    }
+    const int m = n - c - 1;
+    const double inv2 = inv * inv;
+    for (int idx = threadIdx.x; idx < m * m; idx += CT) {
+      const int r = c + 1 + idx / m, s = c + 1 + idx % m;
+      if (s <= r) {
+        const double2 u = cmulc_(S[r * PITCH + c], S[s * PITCH + c]);
+        S[r * PITCH + s].x -= u.x * inv2;
+        S[r * PITCH + s].y -= u.y * inv2;
+      }
+    }
+    if (threadIdx.x == 0) {
+      if (!good) *bad = 1;
+      *ld_acc += log(d);
+    }
+    prev_inv = inv;
+    prev_d = d;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) S[(n - 1) * PITCH + n - 1] = make_double2(prev_d, 0.0);
+  __syncthreads();
+}
+
+// Sinv = inverse of the lower-triangular S (n x n): forward substitution with one column
+// per group of 4 lanes (partial dot products reduced by shuffles).
+__device__ void invert_lower(const double2* S, double2* Sinv, int n) {
+  for (int i = threadIdx.x; i < CB * CB; i += CT) Sinv[(i / CB) * PITCH + i % CB] = make_double2(0, 0);
+  __syncthreads();
+  const int c = threadIdx.x >> 2, sub = threadIdx.x & 3;
+  const bool col = c < n;
+  if (col && sub == 0) Sinv[c * PITCH + c] = make_double2(1.0 / S[c * PITCH + c].x, 0.0);
+  __syncwarp();
+  for (int r = 1; r < n; ++r) {
+    double ax = 0, ay = 0;
+    if (col && r > c)
+      for (int k = c + sub; k < r; k += 4) {
+        const double2 u = cmul_(S[r * PITCH + k], Sinv[k * PITCH + c]);
+        ax += u.x;
+        ay += u.y;
+      }
+    ax += __shfl_xor_sync(0xffffffffu, ax, 1);
+    ay += __shfl_xor_sync(0xffffffffu, ay, 1);
+    ax += __shfl_xor_sync(0xffffffffu, ax, 2);
+    ay += __shfl_xor_sync(0xffffffffu, ay, 2);
+    if (col && r > c && sub == 0) {
+      const double inv = -1.0 / S[r * PITCH + r].x;
+      Sinv[r * PITCH + c] = make_double2(ax * inv, ay * inv);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ Mall,
+                                                    double2* __restrict__ Aall, float2* Zall,
+                                                    double* __restrict__ logdet,
+                                                    double2* __restrict__ trace,
+                                                    int* __restrict__ info, int64_t n) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* S0 = reinterpret_cast<double2*>(smem_raw);
+  double2* S1 = S0 + CB * PITCH;
+  double2* S2 = S1 + CB * PITCH;
+  __shared__ double s_ld;
+  __shared__ int s_bad;
+  __shared__ double s_red[2][CT];
+  const int64_t p = blockIdx.x;
+  const float2* M = Mall + p * n * n;
+  double2* A = Aall + p * n * n;
+  float2* Z = INV ? Zall + p * n * n : nullptr;
+  const int nblk = (int)((n + CB - 1) / CB);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+
+  if (threadIdx.x == 0) {
+    s_ld = 0.0;
+    s_bad = 0;
+  }
+  // A = I - M on the lower triangle (FP64), trace of M
+  double tr = 0, ti = 0;
+  for (int64_t i0 = 0; i0 < n * n; i0 += 8 * CT) {
+    float2 m[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t i = i0 + threadIdx.x + u * CT;
+      m[u] = (i < n * n && (i % n) <= (i / n)) ? M[i] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t i = i0 + threadIdx.x + u * CT;
+      if (i < n * n) {
+        const int64_t r = i / n, c = i % n;
+        if (c <= r) {
+          A[i] = make_double2((r == c ? 1.0 : 0.0) - (double)m[u].x, -(double)m[u].y);
+          if (r == c) {
+            tr += m[u].x;
+            ti += m[u].y;
+          }
+        }
+      }
+    }
+  }
+  s_red[0][threadIdx.x] = tr;
+  s_red[1][threadIdx.x] = ti;
+  __syncthreads();
+
+  for (int j = 0; j < nblk; ++j) {
+    const int64_t j0 = (int64_t)j * CB;
+    const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+    // 1. diagonal block: factor and invert
+    load_blk(S0, A, n, j0, j0, jb, jb);
+    __syncthreads();
+    factor_diag(S0, jb, &s_ld, &s_bad);
+    invert_lower(S0, S1, jb);
+    // C_jj is not needed again; the upper triangle of the diagonal block keeps C_jj^{-H}
+    if (INV) store_blk_adjU(S1, A, n, j0, jb);
+    __syncthreads();
+    // 2. panel: L_ib = A_ib C_jj^{-H}
+    for (int ib = j + 1; ib < nblk; ++ib) {
+      const int64_t i0 = (int64_t)ib * CB;
+      const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+      load_blk(S2, A, n, i0, j0, rb, jb);
+      __syncthreads();
+      double2 acc[4][4];
+      zero_acc(acc);
+      mma_tile<true>(S2, S1, jb, acc);
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int r = ty + 16 * i, c = tx + 16 * jj;
+          if (r < rb && c < jb) A[(i0 + r) * n + j0 + c] = acc[i][jj];
+        }
+      __syncthreads();
+    }
+    // 3. trailing update of the lower triangle: A_ik -= L_ij L_kj^H
+    for (int kb = j + 1; kb < nblk; ++kb) {
+      const int64_t k0 = (int64_t)kb * CB;
+      const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
+      load_blk(S0, A, n, k0, j0, kbsz, jb);
+      for (int ib = kb; ib < nblk; ++ib) {
+        const int64_t i0 = (int64_t)ib * CB;
+        const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+        load_blk(S2, A, n, i0, j0, rb, jb);
+        __syncthreads();
+        double2 acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)  // start from the current A block (loads in flight early)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int r = ty + 16 * i, c = tx + 16 * jj;
+            acc[i][jj] = (r < rb && c < kbsz && (ib > kb || c <= r)) ? A[(i0 + r) * n + k0 + c]
+                                                                      : make_double2(0, 0);
+          }
+        mma_tile_sub(S2, S0, jb, acc);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int r = ty + 16 * i, c = tx + 16 * jj;
+            if (r < rb && c < kbsz && (ib > kb || c <= r)) A[(i0 + r) * n + k0 + c] = acc[i][jj];
+          }
+        __syncthreads();
+      }
+    }
+  }
+
+  if (INV) {
+    // X = C^{-1} block column by block column, X^H kept in the upper triangle of A
+    for (int j = 0; j < nblk; ++j) {
+      const int64_t j0 = (int64_t)j * CB;
+      const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+      for (int ib = j + 1; ib < nblk; ++ib) {
+        const int64_t i0 = (int64_t)ib * CB;
+        const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+        double2 acc[4][4];
+        zero_acc(acc);
+        for (int kb = j; kb < ib; ++kb) {
+          const int64_t k0 = (int64_t)kb * CB;
+          const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
+          load_blk(S2, A, n, i0, k0, rb, kbsz);  // C_ik (strictly lower block)
+          if (kb == j)
+            load_blk_adjU(S0, A, n, j0, jb);  // X_jj
+          else
+            load_blk_adj(S0, A, n, j0, k0, jb, kbsz);  // X_kj = (A_jk)^H
+          __syncthreads();
+          mma_tile<false>(S2, S0, kbsz, acc);
+          __syncthreads();
+        }
+        // X_ij = -C_ii^{-1} acc
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) S2[(ty + 16 * i) * PITCH + tx + 16 * jj] = acc[i][jj];
+        load_blk_adjU(S0, A, n, i0, rb);  // C_ii^{-1}
+        __syncthreads();
+        zero_acc(acc);
+        mma_tile<false>(S0, S2, rb, acc);
+        __syncthreads();
+        // A[j0 + c][i0 + r] = conj(X_ij[r][c]) = -conj(acc[r][c])
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int r = ty + 16 * i, c = tx + 16 * jj;
+            if (r < rb && c < jb) A[(j0 + c) * n + i0 + r] = make_double2(-acc[i][jj].x, acc[i][jj].y);
+          }
+        __syncthreads();
+      }
+    }
+    // Z = X^H - I (upper, complex64), zero below the diagonal
+    for (int64_t i0 = 0; i0 < n * n; i0 += 8 * CT) {
+      double2 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t i = i0 + threadIdx.x + u * CT;
+        v[u] = (i < n * n && (i % n) >= (i / n)) ? A[i] : make_double2(0, 0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t i = i0 + threadIdx.x + u * CT;
+        if (i < n * n) {
+          if ((i % n) == (i / n)) v[u].x -= 1.0;
+          Z[i] = make_float2((float)v[u].x, (float)v[u].y);
+        }
+      }
+    }
+  }
+
+  // reductions
+  for (int w = CT / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s_red[0][threadIdx.x] += s_red[0][threadIdx.x + w];
+      s_red[1][threadIdx.x] += s_red[1][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    logdet[p] = 2.0 * s_ld;
+    trace[p] = make_double2(s_red[0][0], s_red[1][0]);
+    info[p] = s_bad;
+  }
+}
+
+}  // namespace
+
+void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, double2* trace,
+                     int* info, int64_t Np, int64_t nprob, cudaStream_t s) {
+  const size_t smem = (size_t)3 * CB * PITCH * sizeof(double2);
+  if (Z) {
+    static bool set = false;
+    if (!set) {
+      CQ_CHECK_CUDA(cudaFuncSetAttribute(k_chol_inv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+      set = true;
+    }
+    k_chol_inv<true><<<(unsigned)nprob, CT, smem, s>>>(M, A, Z, logdet, trace, info, Np);
+  } else {
+    static bool set = false;
+    if (!set) {
+      CQ_CHECK_CUDA(cudaFuncSetAttribute(k_chol_inv<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      set = true;
+    }
+    k_chol_inv<false><<<(unsigned)nprob, CT, smem, s>>>(M, A, Z, logdet, trace, info, Np);
+  }
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+}  // namespace cq

@@ -77,6 +77,7 @@ struct coqui_b200_ctx {
   DevBuf<double2> eps;
   DevBuf<unsigned char> Gp, Gn, PW;  // storage precision, bytes
   DevBuf<unsigned char> dyn;         // Dyson scratch
+  DevBuf<float4> Ls, LHs;            // pre-split L, L^H for the tensor-core Dyson products
   cq::TcOperand Xtc;                 // packed X for the tensor-core projections
 
   // phase timing of the last call
@@ -337,6 +338,8 @@ void coqui_b200_destroy(coqui_b200_ctx* c) {
   c->Gn.release();
   c->PW.release();
   c->dyn.release();
+  c->Ls.release();
+  c->LHs.release();
   c->Xtc.release();
   for (auto& m : c->marks) cudaEventDestroy(m.second);
   if (c->sol) cusolverDnDestroy(c->sol);
@@ -483,7 +486,13 @@ int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_
     int info = cq::cholesky_lower_batched(c->sol, c->L.p, Np, nk, c->st);
     CQ_REQUIRE(info == 0, COQUI_B200_ENOTHPD, "Coulomb matrix V^q is not positive definite");
     cq::launch_zero_upper_and_adjoint(c->L.p, c->LH.p, Np, nk, c->st);
-    if (c->mode == COQUI_B200_MIXED) cq::tc_pack_X(c->Xtc, c->X.p, nk, Np, nb, c->st);
+    if (c->mode == COQUI_B200_MIXED) {
+      cq::tc_pack_X(c->Xtc, c->X.p, nk, Np, nb, c->st);
+      c->Ls.ensure((size_t)nk * Np * Np);
+      c->LHs.ensure((size_t)nk * Np * Np);
+      cq::to_split(c->L.p, c->Ls.p, Np, Np, nk, false, c->st);
+      cq::to_split(c->LH.p, c->LHs.p, Np, Np, nk, false, c->st);
+    }
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->have_thc = true;
     c->w_valid = false;
@@ -577,6 +586,8 @@ void dyson_all(Ctx* c, bool want_w, bool want_e, std::vector<double>* logdet,
   a.L = c->L.p;
   a.LH = c->LH.p;
   a.V = c->V.p;
+  a.Ls = c->Ls.p;
+  a.LHs = c->LHs.p;
   a.want_w = want_w;
   a.want_e = want_e;
   a.mixed = (c->mode == COQUI_B200_MIXED);

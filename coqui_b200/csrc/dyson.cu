@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <string>
 
+#include "chol.cuh"
 #include "dyson.cuh"
 #include "kernels.cuh"
 #include "tc_gemm.cuh"
@@ -39,43 +40,38 @@ __global__ void k_zero_upper_adjoint(double2* __restrict__ L, double2* __restric
   }
 }
 
-// Z[p] = I (complex128), nprob problems
-__global__ void k_set_identity(double2* __restrict__ Z, int64_t Np, int64_t total) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = i % (Np * Np);
-    Z[i] = make_double2(e / Np == e % Np ? 1.0 : 0.0, 0.0);
-  }
-}
-// Z[p] -= I in place
-__global__ void k_sub_identity(double2* __restrict__ Z, int64_t Np, int64_t total) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = i % (Np * Np);
-    if (e / Np == e % Np) Z[i].x -= 1.0;
-  }
-}
-// E = DH + DH^H + F  (32 x 32 tiles through shared memory for the transposed read)
-__global__ void k_herm_sum(const double2* __restrict__ DH, const float2* __restrict__ F,
+// E = DH + DH^H + F with only the lower triangle (i >= j) of the Hermitian F computed
+// (32 x 32 tiles through shared memory for the transposed reads)
+__global__ void k_herm_sum(const float2* __restrict__ DH, const float2* __restrict__ F,
                            float2* __restrict__ E, int64_t Np) {
-  __shared__ double2 tile[32][33];
+  __shared__ float2 tile[32][33];
+  __shared__ float2 ftile[32][33];
   const int64_t p = blockIdx.z;
-  const double2* d = DH + p * Np * Np;
+  const float2* d = DH + p * Np * Np;
+  const float2* f = F + p * Np * Np;
   const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
-  // load DH[j0 + ty][i0 + tx] for the transposed term
+  // transposed block: DH[j0 + ty][i0 + tx], F[j0 + ty][i0 + tx] (read only where lower)
   for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
     const int64_t r = j0 + ty, c = i0 + threadIdx.x;
-    tile[ty][threadIdx.x] = (r < Np && c < Np) ? d[r * Np + c] : make_double2(0, 0);
+    const bool in = r < Np && c < Np;
+    tile[ty][threadIdx.x] = in ? d[r * Np + c] : make_float2(0.f, 0.f);
+    ftile[ty][threadIdx.x] = (in && r >= c) ? f[r * Np + c] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
     const int64_t i = i0 + ty, j = j0 + threadIdx.x;
     if (i < Np && j < Np) {
-      const double2 a = d[i * Np + j];
-      const double2 b = tile[threadIdx.x][ty];  // DH[j][i]
-      const float2 f = F[p * Np * Np + i * Np + j];
+      const float2 a = d[i * Np + j];
+      const float2 b = tile[threadIdx.x][ty];  // DH[j][i]
+      float2 fv;
+      if (i >= j) {
+        fv = f[i * Np + j];
+      } else {
+        const float2 t = ftile[threadIdx.x][ty];  // F[j][i], lower
+        fv = make_float2(t.x, -t.y);
+      }
       E[p * Np * Np + i * Np + j] =
-          make_float2((float)(a.x + b.x + (double)f.x), (float)(a.y - b.y + (double)f.y));
+          make_float2(a.x + b.x + fv.x, a.y - b.y + fv.y);
     }
   }
 }
@@ -125,8 +121,12 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
   const size_t per = NN * (es + es + (a.mixed ? sizeof(double2) : 0) +
                            (a.want_w ? sizeof(double2) : 0)) +
                      4 * sizeof(void*) + sizeof(int) + sizeof(double) + sizeof(double2) + 64;
-  const size_t budget = (size_t)4 << 30;
-  const int64_t nbq = std::max<int64_t>(1, std::min<int64_t>(nq, (int64_t)(budget / per)));
+  // FP64 form: one frequency at a time (cuBLAS strided batches over q); mixed form: chunks of
+  // the flattened (w, q) problem list, per-q operands addressed periodically.
+  const size_t budget = (size_t)(a.mixed ? 8 : 4) << 30;
+  const int64_t nprob = nw * nq;
+  const int64_t nbq = a.mixed ? std::max<int64_t>(1, std::min<int64_t>(nprob, (int64_t)(budget / per)))
+                              : std::max<int64_t>(1, std::min<int64_t>(nq, (int64_t)(budget / per)));
   scratch.ensure(per * nbq + 1024);
   unsigned char* base = scratch.p;
   auto carve = [&](size_t bytes) {
@@ -162,25 +162,44 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
   std::vector<int> info_h(nbq);
 
   const double2 one = make_double2(1, 0), zero = make_double2(0, 0), mone = make_double2(-1, 0);
-  for (int64_t n = 0; n < nw; ++n) {
-    for (int64_t q0 = 0; q0 < nq; q0 += nbq) {
-      const int64_t nb = std::min(nbq, nq - q0);
-      const int64_t p0 = n * nq + q0;
+  // chunk list: (first flattened problem, count)
+  std::vector<std::pair<int64_t, int64_t>> chunks;
+  if (a.mixed) {
+    for (int64_t p0 = 0; p0 < nprob; p0 += nbq) chunks.emplace_back(p0, std::min(nbq, nprob - p0));
+  } else {
+    for (int64_t n = 0; n < nw; ++n)
+      for (int64_t q0 = 0; q0 < nq; q0 += nbq) chunks.emplace_back(n * nq + q0, std::min(nbq, nq - q0));
+  }
+  for (const auto& ch : chunks) {
+    {
+      const int64_t p0 = ch.first, nb = ch.second;
+      const int64_t q0 = p0 % nq;
       unsigned char* Pi = a.PW + (size_t)p0 * NN * es;
+      // the mixed form addresses the per-q factors periodically from their bases
       const double2* L = a.L + q0 * NN;
       const double2* LH = a.LH + q0 * NN;
+      const float4* Ls = a.Ls;    // mixed form: pre-split factors, addressed periodically in q
+      const float4* LHs = a.LHs;
       const double2* V = a.V + q0 * NN;
       // M = L^H (Pi L)
       {
       Prof::Scope sc(a.prof, "dyson_M_gemm");
       if (a.mixed) {
         // P1 = L^H Pi  (Pi Hermitian: B(k, n) = Pi[k][n] = conj(Pi[n][k]))
-        tc_cgemm_nt(LH, true, false, Np, NN, Pi, false, true, Np, NN, (float2*)T1, Np, NN, Np,
-                    Np, Np, nb, s);
+        TcStructure s1;
+        s1.a_upper = true;  // L^H upper triangular
+        s1.a_mod = nq;
+        s1.a_q0 = q0;
+        tc_cgemm_nt(LHs, true, false, Np, NN, Pi, false, true, Np, NN, (float2*)T1, Np, NN, Np,
+                    Np, Np, nb, s, s1);
         // M = P1 L  (B(k, n) = L[k][n] = conj(LH[n][k]))
-        tc_cgemm_nt(T1, false, false, Np, NN, LH, true, true, Np, NN, (float2*)Mb, Np, NN, Np, Np,
-                    Np, nb, s);
-        launch_eye_minus<float>((const float2*)Mb, A, Np, nb, s);
+        TcStructure s2;
+        s2.b_lower = true;     // L lower triangular
+        s2.b_mod = nq;
+        s2.b_q0 = q0;
+        s2.lower_only = true;  // M Hermitian: the Cholesky reads the lower triangle
+        tc_cgemm_nt(T1, false, false, Np, NN, LHs, true, true, Np, NN, (float2*)Mb, Np, NN, Np, Np,
+                    Np, nb, s, s2);
       } else {
         // row-major C = A B  ->  column-major C^T = B^T A^T
         CQ_BLAS(cublasZgemmStridedBatched(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)Np, (int)Np, (int)Np,
@@ -197,12 +216,19 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       }
       }
       // I - M = C C^H (FP64)
-      {
+      if (a.mixed) {
+        Prof::Scope sc(a.prof, "dyson_chol_inv");
+        launch_chol_inv((const float2*)Mb, A, a.want_w ? (float2*)Y : nullptr, dld, dtr, dinfo, Np,
+                        nb, s);
+      } else {
         Prof::Scope sc(a.prof, "dyson_potrf");
         potrf_ptrs(sol, dptrA, Np, dinfo, nb);
       }
       CQ_CHECK_CUDA(cudaMemcpyAsync(info_h.data(), dinfo, nb * sizeof(int), cudaMemcpyDeviceToHost, s));
-      if (a.want_e) {
+      if (a.want_e && a.mixed) {
+        CQ_CHECK_CUDA(cudaMemcpyAsync(ld_h.data(), dld, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CQ_CHECK_CUDA(cudaMemcpyAsync(tr_h.data(), dtr, nb * sizeof(double2), cudaMemcpyDeviceToHost, s));
+      } else if (a.want_e) {
         Prof::Scope sc(a.prof, "rpa_logdet");
         if (a.mixed)
           launch_logdet_trace<float>(A, (const float2*)Mb, dld, dtr, Np, nb, s);
@@ -214,32 +240,32 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       if (a.want_w && a.mixed) {
         // W = L E L^H with E = (I - M)^{-1} - I = D + D^H + D^H D, D = C^{-1} - I: no
         // cancellation against V, so the split-TF32 products keep W to ~1e-8.
-        double2* Z = Y;  // Z = C^{-H}: column-major Z^T conj(C) = I  (right, upper, ^H)
-        {
-          Prof::Scope sc(a.prof, "dyson_trsm");
-          k_set_identity<<<grid_for(nb * NN, 256), 256, 0, s>>>(Z, Np, nb * NN);
-          count_launch();
-          CQ_BLAS(cublasZtrsmBatched(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C,
-                                     CUBLAS_DIAG_NON_UNIT, (int)Np, (int)Np,
-                                     (const cuDoubleComplex*)&one,
-                                     (const cuDoubleComplex* const*)dptrA, (int)Np,
-                                     (cuDoubleComplex* const*)dptrY, (int)Np, (int)nb));
-          k_sub_identity<<<grid_for(nb * NN, 256), 256, 0, s>>>(Z, Np, nb * NN);  // DH = D^H
-          count_launch();
-        }
+        const float2* Z = (const float2*)Y;  // DH = C^{-H} - I from the FP64 factorisation
         Prof::Scope sc(a.prof, "dyson_W_gemm");
         float2* F = (float2*)T1;
         float2* E = (float2*)Mb;
         // F = D^H D  (B(k, n) = D[k][n] = conj(DH[n][k]))
-        tc_cgemm_nt(Z, true, false, Np, NN, Z, true, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s);
+        TcStructure s3;
+        s3.a_upper = true;     // D^H upper
+        s3.b_lower = true;     // D lower
+        s3.lower_only = true;  // F Hermitian
+        tc_cgemm_nt(Z, false, false, Np, NN, Z, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s3);
         dim3 hb(32, 8), hg((unsigned)((Np + 31) / 32), (unsigned)((Np + 31) / 32), (unsigned)nb);
         k_herm_sum<<<hg, hb, 0, s>>>(Z, F, E, Np);
         count_launch();
         // T = L E  (E Hermitian: B(k, n) = conj(E[n][k]))
-        tc_cgemm_nt(L, true, false, Np, NN, E, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s);
+        TcStructure s4;
+        s4.a_lower = true;  // L lower
+        s4.a_mod = nq;
+        s4.a_q0 = q0;
+        tc_cgemm_nt(Ls, true, false, Np, NN, E, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s4);
         // W = T L^H  (B(k, n) = conj(L[n][k])), written over Pi
-        tc_cgemm_nt(F, false, false, Np, NN, L, true, true, Np, NN, (float2*)Pi, Np, NN, Np, Np,
-                    Np, nb, s);
+        TcStructure s5;
+        s5.b_upper = true;  // B(k, n) = conj(L[n][k]) vanishes for k > n
+        s5.b_mod = nq;
+        s5.b_q0 = q0;
+        tc_cgemm_nt(F, false, false, Np, NN, Ls, true, true, Np, NN, (float2*)Pi, Np, NN, Np, Np,
+                    Np, nb, s, s5);
       } else if (a.want_w) {
         // Y = C^{-1} L^H: column-major Y^T C^T = (L^H)^T  (right, upper)
         CQ_CHECK_CUDA(cudaMemcpyAsync(Y, LH, nb * NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
@@ -266,7 +292,8 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       for (int64_t i = 0; i < nb; ++i) {
         if (info_h[i] != 0)
           throw Error(COQUI_B200_ENOTHPD, "I - L^H Pi L is not positive definite at (w=" +
-                                              std::to_string(n) + ", q=" + std::to_string(q0 + i) + ")");
+                                              std::to_string((p0 + i) / nq) + ", q=" +
+                                              std::to_string((p0 + i) % nq) + ")");
         if (a.want_e) {
           (*logdet)[p0 + i] = ld_h[i];
           (*trace)[p0 + i] = tr_h[i];

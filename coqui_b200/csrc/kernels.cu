@@ -142,17 +142,28 @@ __device__ void dft3(C* A, C* B, int n0, int n1, int n2, int sign) {
   __syncthreads();
 }
 
+// Tile loads are issued 8 per thread before the shared-memory stores so that enough
+// requests are in flight to cover DRAM latency.
 template <typename C, int TILE>
 __device__ __forceinline__ void load_tile(C* A, const C* __restrict__ src, int nk, int64_t ncol,
                                           int64_t col0) {
-  for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) {
-    const int k = i / TILE, c = i % TILE;
-    const int64_t col = col0 + c;
-    C v;
-    v.x = 0;
-    v.y = 0;
-    if (col < ncol) v = src[(int64_t)k * ncol + col];
-    A[i] = v;
+  const int total = nk * TILE;
+  for (int i0 = 0; i0 < total; i0 += 8 * 256) {
+    C v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + threadIdx.x + u * 256;
+      const int k = i / TILE, c = i % TILE;
+      const int64_t col = col0 + c;
+      v[u].x = 0;
+      v[u].y = 0;
+      if (i < total && col < ncol) v[u] = src[(int64_t)k * ncol + col];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + threadIdx.x + u * 256;
+      if (i < total) A[i] = v[u];
+    }
   }
 }
 
@@ -351,23 +362,34 @@ __global__ void __launch_bounds__(128) k_ir_transform(cplx_t<R>* __restrict__ bu
         x[t].y = 0;
       }
     }
-    for (int n = 0; n < n_out; ++n) {
-      double ar = 0, ai = 0;
+    for (int n = 0; n < n_out; n += 2) {
+      const bool two = n + 1 < n_out;
+      double ar = 0, ai = 0, br = 0, bi = 0, cr = 0, ci = 0, dr = 0, di = 0;
       const double2* row = sM + n * n_in;
+      const double2* row2 = sM + (two ? n + 1 : n) * n_in;
 #pragma unroll
       for (int t = 0; t < MAXT; ++t) {
         if (t < n_in) {
-          const double2 m = row[t];
+          const double2 m = row[t], m2 = row2[t];
           ar = fma(m.x, x[t].x, ar);
-          ar = fma(-m.y, x[t].y, ar);
+          br = fma(-m.y, x[t].y, br);
           ai = fma(m.x, x[t].y, ai);
-          ai = fma(m.y, x[t].x, ai);
+          bi = fma(m.y, x[t].x, bi);
+          cr = fma(m2.x, x[t].x, cr);
+          dr = fma(-m2.y, x[t].y, dr);
+          ci = fma(m2.x, x[t].y, ci);
+          di = fma(m2.y, x[t].x, di);
         }
       }
       cplx_t<R> o;
-      o.x = (R)ar;
-      o.y = (R)ai;
+      o.x = (R)(ar + br);
+      o.y = (R)(ai + bi);
       buf[(int64_t)n * ncol + e] = o;
+      if (two) {
+        o.x = (R)(cr + dr);
+        o.y = (R)(ci + di);
+        buf[(int64_t)(n + 1) * ncol + e] = o;
+      }
     }
   }
 }

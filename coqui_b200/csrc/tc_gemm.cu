@@ -12,11 +12,13 @@
 // (hi = rna(x), lo = rna(x - hi)); hi*hi + hi*lo + lo*hi accumulate in FP32 in TMEM.
 //
 // CTA tile: 128 rows x BNC complex columns (UMMA M = 128, N = 2 BNC), 16 complex (32 real)
-// of K per pipeline stage = one 128-byte swizzle row.  Warps 0-3 stage operands (global ->
-// registers -> split -> swizzled st.shared) and later drain TMEM; warp 4 allocates TMEM and
-// one of its lanes issues the MMAs.  Waits are bounded by a 2 s global-timer budget that sets
-// an error flag instead of hanging.
+// of K per pipeline stage = one 128-byte swizzle row.  Warps 0-7 stage operands (global ->
+// registers, one stage ahead -> split -> swizzled st.shared) and then drain TMEM through a
+// shared-memory transpose into coalesced rows; warp 8 allocates TMEM and one of its lanes
+// issues the MMAs.  Known triangular structure of A or B trims each tile's K range.  Waits
+// are bounded by a 2 s global-timer budget that sets an error flag instead of hanging.
 #include <cstdint>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "tc_gemm.cuh"
@@ -30,8 +32,8 @@ __device__ int g_tc_error = 0;
 constexpr int kBM = 128;
 constexpr int kBKR = 32;  // real K per stage (128 bytes of fp32)
 constexpr int kStages = 2;
-constexpr int kProducers = 128;
-constexpr int kThreads = 160;
+constexpr int kProducers = 256;  // warps 0-7 stage operands, then drain the accumulator
+constexpr int kThreads = kProducers + 32;  // + warp 8: TMEM allocation and MMA issue
 
 template <int BNC> struct TileCfg {
   static constexpr int NR = 2 * BNC;                   // UMMA N (real columns)
@@ -40,9 +42,13 @@ template <int BNC> struct TileCfg {
   static constexpr int STAGE = 2 * A_PLANE + 2 * B_PLANE;
   static constexpr int SMEM = kStages * STAGE + 1024 /*align*/ + 256 /*barriers*/;
   static constexpr int TMEM_COLS = NR;                 // 64, 128 or 256
+  static constexpr int B_CHUNKS = BNC * 8 / kProducers;  // B chunks per producer thread
   // kind::tf32 dense, F32 accumulate, K-major A and B, M = 128, N = NR
   static constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) |
                                     ((uint32_t)(NR >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+  // epilogue transpose buffer: 32 rows x (NR / 2 + 4) floats per warp
+  static constexpr int EPI_PITCH = NR / 2 + 4;
+  static_assert(8 * 32 * EPI_PITCH * 4 <= kStages * STAGE, "epilogue buffer");
 };
 
 struct TcParams {
@@ -54,6 +60,9 @@ struct TcParams {
   int64_t sA, sB, sC;
   int a64, b64;  // element type is complex128
   int conj_a, conj_b;
+  int a_upper, a_lower, b_lower, b_upper, lower_only;
+  // periodic batch index (0 = off): operand batch = (q0 + b) % mod, for per-q operands
+  int64_t a_mod, a_q0, b_mod, b_q0;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -98,10 +107,9 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
   return r;
 }
 
-// split x (float or double) into TF32 hi + lo
+// split x into TF32 hi + lo (hi = rna(x), lo = rna(x - hi))
 __device__ __forceinline__ void split2(double x, uint32_t& hi, uint32_t& lo) {
-  const float xf = (float)x;
-  hi = to_tf32(xf);
+  hi = to_tf32((float)x);
   lo = to_tf32((float)(x - (double)__uint_as_float(hi)));
 }
 __device__ __forceinline__ void split2(float x, uint32_t& hi, uint32_t& lo) {
@@ -140,76 +148,113 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
                : "memory");
 }
 
-// load two consecutive complex values (k, k+1) of a row as doubles; zero outside [0, kmax)
-template <bool C64>
-__device__ __forceinline__ void load_pair(const void* base, int64_t off, int64_t k, int64_t kmax,
-                                          double v[4]) {
-  if (C64) {
+// Two consecutive complex values (k, k+1) of one operand row, as loaded from global.
+template <bool C128> struct Pair;
+template <> struct Pair<false> {
+  float4 v;
+  __device__ __forceinline__ void load(const void* base, int64_t off, int64_t k, int64_t kmax,
+                                       bool row_ok) {
     const float2* p = reinterpret_cast<const float2*>(base) + off;
-    if (k + 1 < kmax && ((off & 1) == 0)) {
-      const float4 q = *reinterpret_cast<const float4*>(p);
-      v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    if (row_ok && k + 1 < kmax && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+      v = __ldg(reinterpret_cast<const float4*>(p));
     } else {
       float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
-      if (k < kmax) a = p[0];
-      if (k + 1 < kmax) b = p[1];
-      v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+      if (row_ok && k < kmax) a = __ldg(p);
+      if (row_ok && k + 1 < kmax) b = __ldg(p + 1);
+      v = make_float4(a.x, a.y, b.x, b.y);
     }
-  } else {
-    const double2* p = reinterpret_cast<const double2*>(base) + off;
-    double2 a = make_double2(0, 0), b = make_double2(0, 0);
-    if (k < kmax) a = p[0];
-    if (k + 1 < kmax) b = p[1];
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
   }
-}
+  __device__ __forceinline__ void get(float (&x)[4]) const {
+    x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+  }
+};
+// Pre-split operand: one float4 (hi.re, hi.im, lo.re, lo.im) per complex value, hi/lo TF32.
+template <> struct Pair<true> {
+  float4 a, b;
+  __device__ __forceinline__ void load(const void* base, int64_t off, int64_t k, int64_t kmax,
+                                       bool row_ok) {
+    const float4* p = reinterpret_cast<const float4*>(base) + off;
+    a = make_float4(0.f, 0.f, 0.f, 0.f);
+    b = a;
+    if (row_ok && k < kmax) a = __ldg(p);
+    if (row_ok && k + 1 < kmax) b = __ldg(p + 1);
+  }
+};
+template <int BNC, bool A64, bool B64> struct Staging {
+  using Cfg = TileCfg<BNC>;
+  Pair<A64> a[4];
+  Pair<B64> b[Cfg::B_CHUNKS];
 
-template <int BNC, bool A64, bool B64>
-__device__ __forceinline__ void stage_tile(const TcParams& p, int64_t bz, int64_t m0, int64_t n0,
-                                           int64_t k0c, uint32_t sA_hi, uint32_t sA_lo,
-                                           uint32_t sB_hi, uint32_t sB_lo) {
-  const int t = threadIdx.x;  // 0..127
-  const double ca = p.conj_a ? -1.0 : 1.0, cb = p.conj_b ? -1.0 : 1.0;
-  // A: 128 rows x 8 chunks (2 complex each)
-#pragma unroll 2
-  for (int i = t; i < kBM * 8; i += kProducers) {
-    const int r = i >> 3, c = i & 7;
-    const int64_t m = m0 + r, k = k0c + 2 * c;
-    double v[4] = {0, 0, 0, 0};
-    if (m < p.M) load_pair<!A64>(p.A, bz * p.sA + m * p.lda + k, k, p.K, v);
-    v[1] *= ca;
-    v[3] *= ca;
-    uint32_t h[4], l[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) split2(v[j], h[j], l[j]);
-    const uint32_t off = sw128(r, c);
-    st_shared_v4(sA_hi + off, h[0], h[1], h[2], h[3]);
-    st_shared_v4(sA_lo + off, l[0], l[1], l[2], l[3]);
-  }
-  // B: BNC complex rows x 8 chunks -> realified rows 2n, 2n+1
-#pragma unroll 2
-  for (int i = t; i < BNC * 8; i += kProducers) {
-    const int r = i >> 3, c = i & 7;
-    const int64_t n = n0 + r, k = k0c + 2 * c;
-    double v[4] = {0, 0, 0, 0};
-    if (n < p.N) load_pair<!B64>(p.Bt, bz * p.sB + n * p.ldb + k, k, p.K, v);
-    const double br0 = v[0], bi0 = cb * v[1], br1 = v[2], bi1 = cb * v[3];
-    // row 2r: (br, -bi) pairs; row 2r+1: (bi, br) pairs
-    const double e0[4] = {br0, -bi0, br1, -bi1};
-    const double e1[4] = {bi0, br0, bi1, br1};
-    uint32_t h0[4], l0[4], h1[4], l1[4];
+  __device__ __forceinline__ void load(const TcParams& p, int64_t bz, int64_t m0, int64_t n0,
+                                       int64_t k0c) {
+    const int t = threadIdx.x;
+    const int64_t ba = p.a_mod ? (p.a_q0 + bz) % p.a_mod : bz;
+    const int64_t bb = p.b_mod ? (p.b_q0 + bz) % p.b_mod : bz;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      split2(e0[j], h0[j], l0[j]);
-      split2(e1[j], h1[j], l1[j]);
+      const int i = t + j * kProducers;
+      const int r = i >> 3, c = i & 7;
+      const int64_t m = m0 + r, k = k0c + 2 * c;
+      a[j].load(p.A, ba * p.sA + m * p.lda + k, k, p.K, m < p.M);
     }
-    const uint32_t o0 = sw128(2 * r, c), o1 = sw128(2 * r + 1, c);
-    st_shared_v4(sB_hi + o0, h0[0], h0[1], h0[2], h0[3]);
-    st_shared_v4(sB_lo + o0, l0[0], l0[1], l0[2], l0[3]);
-    st_shared_v4(sB_hi + o1, h1[0], h1[1], h1[2], h1[3]);
-    st_shared_v4(sB_lo + o1, l1[0], l1[1], l1[2], l1[3]);
+#pragma unroll
+    for (int j = 0; j < Cfg::B_CHUNKS; ++j) {
+      const int i = t + j * kProducers;
+      const int r = i >> 3, c = i & 7;
+      const int64_t n = n0 + r, k = k0c + 2 * c;
+      b[j].load(p.Bt, bb * p.sB + n * p.ldb + k, k, p.K, n < p.N);
+    }
   }
-}
+
+  // hi/lo TF32 words of the two complex values of a chunk: (re0, im0, re1, im1)
+  template <bool SPLIT>
+  __device__ __forceinline__ static void words(const Pair<SPLIT>& q, float sgn, uint32_t (&h)[4],
+                                               uint32_t (&l)[4]) {
+    if constexpr (SPLIT) {
+      h[0] = __float_as_uint(q.a.x); h[1] = __float_as_uint(sgn * q.a.y);
+      h[2] = __float_as_uint(q.b.x); h[3] = __float_as_uint(sgn * q.b.y);
+      l[0] = __float_as_uint(q.a.z); l[1] = __float_as_uint(sgn * q.a.w);
+      l[2] = __float_as_uint(q.b.z); l[3] = __float_as_uint(sgn * q.b.w);
+    } else {
+      float v[4];
+      q.get(v);
+      v[1] *= sgn;
+      v[3] *= sgn;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) split2(v[j], h[j], l[j]);
+    }
+  }
+
+  __device__ __forceinline__ void store(const TcParams& p, uint32_t sA_hi, uint32_t sA_lo,
+                                        uint32_t sB_hi, uint32_t sB_lo) const {
+    const int t = threadIdx.x;
+    const float ca = p.conj_a ? -1.f : 1.f, cb = p.conj_b ? -1.f : 1.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int i = t + j * kProducers;
+      const int r = i >> 3, c = i & 7;
+      uint32_t h[4], l[4];
+      words<A64>(a[j], ca, h, l);
+      const uint32_t off = sw128(r, c);
+      st_shared_v4(sA_hi + off, h[0], h[1], h[2], h[3]);
+      st_shared_v4(sA_lo + off, l[0], l[1], l[2], l[3]);
+    }
+    constexpr uint32_t SGN = 0x80000000u;
+#pragma unroll
+    for (int j = 0; j < Cfg::B_CHUNKS; ++j) {
+      const int i = t + j * kProducers;
+      const int r = i >> 3, c = i & 7;
+      uint32_t h[4], l[4];  // (br0, bi0, br1, bi1) after conjugation
+      words<B64>(b[j], cb, h, l);
+      // realified rows: 2r = (br, -bi) pairs, 2r+1 = (bi, br) pairs
+      const uint32_t o0 = sw128(2 * r, c), o1 = sw128(2 * r + 1, c);
+      st_shared_v4(sB_hi + o0, h[0], h[1] ^ SGN, h[2], h[3] ^ SGN);
+      st_shared_v4(sB_lo + o0, l[0], l[1] ^ SGN, l[2], l[3] ^ SGN);
+      st_shared_v4(sB_hi + o1, h[1], h[0], h[3], h[2]);
+      st_shared_v4(sB_lo + o1, l[1], l[0], l[3], l[2]);
+    }
+  }
+};
 
 template <int BNC, bool A64, bool B64>
 __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
@@ -222,7 +267,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t bz = blockIdx.z;
   const int64_t m0 = (int64_t)blockIdx.y * kBM, n0 = (int64_t)blockIdx.x * BNC;
-  const int nkb = (int)((p.K + 15) / 16);
+  if (p.lower_only && n0 > m0 + kBM - 1) return;  // tile strictly above the diagonal
+
+  // K blocks (16 complex each) that can be nonzero for this tile
+  int kb_lo = 0, kb_hi = (int)((p.K + 15) / 16);
+  if (p.a_upper) kb_lo = max(kb_lo, (int)(m0 / 16));
+  if (p.b_lower) kb_lo = max(kb_lo, (int)(n0 / 16));
+  if (p.a_lower) kb_hi = min(kb_hi, (int)((m0 + kBM - 1) / 16) + 1);
+  if (p.b_upper) kb_hi = min(kb_hi, (int)((n0 + BNC - 1) / 16) + 1);
+  const int nkb = max(kb_hi - kb_lo, 0);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -232,7 +285,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
     mbar_init(smem_u32(&bars[4]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 4) {
+  if (warp == 8) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
                  "r"((uint32_t)Cfg::TMEM_COLS)
@@ -245,29 +298,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
   const uint32_t tmem = *tmem_slot;
 
   bool ok = true;
-  if (warp < 4) {
-    // ---------------- producers ----------------
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int s = kb % kStages;
-      const uint32_t ph = (uint32_t)(kb / kStages) & 1u;
+  if (warp < 8) {
+    // ---------------- producers: register prefetch one stage ahead ----------------
+    Staging<BNC, A64, B64> st;
+    if (nkb > 0) st.load(p, bz, m0, n0, (int64_t)kb_lo * 16);
+    for (int it = 0; it < nkb; ++it) {
+      const int s = it % kStages;
+      const uint32_t ph = (uint32_t)(it / kStages) & 1u;
       if (!mbar_wait(smem_u32(&bars[kStages + s]), ph ^ 1u)) { ok = false; break; }
-      unsigned char* st = smem + s * Cfg::STAGE;
-      const uint32_t a_hi = smem_u32(st), a_lo = a_hi + Cfg::A_PLANE;
+      unsigned char* sp = smem + s * Cfg::STAGE;
+      const uint32_t a_hi = smem_u32(sp), a_lo = a_hi + Cfg::A_PLANE;
       const uint32_t b_hi = a_lo + Cfg::A_PLANE, b_lo = b_hi + Cfg::B_PLANE;
-      stage_tile<BNC, A64, B64>(p, bz, m0, n0, (int64_t)kb * 16, a_hi, a_lo, b_hi, b_lo);
+      st.store(p, a_hi, a_lo, b_hi, b_lo);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(smem_u32(&bars[s]));
+      if (it + 1 < nkb) st.load(p, bz, m0, n0, (int64_t)(kb_lo + it + 1) * 16);
     }
-    // ---------------- epilogue ----------------
-    if (ok && mbar_wait(smem_u32(&bars[4]), 0u)) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int r = warp * 32 + lane;
-      const int64_t m = m0 + r;
-      float2* crow = p.C + bz * p.sC + m * p.ldc;
-      const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    // ---------------- epilogue: TMEM -> registers -> smem -> coalesced rows ----------------
+    const int q = warp & 3, h = warp >> 2;  // TMEM lane quadrant, column half
+    float* buf = reinterpret_cast<float*>(smem) + warp * 32 * Cfg::EPI_PITCH;
+    bool have = false;
+    if (ok && nkb > 0) {
+      have = mbar_wait(smem_u32(&bars[4]), 0u);
+      if (have) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    // all producers must be past their last smem stage before it is reused
+    asm volatile("bar.sync 1, %0;" ::"r"(kProducers) : "memory");
+    const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * (Cfg::NR / 2));
 #pragma unroll 1
-      for (int j = 0; j < Cfg::NR / 32; ++j) {
-        uint32_t v[32];
+    for (int j = 0; j < Cfg::NR / 64; ++j) {
+      uint32_t v[32];
+      if (have) {
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
             "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
@@ -280,29 +341,40 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
               "=r"(v[31])
             : "r"(trow + (uint32_t)(j * 32)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (m < p.M) {
-          const int64_t nb0 = n0 + j * 16;
-          const bool vec = ((((uintptr_t)(crow + nb0)) & 15) == 0) && (nb0 + 16 <= p.N);
-          if (vec) {
-            float4* dst = reinterpret_cast<float4*>(crow + nb0);
+      } else {
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-              dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
-                                   __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
-          } else {
+        for (int x = 0; x < 32; ++x) v[x] = 0u;
+      }
+      float4* dst = reinterpret_cast<float4*>(buf + lane * Cfg::EPI_PITCH + j * 32);
 #pragma unroll
-            for (int q = 0; q < 16; ++q)
-              if (nb0 + q < p.N)
-                crow[nb0 + q] = make_float2(__uint_as_float(v[2 * q]), __uint_as_float(v[2 * q + 1]));
-          }
+      for (int x = 0; x < 8; ++x)
+        dst[x] = make_float4(__uint_as_float(v[4 * x]), __uint_as_float(v[4 * x + 1]),
+                             __uint_as_float(v[4 * x + 2]), __uint_as_float(v[4 * x + 3]));
+    }
+    __syncwarp();
+    // warp writes its 32 rows; each row half is BNC/2 complex = BNC floats
+    const int64_t nh = n0 + h * (BNC / 2);
+    for (int rr = 0; rr < 32; ++rr) {
+      const int64_t m = m0 + q * 32 + rr;
+      if (m >= p.M) break;
+      float2* crow = p.C + bz * p.sC + m * p.ldc + nh;
+      const float* src = buf + rr * Cfg::EPI_PITCH;
+      for (int x = lane * 4; x < BNC; x += 128) {
+        const int64_t n = nh + x / 2;
+        const float4 val = *reinterpret_cast<const float4*>(src + x);
+        if (n + 1 < p.N && ((reinterpret_cast<uintptr_t>(crow + x / 2) & 15) == 0)) {
+          *reinterpret_cast<float4*>(crow + x / 2) = val;
+        } else {
+          if (n < p.N) crow[x / 2] = make_float2(val.x, val.y);
+          if (n + 1 < p.N) crow[x / 2 + 1] = make_float2(val.z, val.w);
         }
       }
     }
   } else if (lane == 0) {
-    // ---------------- MMA issuer (warp 4, one lane) ----------------
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int s = kb % kStages;
-      const uint32_t ph = (uint32_t)(kb / kStages) & 1u;
+    // ---------------- MMA issuer (warp 8, one lane) ----------------
+    for (int it = 0; it < nkb; ++it) {
+      const int s = it % kStages;
+      const uint32_t ph = (uint32_t)(it / kStages) & 1u;
       if (!mbar_wait(smem_u32(&bars[s]), ph)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a_hi = smem_u32(smem + s * Cfg::STAGE), a_lo = a_hi + Cfg::A_PLANE;
@@ -312,18 +384,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
         const uint32_t o = (uint32_t)kk * 32;  // 8 tf32 = 32 bytes along K
         const uint64_t ah = make_desc(a_hi + o), al = make_desc(a_lo + o);
         const uint64_t bh = make_desc(b_hi + o), bl = make_desc(b_lo + o);
-        const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+        const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
         mma_tf32(tmem, al, bh, Cfg::IDESC, acc);
         mma_tf32(tmem, ah, bl, Cfg::IDESC, 1u);
         mma_tf32(tmem, ah, bh, Cfg::IDESC, 1u);
       }
       mma_commit(smem_u32(&bars[kStages + s]));  // frees the stage once these MMAs retire
     }
-    if (ok) mma_commit(smem_u32(&bars[4]));
+    if (ok && nkb > 0) mma_commit(smem_u32(&bars[4]));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 4) {
+  if (warp == 8) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"((uint32_t)Cfg::TMEM_COLS)
@@ -345,8 +417,14 @@ void launch_tc(const TcParams& p, int64_t batch, cudaStream_t s) {
   for (int64_t b0 = 0; b0 < batch; b0 += 65535) {
     TcParams q = p;
     const int64_t nb = std::min<int64_t>(65535, batch - b0);
-    q.A = (const unsigned char*)p.A + b0 * p.sA * (p.a64 ? 16 : 8);
-    q.Bt = (const unsigned char*)p.Bt + b0 * p.sB * (p.b64 ? 16 : 8);
+    if (p.a_mod)
+      q.a_q0 = (p.a_q0 + b0) % p.a_mod;
+    else
+      q.A = (const unsigned char*)p.A + b0 * p.sA * (p.a64 ? 16 : 8);  // split = 16 B
+    if (p.b_mod)
+      q.b_q0 = (p.b_q0 + b0) % p.b_mod;
+    else
+      q.Bt = (const unsigned char*)p.Bt + b0 * p.sB * (p.b64 ? 16 : 8);
     q.C = p.C + b0 * p.sC;
     dim3 grid((unsigned)((p.N + BNC - 1) / BNC), (unsigned)((p.M + kBM - 1) / kBM), (unsigned)nb);
     fn<<<grid, kThreads, Cfg::SMEM, s>>>(q);
@@ -367,9 +445,11 @@ void dispatch_n(const TcParams& p, int64_t batch, cudaStream_t s) {
 
 }  // namespace
 
-void tc_cgemm_nt(const void* A, bool a_c128, bool conj_a, int64_t lda, int64_t sA, const void* Bt,
-                 bool b_c128, bool conj_b, int64_t ldb, int64_t sB, float2* C, int64_t ldc,
-                 int64_t sC, int64_t M, int64_t N, int64_t K, int64_t batch, cudaStream_t s) {
+void tc_cgemm_nt(const void* A, bool a_split, bool conj_a, int64_t lda, int64_t sA, const void* Bt,
+                 bool b_split, bool conj_b, int64_t ldb, int64_t sB, float2* C, int64_t ldc,
+                 int64_t sC, int64_t M, int64_t N, int64_t K, int64_t batch, cudaStream_t s,
+                 const TcStructure& st) {
+  const bool a_c128 = a_split, b_c128 = b_split;
   CQ_REQUIRE(M > 0 && N > 0 && K > 0 && batch > 0, COQUI_B200_EINVAL, "tc_cgemm: empty problem");
   TcParams p;
   p.A = A;
@@ -388,6 +468,15 @@ void tc_cgemm_nt(const void* A, bool a_c128, bool conj_a, int64_t lda, int64_t s
   p.b64 = b_c128;
   p.conj_a = conj_a;
   p.conj_b = conj_b;
+  p.a_upper = st.a_upper;
+  p.a_lower = st.a_lower;
+  p.b_lower = st.b_lower;
+  p.b_upper = st.b_upper;
+  p.lower_only = st.lower_only;
+  p.a_mod = st.a_mod;
+  p.a_q0 = st.a_q0;
+  p.b_mod = st.b_mod;
+  p.b_q0 = st.b_q0;
   if (a_c128 && b_c128) dispatch_n<true, true>(p, batch, s);
   else if (a_c128) dispatch_n<true, false>(p, batch, s);
   else if (b_c128) dispatch_n<false, true>(p, batch, s);
@@ -402,17 +491,52 @@ int tc_take_error() {
 }
 
 // ---------------------------------------------------------------------------------------
-// projections
+// operand preparation and projections
 // ---------------------------------------------------------------------------------------
-__global__ void k_transpose_X(const double2* __restrict__ X, double2* __restrict__ XT, int64_t Np,
-                              int64_t nb, int64_t nk) {
-  const int64_t total = nk * Np * nb;
+// out (float4 per complex: hi.re, hi.im, lo.re, lo.im) from complex128; if transpose, the
+// (rows x cols) blocks are written transposed (cols x rows).
+__global__ void k_to_split(const double2* __restrict__ in, float4* __restrict__ out, int64_t rows,
+                           int64_t cols, int64_t total, int transpose) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t k = i / (Np * nb), e = i % (Np * nb);
-    const int64_t P = e / nb, a = e % nb;
-    XT[k * Np * nb + a * Np + P] = X[i];
+    const double2 x = in[i];
+    uint32_t hr, lr, hi, li;
+    split2(x.x, hr, lr);
+    split2(x.y, hi, li);
+    int64_t o = i;
+    if (transpose) {
+      const int64_t b = i / (rows * cols), e = i % (rows * cols);
+      o = b * rows * cols + (e % cols) * rows + e / cols;
+    }
+    out[o] = make_float4(__uint_as_float(hr), __uint_as_float(hi), __uint_as_float(lr),
+                         __uint_as_float(li));
   }
+}
+
+// out[b] = in[b]^T as complex64, (rows x cols) blocks of complex128
+__global__ void k_transpose_c64(const double2* __restrict__ in, float2* __restrict__ out,
+                                int64_t rows, int64_t cols, int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / (rows * cols), e = i % (rows * cols);
+    const double2 x = in[i];
+    out[b * rows * cols + (e % cols) * rows + e / cols] = make_float2((float)x.x, (float)x.y);
+  }
+}
+
+__global__ void k_c64_to_c128(const float2* __restrict__ in, double2* __restrict__ out,
+                              int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = make_double2(in[i].x, in[i].y);
+}
+
+void to_split(const double2* in, float4* out, int64_t rows, int64_t cols, int64_t batch,
+              bool transpose, cudaStream_t s) {
+  const int64_t total = rows * cols * batch;
+  k_to_split<<<grid_for(total, 256), 256, 0, s>>>(in, out, rows, cols, total, transpose ? 1 : 0);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
 }
 
 void tc_pack_X(TcOperand& op, const double2* X, int64_t nk, int64_t Np, int64_t nb,
@@ -421,45 +545,45 @@ void tc_pack_X(TcOperand& op, const double2* X, int64_t nk, int64_t Np, int64_t 
   op.nk = nk;
   op.Np = Np;
   op.nb = nb;
-  op.packed.ensure((size_t)nk * Np * nb * sizeof(double2));
-  k_transpose_X<<<grid_for(nk * Np * nb, 256), 256, 0, s>>>(X, (double2*)op.packed.p, Np, nb, nk);
-  count_launch();
-  CQ_CHECK_CUDA(cudaGetLastError());
+  op.packed.ensure((size_t)nk * Np * nb * sizeof(float4) * 2);
+  float4* Xs = (float4*)op.packed.p;
+  to_split(X, Xs, Np, nb, nk, false, s);                 // X   (nk, Np, nb)
+  to_split(X, Xs + nk * Np * nb, Np, nb, nk, true, s);   // X^T (nk, nb, Np)
 }
 
 void tc_project_p2a(TcOperand& op, const double2* Gk, float2* out, int64_t nk, int64_t Np,
                     int64_t nb, cudaStream_t s) {
-  op.tmp.ensure((size_t)nk * Np * nb * sizeof(float2));
+  const float4* Xs = (const float4*)op.packed.p;
+  op.tmp.ensure((size_t)nk * Np * nb * sizeof(float2) + (size_t)nk * nb * nb * sizeof(float2));
   float2* T = (float2*)op.tmp.p;
-  // T = X G  (Np x nb, K = nb) on CUDA cores (small)
-  GemmDesc d{};
-  d.M = Np; d.N = nb; d.K = nb;
-  d.sam = nb; d.sak = 1; d.sbk = nb; d.sbn = 1;
-  d.scm = nb; d.scn = 1;
-  d.batch = nk; d.bsa = Np * nb; d.bsb = nb * nb; d.bsc = Np * nb;
-  d.alpha = make_double2(1, 0); d.beta = make_double2(0, 0);
-  launch_gemm_simt<double2, double2, float2, float>(d, op.X, Gk, T, s);
-  // out = T X^H: B(k=b, n=Q) = conj(X[Q][b]) -> Bt = X with conjugation (tensor cores)
-  tc_cgemm_nt(T, false, false, nb, Np * nb, op.X, true, true, nb, Np * nb, out, Np, Np * Np, Np,
+  float2* Gt = T + nk * Np * nb;
+  const int64_t tg = nk * nb * nb;
+  k_transpose_c64<<<grid_for(tg, 256), 256, 0, s>>>(Gk, Gt, nb, nb, tg);
+  count_launch();
+  // T = X G  (Np x nb, K = nb): Bt[j][i] = G[i][j]
+  tc_cgemm_nt(Xs, true, false, nb, Np * nb, Gt, false, false, nb, nb * nb, T, nb, Np * nb, Np,
+              nb, nb, nk, s);
+  // out = T X^H: B(k=b, n=Q) = conj(X[Q][b])
+  tc_cgemm_nt(T, false, false, nb, Np * nb, Xs, true, true, nb, Np * nb, out, Np, Np * Np, Np,
               Np, nb, nk, s);
 }
 
 void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, int64_t Np,
                     int64_t nb, cudaStream_t s) {
-  op.tmp.ensure((size_t)nk * Np * nb * sizeof(float2));
-  float2* U = (float2*)op.tmp.p;
-  // U = S X  (Np x nb, K = Np): Bt = X^T (nb x Np), tensor cores
-  tc_cgemm_nt(Sk, false, false, Np, Np * Np, op.packed.p, true, false, Np, Np * nb, U, nb,
-              Np * nb, Np, nb, Np, nk, s);
-  // out = X^H U  (nb x nb, K = Np) on CUDA cores (small)
-  GemmDesc e{};
-  e.M = nb; e.N = nb; e.K = Np;
-  e.sam = 1; e.sak = nb; e.conj_a = true;  // A(a, P) = conj(X[P][a])
-  e.sbk = nb; e.sbn = 1;
-  e.scm = nb; e.scn = 1;
-  e.batch = nk; e.bsa = Np * nb; e.bsb = Np * nb; e.bsc = nb * nb;
-  e.alpha = make_double2(1, 0); e.beta = make_double2(0, 0);
-  launch_gemm_simt<double2, float2, double2, double>(e, op.X, U, out, s);
+  const float4* XTs = (const float4*)op.packed.p + nk * Np * nb;
+  op.tmp.ensure((size_t)nk * Np * nb * sizeof(float2) + (size_t)nk * nb * nb * sizeof(float2));
+  float2* UT = (float2*)op.tmp.p;
+  float2* Sab = UT + nk * Np * nb;
+  // U^T = X^T S^T (nb x Np, K = Np): A = X^T, Bt = S
+  tc_cgemm_nt(XTs, true, false, Np, nb * Np, Sk, false, false, Np, Np * Np, UT, Np, nb * Np, nb,
+              Np, Np, nk, s);
+  // Sigma_ab = X^H U (nb x nb, K = Np): A(a, P) = conj(X^T[a][P]), Bt = U^T
+  tc_cgemm_nt(XTs, true, true, Np, nb * Np, UT, false, false, Np, nb * Np, Sab, nb, nb * nb, nb,
+              nb, Np, nk, s);
+  const int64_t t = nk * nb * nb;
+  k_c64_to_c128<<<grid_for(t, 256), 256, 0, s>>>(Sab, out, t);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
 }
 
 }  // namespace cq

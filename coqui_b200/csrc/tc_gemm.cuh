@@ -9,8 +9,8 @@ namespace cq {
 struct TcOperand {
   const double2* X = nullptr;
   int64_t nk = 0, Np = 0, nb = 0;
-  DevBuf<unsigned char> packed;  // X^T per k (nk, nb, Np), complex128
-  DevBuf<unsigned char> tmp;     // per-call intermediate (X G or S X)
+  DevBuf<unsigned char> packed;  // pre-split X (nk, Np, nb) then X^T (nk, nb, Np)
+  DevBuf<unsigned char> tmp;     // per-call intermediates
   void release() {
     packed.release();
     tmp.release();
@@ -28,14 +28,32 @@ void tc_project_p2a(TcOperand& op, const double2* Gk, float2* out, int64_t nk, i
 void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, int64_t Np,
                     int64_t nb, cudaStream_t s);
 
+// Pre-split operand format: one float4 (hi.re, hi.im, lo.re, lo.im) per complex value with
+// hi = rna_tf32(x), lo = rna_tf32(x - hi); built once for operands used by many GEMMs.
+// in: nbatch blocks of (rows x cols) complex128; transpose writes each block transposed.
+void to_split(const double2* in, float4* out, int64_t rows, int64_t cols, int64_t batch,
+              bool transpose, cudaStream_t s);
+
 // Split-TF32 tensor-core GEMM, "NT" form:
 //   C[b](m, n) = sum_k opA(A[b])(m, k) * opB(Bt[b])(n, k)
-// A: row-major M x K (lda), Bt: row-major N x K (ldb), each complex64 or complex128
-// (the *_c128 flags) and optionally conjugated; C: row-major complex64 (ldc).  Strides in
+// A: row-major M x K (lda), Bt: row-major N x K (ldb), each complex64 or pre-split (the
+// *_split flags) and optionally conjugated; C: row-major complex64 (ldc).  Strides in
 // complex elements; sA/sB/sC are the batch strides.
-void tc_cgemm_nt(const void* A, bool a_c128, bool conj_a, int64_t lda, int64_t sA, const void* Bt,
-                 bool b_c128, bool conj_b, int64_t ldb, int64_t sB, float2* C, int64_t ldc,
-                 int64_t sC, int64_t M, int64_t N, int64_t K, int64_t batch, cudaStream_t s);
+// Known zero structure lets a tile skip K blocks (and whole tiles):
+//   a_upper: A(m, k) = 0 for k < m      a_lower: A(m, k) = 0 for k > m
+//   b_lower: B(k, n) = 0 for k < n      b_upper: B(k, n) = 0 for k > n
+//   lower_only: only tiles touching the lower triangle (m >= n) are written.
+// a_mod / b_mod (> 0): the operand's batch index is (q0 + b) % mod (per-q operands shared
+// by every frequency of a flattened (w, q) batch).
+struct TcStructure {
+  bool a_upper = false, a_lower = false, b_lower = false, b_upper = false, lower_only = false;
+  int64_t a_mod = 0, a_q0 = 0, b_mod = 0, b_q0 = 0;
+};
+
+void tc_cgemm_nt(const void* A, bool a_split, bool conj_a, int64_t lda, int64_t sA, const void* Bt,
+                 bool b_split, bool conj_b, int64_t ldb, int64_t sB, float2* C, int64_t ldc,
+                 int64_t sC, int64_t M, int64_t N, int64_t K, int64_t batch, cudaStream_t s,
+                 const TcStructure& st = TcStructure{});
 
 // Returns (and clears) the device flag set when a bounded wait inside a tensor-core kernel
 // gave up (nonzero = a kernel timed out).
