@@ -27,7 +27,7 @@ SYMBOLS = [
     "coqui_b200_primary_to_aux", "coqui_b200_aux_to_primary", "coqui_b200_tau_to_w",
     "coqui_b200_w_to_tau", "coqui_b200_dyson_w", "coqui_b200_last_timings",
     "coqui_b200_kernel_launches", "coqui_b200_gw_iteration", "coqui_b200_set_profiling",
-    "coqui_b200_kernel_stats",
+    "coqui_b200_kernel_stats", "coqui_b200_primary_to_aux_noalloc",
 ]
 
 
@@ -78,6 +78,9 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_gw_iteration.argtypes = [P, P, P, P]
     lib.coqui_b200_set_profiling.argtypes = [P, ctypes.c_int]
     lib.coqui_b200_kernel_stats.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, P, ctypes.c_int]
+    lib.coqui_b200_primary_to_aux_noalloc.argtypes = [P, P, P, ctypes.c_int64, ctypes.c_int64,
+                                                      ctypes.c_int64, P, ctypes.c_char_p,
+                                                      ctypes.c_int]
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -263,6 +266,19 @@ class Context:
 
     def kernel_launches(self) -> int:
         return int(self.lib.coqui_b200_kernel_launches(self.h))
+
+
+def primary_to_aux_noalloc(X_ptr, G_ptr, out_ptr, nk, Np, nb, stream=None):
+    """Projection O = X G X^H on device buffers the caller owns, with no device allocation.
+
+    X_ptr (complex128 (nk, Np, nb)), G_ptr (complex128 (nk, nb, nb)) and out_ptr
+    (complex64 (nk, Np, Np)) are device addresses (ints).  For callers that must not
+    allocate device memory; intermediates use the library's fixed 32 MiB device array."""
+    lib = load()
+    err = ctypes.create_string_buffer(256)
+    rc = lib.coqui_b200_primary_to_aux_noalloc(X_ptr, G_ptr, out_ptr, nk, Np, nb, stream, err, 256)
+    if rc != OK:
+        raise CoquiB200Error(rc, err.value.decode())
 
 
 def version() -> str:

@@ -144,6 +144,23 @@ COQUI_B200_API int coqui_b200_kernel_stats(const coqui_b200_ctx* ctx, char* name
 /* Number of kernels this library launched since the context was created. */
 COQUI_B200_API int64_t coqui_b200_kernel_launches(const coqui_b200_ctx* ctx);
 
+/* Allocation-free primary -> auxiliary projection O^k_PQ = X^k G^k X^k^H for callers that
+   own their device buffers but must not allocate device memory (an application with its
+   own memory pool or a fixed device-memory budget, or code that cannot afford the device
+   synchronisation cudaMalloc/cudaFree imply).  It has no counterpart in the reference: it is
+   an extra entry into the same tensor-core projection that coqui_b200_primary_to_aux runs.
+   X_skPa: device complex128 (nk, Np, nb); O_skab: device complex128 (nk, nb, nb);
+   O_skPQ: device complex64 (nk, Np, Np), written.  Runs on `stream` (a cudaStream_t, NULL =
+   default stream) and returns after the work finished.  All intermediates live in one
+   static 32 MiB device array: larger problems are rejected with COQUI_B200_EINVAL and a
+   message in errbuf (may be NULL).  Every device that loads the library keeps that array
+   until exit; calls share it, so calls that overlap on the GPU race.  The first call on a
+   device looks up the array's address; make it before any stream capture. */
+COQUI_B200_API int coqui_b200_primary_to_aux_noalloc(const double* X_skPa, const double* O_skab,
+                                                     float* O_skPQ, int64_t nk, int64_t Np,
+                                                     int64_t nb, void* stream, char* errbuf,
+                                                     int errlen);
+
 #ifdef __cplusplus
 }
 #endif
