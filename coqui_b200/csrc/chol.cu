@@ -4,11 +4,14 @@
 //   A = C C^H (C lower, FP64), logdet = 2 sum_i ln C_ii, trace = sum_i M_ii,
 //   optional DH = C^{-H} - I (upper triangular, FP64) for W = L (D + D^H + D^H D) L^H.
 //
-// Right-looking blocked algorithm with 64 x 64 blocks: the diagonal block is factored and
+// Right-looking blocked algorithm with 32 x 32 blocks: the diagonal block is factored and
 // inverted in shared memory, the panel below is L_ib = A_ib C_jj^{-H}, the trailing lower
 // triangle gets A_ik -= L_ij L_kj^H.  The inverse is formed block column by block column:
 // X_ij = -C_ii^{-1} sum_{k=j}^{i-1} C_ik X_kj.  Block products use 4 x 4 register tiles per
-// thread (256 threads per 64 x 64 output), operands staged in shared memory.
+// thread (64 threads per 32 x 32 output), operands staged in shared memory; ~50 KB of
+// shared memory per problem lets four problems share an SM so that one problem's barriers
+// and loads overlap another's FP64 arithmetic.  A = I - M is set up and D^H written out by
+// separate element-wise kernels.
 #include <cstdint>
 
 #include "chol.cuh"
@@ -17,8 +20,9 @@ namespace cq {
 
 namespace {
 
-constexpr int CB = 64;       // block size
-constexpr int CT = 256;      // threads per CTA
+constexpr int CB = 32;       // block size
+constexpr int CT = 64;       // threads per CTA
+constexpr int TW = 8;        // thread grid edge: (TW x TW) threads x (4 x 4) outputs = CB x CB
 constexpr int PITCH = CB + 1;  // smem row pitch (double2 elements)
 
 __device__ __forceinline__ double2 cmul_(double2 a, double2 b) {
@@ -101,19 +105,19 @@ __device__ __forceinline__ void store_blk(const double2* S, double2* G, int64_t 
   }
 }
 
-// acc[i][j] (rows ty + 16 i, cols tx + 16 j) += sum_k X[r][k] * Y'[k][c] over k < K, where
+// acc[i][j] (rows ty + TW i, cols tx + TW j) += sum_k X[r][k] * Y'[k][c] over k < K, where
 // Y'(k, c) = conj(Y[c][k]) if ADJ_Y (product with Y^H) else Y[k][c].
 template <bool ADJ_Y>
 __device__ __forceinline__ void mma_tile(const double2* X, const double2* Y, int K,
                                          double2 (&acc)[4][4]) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
   for (int k = 0; k < K; ++k) {
     double2 a[4], b[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = X[(ty + 16 * i) * PITCH + k];
+    for (int i = 0; i < 4; ++i) a[i] = X[(ty + TW * i) * PITCH + k];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-      b[j] = ADJ_Y ? conj_(Y[(tx + 16 * j) * PITCH + k]) : Y[k * PITCH + tx + 16 * j];
+      b[j] = ADJ_Y ? conj_(Y[(tx + TW * j) * PITCH + k]) : Y[k * PITCH + tx + TW * j];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -127,13 +131,13 @@ __device__ __forceinline__ void mma_tile(const double2* X, const double2* Y, int
 // acc[i][j] -= sum_k X[r][k] conj(Y[c][k])  (A - X Y^H)
 __device__ __forceinline__ void mma_tile_sub(const double2* X, const double2* Y, int K,
                                              double2 (&acc)[4][4]) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
   for (int k = 0; k < K; ++k) {
     double2 a[4], b[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = X[(ty + 16 * i) * PITCH + k];
+    for (int i = 0; i < 4; ++i) a[i] = X[(ty + TW * i) * PITCH + k];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) b[j] = Y[(tx + 16 * j) * PITCH + k];
+    for (int j = 0; j < 4; ++j) b[j] = Y[(tx + TW * j) * PITCH + k];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -193,26 +197,24 @@ __device__ void factor_diag(double2* S, int n, double* ld_acc, int* bad) {
 }
 
 // Sinv = inverse of the lower-triangular S (n x n): forward substitution with one column
-// per group of 4 lanes (partial dot products reduced by shuffles).
+// per pair of lanes (partial dot products reduced by a shuffle).
 __device__ void invert_lower(const double2* S, double2* Sinv, int n) {
   for (int i = threadIdx.x; i < CB * CB; i += CT) Sinv[(i / CB) * PITCH + i % CB] = make_double2(0, 0);
   __syncthreads();
-  const int c = threadIdx.x >> 2, sub = threadIdx.x & 3;
+  const int c = threadIdx.x >> 1, sub = threadIdx.x & 1;
   const bool col = c < n;
   if (col && sub == 0) Sinv[c * PITCH + c] = make_double2(1.0 / S[c * PITCH + c].x, 0.0);
   __syncwarp();
   for (int r = 1; r < n; ++r) {
     double ax = 0, ay = 0;
     if (col && r > c)
-      for (int k = c + sub; k < r; k += 4) {
+      for (int k = c + sub; k < r; k += 2) {
         const double2 u = cmul_(S[r * PITCH + k], Sinv[k * PITCH + c]);
         ax += u.x;
         ay += u.y;
       }
     ax += __shfl_xor_sync(0xffffffffu, ax, 1);
     ay += __shfl_xor_sync(0xffffffffu, ay, 1);
-    ax += __shfl_xor_sync(0xffffffffu, ax, 2);
-    ay += __shfl_xor_sync(0xffffffffu, ay, 2);
     if (col && r > c && sub == 0) {
       const double inv = -1.0 / S[r * PITCH + r].x;
       Sinv[r * PITCH + c] = make_double2(ax * inv, ay * inv);
@@ -223,8 +225,8 @@ __device__ void invert_lower(const double2* S, double2* Sinv, int n) {
 }
 
 template <bool INV>
-__global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ Mall,
-                                                    double2* __restrict__ Aall, float2* Zall,
+__global__ void __launch_bounds__(CT, 4) k_chol_inv(const float2* __restrict__ Mall,
+                                                    double2* __restrict__ Aall,
                                                     double* __restrict__ logdet,
                                                     double2* __restrict__ trace,
                                                     int* __restrict__ info, int64_t n) {
@@ -238,37 +240,19 @@ __global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ M
   const int64_t p = blockIdx.x;
   const float2* M = Mall + p * n * n;
   double2* A = Aall + p * n * n;
-  float2* Z = INV ? Zall + p * n * n : nullptr;
   const int nblk = (int)((n + CB - 1) / CB);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
 
   if (threadIdx.x == 0) {
     s_ld = 0.0;
     s_bad = 0;
   }
-  // A = I - M on the lower triangle (FP64), trace of M
+  // trace of M (A = I - M was set up by k_chol_prep)
   double tr = 0, ti = 0;
-  for (int64_t i0 = 0; i0 < n * n; i0 += 8 * CT) {
-    float2 m[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int64_t i = i0 + threadIdx.x + u * CT;
-      m[u] = (i < n * n && (i % n) <= (i / n)) ? M[i] : make_float2(0.f, 0.f);
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int64_t i = i0 + threadIdx.x + u * CT;
-      if (i < n * n) {
-        const int64_t r = i / n, c = i % n;
-        if (c <= r) {
-          A[i] = make_double2((r == c ? 1.0 : 0.0) - (double)m[u].x, -(double)m[u].y);
-          if (r == c) {
-            tr += m[u].x;
-            ti += m[u].y;
-          }
-        }
-      }
-    }
+  for (int64_t i = threadIdx.x; i < n; i += CT) {
+    const float2 m = M[i * n + i];
+    tr += m.x;
+    ti += m.y;
   }
   s_red[0][threadIdx.x] = tr;
   s_red[1][threadIdx.x] = ti;
@@ -299,7 +283,7 @@ __global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ M
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
-          const int r = ty + 16 * i, c = tx + 16 * jj;
+          const int r = ty + TW * i, c = tx + TW * jj;
           if (r < rb && c < jb) A[(i0 + r) * n + j0 + c] = acc[i][jj];
         }
       __syncthreads();
@@ -319,7 +303,7 @@ __global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ M
         for (int i = 0; i < 4; ++i)  // start from the current A block (loads in flight early)
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) {
-            const int r = ty + 16 * i, c = tx + 16 * jj;
+            const int r = ty + TW * i, c = tx + TW * jj;
             acc[i][jj] = (r < rb && c < kbsz && (ib > kb || c <= r)) ? A[(i0 + r) * n + k0 + c]
                                                                       : make_double2(0, 0);
           }
@@ -328,7 +312,7 @@ __global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ M
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) {
-            const int r = ty + 16 * i, c = tx + 16 * jj;
+            const int r = ty + TW * i, c = tx + TW * jj;
             if (r < rb && c < kbsz && (ib > kb || c <= r)) A[(i0 + r) * n + k0 + c] = acc[i][jj];
           }
         __syncthreads();
@@ -362,7 +346,7 @@ __global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ M
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) S2[(ty + 16 * i) * PITCH + tx + 16 * jj] = acc[i][jj];
+          for (int jj = 0; jj < 4; ++jj) S2[(ty + TW * i) * PITCH + tx + TW * jj] = acc[i][jj];
         load_blk_adjU(S0, A, n, i0, rb);  // C_ii^{-1}
         __syncthreads();
         zero_acc(acc);
@@ -373,27 +357,10 @@ __global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ M
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int jj = 0; jj < 4; ++jj) {
-            const int r = ty + 16 * i, c = tx + 16 * jj;
+            const int r = ty + TW * i, c = tx + TW * jj;
             if (r < rb && c < jb) A[(j0 + c) * n + i0 + r] = make_double2(-acc[i][jj].x, acc[i][jj].y);
           }
         __syncthreads();
-      }
-    }
-    // Z = X^H - I (upper, complex64), zero below the diagonal
-    for (int64_t i0 = 0; i0 < n * n; i0 += 8 * CT) {
-      double2 v[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int64_t i = i0 + threadIdx.x + u * CT;
-        v[u] = (i < n * n && (i % n) >= (i / n)) ? A[i] : make_double2(0, 0);
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int64_t i = i0 + threadIdx.x + u * CT;
-        if (i < n * n) {
-          if ((i % n) == (i / n)) v[u].x -= 1.0;
-          Z[i] = make_float2((float)v[u].x, (float)v[u].y);
-        }
       }
     }
   }
@@ -413,11 +380,43 @@ __global__ void __launch_bounds__(CT, 1) k_chol_inv(const float2* __restrict__ M
   }
 }
 
+// A = I - M on the lower triangle of every problem (FP64)
+__global__ void k_chol_prep(const float2* __restrict__ M, double2* __restrict__ A, int64_t n,
+                            int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = i % (n * n), r = e / n, c = e % n;
+    if (c <= r) {
+      const float2 m = M[i];
+      A[i] = make_double2((r == c ? 1.0 : 0.0) - (double)m.x, -(double)m.y);
+    }
+  }
+}
+
+// Z = X^H - I from the upper triangle of A (complex64), zero below the diagonal
+__global__ void k_chol_final(const double2* __restrict__ A, float2* __restrict__ Z, int64_t n,
+                             int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = i % (n * n), r = e / n, c = e % n;
+    float2 z = make_float2(0.f, 0.f);
+    if (c >= r) {
+      const double2 a = A[i];
+      z = make_float2((float)(a.x - (r == c ? 1.0 : 0.0)), (float)a.y);
+    }
+    Z[i] = z;
+  }
+}
+
 }  // namespace
 
 void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, double2* trace,
                      int* info, int64_t Np, int64_t nprob, cudaStream_t s) {
   const size_t smem = (size_t)3 * CB * PITCH * sizeof(double2);
+  const int64_t total = Np * Np * nprob;
+  k_chol_prep<<<grid_for(total, 256), 256, 0, s>>>(M, A, Np, total);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
   if (Z) {
     static bool set = false;
     if (!set) {
@@ -425,7 +424,10 @@ void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, dou
                                          (int)smem));
       set = true;
     }
-    k_chol_inv<true><<<(unsigned)nprob, CT, smem, s>>>(M, A, Z, logdet, trace, info, Np);
+    k_chol_inv<true><<<(unsigned)nprob, CT, smem, s>>>(M, A, logdet, trace, info, Np);
+    count_launch();
+    CQ_CHECK_CUDA(cudaGetLastError());
+    k_chol_final<<<grid_for(total, 256), 256, 0, s>>>(A, Z, Np, total);
   } else {
     static bool set = false;
     if (!set) {
@@ -433,7 +435,7 @@ void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, dou
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       set = true;
     }
-    k_chol_inv<false><<<(unsigned)nprob, CT, smem, s>>>(M, A, Z, logdet, trace, info, Np);
+    k_chol_inv<false><<<(unsigned)nprob, CT, smem, s>>>(M, A, logdet, trace, info, Np);
   }
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());

@@ -73,6 +73,8 @@ struct coqui_b200_ctx {
 
   // device data
   DevBuf<double2> X, V, L, LH, chi, G, Sig, Tproj, stage, dTwt, dTtw;
+  DevBuf<double> dTwtR, dTtwR;  // real parts, used when the PH matrices are real
+  bool ir_real = false;
   DevBuf<double> fac;
   DevBuf<double2> eps;
   DevBuf<unsigned char> Gp, Gn, PW;  // storage precision, bytes
@@ -229,6 +231,14 @@ void eval_pi_device(Ctx* c) {
 void ir_inplace(Ctx* c, int n_in, int n_out, const double2* M) {
   cq::Prof::Scope sc(&c->prof, "ir_transform");
   const int64_t ncol = c->nq * c->Np * c->Np;
+  if (c->ir_real) {
+    const double* Mr = (M == c->dTwt.p) ? c->dTwtR.p : c->dTtwR.p;
+    if (c->mode == COQUI_B200_FP64)
+      cq::launch_ir_transform_real<double>((double2*)c->PW.p, ncol, n_in, n_out, Mr, c->st);
+    else
+      cq::launch_ir_transform_real<float>((float2*)c->PW.p, ncol, n_in, n_out, Mr, c->st);
+    return;
+  }
   if (c->mode == COQUI_B200_FP64)
     cq::launch_ir_transform<double>((double2*)c->PW.p, ncol, n_in, n_out, M, c->st);
   else
@@ -334,6 +344,8 @@ void coqui_b200_destroy(coqui_b200_ctx* c) {
                   &c->dTwt, &c->dTtw, &c->eps})
     b->release();
   c->fac.release();
+  c->dTwtR.release();
+  c->dTtwR.release();
   c->Gp.release();
   c->Gn.release();
   c->PW.release();
@@ -416,6 +428,25 @@ int coqui_b200_set_ir(coqui_b200_ctx* c, const double* Twt_bb, const double* Ttw
     c->dTtw.ensure(c->Ttw_pos.size());
     upload(c, c->dTwt.p, c->Twt_pos.data(), c->Twt_pos.size() * sizeof(double2));
     upload(c, c->dTtw.p, c->Ttw_pos.data(), c->Ttw_pos.size() * sizeof(double2));
+    // The particle-hole symmetric matrices are real up to rounding (|Im| ~ 1e-15 |Re|);
+    // then the transform runs with the real parts only.
+    double re_max = 0, im_max = 0;
+    for (const auto* v : {&c->Twt_pos, &c->Ttw_pos})
+      for (const double2& z : *v) {
+        re_max = std::max(re_max, std::abs(z.x));
+        im_max = std::max(im_max, std::abs(z.y));
+      }
+    c->ir_real = im_max <= 1e-12 * re_max;
+    if (c->ir_real) {
+      std::vector<double> a(c->Twt_pos.size()), b(c->Ttw_pos.size());
+      for (size_t i = 0; i < a.size(); ++i) a[i] = c->Twt_pos[i].x;
+      for (size_t i = 0; i < b.size(); ++i) b[i] = c->Ttw_pos[i].x;
+      c->dTwtR.ensure(a.size());
+      c->dTtwR.ensure(b.size());
+      upload(c, c->dTwtR.p, a.data(), a.size() * sizeof(double));
+      upload(c, c->dTtwR.p, b.data(), b.size() * sizeof(double));
+      CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    }
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->have_ir = true;
   });

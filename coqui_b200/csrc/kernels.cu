@@ -411,6 +411,74 @@ void launch_ir_transform(cplx_t<R>* buf, int64_t ncol, int n_in, int n_out, cons
   CQ_LAUNCHED();
 }
 
+// Real transform matrix (the particle-hole symmetric IR matrices are real): four outputs
+// per pass, 2 FP64 FMAs per (output, input) pair.
+template <typename R, int MAXT>
+__global__ void __launch_bounds__(128) k_ir_transform_real(cplx_t<R>* __restrict__ buf,
+                                                           int64_t ncol, int n_in, int n_out,
+                                                           const double* __restrict__ M) {
+  extern __shared__ double sMr[];
+  for (int i = threadIdx.x; i < n_in * n_out; i += blockDim.x) sMr[i] = M[i];
+  __syncthreads();
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ncol;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    double2 x[MAXT];
+#pragma unroll
+    for (int t = 0; t < MAXT; ++t) {
+      if (t < n_in) {
+        const cplx_t<R> v = buf[(int64_t)t * ncol + e];
+        x[t].x = v.x;
+        x[t].y = v.y;
+      } else {
+        x[t].x = 0;
+        x[t].y = 0;
+      }
+    }
+    for (int n = 0; n < n_out; n += 4) {
+      double acc[4][2] = {};
+      const double* rows[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) rows[q] = sMr + (n + q < n_out ? n + q : n) * n_in;
+#pragma unroll
+      for (int t = 0; t < MAXT; ++t) {
+        if (t < n_in) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const double m = rows[q][t];
+            acc[q][0] = fma(m, x[t].x, acc[q][0]);
+            acc[q][1] = fma(m, x[t].y, acc[q][1]);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (n + q < n_out) {
+          cplx_t<R> o;
+          o.x = (R)acc[q][0];
+          o.y = (R)acc[q][1];
+          buf[(int64_t)(n + q) * ncol + e] = o;
+        }
+    }
+  }
+}
+
+template <typename R>
+void launch_ir_transform_real(cplx_t<R>* buf, int64_t ncol, int n_in, int n_out, const double* M,
+                              cudaStream_t s) {
+  CQ_REQUIRE(n_in >= 1 && n_in <= 96 && n_out >= 1, COQUI_B200_EUNSUPPORTED,
+             "IR transform supports at most 96 input points");
+  const size_t smem = (size_t)n_in * n_out * sizeof(double);
+  const unsigned grid = grid_for(ncol, 128, 148 * 32);
+  if (n_in <= 32) {
+    set_smem((const void*)k_ir_transform_real<R, 32>, smem);
+    k_ir_transform_real<R, 32><<<grid, 128, smem, s>>>(buf, ncol, n_in, n_out, M);
+  } else {
+    set_smem((const void*)k_ir_transform_real<R, 96>, smem);
+    k_ir_transform_real<R, 96><<<grid, 128, smem, s>>>(buf, ncol, n_in, n_out, M);
+  }
+  CQ_LAUNCHED();
+}
+
 // ---------------------------------------------------------------------------------------
 // conversions, layout changes
 // ---------------------------------------------------------------------------------------
@@ -694,6 +762,8 @@ void launch_gemm_simt(const GemmDesc& d, const TA* A, const TB* B, TC* C, cudaSt
                                     cudaStream_t);                                              \
   template void launch_ir_transform<R>(cplx_t<R>*, int64_t, int, int, const double2*,           \
                                        cudaStream_t);                                           \
+  template void launch_ir_transform_real<R>(cplx_t<R>*, int64_t, int, int, const double*,       \
+                                            cudaStream_t);                                      \
   template void launch_from_c128<R>(const double2*, cplx_t<R>*, int64_t, cudaStream_t);         \
   template void launch_to_c128<R>(const cplx_t<R>*, double2*, int64_t, cudaStream_t);           \
   template void launch_eye_minus<R>(const cplx_t<R>*, double2*, int64_t, int64_t, cudaStream_t); \

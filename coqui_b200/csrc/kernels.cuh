@@ -39,6 +39,11 @@ template <typename R>
 void launch_ir_transform(cplx_t<R>* buf, int64_t ncol, int n_in, int n_out, const double2* M,
                          cudaStream_t s);
 
+// Same with a real matrix M (n_out, n_in) (FP64).
+template <typename R>
+void launch_ir_transform_real(cplx_t<R>* buf, int64_t ncol, int n_in, int n_out, const double* M,
+                              cudaStream_t s);
+
 // complex128 -> storage precision (and back) element-wise conversions.
 template <typename R>
 void launch_from_c128(const double2* in, cplx_t<R>* out, int64_t n, cudaStream_t s);
