@@ -257,6 +257,7 @@ def run_ours(args, rank, world, local):
         ctx.gw_iteration(Gh, sigma_out=Sh)
         e2e.append(total_ms(ctx))
     t_e2e = float(np.mean(e2e))
+    e2e_phases = dict(ctx.timings())
 
     # RPA energy time (resident G) and E_c
     ctx.rpa_energy(Gh)
@@ -265,6 +266,7 @@ def run_ours(args, rank, world, local):
         e_c = ctx.rpa_energy(None)
         rpa.append(total_ms(ctx))
     t_rpa = float(np.mean(rpa))
+    rpa_phases = dict(ctx.timings())
 
     fp64 = None
     if not args.no_fp64:
@@ -358,6 +360,8 @@ def run_ours(args, rank, world, local):
         "rpa_energy_ms": t_rpa, "E_c": e_c,
         "fp64_form": fp64,
         "phases_ms": phases,
+        "e2e_phases_ms": e2e_phases,
+        "rpa_phases_ms": rpa_phases,
         "kernel_groups": groups,
         "roofline": roof,
         "cpu_baseline": cpu,

@@ -123,7 +123,14 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
                      4 * sizeof(void*) + sizeof(int) + sizeof(double) + sizeof(double2) + 64;
   // FP64 form: one frequency at a time (cuBLAS strided batches over q); mixed form: chunks of
   // the flattened (w, q) problem list, per-q operands addressed periodically.
-  const size_t budget = (size_t)(a.mixed ? 8 : 4) << 30;
+  // mixed form: as many problems per chunk as ~60% of the free device memory allows, so the
+  // FP64 factorisation kernel sees whole waves of problems (one CTA per problem)
+  size_t budget = (size_t)4 << 30;
+  if (a.mixed) {
+    size_t fr = 0, tot = 0;
+    CQ_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+    budget = std::max(scratch.n, (size_t)(0.6 * (double)(fr + scratch.n)));
+  }
   const int64_t nprob = nw * nq;
   const int64_t nbq = a.mixed ? std::max<int64_t>(1, std::min<int64_t>(nprob, (int64_t)(budget / per)))
                               : std::max<int64_t>(1, std::min<int64_t>(nq, (int64_t)(budget / per)));

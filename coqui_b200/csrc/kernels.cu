@@ -142,6 +142,28 @@ __device__ void dft3(C* A, C* B, int n0, int n1, int n2, int sign) {
   __syncthreads();
 }
 
+// 3D DFT of one or two tiles on an NC x NC x NC grid known at compile time (NC > 0), else
+// the runtime-shaped dft3; constant strides remove the index arithmetic from the loops.
+template <typename C, int TILE, int NC>
+__device__ __forceinline__ void dft3c(C* A, C* B, int n0, int n1, int n2, int sign) {
+  if constexpr (NC == 0) {
+    dft3<C, TILE>(A, B, n0, n1, n2, sign);
+  } else {
+    constexpr int NK = NC * NC * NC;
+    if constexpr (NC > 1) {
+      dft_dim_n<C, TILE, NC>(A, 1, NK, sign);
+      if (B) dft_dim_n<C, TILE, NC>(B, 1, NK, sign);
+      __syncthreads();
+      dft_dim_n<C, TILE, NC>(A, NC, NK, sign);
+      if (B) dft_dim_n<C, TILE, NC>(B, NC, NK, sign);
+      __syncthreads();
+      dft_dim_n<C, TILE, NC>(A, NC * NC, NK, sign);
+      if (B) dft_dim_n<C, TILE, NC>(B, NC * NC, NK, sign);
+    }
+    __syncthreads();
+  }
+}
+
 // Tile loads are issued 8 per thread before the shared-memory stores so that enough
 // requests are in flight to cover DRAM latency.
 template <typename C, int TILE>
@@ -177,13 +199,14 @@ __device__ __forceinline__ void store_tile(const C* A, C* dst, int nk, int64_t n
   }
 }
 
-template <typename R, int TILE>
+template <typename R, int TILE, int NC>
 __global__ void __launch_bounds__(256) k_pi_fused(const cplx_t<R>* __restrict__ Gp,
                                                   const cplx_t<R>* __restrict__ Gn,
                                                   cplx_t<R>* __restrict__ Pi, int64_t ncol,
-                                                  int n0, int n1, int n2, R scale) {
+                                                  int rn0, int rn1, int rn2, R scale) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n0 = NC ? NC : rn0, n1 = NC ? NC : rn1, n2 = NC ? NC : rn2;
   const int nk = n0 * n1 * n2;
   C* A = reinterpret_cast<C*>(smem_raw);
   C* B = A + nk * TILE;
@@ -193,22 +216,23 @@ __global__ void __launch_bounds__(256) k_pi_fused(const cplx_t<R>* __restrict__ 
     load_tile<C, TILE>(A, Gp, nk, ncol, col0);
     load_tile<C, TILE>(B, Gn, nk, ncol, col0);
     __syncthreads();
-    dft3<C, TILE>(A, B, n0, n1, n2, -1);
+    dft3c<C, TILE, NC>(A, B, n0, n1, n2, -1);
     for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) A[i] = cscale(cmulc(A[i], B[i]), scale);
     __syncthreads();
-    dft3<C, TILE>(A, (C*)nullptr, n0, n1, n2, +1);
+    dft3c<C, TILE, NC>(A, (C*)nullptr, n0, n1, n2, +1);
     store_tile<C, TILE>(A, Pi, nk, ncol, col0);
     __syncthreads();
   }
 }
 
-template <typename R, int TILE>
+template <typename R, int TILE, int NC>
 __global__ void __launch_bounds__(256) k_sigma_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gm,
                                                      const cplx_t<R>* __restrict__ WR,
                                                      cplx_t<R>* Sp, cplx_t<R>* Sm, int64_t ncol,
-                                                     int n0, int n1, int n2, R scale) {
+                                                     int rn0, int rn1, int rn2, R scale) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n0 = NC ? NC : rn0, n1 = NC ? NC : rn1, n2 = NC ? NC : rn2;
   const int nk = n0 * n1 * n2;
   C* A = reinterpret_cast<C*>(smem_raw);
   C* B = A + nk * TILE;
@@ -221,26 +245,27 @@ __global__ void __launch_bounds__(256) k_sigma_fused(const cplx_t<R>* Gp, const 
     if (has_m) load_tile<C, TILE>(B, Gm, nk, ncol, col0);
     load_tile<C, TILE>(Wt, WR, nk, ncol, col0);
     __syncthreads();
-    dft3<C, TILE>(A, has_m ? B : (C*)nullptr, n0, n1, n2, -1);
+    dft3c<C, TILE, NC>(A, has_m ? B : (C*)nullptr, n0, n1, n2, -1);
     for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) {
       const C w = cscale(Wt[i], scale);
       A[i] = cmul(A[i], w);
       if (has_m) B[i] = cmul(B[i], w);
     }
     __syncthreads();
-    dft3<C, TILE>(A, has_m ? B : (C*)nullptr, n0, n1, n2, +1);
+    dft3c<C, TILE, NC>(A, has_m ? B : (C*)nullptr, n0, n1, n2, +1);
     store_tile<C, TILE>(A, Sp, nk, ncol, col0);
     if (has_m) store_tile<C, TILE>(B, Sm, nk, ncol, col0);
     __syncthreads();
   }
 }
 
-template <typename R, int TILE>
+template <typename R, int TILE, int NC>
 __global__ void __launch_bounds__(256) k_dft_plain(cplx_t<R>* __restrict__ buf, int64_t ncol,
-                                                   int n0, int n1, int n2, int sign, R scale,
+                                                   int rn0, int rn1, int rn2, int sign, R scale,
                                                    int64_t nbatch, int64_t bstride) {
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n0 = NC ? NC : rn0, n1 = NC ? NC : rn1, n2 = NC ? NC : rn2;
   const int nk = n0 * n1 * n2;
   C* A = reinterpret_cast<C*>(smem_raw);
   const int64_t ntiles = (ncol + TILE - 1) / TILE;
@@ -250,7 +275,7 @@ __global__ void __launch_bounds__(256) k_dft_plain(cplx_t<R>* __restrict__ buf, 
     C* base = buf + b * bstride;
     load_tile<C, TILE>(A, base, nk, ncol, col0);
     __syncthreads();
-    dft3<C, TILE>(A, (C*)nullptr, n0, n1, n2, sign);
+    dft3c<C, TILE, NC>(A, (C*)nullptr, n0, n1, n2, sign);
     for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) A[i] = cscale(A[i], scale);
     __syncthreads();
     store_tile<C, TILE>(A, base, nk, ncol, col0);
@@ -276,6 +301,23 @@ static void set_smem(const void* fn, size_t bytes) {
     CQ_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
+// cubic grid edge compiled as a constant (0 = runtime shape)
+static int cubic_edge(KGrid g) {
+  if (g.n0 == g.n1 && g.n1 == g.n2 && (g.n0 == 1 || g.n0 == 2 || g.n0 == 3 || g.n0 == 4 || g.n0 == 6))
+    return g.n0;
+  return 0;
+}
+
+#define CQ_DISPATCH_NC(g, ...)                 \
+  switch (cubic_edge(g)) {                     \
+    case 1: { constexpr int NCV = 1; __VA_ARGS__; } break; \
+    case 2: { constexpr int NCV = 2; __VA_ARGS__; } break; \
+    case 3: { constexpr int NCV = 3; __VA_ARGS__; } break; \
+    case 4: { constexpr int NCV = 4; __VA_ARGS__; } break; \
+    case 6: { constexpr int NCV = 6; __VA_ARGS__; } break; \
+    default: { constexpr int NCV = 0; __VA_ARGS__; } break; \
+  }
+
 template <typename R>
 void launch_pi_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gn, cplx_t<R>* Pi, int64_t ncol,
                      KGrid g, double sp, cudaStream_t s) {
@@ -287,11 +329,11 @@ void launch_pi_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gn, cplx_t<R>* Pi, in
   const int64_t ntiles = (ncol + tile - 1) / tile;
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, 148 * 16);
   if (tile == 32) {
-    set_smem((const void*)k_pi_fused<R, 32>, smem);
-    k_pi_fused<R, 32><<<grid, 256, smem, s>>>(Gp, Gn, Pi, ncol, g.n0, g.n1, g.n2, scale);
+    CQ_DISPATCH_NC(g, set_smem((const void*)k_pi_fused<R, 32, NCV>, smem);
+                   k_pi_fused<R, 32, NCV><<<grid, 256, smem, s>>>(Gp, Gn, Pi, ncol, g.n0, g.n1, g.n2, scale))
   } else {
-    set_smem((const void*)k_pi_fused<R, 16>, smem);
-    k_pi_fused<R, 16><<<grid, 256, smem, s>>>(Gp, Gn, Pi, ncol, g.n0, g.n1, g.n2, scale);
+    CQ_DISPATCH_NC(g, set_smem((const void*)k_pi_fused<R, 16, NCV>, smem);
+                   k_pi_fused<R, 16, NCV><<<grid, 256, smem, s>>>(Gp, Gn, Pi, ncol, g.n0, g.n1, g.n2, scale))
   }
   CQ_LAUNCHED();
 }
@@ -308,11 +350,13 @@ void launch_sigma_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gm, const cplx_t<R
   const int64_t ntiles = (ncol + tile - 1) / tile;
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, 148 * 16);
   if (tile == 32) {
-    set_smem((const void*)k_sigma_fused<R, 32>, smem);
-    k_sigma_fused<R, 32><<<grid, 256, smem, s>>>(Gp, Gm, WR, Sp, Sm, ncol, g.n0, g.n1, g.n2, scale);
+    CQ_DISPATCH_NC(g, set_smem((const void*)k_sigma_fused<R, 32, NCV>, smem);
+                   k_sigma_fused<R, 32, NCV><<<grid, 256, smem, s>>>(Gp, Gm, WR, Sp, Sm, ncol, g.n0,
+                                                                     g.n1, g.n2, scale))
   } else {
-    set_smem((const void*)k_sigma_fused<R, 16>, smem);
-    k_sigma_fused<R, 16><<<grid, 256, smem, s>>>(Gp, Gm, WR, Sp, Sm, ncol, g.n0, g.n1, g.n2, scale);
+    CQ_DISPATCH_NC(g, set_smem((const void*)k_sigma_fused<R, 16, NCV>, smem);
+                   k_sigma_fused<R, 16, NCV><<<grid, 256, smem, s>>>(Gp, Gm, WR, Sp, Sm, ncol, g.n0,
+                                                                     g.n1, g.n2, scale))
   }
   CQ_LAUNCHED();
 }
@@ -327,13 +371,13 @@ void launch_dft_plain(cplx_t<R>* buf, int64_t ncol, KGrid g, int sign, double sc
   const int64_t ntiles = (ncol + tile - 1) / tile * nbatch;
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, 148 * 16);
   if (tile == 32) {
-    set_smem((const void*)k_dft_plain<R, 32>, smem);
-    k_dft_plain<R, 32><<<grid, 256, smem, s>>>(buf, ncol, g.n0, g.n1, g.n2, sign, (R)scale,
-                                               nbatch, bstride);
+    CQ_DISPATCH_NC(g, set_smem((const void*)k_dft_plain<R, 32, NCV>, smem);
+                   k_dft_plain<R, 32, NCV><<<grid, 256, smem, s>>>(buf, ncol, g.n0, g.n1, g.n2, sign,
+                                                                   (R)scale, nbatch, bstride))
   } else {
-    set_smem((const void*)k_dft_plain<R, 16>, smem);
-    k_dft_plain<R, 16><<<grid, 256, smem, s>>>(buf, ncol, g.n0, g.n1, g.n2, sign, (R)scale,
-                                               nbatch, bstride);
+    CQ_DISPATCH_NC(g, set_smem((const void*)k_dft_plain<R, 16, NCV>, smem);
+                   k_dft_plain<R, 16, NCV><<<grid, 256, smem, s>>>(buf, ncol, g.n0, g.n1, g.n2, sign,
+                                                                   (R)scale, nbatch, bstride))
   }
   CQ_LAUNCHED();
 }

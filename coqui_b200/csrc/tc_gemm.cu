@@ -31,24 +31,32 @@ __device__ int g_tc_error = 0;
 
 constexpr int kBM = 128;
 constexpr int kBKR = 32;  // real K per stage (128 bytes of fp32)
-constexpr int kStages = 2;
-constexpr int kProducers = 256;  // warps 0-7 stage operands, then drain the accumulator
-constexpr int kThreads = kProducers + 32;  // + warp 8: TMEM allocation and MMA issue
-
-template <int BNC> struct TileCfg {
+// BNC complex columns per tile; NP producer threads (warps 0..NP/32-1 stage operands, then
+// drain the accumulator; warp NP/32 allocates TMEM and issues MMAs); ST pipeline stages.
+// Long-K products use (NP = 256, ST = 2); short-K ones (K <= 64) use (NP = 128, ST = 1), whose
+// smaller footprint lets several CTAs share an SM so one tile's epilogue overlaps another's
+// main loop.
+template <int BNC, int NP, int ST> struct TileCfg {
   static constexpr int NR = 2 * BNC;                   // UMMA N (real columns)
+  static constexpr int NPROD = NP;
+  static constexpr int NPW = NP / 32;
+  static constexpr int STAGES = ST;
+  static constexpr int THREADS = NP + 32;
   static constexpr int A_PLANE = kBM * 128;            // bytes of one A plane
   static constexpr int B_PLANE = NR * 128;             // bytes of one B plane
   static constexpr int STAGE = 2 * A_PLANE + 2 * B_PLANE;
-  static constexpr int SMEM = kStages * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+  static constexpr int SMEM = ST * STAGE + 1024 /*align*/ + 256 /*barriers*/;
   static constexpr int TMEM_COLS = NR;                 // 64, 128 or 256
-  static constexpr int B_CHUNKS = BNC * 8 / kProducers;  // B chunks per producer thread
+  static constexpr int A_CHUNKS = kBM * 8 / NP;        // A chunks per producer thread
+  static constexpr int B_CHUNKS = BNC * 8 / NP;        // B chunks per producer thread
   // kind::tf32 dense, F32 accumulate, K-major A and B, M = 128, N = NR
   static constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) |
                                     ((uint32_t)(NR >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
-  // epilogue transpose buffer: 32 rows x (NR / 2 + 4) floats per warp
+  // epilogue: each warp drains NR / 2 columns at a time through a 32 x (NR / 2 + 4) buffer
+  static constexpr int HALVES = 8 / NPW;
   static constexpr int EPI_PITCH = NR / 2 + 4;
-  static_assert(8 * 32 * EPI_PITCH * 4 <= kStages * STAGE, "epilogue buffer");
+  static_assert(NPW * 32 * EPI_PITCH * 4 <= ST * STAGE, "epilogue buffer");
+  static_assert(B_CHUNKS >= 1, "tile too narrow for the producer count");
 };
 
 struct TcParams {
@@ -180,9 +188,8 @@ template <> struct Pair<true> {
     if (row_ok && k + 1 < kmax) b = __ldg(p + 1);
   }
 };
-template <int BNC, bool A64, bool B64> struct Staging {
-  using Cfg = TileCfg<BNC>;
-  Pair<A64> a[4];
+template <class Cfg, bool A64, bool B64> struct Staging {
+  Pair<A64> a[Cfg::A_CHUNKS];
   Pair<B64> b[Cfg::B_CHUNKS];
 
   __device__ __forceinline__ void load(const TcParams& p, int64_t bz, int64_t m0, int64_t n0,
@@ -191,15 +198,15 @@ template <int BNC, bool A64, bool B64> struct Staging {
     const int64_t ba = p.a_mod ? (p.a_q0 + bz) % p.a_mod : bz;
     const int64_t bb = p.b_mod ? (p.b_q0 + bz) % p.b_mod : bz;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int i = t + j * kProducers;
+    for (int j = 0; j < Cfg::A_CHUNKS; ++j) {
+      const int i = t + j * Cfg::NPROD;
       const int r = i >> 3, c = i & 7;
       const int64_t m = m0 + r, k = k0c + 2 * c;
       a[j].load(p.A, ba * p.sA + m * p.lda + k, k, p.K, m < p.M);
     }
 #pragma unroll
     for (int j = 0; j < Cfg::B_CHUNKS; ++j) {
-      const int i = t + j * kProducers;
+      const int i = t + j * Cfg::NPROD;
       const int r = i >> 3, c = i & 7;
       const int64_t n = n0 + r, k = k0c + 2 * c;
       b[j].load(p.Bt, bb * p.sB + n * p.ldb + k, k, p.K, n < p.N);
@@ -230,8 +237,8 @@ template <int BNC, bool A64, bool B64> struct Staging {
     const int t = threadIdx.x;
     const float ca = p.conj_a ? -1.f : 1.f, cb = p.conj_b ? -1.f : 1.f;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int i = t + j * kProducers;
+    for (int j = 0; j < Cfg::A_CHUNKS; ++j) {
+      const int i = t + j * Cfg::NPROD;
       const int r = i >> 3, c = i & 7;
       uint32_t h[4], l[4];
       words<A64>(a[j], ca, h, l);
@@ -242,7 +249,7 @@ template <int BNC, bool A64, bool B64> struct Staging {
     constexpr uint32_t SGN = 0x80000000u;
 #pragma unroll
     for (int j = 0; j < Cfg::B_CHUNKS; ++j) {
-      const int i = t + j * kProducers;
+      const int i = t + j * Cfg::NPROD;
       const int r = i >> 3, c = i & 7;
       uint32_t h[4], l[4];  // (br0, bi0, br1, bi1) after conjugation
       words<B64>(b[j], cb, h, l);
@@ -256,14 +263,16 @@ template <int BNC, bool A64, bool B64> struct Staging {
   }
 };
 
-template <int BNC, bool A64, bool B64>
-__global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
-  using Cfg = TileCfg<BNC>;
+template <int BNC, int NP, int ST, bool A64, bool B64>
+__global__ void __launch_bounds__(NP + 32, (NP == 128 ? 2 : 1)) k_tc_cgemm(TcParams p) {
+  using Cfg = TileCfg<BNC, NP, ST>;
+  constexpr int kStages = ST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * Cfg::STAGE);
-  // bars[0..1] full, bars[2..3] empty, bars[4] accumulator ready; bars[5] holds the TMEM base
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 5);
+  // bars[0..ST) full, bars[ST..2ST) empty, bars[2ST] accumulator ready, then the TMEM base
+  uint64_t* acc_bar = bars + 2 * kStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t bz = blockIdx.z;
   const int64_t m0 = (int64_t)blockIdx.y * kBM, n0 = (int64_t)blockIdx.x * BNC;
@@ -279,13 +288,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(smem_u32(&bars[s]), kProducers);
+      mbar_init(smem_u32(&bars[s]), Cfg::NPROD);
       mbar_init(smem_u32(&bars[kStages + s]), 1);
     }
-    mbar_init(smem_u32(&bars[4]), 1);
+    mbar_init(smem_u32(acc_bar), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 8) {
+  if (warp == Cfg::NPW) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
                  "r"((uint32_t)Cfg::TMEM_COLS)
@@ -298,9 +307,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
   const uint32_t tmem = *tmem_slot;
 
   bool ok = true;
-  if (warp < 8) {
+  if (warp < Cfg::NPW) {
     // ---------------- producers: register prefetch one stage ahead ----------------
-    Staging<BNC, A64, B64> st;
+    Staging<Cfg, A64, B64> st;
     if (nkb > 0) st.load(p, bz, m0, n0, (int64_t)kb_lo * 16);
     for (int it = 0; it < nkb; ++it) {
       const int s = it % kStages;
@@ -315,63 +324,68 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
       if (it + 1 < nkb) st.load(p, bz, m0, n0, (int64_t)(kb_lo + it + 1) * 16);
     }
     // ---------------- epilogue: TMEM -> registers -> smem -> coalesced rows ----------------
-    const int q = warp & 3, h = warp >> 2;  // TMEM lane quadrant, column half
+    const int q = warp & 3;  // TMEM lane quadrant
     float* buf = reinterpret_cast<float*>(smem) + warp * 32 * Cfg::EPI_PITCH;
     bool have = false;
     if (ok && nkb > 0) {
-      have = mbar_wait(smem_u32(&bars[4]), 0u);
+      have = mbar_wait(smem_u32(acc_bar), 0u);
       if (have) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
     // all producers must be past their last smem stage before it is reused
-    asm volatile("bar.sync 1, %0;" ::"r"(kProducers) : "memory");
-    const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * (Cfg::NR / 2));
+    asm volatile("bar.sync 1, %0;" ::"r"(Cfg::NPROD) : "memory");
 #pragma unroll 1
-    for (int j = 0; j < Cfg::NR / 64; ++j) {
-      uint32_t v[32];
-      if (have) {
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-            "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-            "%28, %29, %30, %31}, [%32];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-              "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-              "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
-              "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-              "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
-              "=r"(v[31])
-            : "r"(trow + (uint32_t)(j * 32)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      } else {
-#pragma unroll
-        for (int x = 0; x < 32; ++x) v[x] = 0u;
-      }
-      float4* dst = reinterpret_cast<float4*>(buf + lane * Cfg::EPI_PITCH + j * 32);
-#pragma unroll
-      for (int x = 0; x < 8; ++x)
-        dst[x] = make_float4(__uint_as_float(v[4 * x]), __uint_as_float(v[4 * x + 1]),
-                             __uint_as_float(v[4 * x + 2]), __uint_as_float(v[4 * x + 3]));
-    }
-    __syncwarp();
-    // warp writes its 32 rows; each row half is BNC/2 complex = BNC floats
-    const int64_t nh = n0 + h * (BNC / 2);
-    for (int rr = 0; rr < 32; ++rr) {
-      const int64_t m = m0 + q * 32 + rr;
-      if (m >= p.M) break;
-      float2* crow = p.C + bz * p.sC + m * p.ldc + nh;
-      const float* src = buf + rr * Cfg::EPI_PITCH;
-      for (int x = lane * 4; x < BNC; x += 128) {
-        const int64_t n = nh + x / 2;
-        const float4 val = *reinterpret_cast<const float4*>(src + x);
-        if (n + 1 < p.N && ((reinterpret_cast<uintptr_t>(crow + x / 2) & 15) == 0)) {
-          *reinterpret_cast<float4*>(crow + x / 2) = val;
+    for (int hp = 0; hp < Cfg::HALVES; ++hp) {
+      const int h = (warp >> 2) * Cfg::HALVES + hp;  // column half
+      const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * (Cfg::NR / 2));
+#pragma unroll 1
+      for (int j = 0; j < Cfg::NR / 64; ++j) {
+        uint32_t v[32];
+        if (have) {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+              "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+              "%28, %29, %30, %31}, [%32];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+                "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+                "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+                "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+                "=r"(v[31])
+              : "r"(trow + (uint32_t)(j * 32)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         } else {
-          if (n < p.N) crow[x / 2] = make_float2(val.x, val.y);
-          if (n + 1 < p.N) crow[x / 2 + 1] = make_float2(val.z, val.w);
+#pragma unroll
+          for (int x = 0; x < 32; ++x) v[x] = 0u;
+        }
+        float4* dst = reinterpret_cast<float4*>(buf + lane * Cfg::EPI_PITCH + j * 32);
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+          dst[x] = make_float4(__uint_as_float(v[4 * x]), __uint_as_float(v[4 * x + 1]),
+                               __uint_as_float(v[4 * x + 2]), __uint_as_float(v[4 * x + 3]));
+      }
+      __syncwarp();
+      // warp writes its 32 rows; each row half is BNC/2 complex = BNC floats
+      const int64_t nh = n0 + h * (BNC / 2);
+      for (int rr = 0; rr < 32; ++rr) {
+        const int64_t m = m0 + q * 32 + rr;
+        if (m >= p.M) break;
+        float2* crow = p.C + bz * p.sC + m * p.ldc + nh;
+        const float* src = buf + rr * Cfg::EPI_PITCH;
+        for (int x = lane * 4; x < BNC; x += 128) {
+          const int64_t n = nh + x / 2;
+          const float4 val = *reinterpret_cast<const float4*>(src + x);
+          if (n + 1 < p.N && ((reinterpret_cast<uintptr_t>(crow + x / 2) & 15) == 0)) {
+            *reinterpret_cast<float4*>(crow + x / 2) = val;
+          } else {
+            if (n < p.N) crow[x / 2] = make_float2(val.x, val.y);
+            if (n + 1 < p.N) crow[x / 2 + 1] = make_float2(val.z, val.w);
+          }
         }
       }
+      __syncwarp();
     }
   } else if (lane == 0) {
-    // ---------------- MMA issuer (warp 8, one lane) ----------------
+    // ---------------- MMA issuer (one lane of the last warp) ----------------
     for (int it = 0; it < nkb; ++it) {
       const int s = it % kStages;
       const uint32_t ph = (uint32_t)(it / kStages) & 1u;
@@ -391,11 +405,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
       }
       mma_commit(smem_u32(&bars[kStages + s]));  // frees the stage once these MMAs retire
     }
-    if (ok && nkb > 0) mma_commit(smem_u32(&bars[4]));
+    if (ok && nkb > 0) mma_commit(smem_u32(acc_bar));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 8) {
+  if (warp == Cfg::NPW) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"((uint32_t)Cfg::TMEM_COLS)
@@ -403,10 +417,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm(TcParams p) {
   }
 }
 
-template <int BNC, bool A64, bool B64>
+template <int BNC, int NP, int ST, bool A64, bool B64>
 void launch_tc(const TcParams& p, int64_t batch, cudaStream_t s) {
-  using Cfg = TileCfg<BNC>;
-  auto fn = k_tc_cgemm<BNC, A64, B64>;
+  using Cfg = TileCfg<BNC, NP, ST>;
+  auto fn = k_tc_cgemm<BNC, NP, ST, A64, B64>;
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -427,7 +441,7 @@ void launch_tc(const TcParams& p, int64_t batch, cudaStream_t s) {
       q.Bt = (const unsigned char*)p.Bt + b0 * p.sB * (p.b64 ? 16 : 8);
     q.C = p.C + b0 * p.sC;
     dim3 grid((unsigned)((p.N + BNC - 1) / BNC), (unsigned)((p.M + kBM - 1) / kBM), (unsigned)nb);
-    fn<<<grid, kThreads, Cfg::SMEM, s>>>(q);
+    fn<<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(q);
     count_launch();
     CQ_CHECK_CUDA(cudaGetLastError());
   }
@@ -435,12 +449,21 @@ void launch_tc(const TcParams& p, int64_t batch, cudaStream_t s) {
 
 template <bool A64, bool B64>
 void dispatch_n(const TcParams& p, int64_t batch, cudaStream_t s) {
-  if (p.N >= 128)
-    launch_tc<128, A64, B64>(p, batch, s);
-  else if (p.N > 32)
-    launch_tc<64, A64, B64>(p, batch, s);
-  else
-    launch_tc<32, A64, B64>(p, batch, s);
+  if (p.K <= 64) {  // short K: one stage, four producer warps, several CTAs per SM
+    if (p.N >= 128)
+      launch_tc<128, 128, 1, A64, B64>(p, batch, s);
+    else if (p.N > 32)
+      launch_tc<64, 128, 1, A64, B64>(p, batch, s);
+    else
+      launch_tc<32, 128, 1, A64, B64>(p, batch, s);
+  } else {
+    if (p.N >= 128)
+      launch_tc<128, 256, 2, A64, B64>(p, batch, s);
+    else if (p.N > 32)
+      launch_tc<64, 256, 2, A64, B64>(p, batch, s);
+    else
+      launch_tc<32, 256, 2, A64, B64>(p, batch, s);
+  }
 }
 
 }  // namespace
