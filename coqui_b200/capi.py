@@ -181,9 +181,10 @@ class Context:
         self._check(self.lib.coqui_b200_set_w(self.h, _ptr(W, "W")))
 
     def eval_sigma(self, G, out=None):
-        G = self._G(G)
+        """G = None reuses the device-resident G of the previous call."""
+        G = None if G is None else self._G(G)
         if out is None:
-            out = np.empty_like(G)
+            out = np.empty((self.nt, 1, self.nk, self.nb, self.nb), np.complex128)
         self._check(self.lib.coqui_b200_eval_sigma(self.h, _ptr(G, "G"), _ptr(out, "Sigma")))
         return out
 

@@ -85,6 +85,7 @@ template <typename T> struct DevBuf {
     cudaError_t e = cudaMalloc((void**)&p, (count ? count : 1) * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;
+      cudaGetLastError();  // the failed allocation is not a sticky error: clear it
       throw Error(COQUI_B200_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     }
     n = count;

@@ -81,6 +81,19 @@ struct coqui_b200_ctx {
   DevBuf<unsigned char> dyn;         // Dyson scratch
   DevBuf<float4> Ls, LHs;            // pre-split L, L^H for the tensor-core Dyson products
   cq::TcOperand Xtc;                 // packed X for the tensor-core projections
+  DevBuf<double2> Gx;                // primary_to_aux staging (the resident G stays intact)
+
+  // G_PQ(tau) for every tau, computed by the polarizability and reused (then overwritten in
+  // place) by the self-energy of the same G; allocated when it fits in half the free memory
+  DevBuf<unsigned char> Gcache;
+  bool gcache_valid = false;
+
+  // pipelined host transfers: G arrives in tau chunks on the copy stream (one event per
+  // chunk) and Sigma leaves chunk by chunk while later chunks are computed
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ev_st = nullptr;  // compute stream -> copy stream ordering
+  std::vector<cudaEvent_t> up_ev;
+  bool g_pipelined = false;
 
   // phase timing of the last call
   std::vector<std::pair<std::string, cudaEvent_t>> marks;
@@ -117,24 +130,35 @@ namespace {
 
 using Ctx = coqui_b200_ctx;
 
+// After an error: let queued work and host copies finish before returning to the caller,
+// whose host buffers they may still reference.
+void settle(Ctx* c) {
+  if (c->st) (void)cudaStreamSynchronize(c->st);
+  if (c->cs) (void)cudaStreamSynchronize(c->cs);
+}
+
 template <typename F> int guarded(Ctx* c, F&& f) {
   if (!c) return COQUI_B200_EINVAL;
   try {
     CQ_CHECK_CUDA(cudaSetDevice(c->dev));
     f();
     if (c->st) CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    if (c->cs) CQ_CHECK_CUDA(cudaStreamSynchronize(c->cs));
     if (cq::tc_take_error())
       throw Error(COQUI_B200_ETIMEDOUT, "a tensor-core kernel gave up a bounded wait");
     c->err.clear();
     return COQUI_B200_OK;
   } catch (const Error& e) {
     c->err = e.what();
+    settle(c);
     return e.code;
   } catch (const std::bad_alloc&) {
     c->err = "host allocation failed";
+    settle(c);
     return COQUI_B200_ENOMEM;
   } catch (const std::exception& e) {
     c->err = e.what();
+    settle(c);
     return COQUI_B200_EINVAL;
   }
 }
@@ -169,65 +193,131 @@ void require_ready(Ctx* c, bool thc, bool ir, bool k) {
 // projections: O_PQ = X G X^H (primary -> aux) and O_ab = X^H O X (aux -> primary)
 // ---------------------------------------------------------------------------------------
 
-// G_k (nk, nb, nb) complex128 on device -> out (nk, Np, Np) in storage precision.
-void project_p2a(Ctx* c, const double2* Gk, void* out) {
+// ntau consecutive G slices (ntau, nk, nb, nb) complex128 on the device -> out (ntau, nk,
+// Np, Np) in storage precision.  The tensor-core form batches all ntau * nk problems.
+void project_p2a(Ctx* c, const double2* Gk, void* out, int64_t ntau = 1) {
   cq::Prof::Scope sc(&c->prof, "proj_p2a");
   const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
   if (c->mode == COQUI_B200_FP64) {
     c->Tproj.ensure((size_t)nk * Np * nb);
-    // T = X G  (Np x nb)
-    zgemm_rm(c, 'N', 'N', Np, nb, nb, make_double2(1, 0), c->X.p, nb, Np * nb, Gk, nb, nb * nb,
-             make_double2(0, 0), c->Tproj.p, nb, Np * nb, nk);
-    // O = T X^H  (Np x Np)
-    zgemm_rm(c, 'N', 'C', Np, Np, nb, make_double2(1, 0), c->Tproj.p, nb, Np * nb, c->X.p, nb,
-             Np * nb, make_double2(0, 0), (double2*)out, Np, Np * Np, nk);
+    for (int64_t t = 0; t < ntau; ++t) {
+      const double2* G = Gk + t * nk * nb * nb;
+      double2* O = (double2*)out + t * nk * Np * Np;
+      // T = X G  (Np x nb)
+      zgemm_rm(c, 'N', 'N', Np, nb, nb, make_double2(1, 0), c->X.p, nb, Np * nb, G, nb, nb * nb,
+               make_double2(0, 0), c->Tproj.p, nb, Np * nb, nk);
+      // O = T X^H  (Np x Np)
+      zgemm_rm(c, 'N', 'C', Np, Np, nb, make_double2(1, 0), c->Tproj.p, nb, Np * nb, c->X.p, nb,
+               Np * nb, make_double2(0, 0), O, Np, Np * Np, nk);
+    }
   } else {
-    cq::tc_project_p2a(c->Xtc, Gk, (float2*)out, nk, Np, nb, c->st);
+    cq::tc_project_p2a(c->Xtc, Gk, (float2*)out, nk, Np, nb, ntau * nk, c->st);
   }
 }
-
-// S_k (nk, Np, Np) storage -> out (nk, nb, nb) complex128 (device).
-void project_a2p(Ctx* c, const void* Sk, double2* out) {
+// ntau consecutive slices (ntau, nk, Np, Np) in storage precision -> out (ntau, nk, nb, nb)
+// complex128.
+void project_a2p(Ctx* c, const void* Sk, double2* out, int64_t ntau = 1) {
   cq::Prof::Scope sc(&c->prof, "proj_a2p");
   const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
   if (c->mode == COQUI_B200_FP64) {
     c->Tproj.ensure((size_t)nk * Np * nb);
-    // T = X^H S  (nb x Np)
-    zgemm_rm(c, 'C', 'N', nb, Np, Np, make_double2(1, 0), c->X.p, nb, Np * nb,
-             (const double2*)Sk, Np, Np * Np, make_double2(0, 0), c->Tproj.p, Np, Np * nb, nk);
-    // O = T X  (nb x nb)
-    zgemm_rm(c, 'N', 'N', nb, nb, Np, make_double2(1, 0), c->Tproj.p, Np, Np * nb, c->X.p, nb,
-             Np * nb, make_double2(0, 0), out, nb, nb * nb, nk);
+    for (int64_t t = 0; t < ntau; ++t) {
+      const double2* S = (const double2*)Sk + t * nk * Np * Np;
+      double2* O = out + t * nk * nb * nb;
+      // T = X^H S  (nb x Np)
+      zgemm_rm(c, 'C', 'N', nb, Np, Np, make_double2(1, 0), c->X.p, nb, Np * nb, S, Np, Np * Np,
+               make_double2(0, 0), c->Tproj.p, Np, Np * nb, nk);
+      // O = T X  (nb x nb)
+      zgemm_rm(c, 'N', 'N', nb, nb, Np, make_double2(1, 0), c->Tproj.p, Np, Np * nb, c->X.p, nb,
+               Np * nb, make_double2(0, 0), O, nb, nb * nb, nk);
+    }
   } else {
-    cq::tc_project_a2p(c->Xtc, (const float2*)Sk, out, nk, Np, nb, c->st);
+    cq::tc_project_a2p(c->Xtc, (const float2*)Sk, out, nk, Np, nb, ntau * nk, c->st);
   }
 }
 
 // ---------------------------------------------------------------------------------------
-// Pi(tau) for all tau in [0, nt_half) into the PW buffer (rpa_pi.icc:102-176)
+// tau chunks: chunk i covers the tau pairs it in [a, b), i.e. the slices [a, b) and
+// [nt - b, nt - a), in the order the polarizability consumes them (Pi(it) needs G(it) and
+// G(nt - 1 - it), rpa_pi.icc:102-176).  At least 256 (tau, k) problems per chunk so that each
+// batched projection fills the GPU.
 // ---------------------------------------------------------------------------------------
+int64_t tau_chunk(Ctx* c) {
+  const int64_t want = (256 + c->nk - 1) / c->nk;
+  return std::min<int64_t>(c->nth, std::max<int64_t>(4, want));
+}
+int64_t n_tau_chunks(Ctx* c) { return (c->nth + tau_chunk(c) - 1) / tau_chunk(c); }
+void tau_chunk_range(Ctx* c, int64_t i, int64_t* a, int64_t* b) {
+  *a = i * tau_chunk(c);
+  *b = std::min<int64_t>(c->nth, *a + tau_chunk(c));
+}
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// make the compute stream wait for the G slices of chunk i (pipelined upload only)
+void wait_G_chunk(Ctx* c, int64_t i) {
+  if (c->g_pipelined) CQ_CHECK_CUDA(cudaStreamWaitEvent(c->st, c->up_ev[(size_t)i], 0));
+}
+
+// Projected-G cache (nt slabs); nullptr when it does not fit in half the free memory.
+unsigned char* gcache(Ctx* c) {
+  const size_t bytes = (size_t)c->nt * c->nk * c->Np * c->Np * c->elem();
+  if (c->Gcache.n >= bytes) return c->Gcache.p;
+  size_t fr = 0, tot = 0;
+  CQ_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+  if (bytes > fr / 2) return nullptr;
+  c->Gcache.ensure(bytes);
+  return c->Gcache.p;
+}
+
 void eval_pi_device(Ctx* c) {
-  const int64_t nk = c->nk, Np = c->Np, ncol = Np * Np, nt = c->nt;
+  const int64_t nk = c->nk, nb = c->nb, Np = c->Np, ncol = Np * Np, nt = c->nt;
   const size_t slab = (size_t)nk * ncol * c->elem();
+  const size_t gsz = (size_t)nk * nb * nb;
   c->Gp.ensure(slab);
   c->Gn.ensure(slab);
   c->PW.ensure((size_t)c->nmax * c->nq * ncol * c->elem());
+  unsigned char* cache = gcache(c);
+  c->gcache_valid = false;
   const double sp = (c->ns == 2) ? -1.0 : -2.0;
-  for (int64_t it = 0; it < c->nth; ++it) {
-    project_p2a(c, c->G.p + it * nk * c->nb * c->nb, c->Gp.p);
-    project_p2a(c, c->G.p + (nt - it - 1) * nk * c->nb * c->nb, c->Gn.p);
-    unsigned char* dst = c->PW.p + (size_t)it * c->nq * ncol * c->elem();
-    cq::Prof::Scope sc(&c->prof, "pi_fused");
-    if (c->mode == COQUI_B200_FP64)
-      cq::launch_pi_fused<double>((double2*)c->Gp.p, (double2*)c->Gn.p, (double2*)dst, ncol, c->g,
-                                  sp, c->st);
-    else
-      cq::launch_pi_fused<float>((float2*)c->Gp.p, (float2*)c->Gn.p, (float2*)dst, ncol, c->g, sp,
-                                 c->st);
+  for (int64_t i = 0; i < n_tau_chunks(c); ++i) {
+    int64_t a, b;
+    tau_chunk_range(c, i, &a, &b);
+    wait_G_chunk(c, i);
+    if (cache) {
+      project_p2a(c, c->G.p + a * gsz, cache + a * slab, b - a);
+      project_p2a(c, c->G.p + (nt - b) * gsz, cache + (nt - b) * slab, b - a);
+    }
+    for (int64_t it = a; it < b; ++it) {
+      const unsigned char* gp = c->Gp.p;
+      const unsigned char* gn = c->Gn.p;
+      if (cache) {
+        gp = cache + it * slab;
+        gn = cache + (nt - it - 1) * slab;
+      } else {
+        project_p2a(c, c->G.p + it * gsz, c->Gp.p);
+        project_p2a(c, c->G.p + (nt - it - 1) * gsz, c->Gn.p);
+      }
+      unsigned char* dst = c->PW.p + (size_t)it * c->nq * ncol * c->elem();
+      cq::Prof::Scope sc(&c->prof, "pi_fused");
+      if (c->mode == COQUI_B200_FP64)
+        cq::launch_pi_fused<double>((const double2*)gp, (const double2*)gn, (double2*)dst, ncol,
+                                    c->g, sp, c->st);
+      else
+        cq::launch_pi_fused<float>((const float2*)gp, (const float2*)gn, (float2*)dst, ncol, c->g,
+                                   sp, c->st);
+    }
   }
+  c->gcache_valid = (cache != nullptr);
   c->w_valid = false;
 }
-
 void ir_inplace(Ctx* c, int n_in, int n_out, const double2* M) {
   cq::Prof::Scope sc(&c->prof, "ir_transform");
   const int64_t ncol = c->nq * c->Np * c->Np;
@@ -245,16 +335,42 @@ void ir_inplace(Ctx* c, int n_in, int n_out, const double2* M) {
     cq::launch_ir_transform<float>((float2*)c->PW.p, ncol, n_in, n_out, M, c->st);
 }
 
-// G_tskij == NULL reuses the G already resident on the device.
 void upload_G(Ctx* c, const double* G_tskij) {
-  const size_t n = (size_t)c->nt * c->nk * c->nb * c->nb;
+  const size_t gsz = (size_t)c->nk * c->nb * c->nb;
+  const size_t n = (size_t)c->nt * gsz;
   if (!G_tskij) {
     CQ_REQUIRE(c->g_resident, COQUI_B200_EINVAL, "G_tskij is null and no G is resident");
     return;
   }
   c->G.ensure(n);
-  upload(c, c->G.p, G_tskij, n * sizeof(double2));
+  c->gcache_valid = false;
   c->g_resident = true;
+  if (!is_pinned(G_tskij)) {
+    c->g_pipelined = false;
+    upload(c, c->G.p, G_tskij, n * sizeof(double2));
+    return;
+  }
+  // page-locked source: copy chunk by chunk on the copy stream; the projections of chunk i
+  // start once its event fired, while later chunks are still crossing the bus
+  const int64_t nch = n_tau_chunks(c);
+  while ((int64_t)c->up_ev.size() < nch) {
+    cudaEvent_t e;
+    CQ_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->up_ev.push_back(e);
+  }
+  CQ_CHECK_CUDA(cudaEventRecord(c->ev_st, c->st));  // earlier readers of the G buffer
+  CQ_CHECK_CUDA(cudaStreamWaitEvent(c->cs, c->ev_st, 0));
+  const double2* h = reinterpret_cast<const double2*>(G_tskij);
+  for (int64_t i = 0; i < nch; ++i) {
+    int64_t a, b;
+    tau_chunk_range(c, i, &a, &b);
+    const size_t bytes = (size_t)(b - a) * gsz * sizeof(double2);
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->G.p + a * gsz, h + a * gsz, bytes, cudaMemcpyHostToDevice, c->cs));
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->G.p + (c->nt - b) * gsz, h + (c->nt - b) * gsz, bytes,
+                                  cudaMemcpyHostToDevice, c->cs));
+    CQ_CHECK_CUDA(cudaEventRecord(c->up_ev[(size_t)i], c->cs));
+  }
+  c->g_pipelined = true;
 }
 
 // E_c accumulation (thc_rpa.icc:130-173) from per-(w, q) log det and traces.
@@ -319,6 +435,8 @@ int coqui_b200_create(coqui_b200_ctx** out, const coqui_b200_dims* dims) {
                "k-grid edges above 8 are not supported");
     c->mode = d.precision_mode;
     CQ_CHECK_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CQ_CHECK_CUDA(cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking));
+    CQ_CHECK_CUDA(cudaEventCreateWithFlags(&c->ev_st, cudaEventDisableTiming));
     CQ_CHECK_BLAS(cublasCreate(&c->blas));
     CQ_CHECK_BLAS(cublasSetStream(c->blas, c->st));
     CQ_CHECK_BLAS(cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
@@ -340,9 +458,14 @@ void coqui_b200_destroy(coqui_b200_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
+  if (c->cs) cudaStreamSynchronize(c->cs);
   for (auto* b : {&c->X, &c->V, &c->L, &c->LH, &c->chi, &c->G, &c->Sig, &c->Tproj, &c->stage,
-                  &c->dTwt, &c->dTtw, &c->eps})
+                  &c->dTwt, &c->dTtw, &c->eps, &c->Gx})
     b->release();
+  c->Gcache.release();
+  for (cudaEvent_t e : c->up_ev) cudaEventDestroy(e);
+  if (c->ev_st) cudaEventDestroy(c->ev_st);
+  if (c->cs) cudaStreamDestroy(c->cs);
   c->fac.release();
   c->dTwtR.release();
   c->dTtwR.release();
@@ -449,6 +572,7 @@ int coqui_b200_set_ir(coqui_b200_ctx* c, const double* Twt_bb, const double* Ttw
     }
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->have_ir = true;
+    c->gcache_valid = false;
   });
 }
 
@@ -498,6 +622,7 @@ int coqui_b200_set_kmesh(coqui_b200_ctx* c, const double* kpts, const double* la
       CQ_CHECK_CUDA(cudaMemsetAsync(c->chi.p, 0, (size_t)nk * c->Np * sizeof(double2), c->st));
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->have_k = true;
+    c->gcache_valid = false;
   });
 }
 
@@ -526,6 +651,7 @@ int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_
     }
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->have_thc = true;
+    c->gcache_valid = false;
     c->w_valid = false;
   });
 }
@@ -537,12 +663,12 @@ int coqui_b200_primary_to_aux(coqui_b200_ctx* c, int64_t n_tau, const double* O_
     CQ_REQUIRE(n_tau >= 1 && O_tskab && O_tskPQ, COQUI_B200_EINVAL, "bad arguments");
     const int64_t nk = c->nk, nb = c->nb, Np = c->Np, ncol = Np * Np;
     const size_t gsz = (size_t)nk * nb * nb;
-    c->G.ensure(gsz);
+    c->Gx.ensure(gsz);  // not c->G: a resident G stays valid
     c->Gp.ensure((size_t)nk * ncol * c->elem());
     c->stage.ensure((size_t)nk * ncol);
     for (int64_t t = 0; t < n_tau; ++t) {
-      upload(c, c->G.p, O_tskab + 2 * t * gsz, gsz * sizeof(double2));
-      project_p2a(c, c->G.p, c->Gp.p);
+      upload(c, c->Gx.p, O_tskab + 2 * t * gsz, gsz * sizeof(double2));
+      project_p2a(c, c->Gx.p, c->Gp.p);
       const double2* src = (const double2*)c->Gp.p;
       if (c->mode == COQUI_B200_MIXED) {
         cq::launch_to_c128<float>((float2*)c->Gp.p, c->stage.p, nk * ncol, c->st);
@@ -679,7 +805,9 @@ void download_w_qt(Ctx* c, double* dW_qtPQ) {
 }
 
 // Sigma(tau) for all tau into c->Sig (device, complex128), thc_gw.icc:70-213 twice.
-void sigma_device(Ctx* c) {
+// host_out (may be null) receives Sigma_tskij; from page-locked memory it is filled chunk by
+// chunk on the copy stream while the following chunks are computed.
+void sigma_device(Ctx* c, double* host_out) {
   CQ_REQUIRE(c->w_valid, COQUI_B200_EINVAL, "no screened interaction: call update_w or set_w");
   const int64_t nk = c->nk, nb = c->nb, Np = c->Np, ncol = Np * Np, nt = c->nt;
   const size_t slab = (size_t)nk * ncol * c->elem();
@@ -700,26 +828,66 @@ void sigma_device(Ctx* c) {
     c->w_in_R = true;
   }
   c->mark("SIGMA_FT_W");
-  for (int64_t it = 0; it < c->nth; ++it) {
-    const bool minus = it < nt / 2;  // thc_gw.icc:59-61 writes Sigma(nt-1-it) for it < nt/2
-    project_p2a(c, c->G.p + it * gsz, c->Gp.p);
-    if (minus) project_p2a(c, c->G.p + (nt - it - 1) * gsz, c->Gn.p);
-    unsigned char* WR = c->PW.p + (size_t)it * c->nq * ncol * c->elem();
-    {
-      cq::Prof::Scope sc(&c->prof, "sigma_fused");
-      if (c->mode == COQUI_B200_FP64)
-        cq::launch_sigma_fused<double>((double2*)c->Gp.p, minus ? (double2*)c->Gn.p : nullptr,
-                                       (double2*)WR, (double2*)c->Gp.p,
-                                       minus ? (double2*)c->Gn.p : nullptr, ncol, c->g, c->st);
-      else
-        cq::launch_sigma_fused<float>((float2*)c->Gp.p, minus ? (float2*)c->Gn.p : nullptr,
-                                      (float2*)WR, (float2*)c->Gp.p,
-                                      minus ? (float2*)c->Gn.p : nullptr, ncol, c->g, c->st);
+  // G_PQ(tau) of this G is still in the cache when the polarizability just ran: Sigma_PQ is
+  // then formed in place there and projected back in batches
+  unsigned char* cache = c->gcache_valid ? c->Gcache.p : nullptr;
+  c->gcache_valid = false;
+  const bool pipe_out = host_out && is_pinned(host_out);
+  for (int64_t i = 0; i < n_tau_chunks(c); ++i) {
+    int64_t a, b;
+    tau_chunk_range(c, i, &a, &b);
+    if (!cache) wait_G_chunk(c, i);
+    for (int64_t it = a; it < b; ++it) {
+      const bool minus = it < nt / 2;  // thc_gw.icc:59-61 writes Sigma(nt-1-it) for it < nt/2
+      unsigned char* gp = c->Gp.p;
+      unsigned char* gn = minus ? c->Gn.p : nullptr;
+      if (cache) {
+        gp = cache + it * slab;
+        gn = minus ? cache + (nt - it - 1) * slab : nullptr;
+      } else {
+        project_p2a(c, c->G.p + it * gsz, gp);
+        if (minus) project_p2a(c, c->G.p + (nt - it - 1) * gsz, gn);
+      }
+      unsigned char* WR = c->PW.p + (size_t)it * c->nq * ncol * c->elem();
+      {
+        cq::Prof::Scope sc(&c->prof, "sigma_fused");
+        if (c->mode == COQUI_B200_FP64)
+          cq::launch_sigma_fused<double>((double2*)gp, (double2*)gn, (double2*)WR, (double2*)gp,
+                                         (double2*)gn, ncol, c->g, c->st);
+        else
+          cq::launch_sigma_fused<float>((float2*)gp, (float2*)gn, (float2*)WR, (float2*)gp,
+                                        (float2*)gn, ncol, c->g, c->st);
+      }
+      if (!cache) {
+        project_a2p(c, gp, c->Sig.p + it * gsz);
+        if (minus) project_a2p(c, gn, c->Sig.p + (nt - it - 1) * gsz);
+      }
     }
-    project_a2p(c, c->Gp.p, c->Sig.p + it * gsz);
-    if (minus) project_a2p(c, c->Gn.p, c->Sig.p + (nt - it - 1) * gsz);
+    if (cache) {
+      // for odd nt the middle slice is in both ranges (same values written twice)
+      project_a2p(c, cache + a * slab, c->Sig.p + a * gsz, b - a);
+      project_a2p(c, cache + (nt - b) * slab, c->Sig.p + (nt - b) * gsz, b - a);
+    }
+    if (pipe_out) {
+      const size_t bytes = (size_t)(b - a) * gsz * sizeof(double2);
+      double2* h = reinterpret_cast<double2*>(host_out);
+      CQ_CHECK_CUDA(cudaEventRecord(c->ev_st, c->st));
+      CQ_CHECK_CUDA(cudaStreamWaitEvent(c->cs, c->ev_st, 0));
+      CQ_CHECK_CUDA(cudaMemcpyAsync(h + a * gsz, c->Sig.p + a * gsz, bytes, cudaMemcpyDeviceToHost, c->cs));
+      CQ_CHECK_CUDA(cudaMemcpyAsync(h + (nt - b) * gsz, c->Sig.p + (nt - b) * gsz, bytes,
+                                    cudaMemcpyDeviceToHost, c->cs));
+    }
   }
   c->mark("EVALUATE_SIGMA_R");
+  if (host_out) {
+    if (pipe_out) {  // the compute stream's timeline ends when the last copy landed
+      CQ_CHECK_CUDA(cudaEventRecord(c->ev_st, c->cs));
+      CQ_CHECK_CUDA(cudaStreamWaitEvent(c->st, c->ev_st, 0));
+    } else {
+      download(c, host_out, c->Sig.p, (size_t)nt * gsz * sizeof(double2));
+    }
+    c->mark("d2h_Sigma");
+  }
 }
 
 [[maybe_unused]] void w_to_q_space(Ctx* c) {
@@ -782,11 +950,7 @@ int coqui_b200_eval_sigma(coqui_b200_ctx* c, const double* G_tskij, double* Sigm
     c->begin_timing();
     upload_G(c, G_tskij);
     c->mark("h2d_G");
-    sigma_device(c);
-    if (Sigma_tskij) {
-      download(c, Sigma_tskij, c->Sig.p, (size_t)c->nt * c->nk * c->nb * c->nb * sizeof(double2));
-      c->mark("d2h_Sigma");
-    }
+    sigma_device(c, Sigma_tskij);
     c->end_timing();
   });
 }
@@ -803,11 +967,7 @@ int coqui_b200_gw_iteration(coqui_b200_ctx* c, const double* G_tskij, double* Si
       eps_head(c, eps_inv_head);
       c->mark("EPS_INV_HEAD");
     }
-    sigma_device(c);
-    if (Sigma_tskij) {
-      download(c, Sigma_tskij, c->Sig.p, (size_t)c->nt * c->nk * c->nb * c->nb * sizeof(double2));
-      c->mark("d2h_Sigma");
-    }
+    sigma_device(c, Sigma_tskij);
     c->end_timing();
   });
 }

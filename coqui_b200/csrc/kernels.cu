@@ -4,6 +4,7 @@
 // All large arrays are (leading index, ncol) row-major with ncol = Np * Np consecutive
 // auxiliary-basis elements, so every kernel reads and writes whole 32-column runs per warp.
 #include <atomic>
+#include <type_traits>
 #include <mutex>
 
 #include "kernels.cuh"
@@ -506,11 +507,77 @@ __global__ void __launch_bounds__(128) k_ir_transform_real(cplx_t<R>* __restrict
   }
 }
 
+// Complex64 storage with FP32 accumulation (mixed-precision form): the 2 n_in FMAs per output
+// then cost half the FP64 form's issue slots, so the transform stays bound by its HBM
+// traffic.  The accumulation error is of the order of the complex64 rounding of the inputs
+// (the IR rows are sums of same-sign weights for the low frequencies, at most |T| ~ 1e3).
+// M (n_out, n_in) FP64 is staged into shared memory as FP32, rows padded to MAXT entries and
+// the row count to a multiple of 4 with zeros, so that one float4 read feeds 8 FMAs.
+template <int MAXT>
+__global__ void __launch_bounds__(256) k_ir_transform_f32(float2* __restrict__ buf, int64_t ncol,
+                                                          int n_in, int n_out,
+                                                          const double* __restrict__ M) {
+  static_assert(MAXT % 4 == 0, "MAXT must be a multiple of 4");
+  extern __shared__ float4 sM4[];
+  float* sMf = reinterpret_cast<float*>(sM4);
+  const int n_out4 = (n_out + 3) / 4;
+  for (int i = threadIdx.x; i < n_out4 * 4 * MAXT; i += blockDim.x) {
+    const int o = i / MAXT, t = i % MAXT;
+    sMf[i] = (o < n_out && t < n_in) ? (float)M[o * n_in + t] : 0.f;
+  }
+  __syncthreads();
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ncol;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    float2 x[MAXT];
+#pragma unroll
+    for (int t = 0; t < MAXT; ++t)
+      x[t] = (t < n_in) ? buf[(int64_t)t * ncol + e] : make_float2(0.f, 0.f);
+    for (int o4 = 0; o4 < n_out4; ++o4) {
+      float ar[4] = {0.f, 0.f, 0.f, 0.f}, ai[4] = {0.f, 0.f, 0.f, 0.f};
+      const float4* rows = sM4 + (size_t)o4 * 4 * (MAXT / 4);
+#pragma unroll
+      for (int t4 = 0; t4 < MAXT / 4; ++t4) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 m = rows[q * (MAXT / 4) + t4];
+          ar[q] = fmaf(m.x, x[4 * t4 + 0].x, ar[q]);
+          ai[q] = fmaf(m.x, x[4 * t4 + 0].y, ai[q]);
+          ar[q] = fmaf(m.y, x[4 * t4 + 1].x, ar[q]);
+          ai[q] = fmaf(m.y, x[4 * t4 + 1].y, ai[q]);
+          ar[q] = fmaf(m.z, x[4 * t4 + 2].x, ar[q]);
+          ai[q] = fmaf(m.z, x[4 * t4 + 2].y, ai[q]);
+          ar[q] = fmaf(m.w, x[4 * t4 + 3].x, ar[q]);
+          ai[q] = fmaf(m.w, x[4 * t4 + 3].y, ai[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (o4 * 4 + q < n_out) __stcs(buf + (int64_t)(o4 * 4 + q) * ncol + e, make_float2(ar[q], ai[q]));
+    }
+  }
+}
+
+template <int MAXT>
+static void launch_ir_f32(float2* buf, int64_t ncol, int n_in, int n_out, const double* M,
+                          cudaStream_t s) {
+  const size_t smem = (size_t)((n_out + 3) / 4) * 4 * MAXT * sizeof(float);
+  set_smem((const void*)k_ir_transform_f32<MAXT>, smem);
+  k_ir_transform_f32<MAXT><<<grid_for(ncol, 256, 148 * 16), 256, smem, s>>>(buf, ncol, n_in, n_out, M);
+  CQ_LAUNCHED();
+}
+
 template <typename R>
 void launch_ir_transform_real(cplx_t<R>* buf, int64_t ncol, int n_in, int n_out, const double* M,
                               cudaStream_t s) {
   CQ_REQUIRE(n_in >= 1 && n_in <= 96 && n_out >= 1, COQUI_B200_EUNSUPPORTED,
              "IR transform supports at most 96 input points");
+  if constexpr (std::is_same<R, float>::value) {
+    float2* b = reinterpret_cast<float2*>(buf);
+    if (n_in <= 16) return launch_ir_f32<16>(b, ncol, n_in, n_out, M, s);
+    if (n_in <= 24) return launch_ir_f32<24>(b, ncol, n_in, n_out, M, s);
+    if (n_in <= 32) return launch_ir_f32<32>(b, ncol, n_in, n_out, M, s);
+    if (n_in <= 48) return launch_ir_f32<48>(b, ncol, n_in, n_out, M, s);
+  }
   const size_t smem = (size_t)n_in * n_out * sizeof(double);
   const unsigned grid = grid_for(ncol, 128, 148 * 32);
   if (n_in <= 32) {

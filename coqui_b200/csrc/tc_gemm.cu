@@ -575,35 +575,41 @@ void tc_pack_X(TcOperand& op, const double2* X, int64_t nk, int64_t Np, int64_t 
 }
 
 void tc_project_p2a(TcOperand& op, const double2* Gk, float2* out, int64_t nk, int64_t Np,
-                    int64_t nb, cudaStream_t s) {
+                    int64_t nb, int64_t nbatch, cudaStream_t s) {
   const float4* Xs = (const float4*)op.packed.p;
-  op.tmp.ensure((size_t)nk * Np * nb * sizeof(float2) + (size_t)nk * nb * nb * sizeof(float2));
+  op.tmp.ensure((size_t)nbatch * Np * nb * sizeof(float2) + (size_t)nbatch * nb * nb * sizeof(float2));
   float2* T = (float2*)op.tmp.p;
-  float2* Gt = T + nk * Np * nb;
-  const int64_t tg = nk * nb * nb;
+  float2* Gt = T + nbatch * Np * nb;
+  const int64_t tg = nbatch * nb * nb;
   k_transpose_c64<<<grid_for(tg, 256), 256, 0, s>>>(Gk, Gt, nb, nb, tg);
   count_launch();
+  // problem b = (tau, k) uses X^k: X is addressed periodically with period nk
+  TcStructure sx_a, sx_b;
+  sx_a.a_mod = nk;
+  sx_b.b_mod = nk;
   // T = X G  (Np x nb, K = nb): Bt[j][i] = G[i][j]
   tc_cgemm_nt(Xs, true, false, nb, Np * nb, Gt, false, false, nb, nb * nb, T, nb, Np * nb, Np,
-              nb, nb, nk, s);
+              nb, nb, nbatch, s, sx_a);
   // out = T X^H: B(k=b, n=Q) = conj(X[Q][b])
   tc_cgemm_nt(T, false, false, nb, Np * nb, Xs, true, true, nb, Np * nb, out, Np, Np * Np, Np,
-              Np, nb, nk, s);
+              Np, nb, nbatch, s, sx_b);
 }
 
 void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, int64_t Np,
-                    int64_t nb, cudaStream_t s) {
+                    int64_t nb, int64_t nbatch, cudaStream_t s) {
   const float4* XTs = (const float4*)op.packed.p + nk * Np * nb;
-  op.tmp.ensure((size_t)nk * Np * nb * sizeof(float2) + (size_t)nk * nb * nb * sizeof(float2));
+  op.tmp.ensure((size_t)nbatch * Np * nb * sizeof(float2) + (size_t)nbatch * nb * nb * sizeof(float2));
   float2* UT = (float2*)op.tmp.p;
-  float2* Sab = UT + nk * Np * nb;
+  float2* Sab = UT + nbatch * Np * nb;
+  TcStructure sx;
+  sx.a_mod = nk;
   // U^T = X^T S^T (nb x Np, K = Np): A = X^T, Bt = S
   tc_cgemm_nt(XTs, true, false, Np, nb * Np, Sk, false, false, Np, Np * Np, UT, Np, nb * Np, nb,
-              Np, Np, nk, s);
+              Np, Np, nbatch, s, sx);
   // Sigma_ab = X^H U (nb x nb, K = Np): A(a, P) = conj(X^T[a][P]), Bt = U^T
   tc_cgemm_nt(XTs, true, true, Np, nb * Np, UT, false, false, Np, nb * Np, Sab, nb, nb * nb, nb,
-              nb, Np, nk, s);
-  const int64_t t = nk * nb * nb;
+              nb, Np, nbatch, s, sx);
+  const int64_t t = nbatch * nb * nb;
   k_c64_to_c128<<<grid_for(t, 256), 256, 0, s>>>(Sab, out, t);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());

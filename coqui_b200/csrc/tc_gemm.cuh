@@ -20,13 +20,15 @@ struct TcOperand {
 void tc_pack_X(TcOperand& op, const double2* X, int64_t nk, int64_t Np, int64_t nb,
                cudaStream_t s);
 
-// out[k] = X^k G^k X^k^H  (Np x Np, complex64), G (nk, nb, nb) complex128.
+// out[b] = X^k G^b X^k^H  (Np x Np, complex64) for nbatch problems b = (tau, k), k = b % nk;
+// G (nbatch, nb, nb) complex128.
 void tc_project_p2a(TcOperand& op, const double2* Gk, float2* out, int64_t nk, int64_t Np,
-                    int64_t nb, cudaStream_t s);
+                    int64_t nb, int64_t nbatch, cudaStream_t s);
 
-// out[k] = X^k^H S^k X^k  (nb x nb, complex128), S (nk, Np, Np) complex64.
+// out[b] = X^k^H S^b X^k  (nb x nb, complex128) for nbatch problems, k = b % nk; S (nbatch,
+// Np, Np) complex64.
 void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, int64_t Np,
-                    int64_t nb, cudaStream_t s);
+                    int64_t nb, int64_t nbatch, cudaStream_t s);
 
 // Pre-split operand format: one float4 (hi.re, hi.im, lo.re, lo.im) per complex value with
 // hi = rna_tf32(x), lo = rna_tf32(x - hi); built once for operands used by many GEMMs.
