@@ -224,12 +224,15 @@ __device__ void invert_lower(const double2* S, double2* Sinv, int n) {
   __syncthreads();
 }
 
+// inv_group: the inverse is formed within diagonal groups of inv_group blocks only (the
+// whole matrix when inv_group >= nblk); the tensor-core levels fill in the rest.
 template <bool INV>
 __global__ void __launch_bounds__(CT, 4) k_chol_inv(const float2* __restrict__ Mall,
                                                     double2* __restrict__ Aall,
                                                     double* __restrict__ logdet,
                                                     double2* __restrict__ trace,
-                                                    int* __restrict__ info, int64_t n) {
+                                                    int* __restrict__ info, int64_t n,
+                                                    int inv_group) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* S0 = reinterpret_cast<double2*>(smem_raw);
   double2* S1 = S0 + CB * PITCH;
@@ -325,7 +328,8 @@ __global__ void __launch_bounds__(CT, 4) k_chol_inv(const float2* __restrict__ M
     for (int j = 0; j < nblk; ++j) {
       const int64_t j0 = (int64_t)j * CB;
       const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
-      for (int ib = j + 1; ib < nblk; ++ib) {
+      const int gend = min(nblk, (j / inv_group + 1) * inv_group);
+      for (int ib = j + 1; ib < gend; ++ib) {
         const int64_t i0 = (int64_t)ib * CB;
         const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
         double2 acc[4][4];
@@ -408,6 +412,87 @@ __global__ void k_chol_final(const double2* __restrict__ A, float2* __restrict__
   }
 }
 
+// Operands of the tensor-core inverse levels from A (C in the lower triangle, U = C^{-H} in
+// the upper triangle of each kInvGroup diagonal group):
+//   Z  = U - I inside the diagonal groups' upper triangles, 0 below the diagonal (the levels
+//        write the upper off-group blocks);
+//   Zl = U^H - I = C^{-1} - I inside the diagonal groups' lower triangles, 0 elsewhere (the
+//        levels write the lower off-group blocks they need later);
+//   Zc = -C on the strictly lower off-group blocks (other entries are not written).
+// 32 x 32 tiles; the transposed reads of Zl go through shared memory.
+__global__ void __launch_bounds__(256) k_chol_split(const double2* __restrict__ Aall,
+                                                   float2* __restrict__ Zall,
+                                                   float2* __restrict__ Zlall,
+                                                   float2* __restrict__ Zcall, int64_t n) {
+  __shared__ double2 tile[32][33];
+  const int64_t p = blockIdx.z;
+  const double2* A = Aall + p * n * n;
+  float2* Z = Zall + p * n * n;
+  float2* Zl = Zlall + p * n * n;
+  float2* Zc = Zcall + p * n * n;
+  const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
+  const bool same_group = (i0 / kInvGroup) == (j0 / kInvGroup);
+  const bool mirror = same_group && i0 >= j0;  // lower tile of a group: needs U^H
+  if (mirror) {
+    for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+      const int64_t r = j0 + ty, c = i0 + threadIdx.x;  // upper tile (j0, i0)
+      tile[ty][threadIdx.x] = (r < n && c < n && c >= r) ? A[r * n + c] : make_double2(0, 0);
+    }
+  }
+  __syncthreads();
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t i = i0 + ty, j = j0 + threadIdx.x;
+    if (i >= n || j >= n) continue;
+    const int64_t e = i * n + j;
+    const float d = (i == j) ? 1.f : 0.f;
+    if (j >= i) {
+      if (same_group) {
+        const double2 a = A[e];
+        Z[e] = make_float2((float)(a.x - d), (float)a.y);
+      }
+    } else {
+      Z[e] = make_float2(0.f, 0.f);
+      if (!same_group) {
+        const double2 a = A[e];
+        Zc[e] = make_float2((float)(-a.x), (float)(-a.y));
+      }
+    }
+    if (i >= j) {
+      if (mirror) {
+        const double2 u = tile[threadIdx.x][ty];  // A[j][i] = U[j][i]
+        Zl[e] = make_float2((float)(u.x - d), (float)(-u.y));
+      } else {
+        Zl[e] = make_float2(0.f, 0.f);
+      }
+    } else {
+      Zl[e] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
+// Zl[r1 + c][r0 + r] = conj(Z[r0 + r][r1 + c]) for r < b, c < b1 (a level's result, kept as
+// the lower-triangle operand of the next level)
+__global__ void k_block_adjoint(const float2* __restrict__ Zall, float2* __restrict__ Zlall,
+                                int64_t n, int64_t r0, int64_t r1, int64_t b, int64_t b1) {
+  __shared__ float2 tile[32][33];
+  const int64_t p = blockIdx.z;
+  const float2* Z = Zall + p * n * n;
+  float2* Zl = Zlall + p * n * n;
+  const int64_t rt = (int64_t)blockIdx.y * 32, ct = (int64_t)blockIdx.x * 32;
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t r = rt + ty, c = ct + threadIdx.x;
+    tile[ty][threadIdx.x] = (r < b && c < b1) ? Z[(r0 + r) * n + r1 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t c = ct + ty, r = rt + threadIdx.x;  // output row r1 + c, column r0 + r
+    if (r < b && c < b1) {
+      const float2 v = tile[threadIdx.x][ty];
+      Zl[(r1 + c) * n + r0 + r] = make_float2(v.x, -v.y);
+    }
+  }
+}
+
 }  // namespace
 
 void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, double2* trace,
@@ -424,7 +509,7 @@ void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, dou
                                          (int)smem));
       set = true;
     }
-    k_chol_inv<true><<<(unsigned)nprob, CT, smem, s>>>(M, A, logdet, trace, info, Np);
+    k_chol_inv<true><<<(unsigned)nprob, CT, smem, s>>>(M, A, logdet, trace, info, Np, 1 << 30);
     count_launch();
     CQ_CHECK_CUDA(cudaGetLastError());
     k_chol_final<<<grid_for(total, 256), 256, 0, s>>>(A, Z, Np, total);
@@ -435,8 +520,45 @@ void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, dou
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       set = true;
     }
-    k_chol_inv<false><<<(unsigned)nprob, CT, smem, s>>>(M, A, logdet, trace, info, Np);
+    k_chol_inv<false><<<(unsigned)nprob, CT, smem, s>>>(M, A, logdet, trace, info, Np, 1 << 30);
   }
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+void launch_chol_group_inv(const float2* M, double2* A, double* logdet, double2* trace, int* info,
+                           int64_t Np, int64_t nprob, cudaStream_t s) {
+  const size_t smem = (size_t)3 * CB * PITCH * sizeof(double2);
+  const int64_t total = Np * Np * nprob;
+  k_chol_prep<<<grid_for(total, 256), 256, 0, s>>>(M, A, Np, total);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+  static bool set = false;
+  if (!set) {
+    CQ_CHECK_CUDA(cudaFuncSetAttribute(k_chol_inv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    set = true;
+  }
+  k_chol_inv<true><<<(unsigned)nprob, CT, smem, s>>>(M, A, logdet, trace, info, Np, kInvGroup / CB);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+void launch_chol_split(const double2* A, float2* Z, float2* Zl, float2* Zc, int64_t Np,
+                       int64_t nprob, cudaStream_t s) {
+  CQ_REQUIRE(nprob <= 65535, COQUI_B200_EINVAL, "chol_split: too many problems per launch");
+  const unsigned nt = (unsigned)((Np + 31) / 32);
+  k_chol_split<<<dim3(nt, nt, (unsigned)nprob), dim3(32, 8), 0, s>>>(A, Z, Zl, Zc, Np);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+void launch_block_adjoint(const float2* Z, float2* Zl, int64_t Np, int64_t r0, int64_t r1,
+                          int64_t b, int64_t b1, int64_t nprob, cudaStream_t s) {
+  CQ_REQUIRE(nprob <= 65535 && r0 + b <= r1 && r1 + b1 <= Np, COQUI_B200_EINVAL,
+             "block_adjoint: bad block");
+  const dim3 g((unsigned)((b1 + 31) / 32), (unsigned)((b + 31) / 32), (unsigned)nprob);
+  k_block_adjoint<<<g, dim3(32, 8), 0, s>>>(Z, Zl, Np, r0, r1, b, b1);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
 }

@@ -12,4 +12,22 @@ namespace cq {
 void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, double2* trace,
                      int* info, int64_t Np, int64_t nprob, cudaStream_t s);
 
+// Diagonal group edge of the FP64 inverse when the tensor cores form the off-group blocks.
+constexpr int64_t kInvGroup = 128;
+
+// As launch_chol_inv without Z, but the inverse U = C^{-H} is formed only inside the
+// kInvGroup x kInvGroup diagonal groups (upper triangle of A there).
+void launch_chol_group_inv(const float2* M, double2* A, double* logdet, double2* trace, int* info,
+                           int64_t Np, int64_t nprob, cudaStream_t s);
+
+// Complex64 operands of the tensor-core inverse levels (all Np x Np per problem):
+// Z = U - I (group upper triangles; 0 below the diagonal), Zl = U^H - I (group lower
+// triangles; 0 elsewhere), Zc = -C (strictly lower off-group blocks only).
+void launch_chol_split(const double2* A, float2* Z, float2* Zl, float2* Zc, int64_t Np,
+                       int64_t nprob, cudaStream_t s);
+
+// Zl[r1 + c][r0 + r] = conj(Z[r0 + r][r1 + c]), r < b, c < b1.
+void launch_block_adjoint(const float2* Z, float2* Zl, int64_t Np, int64_t r0, int64_t r1,
+                          int64_t b, int64_t b1, int64_t nprob, cudaStream_t s);
+
 }  // namespace cq

@@ -223,10 +223,15 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       }
       }
       // I - M = C C^H (FP64)
+      // above one kInvGroup the off-group blocks of the inverse come from the tensor cores
+      const bool tc_inverse = a.mixed && a.want_w && Np > kInvGroup;
       if (a.mixed) {
         Prof::Scope sc(a.prof, "dyson_chol_inv");
-        launch_chol_inv((const float2*)Mb, A, a.want_w ? (float2*)Y : nullptr, dld, dtr, dinfo, Np,
-                        nb, s);
+        if (tc_inverse)
+          launch_chol_group_inv((const float2*)Mb, A, dld, dtr, dinfo, Np, nb, s);
+        else
+          launch_chol_inv((const float2*)Mb, A, a.want_w ? (float2*)Y : nullptr, dld, dtr, dinfo,
+                          Np, nb, s);
       } else {
         Prof::Scope sc(a.prof, "dyson_potrf");
         potrf_ptrs(sol, dptrA, Np, dinfo, nb);
@@ -247,7 +252,38 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       if (a.want_w && a.mixed) {
         // W = L E L^H with E = (I - M)^{-1} - I = D + D^H + D^H D, D = C^{-1} - I: no
         // cancellation against V, so the split-TF32 products keep W to ~1e-8.
-        const float2* Z = (const float2*)Y;  // DH = C^{-H} - I from the FP64 factorisation
+        if (tc_inverse) {
+          // U = C^{-H} by doubling: FP64 inverses of the kInvGroup diagonal groups, then for
+          // each level b the pairs of diagonal blocks (r0: b, r1: b1) get
+          //   U01 = -U00 C10^H U11
+          // as two split-TF32 products.  Z holds U - I (the D^H of the W products), Zl holds
+          // U^H - I where a later level needs it, Zc = -C off the groups.
+          Prof::Scope sc(a.prof, "dyson_tc_inverse");
+          float2* Z = (float2*)Y;
+          float2* Zl = (float2*)Y + nbq * NN;
+          float2* Zc = (float2*)T1;
+          float2* S = (float2*)Mb;
+          launch_chol_split(A, Z, Zl, Zc, Np, nb, s);
+          for (int64_t b = kInvGroup; b < Np; b *= 2) {
+            for (int64_t r0 = 0; r0 + b < Np; r0 += 2 * b) {
+              const int64_t r1 = r0 + b, b1 = std::min(b, Np - r1);
+              // S = U00 (-C10)^H  (b x b1, K = b): A = Z + I on the 00 block (upper)
+              TcStructure t1;
+              t1.a_upper = true;
+              t1.a_ident = true;
+              tc_cgemm_nt(Z + r0 * Np + r0, false, false, Np, NN, Zc + r1 * Np + r0, false, true,
+                          Np, NN, S + r0 * Np + r1, Np, NN, b, b1, b, nb, s, t1);
+              // U01 = S U11 with U11(k, n) = conj(Zl[n][k]) + delta  (b x b1, K = b1)
+              TcStructure t2;
+              t2.b_upper = true;
+              t2.b_ident = true;
+              tc_cgemm_nt(S + r0 * Np + r1, false, false, Np, NN, Zl + r1 * Np + r1, false, true,
+                          Np, NN, Z + r0 * Np + r1, Np, NN, b, b1, b1, nb, s, t2);
+              if (2 * b < Np) launch_block_adjoint(Z, Zl, Np, r0, r1, b, b1, nb, s);
+            }
+          }
+        }
+        const float2* Z = (const float2*)Y;  // DH = C^{-H} - I
         Prof::Scope sc(a.prof, "dyson_W_gemm");
         float2* F = (float2*)T1;
         float2* E = (float2*)Mb;

@@ -69,6 +69,7 @@ struct TcParams {
   int a64, b64;  // element type is complex128
   int conj_a, conj_b;
   int a_upper, a_lower, b_lower, b_upper, lower_only;
+  int a_ident, b_ident;  // operand + identity (complex64 operands only)
   // periodic batch index (0 = off): operand batch = (q0 + b) % mod, for per-q operands
   int64_t a_mod, a_q0, b_mod, b_q0;
 };
@@ -175,6 +176,11 @@ template <> struct Pair<false> {
   __device__ __forceinline__ void get(float (&x)[4]) const {
     x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
   }
+  // adds 1 to the real part of the first (e = 0) or second (e = 1) value
+  __device__ __forceinline__ void add_one(int e) {
+    if (e == 0) v.x += 1.f;
+    else v.z += 1.f;
+  }
 };
 // Pre-split operand: one float4 (hi.re, hi.im, lo.re, lo.im) per complex value, hi/lo TF32.
 template <> struct Pair<true> {
@@ -187,6 +193,7 @@ template <> struct Pair<true> {
     if (row_ok && k < kmax) a = __ldg(p);
     if (row_ok && k + 1 < kmax) b = __ldg(p + 1);
   }
+  __device__ __forceinline__ void add_one(int) {}  // not used: rejected on the host
 };
 template <class Cfg, bool A64, bool B64> struct Staging {
   Pair<A64> a[Cfg::A_CHUNKS];
@@ -203,6 +210,10 @@ template <class Cfg, bool A64, bool B64> struct Staging {
       const int r = i >> 3, c = i & 7;
       const int64_t m = m0 + r, k = k0c + 2 * c;
       a[j].load(p.A, ba * p.sA + m * p.lda + k, k, p.K, m < p.M);
+      if (p.a_ident && m < p.M) {
+        if (m == k && k < p.K) a[j].add_one(0);
+        if (m == k + 1 && k + 1 < p.K) a[j].add_one(1);
+      }
     }
 #pragma unroll
     for (int j = 0; j < Cfg::B_CHUNKS; ++j) {
@@ -210,6 +221,10 @@ template <class Cfg, bool A64, bool B64> struct Staging {
       const int r = i >> 3, c = i & 7;
       const int64_t n = n0 + r, k = k0c + 2 * c;
       b[j].load(p.Bt, bb * p.sB + n * p.ldb + k, k, p.K, n < p.N);
+      if (p.b_ident && n < p.N) {
+        if (n == k && k < p.K) b[j].add_one(0);
+        if (n == k + 1 && k + 1 < p.K) b[j].add_one(1);
+      }
     }
   }
 
@@ -496,6 +511,10 @@ void tc_cgemm_nt(const void* A, bool a_split, bool conj_a, int64_t lda, int64_t 
   p.b_lower = st.b_lower;
   p.b_upper = st.b_upper;
   p.lower_only = st.lower_only;
+  CQ_REQUIRE(!(st.a_ident && a_c128) && !(st.b_ident && b_c128), COQUI_B200_EINVAL,
+             "tc_cgemm: identity shift needs a complex64 operand");
+  p.a_ident = st.a_ident;
+  p.b_ident = st.b_ident;
   p.a_mod = st.a_mod;
   p.a_q0 = st.a_q0;
   p.b_mod = st.b_mod;

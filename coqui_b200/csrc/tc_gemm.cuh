@@ -47,8 +47,11 @@ void to_split(const double2* in, float4* out, int64_t rows, int64_t cols, int64_
 //   lower_only: only tiles touching the lower triangle (m >= n) are written.
 // a_mod / b_mod (> 0): the operand's batch index is (q0 + b) % mod (per-q operands shared
 // by every frequency of a flattened (w, q) batch).
+// a_ident / b_ident: the operand is used as (stored values + identity), with the identity on
+// the operand's own diagonal (m == k for A, n == k for B); complex64 operands only.
 struct TcStructure {
   bool a_upper = false, a_lower = false, b_lower = false, b_upper = false, lower_only = false;
+  bool a_ident = false, b_ident = false;
   int64_t a_mod = 0, a_q0 = 0, b_mod = 0, b_q0 = 0;
 };
 

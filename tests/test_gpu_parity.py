@@ -136,6 +136,22 @@ def test_edge_cases(mode, tol, grid, nb, nocc, Np, lam):
     assert abs(c.rpa_energy(cs.G) - cs.e_rpa) < tol
 
 
+@pytest.mark.parametrize("grid,Np", [
+    (1, 300),  # groups 128 + 128 + 44: a ragged level-256 pair (256 x 44)
+    ((1, 1, 2), 512),  # two doubling levels (128, 256)
+])
+def test_dyson_tensor_core_inverse(grid, Np):
+    """Above 128 auxiliary functions the off-group blocks of C^{-1} come from the tensor
+    cores (mixed mode); W must stay within the mixed tolerance of the FP64 oracle."""
+    cs = Case(grid, 16, 8, Np, seed=13)
+    c = cs.ctx(capi.MIXED)
+    assert maxabs(c.dyson_w(cs.Pi_w), cs.W_w) < 1e-6
+    W, _ = c.update_w(cs.G)
+    assert maxabs(W, cs.dW) < 1e-6
+    assert maxabs(c.eval_sigma(cs.G), cs.Sigma) < 1e-6
+    c.close()
+
+
 def test_solver_mirror_matches_oracle(base):
     thc = solvers.THCData.from_synthetic(base.s)
     scr = solvers.scr_coulomb_t(base.pft)
