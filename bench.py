@@ -124,12 +124,13 @@ def algorithmic_work(w, s, ft):
     amount per iteration or None).  Flops count a complex multiply-add as 8 (FP64-equivalent
     count of the product actually formed, triangular structure included); bytes are the
     compulsory complex64 reads + writes."""
-    nk, nb, Np, nth, nwh = s.nk, s.nb, s.Np, ft.nt_half, ft.nw_half
+    nk, nb, Np, nth, nwh, nt = s.nk, s.nb, s.Np, ft.nt_half, ft.nw_half, ft.nt_f
     ncol, P = Np * Np, nk * nwh  # Dyson problems per iteration
     n3 = float(Np) ** 3
     return {
-        "proj_p2a": ("tensor", nk * (gemm_flops_c(Np, nb, nb) + gemm_flops_c(Np, Np, nb)), None),
-        "proj_a2p": ("tensor", nk * (gemm_flops_c(nb, Np, Np) + gemm_flops_c(nb, nb, Np)), None),
+        # every G(tau) projected once and every Sigma(tau) once (tau-batched launches)
+        "proj_p2a": ("tensor", None, nt * nk * (gemm_flops_c(Np, nb, nb) + gemm_flops_c(Np, Np, nb))),
+        "proj_a2p": ("tensor", None, nt * nk * (gemm_flops_c(nb, Np, Np) + gemm_flops_c(nb, nb, Np))),
         "pi_fused": ("hbm", 3 * nk * ncol * 8, None),
         "sigma_fused": ("hbm", 5 * nk * ncol * 8, None),
         "dft_w": ("hbm", 2 * nth * nk * ncol * 8, None),
@@ -138,8 +139,11 @@ def algorithmic_work(w, s, ft):
         "dyson_M_gemm": ("tensor", None, 0.75 * 8 * n3 * P),
         # F = D^H D (1/6), T = L E (1/2), W = T L^H (1/2)
         "dyson_W_gemm": ("tensor", None, (1 / 6 + 0.5 + 0.5) * 8 * n3 * P),
-        # Cholesky + triangular inverse: Np^3 / 3 complex multiply-adds
-        "dyson_chol_inv": ("fp64", None, 8 * n3 / 3 * P),
+        # FP64 Cholesky (Np^3 / 6 complex multiply-adds) + inverse of the 128 x 128 diagonal
+        # groups (Np 128^2 / 6); the whole inverse (Np^3 / 6) when Np <= 128
+        "dyson_chol_inv": ("fp64", None, 8 * (n3 / 6 + (Np * min(Np, 128) ** 2) / 6) * P),
+        # the rest of the triangular inverse on the tensor cores
+        "dyson_tc_inverse": ("tensor", None, 8 * max(0.0, n3 - Np * min(Np, 128) ** 2) / 6 * P),
     }
 
 

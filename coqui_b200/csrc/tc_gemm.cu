@@ -323,20 +323,37 @@ __global__ void __launch_bounds__(NP + 32, (NP == 128 ? 2 : 1)) k_tc_cgemm(TcPar
 
   bool ok = true;
   if (warp < Cfg::NPW) {
-    // ---------------- producers: register prefetch one stage ahead ----------------
-    Staging<Cfg, A64, B64> st;
-    if (nkb > 0) st.load(p, bz, m0, n0, (int64_t)kb_lo * 16);
-    for (int it = 0; it < nkb; ++it) {
+    // ---------------- producers: register prefetch ----------------
+    // Long K (eight producer warps): two register sets alternate, so a K block's global
+    // loads have two stage times to arrive before its split values go to shared memory.
+    // Short K (four producer warps, twice the values per thread): one set, one stage ahead.
+    constexpr int kAhead = (NP == 256) ? 2 : 1;
+    auto step = [&](Staging<Cfg, A64, B64>& st, int it) -> bool {
       const int s = it % kStages;
       const uint32_t ph = (uint32_t)(it / kStages) & 1u;
-      if (!mbar_wait(smem_u32(&bars[kStages + s]), ph ^ 1u)) { ok = false; break; }
+      if (!mbar_wait(smem_u32(&bars[kStages + s]), ph ^ 1u)) return false;
       unsigned char* sp = smem + s * Cfg::STAGE;
       const uint32_t a_hi = smem_u32(sp), a_lo = a_hi + Cfg::A_PLANE;
       const uint32_t b_hi = a_lo + Cfg::A_PLANE, b_lo = b_hi + Cfg::B_PLANE;
       st.store(p, a_hi, a_lo, b_hi, b_lo);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(smem_u32(&bars[s]));
-      if (it + 1 < nkb) st.load(p, bz, m0, n0, (int64_t)(kb_lo + it + 1) * 16);
+      if (it + kAhead < nkb) st.load(p, bz, m0, n0, (int64_t)(kb_lo + it + kAhead) * 16);
+      return true;
+    };
+    if constexpr (kAhead == 2) {
+      Staging<Cfg, A64, B64> st0, st1;
+      if (nkb > 0) st0.load(p, bz, m0, n0, (int64_t)kb_lo * 16);
+      if (nkb > 1) st1.load(p, bz, m0, n0, (int64_t)(kb_lo + 1) * 16);
+      for (int it = 0; it < nkb; it += 2) {
+        if (!step(st0, it)) { ok = false; break; }
+        if (it + 1 < nkb && !step(st1, it + 1)) { ok = false; break; }
+      }
+    } else {
+      Staging<Cfg, A64, B64> st0;
+      if (nkb > 0) st0.load(p, bz, m0, n0, (int64_t)kb_lo * 16);
+      for (int it = 0; it < nkb; ++it)
+        if (!step(st0, it)) { ok = false; break; }
     }
     // ---------------- epilogue: TMEM -> registers -> smem -> coalesced rows ----------------
     const int q = warp & 3;  // TMEM lane quadrant
