@@ -28,6 +28,9 @@ SYMBOLS = [
     "coqui_b200_w_to_tau", "coqui_b200_dyson_w", "coqui_b200_last_timings",
     "coqui_b200_kernel_launches", "coqui_b200_gw_iteration", "coqui_b200_set_profiling",
     "coqui_b200_kernel_stats", "coqui_b200_primary_to_aux_noalloc",
+    "coqui_b200_set_ir_fermi", "coqui_b200_set_mean_field", "coqui_b200_set_iter_alg",
+    "coqui_b200_scgw_iteration", "coqui_b200_get_scgw_state", "coqui_b200_dyson_g",
+    "coqui_b200_gm_energy",
 ]
 
 
@@ -81,6 +84,14 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_primary_to_aux_noalloc.argtypes = [P, P, P, ctypes.c_int64, ctypes.c_int64,
                                                       ctypes.c_int64, P, ctypes.c_char_p,
                                                       ctypes.c_int]
+    D, I64 = ctypes.c_double, ctypes.c_int64
+    lib.coqui_b200_set_ir_fermi.argtypes = [P, P, P, P, I64, D]
+    lib.coqui_b200_set_mean_field.argtypes = [P, P, P, P, D]
+    lib.coqui_b200_set_iter_alg.argtypes = [P, ctypes.c_int, D, I64, I64]
+    lib.coqui_b200_scgw_iteration.argtypes = [P, P, I64, P]
+    lib.coqui_b200_get_scgw_state.argtypes = [P, P, P, P]
+    lib.coqui_b200_dyson_g.argtypes = [P, P, P, P]
+    lib.coqui_b200_gm_energy.argtypes = [P, P, P, ctypes.POINTER(D)]
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -141,6 +152,58 @@ class Context:
         x = np.ascontiguousarray(ft.tau_mesh_x, np.float64)
         self._check(self.lib.coqui_b200_set_ir(self.h, _ptr(Twt, "Twt"), _ptr(Ttw, "Ttw"),
                                                _ptr(Tb, "Tb"), _ptr(x, "tau")))
+
+    def set_ir_fermi(self, ft):
+        """Fermionic IR tables of the self-consistent loop (Twt_ff, Ttw_ff, wn_mesh_f, beta)."""
+        nt, nw = self.nt, int(ft.Twt_ff.shape[0])
+        Twt = _c128(ft.Twt_ff, (nw, nt), "Twt_ff")
+        Ttw = _c128(ft.Ttw_ff, (nt, nw), "Ttw_ff")
+        wn = np.ascontiguousarray(ft.wn_mesh_f, np.int64).reshape(nw)
+        self.nw_f = nw
+        self._check(self.lib.coqui_b200_set_ir_fermi(self.h, _ptr(Twt, "Twt"), _ptr(Ttw, "Ttw"),
+                                                     _ptr(wn, "wn"), nw, float(ft.beta)))
+
+    def set_mean_field(self, H0, S, F, mu=0.0):
+        sh = (1, self.nk, self.nb, self.nb)
+        H0, S, F = _c128(H0, sh, "H0"), _c128(S, sh, "S"), _c128(F, sh, "F")
+        self._check(self.lib.coqui_b200_set_mean_field(self.h, _ptr(H0, "H0"), _ptr(S, "S"),
+                                                       _ptr(F, "F"), float(mu)))
+
+    def set_iter_alg(self, alg="damping", mixing=0.7, max_subsp=5, diis_start=5):
+        a = {"damping": 0, "diis": 1}[alg]
+        self._check(self.lib.coqui_b200_set_iter_alg(self.h, a, float(mixing), int(max_subsp),
+                                                     int(diis_start)))
+
+    def scgw_iteration(self, it, G=None):
+        """One self-consistent GW iteration; G (iteration 1) uploads the starting G."""
+        G = None if G is None else self._G(G)
+        st = np.zeros(5, np.float64)
+        self._check(self.lib.coqui_b200_scgw_iteration(self.h, _ptr(G, "G"), int(it), _ptr(st, "st")))
+        return dict(conv_F=st[0], conv_Sigma=st[1], e_1e=st[2], e_hf=st[3], e_corr=st[4],
+                    e_tot=st[2] + st[3] + st[4])
+
+    def get_scgw_state(self):
+        G = np.empty((self.nt, 1, self.nk, self.nb, self.nb), np.complex128)
+        S = np.empty_like(G)
+        Dm = np.empty((1, self.nk, self.nb, self.nb), np.complex128)
+        self._check(self.lib.coqui_b200_get_scgw_state(self.h, _ptr(G, "G"), _ptr(S, "S"),
+                                                       _ptr(Dm, "Dm")))
+        return G, S, Dm
+
+    def dyson_g(self, Sigma):
+        S = self._G(Sigma)
+        G = np.empty_like(S)
+        Dm = np.empty((1, self.nk, self.nb, self.nb), np.complex128)
+        self._check(self.lib.coqui_b200_dyson_g(self.h, _ptr(S, "Sigma"), _ptr(G, "G"),
+                                                _ptr(Dm, "Dm")))
+        return G, Dm
+
+    def gm_energy(self, G, Sigma):
+        G, S = self._G(G), self._G(Sigma)
+        e = ctypes.c_double(0.0)
+        self._check(self.lib.coqui_b200_gm_energy(self.h, _ptr(G, "G"), _ptr(S, "Sigma"),
+                                                  ctypes.byref(e)))
+        return e.value
 
     def set_kmesh(self, kpts, lattv, chi_bar=None):
         k = np.ascontiguousarray(kpts, np.float64).reshape(self.nk, 3)

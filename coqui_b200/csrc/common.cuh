@@ -79,6 +79,10 @@ inline unsigned grid_for(int64_t n, int block, int64_t cap = 148 * 64) {
 template <typename T> struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
   void ensure(size_t count) {
     if (count <= n) return;
     release();

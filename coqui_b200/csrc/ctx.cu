@@ -20,6 +20,7 @@
 
 #include "dyson.cuh"
 #include "kernels.cuh"
+#include "scgw.cuh"
 #include "tc_gemm.cuh"
 
 using cq::Error;
@@ -87,6 +88,28 @@ struct coqui_b200_ctx {
   // place) by the self-energy of the same G; allocated when it fits in half the free memory
   DevBuf<unsigned char> Gcache;
   bool gcache_valid = false;
+
+  // self-consistent loop: fermionic IR grid, mean field, iteration state
+  bool have_irf = false, have_mf = false;
+  int64_t nwf = 0;
+  double beta = 0, mu = 0;
+  std::vector<int64_t> wnf;
+  std::vector<double2> Ttw_ff_h;           // (nt, nwf)
+  DevBuf<int64_t> dwnf;
+  DevBuf<double2> dTwt_ff, dTtw_ff;        // (nwf, nt), (nt, nwf)
+  DevBuf<double2> H0, Sov, F, F_mf, Dm;    // (nk, nb, nb)
+  DevBuf<double2> Gw, Sw, Xw;              // (nwf, nk, nb, nb)
+  DevBuf<double2> Gin;                     // G(tau) that produced the current Sigma
+  DevBuf<double2> FS, prevFS;              // this / the previous iteration's (F, Sigma)
+  DevBuf<int> ginfo;
+  DevBuf<double> red;
+  DevBuf<double2> trc;
+  int iter_alg = 0;                        // 0 damping, 1 commutator DIIS
+  double mixing = 0.7;
+  int64_t max_subsp = 5, diis_start = 5;
+  std::vector<std::unique_ptr<DevBuf<double2>>> dx;  // DIIS x-vectors (F then Sigma)
+  std::vector<std::unique_ptr<DevBuf<double2>>> dr;  // DIIS residuals (Sigma part)
+  std::vector<std::complex<double>> dB;              // residual overlaps (row-major nB x nB)
 
   // pipelined host transfers: G arrives in tau chunks on the copy stream (one event per
   // chunk) and Sigma leaves chunk by chunk while later chunks are computed
@@ -400,6 +423,213 @@ double rpa_energy_from(Ctx* c, const std::vector<double>& logdet, const std::vec
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------------------
+// self-consistent loop (scf_driver.cpp:90-173 for GW, hf = nullptr, constant mu)
+// ---------------------------------------------------------------------------------------
+// Fermionic IR transforms of n columns: out (nwf, n) = Twt_ff in (nt, n) and back.
+void tau_to_w_ff(Ctx* c, const double2* in, double2* out, int64_t n) {
+  zgemm_rm(c, 'N', 'N', c->nwf, n, c->nt, make_double2(1, 0), c->dTwt_ff.p, c->nt, 0, in, n, 0,
+           make_double2(0, 0), out, n, 0, 1);
+}
+void w_to_tau_ff(Ctx* c, const double2* in, double2* out, int64_t n) {
+  zgemm_rm(c, 'N', 'N', c->nt, n, c->nwf, make_double2(1, 0), c->dTtw_ff.p, c->nwf, 0, in, n, 0,
+           make_double2(0, 0), out, n, 0, 1);
+}
+
+void require_scgw(Ctx* c) {
+  require_ready(c, true, true, true);
+  CQ_REQUIRE(c->have_irf, COQUI_B200_EINVAL, "set_ir_fermi not called");
+  CQ_REQUIRE(c->have_mf, COQUI_B200_EINVAL, "set_mean_field not called");
+}
+
+// simple_dyson.cpp:66-123 with the hermitization of scf_driver.cpp:140-143: c->G <- G(tau)
+// from Sigma(tau) (device, (nt, nk, nb, nb)), c->Dm <- -G(beta^-).
+void dyson_g_device(Ctx* c, const double2* Sig) {
+  cq::Prof::Scope sc(&c->prof, "scgw_dyson_g");
+  const int64_t nk = c->nk, nb = c->nb, ncol = nk * nb * nb, nw = c->nwf;
+  c->Sw.ensure(nw * ncol);
+  c->Xw.ensure(nw * ncol);
+  c->ginfo.ensure(nw * nk);
+  c->G.ensure(c->nt * ncol);
+  c->Dm.ensure(ncol);
+  tau_to_w_ff(c, Sig, c->Sw.p, ncol);
+  cq::build_dyson_matrix(c->Sov.p, c->H0.p, c->F.p, c->Sw.p, c->Xw.p, c->dwnf.p, c->beta, c->mu,
+                         nw, nk, nb, c->st);
+  cq::invert_batched(c->Xw.p, nb, nw * nk, c->ginfo.p, c->blas, c->st);
+  w_to_tau_ff(c, c->Xw.p, c->G.p, ncol);
+  // Dm = -sum_t T_beta(t) G(t)  (IAFT.icc:226-238, simple_dyson.cpp:119-121)
+  c->trc.ensure(c->nt);
+  upload(c, c->trc.p, c->T_beta.data(), c->nt * sizeof(double2));
+  zgemm_rm(c, 'N', 'N', 1, ncol, c->nt, make_double2(-1, 0), c->trc.p, c->nt, 0, c->G.p, ncol, 0,
+           make_double2(0, 0), c->Dm.p, ncol, 0, 1);
+  cq::hermitize_c128(c->Dm.p, nb, nk, c->st);
+  cq::hermitize_c128(c->G.p, nb, c->nt * nk, c->st);
+  std::vector<int> info(nw * nk);
+  CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), c->ginfo.p, info.size() * sizeof(int),
+                                cudaMemcpyDeviceToHost, c->st));
+  CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+  for (int v : info)
+    CQ_REQUIRE(v == 0, COQUI_B200_ENOTHPD, "singular Dyson matrix (i w + mu) S - H0 - F - Sigma");
+  // the resident G changed: no pipelined chunks, no cached projections
+  c->g_resident = true;
+  c->g_pipelined = false;
+  c->gcache_valid = false;
+}
+
+// sum_k w_k sum_ij A_ij B_ji per leading index (w_k = 1/nk): out (nlead)
+std::vector<std::complex<double>> k_traces(Ctx* c, const double2* A, const double2* B, int64_t nlead,
+                                           int64_t b_mod) {
+  const int64_t nk = c->nk, nb = c->nb;
+  c->trc.ensure(nlead * nk);
+  cq::trace_products(A, B, c->trc.p, nb, nlead * nk, b_mod, c->st);
+  std::vector<double2> h(nlead * nk);
+  CQ_CHECK_CUDA(cudaMemcpyAsync(h.data(), c->trc.p, h.size() * sizeof(double2),
+                                cudaMemcpyDeviceToHost, c->st));
+  CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+  std::vector<std::complex<double>> out(nlead, 0.0);
+  for (int64_t l = 0; l < nlead; ++l)
+    for (int64_t k = 0; k < nk; ++k)
+      out[l] += std::complex<double>(h[l * nk + k].x, h[l * nk + k].y) / (double)nk;
+  return out;
+}
+
+// Galitskii-Migdal energy (scf_common.cpp:87-136) of G(tau), Sigma(tau) on the device.
+double gm_energy_device(Ctx* c, const double2* G, const double2* Sig) {
+  cq::Prof::Scope sc(&c->prof, "scgw_energy");
+  const int64_t ncol = c->nk * c->nb * c->nb, nw = c->nwf;
+  c->Sw.ensure(nw * ncol);
+  c->Gw.ensure(nw * ncol);
+  tau_to_w_ff(c, Sig, c->Sw.p, ncol);
+  tau_to_w_ff(c, G, c->Gw.p, ncol);
+  const auto e_w = k_traces(c, c->Sw.p, c->Gw.p, nw, 0);
+  std::complex<double> e = 0;
+  for (int64_t t = 0; t < c->nt; ++t) {
+    std::complex<double> et = 0;
+    for (int64_t w = 0; w < nw; ++w) {
+      const double2 T = c->Ttw_ff_h[t * nw + w];
+      et += std::complex<double>(T.x, T.y) * e_w[w];
+    }
+    e += std::complex<double>(c->T_beta[t].x, c->T_beta[t].y) * et;
+  }
+  return (-0.5 * 2.0 * e).real();  // spin factor 2 for ns = 1
+}
+
+// e_1e = 2 sum_k w_k Tr[Dm H0], e_hf = 2 sum_k w_k Tr[Dm F] / 2 (scf_common.cpp:44-77)
+void hf_energy_device(Ctx* c, double* e_1e, double* e_hf) {
+  *e_1e = 2.0 * k_traces(c, c->Dm.p, c->H0.p, 1, 0)[0].real();
+  *e_hf = 2.0 * 0.5 * k_traces(c, c->Dm.p, c->F.p, 1, 0)[0].real();
+}
+
+// Commutator residual (vspace_fock_sigma.hpp commutator_t) of (F, Sigma) with G_in:
+// out(tau) = w_to_tau[G(iw) X(iw) - X(iw) G(iw)], X = (iw + mu) S - H0 - F - Sigma(iw).
+void commutator_device(Ctx* c, const double2* F, const double2* Sig, const double2* Gin,
+                       double2* out) {
+  const int64_t nk = c->nk, nb = c->nb, ncol = nk * nb * nb, nw = c->nwf;
+  c->Sw.ensure(nw * ncol);
+  c->Gw.ensure(nw * ncol);
+  c->Xw.ensure(nw * ncol);
+  tau_to_w_ff(c, Gin, c->Gw.p, ncol);
+  tau_to_w_ff(c, Sig, c->Sw.p, ncol);
+  cq::build_dyson_matrix(c->Sov.p, c->H0.p, F, c->Sw.p, c->Xw.p, c->dwnf.p, c->beta, c->mu, nw, nk,
+                         nb, c->st);
+  // C = G X, then C -= X G (C in the Sigma(iw) buffer)
+  zgemm_rm(c, 'N', 'N', nb, nb, nb, make_double2(1, 0), c->Gw.p, nb, nb * nb, c->Xw.p, nb, nb * nb,
+           make_double2(0, 0), c->Sw.p, nb, nb * nb, nw * nk);
+  zgemm_rm(c, 'N', 'N', nb, nb, nb, make_double2(-1, 0), c->Xw.p, nb, nb * nb, c->Gw.p, nb, nb * nb,
+           make_double2(1, 0), c->Sw.p, nb, nb * nb, nw * nk);
+  w_to_tau_ff(c, c->Sw.p, out, ncol);
+}
+
+// Commutator DIIS step (diis_t::solve, diis_t.hpp:58-100) on the device vectors.  FS holds
+// (F, Sigma) contiguous; returns (conv_F, conv_Sigma) and overwrites FS with the new state.
+std::pair<double, double> diis_device(Ctx* c, double2* FS, int64_t it) {
+  const int64_t nF = c->nk * c->nb * c->nb, nS = c->nt * nF, nFS = nF + nS;
+  auto new_vec = [&](int64_t n) {
+    auto b = std::make_unique<DevBuf<double2>>();
+    b->ensure(n);
+    return b;
+  };
+  auto copy = [&](double2* dst, const double2* src, int64_t n) {
+    CQ_CHECK_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  };
+  auto damping = [&]() {
+    const double m = c->mixing;
+    cq::axpby_c128(c->prevFS.p, FS, 1.0 - m, m, nFS, c->st);
+    return std::make_pair(cq::maxabs_diff(c->prevFS.p, FS, nF, c->red, c->st),
+                          cq::maxabs_diff(c->prevFS.p + nF, FS + nF, nS, c->red, c->st));
+  };
+  // add (x = FS, residual of FS) to the subspaces, dropping the oldest pair when full
+  auto add_residual = [&]() {
+    if ((int64_t)c->dr.size() >= c->max_subsp) {
+      c->dr.erase(c->dr.begin());
+      c->dx.erase(c->dx.begin());
+      const int64_t n = (int64_t)std::llround(std::sqrt((double)c->dB.size()));
+      std::vector<std::complex<double>> B((n - 1) * (n - 1));
+      for (int64_t i = 1; i < n; ++i)
+        for (int64_t j = 1; j < n; ++j) B[(i - 1) * (n - 1) + (j - 1)] = c->dB[i * n + j];
+      c->dB = B;
+    }
+    auto r = new_vec(nS);
+    commutator_device(c, FS, FS + nF, c->Gin.p, r->p);
+    const int64_t n = (int64_t)c->dr.size();
+    std::vector<std::complex<double>> B((n + 1) * (n + 1));
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t j = 0; j < n; ++j) B[i * (n + 1) + j] = c->dB[i * n + j];
+    for (int64_t i = 0; i < n; ++i) {
+      const std::complex<double> o = cq::dotc(c->dr[i]->p, r->p, nS, c->red, c->st);
+      B[i * (n + 1) + n] = o;
+      B[n * (n + 1) + i] = std::conj(o);
+    }
+    B[n * (n + 1) + n] = cq::dotc(r->p, r->p, nS, c->red, c->st);
+    c->dB = B;
+    c->dr.push_back(std::move(r));
+    auto x = new_vec(nFS);
+    copy(x->p, FS, nFS);
+    c->dx.push_back(std::move(x));
+  };
+  if ((int64_t)c->dx.size() == 1 || it < c->diis_start) {
+    if (c->dx.size() <= 1) {
+      auto x = new_vec(nFS);
+      copy(x->p, FS, nFS);
+      c->dx.push_back(std::move(x));
+    } else {
+      add_residual();
+    }
+    return damping();
+  }
+  add_residual();
+  const int64_t n = (int64_t)c->dr.size();
+  if (n <= 1) return damping();
+  // compute_coefs_c1 (diis_alg.hpp:330-370): pseudo-inverse of Re B on its eigenbasis
+  std::vector<double> B(n * n);
+  for (int64_t i = 0; i < n * n; ++i) B[i] = c->dB[i].real();
+  std::vector<double> ev, U;
+  cq::sym_eigen(B, n, ev, U);
+  const double emax = *std::max_element(ev.begin(), ev.end());
+  const double emin = *std::min_element(ev.begin(), ev.end());
+  const double cond = emax / emin;
+  std::vector<double> xcoef(n, 0.0);
+  for (int64_t k = 0; k < n; ++k) {
+    if (!(ev[k] * cond > 1e-12)) continue;
+    double proj = 0;  // u_k . 1
+    for (int64_t i = 0; i < n; ++i) proj += U[i * n + k];
+    for (int64_t i = 0; i < n; ++i) xcoef[i] += U[i * n + k] * proj / ev[k];
+  }
+  double sum = 0;
+  for (double v : xcoef) sum += v;
+  // make_linear_comb (vspace.h): coefficients aligned with the newest x-vectors
+  c->Sw.ensure(std::max<int64_t>(nFS, c->nwf * nF));
+  double2* R = c->Sw.p;
+  CQ_CHECK_CUDA(cudaMemsetAsync(R, 0, nFS * sizeof(double2), c->st));
+  const int64_t nx = (int64_t)c->dx.size();
+  for (int64_t i = 0; i < std::min(nx, n); ++i)
+    cq::axpy_c128(c->dx[nx - 1 - i]->p, R, make_double2(xcoef[n - 1 - i] / sum, 0.0), nFS, c->st);
+  const double cF = cq::maxabs_diff(FS, R, nF, c->red, c->st);
+  const double cS = cq::maxabs_diff(FS + nF, R + nF, nS, c->red, c->st);
+  copy(FS, R, nFS);
+  return {cF, cS};
+}
 
 // =======================================================================================
 // ABI
@@ -1095,6 +1325,177 @@ int coqui_b200_dyson_w(coqui_b200_ctx* c, const double* Pi_wqPQ, double* W_wqPQ)
     }
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->w_valid = false;
+  });
+}
+
+
+int coqui_b200_set_ir_fermi(coqui_b200_ctx* c, const double* Twt_ff, const double* Ttw_ff,
+                            const int64_t* wn_mesh_f, int64_t nw_f, double beta) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(Twt_ff && Ttw_ff && wn_mesh_f && nw_f >= 1 && beta > 0, COQUI_B200_EINVAL,
+               "bad fermionic IR tables");
+    const int64_t nt = c->nt;
+    c->nwf = nw_f;
+    c->beta = beta;
+    c->wnf.assign(wn_mesh_f, wn_mesh_f + nw_f);
+    c->Ttw_ff_h.resize(nt * nw_f);
+    for (int64_t i = 0; i < nt * nw_f; ++i) c->Ttw_ff_h[i] = make_double2(Ttw_ff[2 * i], Ttw_ff[2 * i + 1]);
+    c->dTwt_ff.ensure(nw_f * nt);
+    c->dTtw_ff.ensure(nt * nw_f);
+    c->dwnf.ensure(nw_f);
+    upload(c, c->dTwt_ff.p, Twt_ff, nw_f * nt * sizeof(double2));
+    upload(c, c->dTtw_ff.p, Ttw_ff, nt * nw_f * sizeof(double2));
+    upload(c, c->dwnf.p, wn_mesh_f, nw_f * sizeof(int64_t));
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->have_irf = true;
+  });
+}
+
+int coqui_b200_set_mean_field(coqui_b200_ctx* c, const double* H0_skij, const double* S_skij,
+                              const double* F_skij, double mu) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(H0_skij && S_skij && F_skij, COQUI_B200_EINVAL, "null mean-field arrays");
+    const int64_t n = c->nk * c->nb * c->nb;
+    for (auto* b : {&c->H0, &c->Sov, &c->F, &c->F_mf}) b->ensure(n);
+    upload(c, c->H0.p, H0_skij, n * sizeof(double2));
+    upload(c, c->Sov.p, S_skij, n * sizeof(double2));
+    upload(c, c->F.p, F_skij, n * sizeof(double2));
+    upload(c, c->F_mf.p, F_skij, n * sizeof(double2));
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    c->mu = mu;
+    c->have_mf = true;
+    c->dx.clear();
+    c->dr.clear();
+    c->dB.clear();
+  });
+}
+
+int coqui_b200_set_iter_alg(coqui_b200_ctx* c, int alg, double mixing, int64_t max_subsp,
+                            int64_t diis_start) {
+  return guarded(c, [&] {
+    CQ_REQUIRE((alg == 0 || alg == 1) && mixing > 0 && mixing <= 1 && max_subsp >= 2,
+               COQUI_B200_EINVAL, "bad iteration parameters");
+    c->iter_alg = alg;
+    c->mixing = mixing;
+    c->max_subsp = max_subsp;
+    c->diis_start = diis_start;
+  });
+}
+
+int coqui_b200_scgw_iteration(coqui_b200_ctx* c, const double* G_tskij, int64_t it, double* stats) {
+  return guarded(c, [&] {
+    require_scgw(c);
+    CQ_REQUIRE(it >= 1 && stats, COQUI_B200_EINVAL, "bad iteration arguments");
+    const int64_t nF = c->nk * c->nb * c->nb, nS = c->nt * nF;
+    CQ_REQUIRE(it == 1 || c->prevFS.n >= (size_t)(nF + nS), COQUI_B200_EINVAL,
+               "iteration > 1 without a previous iteration");
+    c->begin_timing();
+    upload_G(c, G_tskij);
+    c->mark("h2d_G");
+    if (c->iter_alg == 1) {  // the residual of this step is taken with the incoming G
+      c->Gin.ensure(nS);
+      CQ_CHECK_CUDA(cudaMemcpyAsync(c->Gin.p, c->G.p, nS * sizeof(double2),
+                                    cudaMemcpyDeviceToDevice, c->st));
+    }
+    update_w_device(c);
+    sigma_device(c, nullptr);
+    // scf_driver.cpp:126-129
+    cq::hermitize_c128(c->F.p, c->nb, c->nk, c->st);
+    cq::hermitize_c128(c->Sig.p, c->nb, c->nt * c->nk, c->st);
+    c->FS.ensure(nF + nS);
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->FS.p, c->F.p, nF * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->FS.p + nF, c->Sig.p, nS * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, c->st));
+    double cF = 0, cS = 0;
+    {
+      cq::Prof::Scope sc(&c->prof, "scgw_iterate");
+      if (it == 1) {  // solve_iterative, it == 1 (scf_common.cpp:320-347)
+        cF = cq::maxabs_diff(c->F_mf.p, c->FS.p, nF, c->red, c->st);
+        cS = cq::maxabs_diff(c->FS.p + nF, nullptr, nS, c->red, c->st);
+        c->dx.clear();
+        c->dr.clear();
+        c->dB.clear();
+        if (c->iter_alg == 1) {
+          auto x = std::make_unique<DevBuf<double2>>();
+          x->ensure(nF + nS);
+          CQ_CHECK_CUDA(cudaMemcpyAsync(x->p, c->FS.p, (nF + nS) * sizeof(double2),
+                                        cudaMemcpyDeviceToDevice, c->st));
+          c->dx.push_back(std::move(x));
+        }
+      } else if (c->iter_alg == 0) {  // damp_t (damp_t.hpp:34-57)
+        const double m = c->mixing;
+        cq::axpby_c128(c->prevFS.p, c->FS.p, 1.0 - m, m, nF + nS, c->st);
+        cF = cq::maxabs_diff(c->prevFS.p, c->FS.p, nF, c->red, c->st);
+        cS = cq::maxabs_diff(c->prevFS.p + nF, c->FS.p + nF, nS, c->red, c->st);
+      } else {
+        std::tie(cF, cS) = diis_device(c, c->FS.p, it);
+      }
+    }
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->F.p, c->FS.p, nF * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->Sig.p, c->FS.p + nF, nS * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, c->st));
+    c->prevFS.ensure(nF + nS);
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->prevFS.p, c->FS.p, (nF + nS) * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, c->st));
+    c->mark("ITERATIVE");
+    dyson_g_device(c, c->Sig.p);
+    c->mark("DYSON");
+    double e1 = 0, ehf = 0;
+    hf_energy_device(c, &e1, &ehf);
+    const double ec = gm_energy_device(c, c->G.p, c->Sig.p);
+    c->mark("ENERGIES");
+    stats[0] = cF;
+    stats[1] = cS;
+    stats[2] = e1;
+    stats[3] = ehf;
+    stats[4] = ec;
+    c->end_timing();
+  });
+}
+
+int coqui_b200_get_scgw_state(coqui_b200_ctx* c, double* G_tskij, double* Sigma_tskij,
+                              double* Dm_skij) {
+  return guarded(c, [&] {
+    const int64_t nF = c->nk * c->nb * c->nb, nS = c->nt * nF;
+    if (G_tskij) {
+      CQ_REQUIRE(c->g_resident && c->G.n >= (size_t)nS, COQUI_B200_EINVAL, "no resident G");
+      download(c, G_tskij, c->G.p, nS * sizeof(double2));
+    }
+    if (Sigma_tskij) {
+      CQ_REQUIRE(c->Sig.n >= (size_t)nS, COQUI_B200_EINVAL, "no self-energy yet");
+      download(c, Sigma_tskij, c->Sig.p, nS * sizeof(double2));
+    }
+    if (Dm_skij) {
+      CQ_REQUIRE(c->Dm.n >= (size_t)nF, COQUI_B200_EINVAL, "no density matrix yet");
+      download(c, Dm_skij, c->Dm.p, nF * sizeof(double2));
+    }
+  });
+}
+
+int coqui_b200_dyson_g(coqui_b200_ctx* c, const double* Sigma_tskij, double* G_tskij,
+                       double* Dm_skij) {
+  return guarded(c, [&] {
+    require_scgw(c);
+    CQ_REQUIRE(Sigma_tskij, COQUI_B200_EINVAL, "null Sigma");
+    const int64_t nF = c->nk * c->nb * c->nb, nS = c->nt * nF;
+    c->Sig.ensure(nS);
+    upload(c, c->Sig.p, Sigma_tskij, nS * sizeof(double2));
+    dyson_g_device(c, c->Sig.p);
+    if (G_tskij) download(c, G_tskij, c->G.p, nS * sizeof(double2));
+    if (Dm_skij) download(c, Dm_skij, c->Dm.p, nF * sizeof(double2));
+  });
+}
+
+int coqui_b200_gm_energy(coqui_b200_ctx* c, const double* G_tskij, const double* Sigma_tskij,
+                         double* e_corr) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(c->have_irf && G_tskij && Sigma_tskij && e_corr, COQUI_B200_EINVAL,
+               "bad arguments (set_ir_fermi first)");
+    const int64_t nS = c->nt * c->nk * c->nb * c->nb;
+    c->stage.ensure(2 * nS);
+    upload(c, c->stage.p, G_tskij, nS * sizeof(double2));
+    upload(c, c->stage.p + nS, Sigma_tskij, nS * sizeof(double2));
+    *e_corr = gm_energy_device(c, c->stage.p, c->stage.p + nS);
   });
 }
 

@@ -50,6 +50,17 @@ class SyntheticSystem:
     def nk(self) -> int:
         return int(self.kpts.shape[0])
 
+    def mean_field(self):
+        """(H0, S, F) of the synthetic mean field, each (1, nk, nb, nb) complex128: H0 holds
+        the orbital energies (C = I), S = I, and the Fock part is zero (the loop runs with a
+        fixed mean-field Fock, scf_driver.cpp:94 with hf = nullptr)."""
+        nk, nb = self.eps.shape[1], self.nb
+        H0 = np.zeros((1, nk, nb, nb), np.complex128)
+        idx = np.arange(nb)
+        H0[0][:, idx, idx] = self.eps[0]
+        S = np.broadcast_to(np.eye(nb, dtype=np.complex128), (1, nk, nb, nb)).copy()
+        return H0, S, np.zeros_like(H0)
+
     def G0(self, ft: IAFT) -> np.ndarray:
         """G0_tskij(tau) for C = I (diagonal), qp_scf_common.cpp:86-93."""
         tau = ft.tau_mesh()

@@ -122,6 +122,49 @@ COQUI_B200_API int coqui_b200_rpa_energy(coqui_b200_ctx* ctx, const double* G_ts
 COQUI_B200_API int coqui_b200_gw_iteration(coqui_b200_ctx* ctx, const double* G_tskij,
                                            double* Sigma_tskij, double* eps_inv_head);
 
+/* ---- self-consistent GW loop (scf_loop, src/methods/SCF/scf_driver.cpp:90-173, for GW with
+   hf = nullptr and a constant chemical potential) ---- */
+
+/* Fermionic IR tables, rescaled by beta as in ir_driver.hpp:68-73: Twt_ff (nw_f, nt_f) and
+   Ttw_ff (nt_f, nw_f) complex128, wn_mesh_f (nw_f) Matsubara integers (omega_n = pi wn / beta,
+   IAFT.hpp:55-57). */
+COQUI_B200_API int coqui_b200_set_ir_fermi(coqui_b200_ctx* ctx, const double* Twt_ff,
+                                           const double* Ttw_ff, const int64_t* wn_mesh_f,
+                                           int64_t nw_f, double beta);
+
+/* Mean field of the loop: H0_skij, S_skij, F_skij (ns, nk, nb, nb) complex128 (F without H0,
+   kept fixed as with hf = nullptr) and the chemical potential mu. */
+COQUI_B200_API int coqui_b200_set_mean_field(coqui_b200_ctx* ctx, const double* H0_skij,
+                                             const double* S_skij, const double* F_skij, double mu);
+
+/* Iteration algorithm of solve_iterative (scf_common.cpp:229-355): alg 0 = damping
+   (damp_t.hpp:34-48, mixing), 1 = commutator DIIS (diis_t.hpp:58-100; mixing of its damping
+   steps, max_subsp, diis_start). */
+COQUI_B200_API int coqui_b200_set_iter_alg(coqui_b200_ctx* ctx, int alg, double mixing,
+                                           int64_t max_subsp, int64_t diis_start);
+
+/* One loop iteration it (>= 1): update_w, Sigma, hermitize, damping/DIIS, Dyson for G
+   (simple_dyson.cpp:11-123, G stays resident for the next iteration), energies.
+   G_tskij != NULL uploads the starting G (iteration 1).  stats[5] = max|dF|, max|dSigma|,
+   e_1e, e_hf, e_corr (Galitskii-Migdal, scf_common.cpp:87-136). */
+COQUI_B200_API int coqui_b200_scgw_iteration(coqui_b200_ctx* ctx, const double* G_tskij,
+                                             int64_t it, double* stats);
+
+/* Copies of the loop state: G_tskij, Sigma_tskij (nt_f, ns, nk, nb, nb), Dm_skij
+   (ns, nk, nb, nb); NULL entries are skipped. */
+COQUI_B200_API int coqui_b200_get_scgw_state(coqui_b200_ctx* ctx, double* G_tskij,
+                                             double* Sigma_tskij, double* Dm_skij);
+
+/* Dyson equation for G from Sigma_tskij (simple_dyson::solve_dyson + Dm = -G(beta^-)); the
+   result replaces the resident G.  G_tskij / Dm_skij outputs may be NULL. */
+COQUI_B200_API int coqui_b200_dyson_g(coqui_b200_ctx* ctx, const double* Sigma_tskij,
+                                      double* G_tskij, double* Dm_skij);
+
+/* Galitskii-Migdal correlation energy of G_tskij and Sigma_tskij (eval_corr_energy,
+   scf_common.cpp:87-136; k weights 1/nk). */
+COQUI_B200_API int coqui_b200_gm_energy(coqui_b200_ctx* ctx, const double* G_tskij,
+                                        const double* Sigma_tskij, double* e_corr);
+
 /* Building blocks (same layouts as the reference's arguments). */
 COQUI_B200_API int coqui_b200_primary_to_aux(coqui_b200_ctx* ctx, int64_t n_tau, const double* O_tskab,
                               double* O_tskPQ);

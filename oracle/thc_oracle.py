@@ -418,3 +418,155 @@ def damp(H, H_prev, mixing=0.7):
 def hermitize(A):
     """scf_driver.cpp:126-129: A <- (A + A^H)/2 over the last two axes."""
     return 0.5 * (A + np.conj(np.swapaxes(A, -1, -2)))
+
+
+# ----------------------------------------------------------------------------------------
+# Self-consistent GW loop pieces (scf_driver.cpp:90-173 with hf = nullptr, const_mu)
+# ----------------------------------------------------------------------------------------
+def eval_hf_energy(Dm_skij, F_skij, H0_skij, k_weight, F_has_H0=False):
+    """scf_common.cpp:44-77: e_1e = spin sum_k w_k Tr[Dm H0], e_hf = spin sum_k w_k Tr[Dm F]/2
+    (F - H0 when F contains H0)."""
+    ns = Dm_skij.shape[0]
+    w = np.asarray(k_weight, np.complex128)
+    e_1e = np.einsum("k,skij,skji->", w, Dm_skij, H0_skij)
+    Fx = F_skij - H0_skij if F_has_H0 else F_skij
+    e_hf = 0.5 * np.einsum("k,skij,skji->", w, Dm_skij, Fx)
+    spin = 1.0 if ns == 2 else 2.0
+    return float((spin * e_1e).real), float((spin * e_hf).real)
+
+
+def dyson_G(H0_skij, S_skij, F_skij, Sigma_tskij, mu, ft: IAFT):
+    """update_G with const_mu (scf_common.cpp:139-145) -> simple_dyson::solve_dyson
+    (simple_dyson.cpp:11-123): G(tau) and Dm = -G(beta^-), then both made Hermitian as the
+    loop does after the Dyson step (scf_driver.cpp:140-143)."""
+    G = solve_dyson(H0_skij, S_skij, F_skij, Sigma_tskij, mu, ft)
+    Dm = -ft.tau_to_beta(G)
+    return hermitize(G), hermitize(Dm)
+
+
+def commutator_t(ft: IAFT, G_tskij, F_skij, Sigma_tskij, mu, S_skij, H0_skij):
+    """vspace_fock_sigma.hpp commutator_t: C(tau) = w_to_tau[G(iw) X(iw) - X(iw) G(iw)],
+    X(iw) = (iw + mu) S - H0 - F - Sigma(iw), all on the fermionic IR grid."""
+    Gw = ft.tau_to_w(G_tskij, "fermi")
+    Sw = ft.tau_to_w(Sigma_tskij, "fermi")
+    Cw = np.empty_like(Gw)
+    for n in range(Gw.shape[0]):
+        om = ft.omega(int(ft.wn_mesh_f[n])) + mu
+        Xm = om * S_skij - H0_skij - F_skij - Sw[n]
+        Cw[n] = Gw[n] @ Xm - Xm @ Gw[n]
+    return ft.w_to_tau(Cw, "fermi")
+
+
+class CommutatorDIIS:
+    """Frequency-dependent commutator DIIS on (F, Sigma(tau)): diis_t.hpp:37-115 driving
+    diis_alg.hpp:100-170 (subspaces as vspace.h keeps them, coefficients as
+    compute_coefs_c1, diis_alg.hpp:330-370) with the residual of com_diis_residual.h.
+    x-vectors are stored undamped; residuals carry Sigma only (their Fock part is zero)."""
+
+    def __init__(self, mixing=0.2, max_subsp_size=5, diis_start=5):
+        self.mixing, self.max_subsp, self.diis_start = mixing, max_subsp_size, diis_start
+        self.x, self.r, self.B = [], [], np.zeros((0, 0), np.complex128)
+
+    def initialize(self, F, Sigma):
+        """init_solver (scf_common.cpp:204-226): the first x-vector is the iteration-1 state."""
+        self.x = [(F.copy(), Sigma.copy())]
+        self.r, self.B = [], np.zeros((0, 0), np.complex128)
+
+    @staticmethod
+    def _dot(a, b):  # FockSigma::dot_prod: conj(a) . b over F and Sigma
+        return np.vdot(a[0], b[0]) + np.vdot(a[1], b[1])
+
+    def _add_residual(self, vec, res):
+        if len(self.r) >= self.max_subsp:  # diis_alg.hpp:125-133: drop the oldest pair
+            self.r.pop(0)
+            self.x.pop(0)
+            self.B = self.B[1:, 1:]
+        n = len(self.r)
+        Bn = np.zeros((n + 1, n + 1), np.complex128)
+        Bn[:n, :n] = self.B
+        for i in range(n):
+            Bn[i, n] = self._dot(self.r[i], res)
+            Bn[n, i] = np.conj(Bn[i, n])
+        Bn[n, n] = self._dot(res, res)
+        self.B = Bn
+        self.r.append(res)
+        self.x.append(vec)
+
+    def coefficients(self):
+        """compute_coefs_c1: pseudo-inverse of Re B on its eigenbasis, c = B^+ 1 / sum."""
+        B = self.B.real
+        ev, U = np.linalg.eigh(B)
+        cond = ev.max() / ev.min()
+        inv = np.array([1.0 / e if e * cond > 1e-12 else 0.0 for e in ev])
+        x = (U * inv) @ U.T @ np.ones(B.shape[0])
+        return x / x.sum()
+
+    def combine(self, c):
+        """vspace.h make_linear_comb: c aligned with the newest vectors."""
+        F = np.zeros_like(self.x[-1][0])
+        S = np.zeros_like(self.x[-1][1])
+        for i in range(min(len(self.x), len(c))):
+            F += c[len(c) - 1 - i] * self.x[-1 - i][0]
+            S += c[len(c) - 1 - i] * self.x[-1 - i][1]
+        return F, S
+
+    def solve(self, F, Sigma, F_prev, Sigma_prev, residual, it):
+        """diis_t::solve for iteration it >= 2.  residual(F, Sigma) gives the commutator of
+        the state.  Returns (F, Sigma, conv_F, conv_Sigma)."""
+        vec = (F.copy(), Sigma.copy())
+        if len(self.x) == 1 or it < self.diis_start:
+            if len(self.x) <= 1:  # grow the x-space without a residual
+                self.x.append(vec)
+            else:
+                self._add_residual(vec, (np.zeros_like(F), residual(F, Sigma)))
+            return damp_pair(F, Sigma, F_prev, Sigma_prev, self.mixing)
+        self._add_residual(vec, (np.zeros_like(F), residual(F, Sigma)))
+        if len(self.r) > 1:
+            Fx, Sx = self.combine(self.coefficients())
+            return Fx, Sx, float(np.abs(F - Fx).max()), float(np.abs(Sigma - Sx).max())
+        return damp_pair(F, Sigma, F_prev, Sigma_prev, self.mixing)
+
+
+def damp_pair(F, Sigma, F_prev, Sigma_prev, mixing):
+    """damp_t::solve on F and Sigma (damp_t.hpp:34-57)."""
+    Fn, cF = damp(F, F_prev, mixing)
+    Sn, cS = damp(Sigma, Sigma_prev, mixing)
+    return Fn, Sn, cF, cS
+
+
+def scgw_loop(G0_tskij, X_skPa, V_qPQ, H0_skij, S_skij, F_skij, mu, ft: IAFT, kpts, lattv,
+              kp_grid, niter, conv_tol, alg="damping", mixing=0.7, max_subsp_size=5,
+              diis_start=5):
+    """scf_loop (scf_driver.cpp:90-173) for GW with hf = nullptr and a constant mu: update_w,
+    evaluate, hermitize, solve_iterative, Dyson, energies; stops when max|dF| and max|dSigma|
+    are below conv_tol.  Returns the per-iteration records and the final (G, Sigma)."""
+    nk = kpts.shape[0]
+    w = np.full(nk, 1.0 / nk)
+    G, F = G0_tskij.copy(), F_skij.copy()
+    F_prev = Sigma_prev = None
+    diis = CommutatorDIIS(mixing, max_subsp_size, diis_start) if alg == "diis" else None
+    hist = []
+    for it in range(1, niter + 1):
+        dW, _, _ = update_w(G, X_skPa, V_qPQ, ft, kpts, lattv, kp_grid)
+        Sigma = eval_Sigma_all_Rspace(G, dW, X_skPa, kpts, lattv, kp_grid)
+        F, Sigma = hermitize(F), hermitize(Sigma)
+        if it == 1:  # solve_iterative, it == 1: changes w.r.t. the mean field only
+            cF, cS = float(np.abs(F_skij - F).max()), float(np.abs(Sigma).max())
+            if diis is not None:
+                diis.initialize(F, Sigma)
+        elif diis is None:
+            F, Sigma, cF, cS = damp_pair(F, Sigma, F_prev, Sigma_prev, mixing)
+        else:
+            G_in = G
+            F, Sigma, cF, cS = diis.solve(
+                F, Sigma, F_prev, Sigma_prev,
+                lambda Fv, Sv: commutator_t(ft, G_in, Fv, Sv, mu, S_skij, H0_skij), it)
+        G, Dm = dyson_G(H0_skij, S_skij, F, Sigma, mu, ft)
+        e_1e, e_hf = eval_hf_energy(Dm, F, H0_skij, w)
+        e_corr = eval_corr_energy(G, Sigma, ft, w)
+        hist.append(dict(it=it, conv_F=cF, conv_Sigma=cS, e_1e=e_1e, e_hf=e_hf, e_corr=e_corr,
+                         e_tot=e_1e + e_hf + e_corr))
+        F_prev, Sigma_prev = F, Sigma
+        if abs(cF) <= abs(conv_tol) and abs(cS) <= abs(conv_tol):
+            break
+    return hist, G, Sigma
