@@ -30,7 +30,11 @@ SYMBOLS = [
     "coqui_b200_kernel_stats", "coqui_b200_primary_to_aux_noalloc",
     "coqui_b200_set_ir_fermi", "coqui_b200_set_mean_field", "coqui_b200_set_iter_alg",
     "coqui_b200_scgw_iteration", "coqui_b200_get_scgw_state", "coqui_b200_dyson_g",
-    "coqui_b200_gm_energy",
+    "coqui_b200_gm_energy", "coqui_b200_mlp_create", "coqui_b200_mlp_destroy",
+    "coqui_b200_mlp_last_error", "coqui_b200_mlp_num_params", "coqui_b200_mlp_set_params",
+    "coqui_b200_mlp_get_params", "coqui_b200_mlp_forward", "coqui_b200_mlp_gradient",
+    "coqui_b200_mlp_train", "coqui_b200_mlp_extrapolate", "coqui_b200_scgw_set_mlp",
+    "coqui_b200_scgw_sigma_diag_w",
 ]
 
 
@@ -92,6 +96,22 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_get_scgw_state.argtypes = [P, P, P, P]
     lib.coqui_b200_dyson_g.argtypes = [P, P, P, P]
     lib.coqui_b200_gm_energy.argtypes = [P, P, P, ctypes.POINTER(D)]
+    lib.coqui_b200_mlp_create.argtypes = [ctypes.POINTER(P), I64, I64, I64, ctypes.c_uint64,
+                                          ctypes.c_int]
+    lib.coqui_b200_mlp_destroy.argtypes = [P]
+    lib.coqui_b200_mlp_destroy.restype = None
+    lib.coqui_b200_mlp_last_error.argtypes = [P]
+    lib.coqui_b200_mlp_last_error.restype = ctypes.c_char_p
+    lib.coqui_b200_mlp_num_params.argtypes = [P]
+    lib.coqui_b200_mlp_num_params.restype = I64
+    lib.coqui_b200_mlp_set_params.argtypes = [P, P]
+    lib.coqui_b200_mlp_get_params.argtypes = [P, P]
+    lib.coqui_b200_mlp_forward.argtypes = [P, P, I64, P]
+    lib.coqui_b200_mlp_gradient.argtypes = [P, P, P, I64, ctypes.POINTER(ctypes.c_float), P]
+    lib.coqui_b200_mlp_train.argtypes = [P, P, P, I64, I64, I64, D, ctypes.c_uint64, P]
+    lib.coqui_b200_mlp_extrapolate.argtypes = [P, P, I64, D, P]
+    lib.coqui_b200_scgw_set_mlp.argtypes = [P, P, ctypes.c_int, D]
+    lib.coqui_b200_scgw_sigma_diag_w.argtypes = [P, P]
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -177,10 +197,22 @@ class Context:
     def scgw_iteration(self, it, G=None):
         """One self-consistent GW iteration; G (iteration 1) uploads the starting G."""
         G = None if G is None else self._G(G)
-        st = np.zeros(5, np.float64)
+        st = np.zeros(8, np.float64)
         self._check(self.lib.coqui_b200_scgw_iteration(self.h, _ptr(G, "G"), int(it), _ptr(st, "st")))
         return dict(conv_F=st[0], conv_Sigma=st[1], e_1e=st[2], e_hf=st[3], e_corr=st[4],
-                    e_tot=st[2] + st[3] + st[4])
+                    e_tot=st[2] + st[3] + st[4], residual=st[5], learned=int(st[6]),
+                    evaluations=int(st[7]))
+
+    def set_mlp(self, mlp, enable=True, max_jump=5.0):
+        """Learned update of the damped loop (mlp: capi.Mlp with 4 inputs, 2 outputs)."""
+        h = mlp.h if (mlp is not None and enable) else None
+        self._check(self.lib.coqui_b200_scgw_set_mlp(self.h, h, 1 if enable else 0, float(max_jump)))
+        self._mlp_ref = mlp  # the network must outlive its use
+
+    def sigma_diag_w(self):
+        out = np.empty((self.nw_f, self.nk, self.nb), np.complex128)
+        self._check(self.lib.coqui_b200_scgw_sigma_diag_w(self.h, _ptr(out, "out")))
+        return out
 
     def get_scgw_state(self):
         G = np.empty((self.nt, 1, self.nk, self.nb, self.nb), np.complex128)
@@ -347,3 +379,73 @@ def primary_to_aux_noalloc(X_ptr, G_ptr, out_ptr, nk, Np, nb, stream=None):
 
 def version() -> str:
     return load().coqui_b200_version().decode()
+
+
+class Mlp:
+    """The learned self-energy update's network (in -> width -> width -> out, tanh), trained
+    and evaluated on the device by the library's own kernels."""
+
+    def __init__(self, din=4, width=256, dout=2, seed=0, device=0):
+        self.lib = load()
+        self.din, self.width, self.dout = din, width, dout
+        self.h = ctypes.c_void_p()
+        rc = self.lib.coqui_b200_mlp_create(ctypes.byref(self.h), din, width, dout, seed, device)
+        if rc != OK:
+            raise CoquiB200Error(rc, "coqui_b200_mlp_create failed")
+        self.nparam = int(self.lib.coqui_b200_mlp_num_params(self.h))
+
+    def close(self):
+        if self.h:
+            self.lib.coqui_b200_mlp_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != OK:
+            raise CoquiB200Error(rc, self.lib.coqui_b200_mlp_last_error(self.h).decode())
+
+    def params(self):
+        p = np.empty(self.nparam, np.float32)
+        self._check(self.lib.coqui_b200_mlp_get_params(self.h, _ptr(p, "params")))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32).reshape(self.nparam)
+        self._check(self.lib.coqui_b200_mlp_set_params(self.h, _ptr(p, "params")))
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, self.din)
+        Y = np.empty((X.shape[0], self.dout), np.float32)
+        self._check(self.lib.coqui_b200_mlp_forward(self.h, _ptr(X, "X"), X.shape[0], _ptr(Y, "Y")))
+        return Y
+
+    def gradient(self, X, T):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, self.din)
+        T = np.ascontiguousarray(T, np.float32).reshape(-1, self.dout)
+        g = np.empty(self.nparam, np.float32)
+        loss = ctypes.c_float(0.0)
+        self._check(self.lib.coqui_b200_mlp_gradient(self.h, _ptr(X, "X"), _ptr(T, "T"), X.shape[0],
+                                                     ctypes.byref(loss), _ptr(g, "g")))
+        return loss.value, g
+
+    def extrapolate(self, hist, max_jump=5.0):
+        """hist (4, n) complex128, oldest first -> learned correction (n,) complex128."""
+        h = np.ascontiguousarray(hist, np.complex128)
+        n = h.shape[1]
+        out = np.empty(n, np.complex128)
+        self._check(self.lib.coqui_b200_mlp_extrapolate(self.h, _ptr(h, "hist"), n,
+                                                        float(max_jump), _ptr(out, "delta")))
+        return out
+
+    def train(self, X, T, batch=4096, epochs=10, lr=1e-3, seed=0):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, self.din)
+        T = np.ascontiguousarray(T, np.float32).reshape(-1, self.dout)
+        hist = np.zeros(epochs, np.float32)
+        self._check(self.lib.coqui_b200_mlp_train(self.h, _ptr(X, "X"), _ptr(T, "T"), X.shape[0],
+                                                  batch, epochs, float(lr), seed, _ptr(hist, "h")))
+        return hist

@@ -20,6 +20,7 @@
 
 #include "dyson.cuh"
 #include "kernels.cuh"
+#include "mlp.cuh"
 #include "scgw.cuh"
 #include "tc_gemm.cuh"
 
@@ -110,6 +111,15 @@ struct coqui_b200_ctx {
   std::vector<std::unique_ptr<DevBuf<double2>>> dx;  // DIIS x-vectors (F then Sigma)
   std::vector<std::unique_ptr<DevBuf<double2>>> dr;  // DIIS residuals (Sigma part)
   std::vector<std::complex<double>> dB;              // residual overlaps (row-major nB x nB)
+  // learned update of the damped loop
+  coqui_b200_mlp* mlp = nullptr;
+  bool mlp_on = false, last_mlp = false;
+  double mlp_max_jump = 5.0, r_prev = 0;
+  int cooldown = 0;
+  int64_t nhist = 0;
+  DevBuf<double2> dhist;       // (4, nwf * nk * nb) diag Sigma_in(i w), oldest first
+  DevBuf<double2> plain_saved; // the damped Sigma that the last proposal replaced
+  DevBuf<double2> dtmp;        // (max(nt, nwf), nk * nb)
 
   // pipelined host transfers: G arrives in tau chunks on the copy stream (one event per
   // chunk) and Sigma leaves chunk by chunk while later chunks are computed
@@ -539,6 +549,38 @@ void commutator_device(Ctx* c, const double2* F, const double2* Sig, const doubl
   zgemm_rm(c, 'N', 'N', nb, nb, nb, make_double2(-1, 0), c->Xw.p, nb, nb * nb, c->Gw.p, nb, nb * nb,
            make_double2(1, 0), c->Sw.p, nb, nb * nb, nw * nk);
   w_to_tau_ff(c, c->Sw.p, out, ncol);
+}
+
+// diag Sigma_ii^k(i w_n) of Sig(tau) into out (nwf, nk * nb)
+void sigma_diag_w(Ctx* c, const double2* Sig, double2* out) {
+  const int64_t nkb = c->nk * c->nb;
+  c->dtmp.ensure(std::max(c->nt, c->nwf) * nkb);
+  cq::extract_diag(Sig, c->dtmp.p, c->nb, c->nt * c->nk, c->st);
+  zgemm_rm(c, 'N', 'N', c->nwf, nkb, c->nt, make_double2(1, 0), c->dTwt_ff.p, c->nt, 0, c->dtmp.p,
+           nkb, 0, make_double2(0, 0), out, nkb, 0, 1);
+}
+
+// Sig(tau) += Ttw_ff diag(delta(i w)), then Hermitian again
+void add_diag_w(Ctx* c, const double2* delta_w, double2* Sig) {
+  const int64_t nkb = c->nk * c->nb;
+  c->dtmp.ensure(std::max(c->nt, c->nwf) * nkb);
+  zgemm_rm(c, 'N', 'N', c->nt, nkb, c->nwf, make_double2(1, 0), c->dTtw_ff.p, c->nwf, 0, delta_w,
+           nkb, 0, make_double2(0, 0), c->dtmp.p, nkb, 0, 1);
+  cq::add_diag(Sig, c->dtmp.p, c->nb, c->nt * c->nk, c->st);
+  cq::hermitize_c128(Sig, c->nb, c->nt * c->nk, c->st);
+}
+
+// append diag Sigma_in(i w) to the four-iterate history (oldest dropped)
+void push_history(Ctx* c, const double2* Sig) {
+  const int64_t nel = c->nwf * c->nk * c->nb;
+  c->dhist.ensure(5 * nel);
+  if (c->nhist == 4) {
+    CQ_CHECK_CUDA(cudaMemcpyAsync(c->dhist.p, c->dhist.p + nel, 3 * nel * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, c->st));
+    c->nhist = 3;
+  }
+  sigma_diag_w(c, Sig, c->dhist.p + c->nhist * nel);
+  ++c->nhist;
 }
 
 // Commutator DIIS step (diis_t::solve, diis_t.hpp:58-100) on the device vectors.  FS holds
@@ -1406,7 +1448,8 @@ int coqui_b200_scgw_iteration(coqui_b200_ctx* c, const double* G_tskij, int64_t 
     CQ_CHECK_CUDA(cudaMemcpyAsync(c->FS.p, c->F.p, nF * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
     CQ_CHECK_CUDA(cudaMemcpyAsync(c->FS.p + nF, c->Sig.p, nS * sizeof(double2),
                                   cudaMemcpyDeviceToDevice, c->st));
-    double cF = 0, cS = 0;
+    double cF = 0, cS = 0, resid = 0;
+    int flag = 0, evals = 1;
     {
       cq::Prof::Scope sc(&c->prof, "scgw_iterate");
       if (it == 1) {  // solve_iterative, it == 1 (scf_common.cpp:320-347)
@@ -1422,12 +1465,55 @@ int coqui_b200_scgw_iteration(coqui_b200_ctx* c, const double* G_tskij, int64_t 
                                         cudaMemcpyDeviceToDevice, c->st));
           c->dx.push_back(std::move(x));
         }
+        resid = cS;
+        c->r_prev = cS;
+        c->nhist = 0;
+        c->last_mlp = false;
+        c->cooldown = 0;
+        if (c->mlp_on) push_history(c, c->FS.p + nF);
       } else if (c->iter_alg == 0) {  // damp_t (damp_t.hpp:34-57)
+        resid = cq::maxabs_diff(c->prevFS.p + nF, c->FS.p + nF, nS, c->red, c->st);
+        if (c->mlp_on && c->last_mlp && resid > c->r_prev) {
+          // the learned proposal raised the residual: evaluate the plain damped Sigma instead
+          CQ_CHECK_CUDA(cudaMemcpyAsync(c->prevFS.p + nF, c->plain_saved.p, nS * sizeof(double2),
+                                        cudaMemcpyDeviceToDevice, c->st));
+          dyson_g_device(c, c->prevFS.p + nF);
+          update_w_device(c);
+          sigma_device(c, nullptr);
+          cq::hermitize_c128(c->Sig.p, c->nb, c->nt * c->nk, c->st);
+          CQ_CHECK_CUDA(cudaMemcpyAsync(c->FS.p + nF, c->Sig.p, nS * sizeof(double2),
+                                        cudaMemcpyDeviceToDevice, c->st));
+          resid = cq::maxabs_diff(c->prevFS.p + nF, c->FS.p + nF, nS, c->red, c->st);
+          c->cooldown = 3;
+          c->nhist = 0;
+          flag = -1;
+          ++evals;
+        }
         const double m = c->mixing;
         cq::axpby_c128(c->prevFS.p, c->FS.p, 1.0 - m, m, nF + nS, c->st);
         cF = cq::maxabs_diff(c->prevFS.p, c->FS.p, nF, c->red, c->st);
         cS = cq::maxabs_diff(c->prevFS.p + nF, c->FS.p + nF, nS, c->red, c->st);
+        if (c->mlp_on) {
+          push_history(c, c->FS.p + nF);
+          c->last_mlp = false;
+          if (c->cooldown > 0) {
+            --c->cooldown;
+          } else if (c->nhist == 4) {
+            const int64_t nel = c->nwf * c->nk * c->nb;
+            c->plain_saved.ensure(nS);
+            CQ_CHECK_CUDA(cudaMemcpyAsync(c->plain_saved.p, c->FS.p + nF, nS * sizeof(double2),
+                                          cudaMemcpyDeviceToDevice, c->st));
+            double2* delta = c->dhist.p + 4 * nel;  // fifth slot of the history buffer
+            cq::mlp_extrapolate(mlp_net(c->mlp), c->dhist.p, nel, c->mlp_max_jump, delta, c->st);
+            add_diag_w(c, delta, c->FS.p + nF);
+            c->last_mlp = true;
+            c->nhist = 0;
+            if (flag == 0) flag = 1;
+          }
+          c->r_prev = resid;
+        }
       } else {
+        resid = cq::maxabs_diff(c->prevFS.p + nF, c->FS.p + nF, nS, c->red, c->st);
         std::tie(cF, cS) = diis_device(c, c->FS.p, it);
       }
     }
@@ -1449,7 +1535,35 @@ int coqui_b200_scgw_iteration(coqui_b200_ctx* c, const double* G_tskij, int64_t 
     stats[2] = e1;
     stats[3] = ehf;
     stats[4] = ec;
+    stats[5] = resid;
+    stats[6] = flag;
+    stats[7] = evals;
     c->end_timing();
+  });
+}
+
+int coqui_b200_scgw_set_mlp(coqui_b200_ctx* c, coqui_b200_mlp* mlp, int enable, double max_jump) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(!enable || (mlp && max_jump > 0), COQUI_B200_EINVAL, "enable needs an mlp");
+    if (enable) CQ_REQUIRE(mlp_net(mlp).din == 4 && mlp_net(mlp).dout == 2, COQUI_B200_EINVAL,
+                           "the learned update takes a network with 4 inputs and 2 outputs");
+    c->mlp = enable ? mlp : nullptr;
+    c->mlp_on = enable != 0;
+    c->mlp_max_jump = max_jump;
+    c->nhist = 0;
+    c->last_mlp = false;
+    c->cooldown = 0;
+  });
+}
+
+int coqui_b200_scgw_sigma_diag_w(coqui_b200_ctx* c, double* out) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(c->have_irf && out, COQUI_B200_EINVAL, "bad arguments (set_ir_fermi first)");
+    const int64_t nS = c->nt * c->nk * c->nb * c->nb, nel = c->nwf * c->nk * c->nb;
+    CQ_REQUIRE(c->Sig.n >= (size_t)nS, COQUI_B200_EINVAL, "no self-energy yet");
+    c->trc.ensure(nel);
+    sigma_diag_w(c, c->Sig.p, c->trc.p);
+    download(c, out, c->trc.p, nel * sizeof(double2));
   });
 }
 

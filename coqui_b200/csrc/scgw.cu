@@ -179,6 +179,26 @@ __global__ void k_axpy(const double2* __restrict__ x, double2* __restrict__ y, d
   }
 }
 
+__global__ void k_extract_diag(const double2* __restrict__ A, double2* __restrict__ out, int64_t nb,
+                               int64_t nmat) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb * nmat;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = i / nb, d = i % nb;
+    out[i] = A[m * nb * nb + d * nb + d];
+  }
+}
+
+__global__ void k_add_diag(double2* __restrict__ A, const double2* __restrict__ dv, int64_t nb,
+                           int64_t nmat) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb * nmat;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = i / nb, d = i % nb;
+    double2& a = A[m * nb * nb + d * nb + d];
+    a.x += dv[i].x;
+    a.y += dv[i].y;
+  }
+}
+
 constexpr int kRedBlocks = 592;
 
 __global__ void __launch_bounds__(256) k_maxabs_diff(const double2* __restrict__ a,
@@ -271,6 +291,18 @@ void invert_batched(double2* A, int64_t nb, int64_t nmat, int* info, cublasHandl
     set = true;
   }
   k_gauss_jordan<<<(unsigned)nmat, 256, smem, s>>>(A, (int)nb, info);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+void extract_diag(const double2* A, double2* out, int64_t nb, int64_t nmat, cudaStream_t s) {
+  k_extract_diag<<<grid_for(nb * nmat, 256), 256, 0, s>>>(A, out, nb, nmat);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+void add_diag(double2* A, const double2* d, int64_t nb, int64_t nmat, cudaStream_t s) {
+  k_add_diag<<<grid_for(nb * nmat, 256), 256, 0, s>>>(A, d, nb, nmat);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
 }

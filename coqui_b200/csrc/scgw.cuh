@@ -42,6 +42,10 @@ double maxabs_diff(const double2* a, const double2* b, int64_t n, DevBuf<double>
 std::complex<double> dotc(const double2* a, const double2* b, int64_t n, DevBuf<double>& part,
                           cudaStream_t s);
 
+// out[m * nb + i] = A[m]_ii, and A[m]_ii += d[m * nb + i], for nmat nb x nb matrices
+void extract_diag(const double2* A, double2* out, int64_t nb, int64_t nmat, cudaStream_t s);
+void add_diag(double2* A, const double2* d, int64_t nb, int64_t nmat, cudaStream_t s);
+
 // Eigen-decomposition of a small real symmetric matrix by cyclic Jacobi rotations (host):
 // A (n x n, row-major) -> ev (n), U (n x n, row-major, column k = eigenvector k).
 void sym_eigen(const std::vector<double>& A, int64_t n, std::vector<double>& ev,

@@ -67,6 +67,7 @@ extern "C" {
                               FP64 Cholesky / log-det */
 
 typedef struct coqui_b200_ctx coqui_b200_ctx;
+typedef struct coqui_b200_mlp coqui_b200_mlp; /* network of the learned self-energy update */
 
 typedef struct {
   int64_t ns;          /* spin components (1 supported) */
@@ -145,10 +146,25 @@ COQUI_B200_API int coqui_b200_set_iter_alg(coqui_b200_ctx* ctx, int alg, double 
 
 /* One loop iteration it (>= 1): update_w, Sigma, hermitize, damping/DIIS, Dyson for G
    (simple_dyson.cpp:11-123, G stays resident for the next iteration), energies.
-   G_tskij != NULL uploads the starting G (iteration 1).  stats[5] = max|dF|, max|dSigma|,
-   e_1e, e_hf, e_corr (Galitskii-Migdal, scf_common.cpp:87-136). */
+   G_tskij != NULL uploads the starting G (iteration 1).  stats[8] = max|dF|, max|dSigma|,
+   e_1e, e_hf, e_corr (Galitskii-Migdal, scf_common.cpp:87-136), the residual
+   max|Sigma_GW - Sigma_in| of this iteration, learned-update flag (1 applied, -1 withdrawn
+   and re-evaluated, 0 none), number of GW evaluations in this call. */
 COQUI_B200_API int coqui_b200_scgw_iteration(coqui_b200_ctx* ctx, const double* G_tskij,
                                              int64_t it, double* stats);
+
+/* Learned update of the damped loop (alg 0): after the damping step, the network extrapolates
+   every diagonal element Sigma_ii^k(i w_n) from its last four iterates and the loop adds the
+   proposal (back on the tau grid, made Hermitian).  The next iteration judges it by the
+   residual max|Sigma_GW - Sigma_in|: if that grew, the proposal is withdrawn, the plain damped
+   Sigma is evaluated instead and the network pauses for three iterations.  mlp NULL or enable 0
+   switches it off.  The mlp must outlive its use by the context. */
+COQUI_B200_API int coqui_b200_scgw_set_mlp(coqui_b200_ctx* ctx, coqui_b200_mlp* mlp, int enable,
+                                           double max_jump);
+
+/* Diagonal of the current loop self-energy on the fermionic frequency grid:
+   out (nw_f, nk, nb) complex128. */
+COQUI_B200_API int coqui_b200_scgw_sigma_diag_w(coqui_b200_ctx* ctx, double* out);
 
 /* Copies of the loop state: G_tskij, Sigma_tskij (nt_f, ns, nk, nb, nb), Dm_skij
    (ns, nk, nb, nb); NULL entries are skipped. */
@@ -164,6 +180,34 @@ COQUI_B200_API int coqui_b200_dyson_g(coqui_b200_ctx* ctx, const double* Sigma_t
    scf_common.cpp:87-136; k weights 1/nk). */
 COQUI_B200_API int coqui_b200_gm_energy(coqui_b200_ctx* ctx, const double* G_tskij,
                                         const double* Sigma_tskij, double* e_corr);
+
+/* ---- learned self-energy update: a small MLP (in -> width -> width -> out, tanh), BF16
+   weights, FP32 accumulation, trained on the device by hand-written kernels.  No counterpart
+   in the reference (its loop has only damping and DIIS). ---- */
+
+COQUI_B200_API int coqui_b200_mlp_create(coqui_b200_mlp** mlp, int64_t in_dim, int64_t width,
+                                         int64_t out_dim, uint64_t seed, int device);
+COQUI_B200_API void coqui_b200_mlp_destroy(coqui_b200_mlp* mlp);
+COQUI_B200_API const char* coqui_b200_mlp_last_error(const coqui_b200_mlp* mlp);
+/* Parameters as FP32 W1 (width, in), b1, W2 (width, width), b2, W3 (out, width), b3. */
+COQUI_B200_API int64_t coqui_b200_mlp_num_params(const coqui_b200_mlp* mlp);
+COQUI_B200_API int coqui_b200_mlp_set_params(coqui_b200_mlp* mlp, const float* params);
+COQUI_B200_API int coqui_b200_mlp_get_params(coqui_b200_mlp* mlp, float* params);
+/* Y (B, out) = MLP(X (B, in)), host arrays. */
+COQUI_B200_API int coqui_b200_mlp_forward(coqui_b200_mlp* mlp, const float* X, int64_t B, float* Y);
+/* Mean squared error of MLP(X) against T (B, out) and its gradient (num_params). */
+COQUI_B200_API int coqui_b200_mlp_gradient(coqui_b200_mlp* mlp, const float* X, const float* T,
+                                           int64_t B, float* loss, float* grad);
+/* Learned extrapolation (4 inputs, 2 outputs): hist (4, n) complex128, the last four iterates of
+   n sequences (oldest first); with d1 = s3 - s2, d2 = s2 - s1, d3 = s1 - s0 the network maps
+   (d1/d2, d2/d3) to (s_inf - s3)/d1; delta (n) complex128 = d1 * output, at most max_jump |d1|,
+   0 where the differences vanish. */
+COQUI_B200_API int coqui_b200_mlp_extrapolate(coqui_b200_mlp* mlp, const double* hist, int64_t n,
+                                              double max_jump, double* delta);
+/* Adam training over shuffled mini-batches; loss_history (epochs) may be NULL. */
+COQUI_B200_API int coqui_b200_mlp_train(coqui_b200_mlp* mlp, const float* X, const float* T,
+                                        int64_t n_samples, int64_t batch, int64_t epochs,
+                                        double lr, uint64_t seed, float* loss_history);
 
 /* Building blocks (same layouts as the reference's arguments). */
 COQUI_B200_API int coqui_b200_primary_to_aux(coqui_b200_ctx* ctx, int64_t n_tau, const double* O_tskab,

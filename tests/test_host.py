@@ -54,3 +54,27 @@ def test_shape_validation_before_device():
         capi._c128(np.zeros((2, 3)), (3, 2), "x")
     with pytest.raises(ValueError):
         capi._ptr(np.zeros((4, 4))[:, ::2], "x")
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(3)
+    din, width, dout = 4, 16, 2
+    n = width * din + width + width * width + width + dout * width + dout
+    p = rng.standard_normal(n) * 0.3
+    X, T = rng.standard_normal((7, din)), rng.standard_normal((7, dout))
+    _, g = M.loss_and_grad(p, X, T, din, width, dout, round_params=False)
+    for i in rng.choice(n, 12, replace=False):
+        e = np.zeros(n)
+        e[i] = 1e-6
+        lp, _ = M.loss_and_grad(p + e, X, T, din, width, dout, round_params=False)
+        lm, _ = M.loss_and_grad(p - e, X, T, din, width, dout, round_params=False)
+        assert abs((lp - lm) / 2e-6 - g[i]) < 1e-7 * max(1.0, abs(g[i]))
+
+
+def test_bf16_rounding_ties_to_even():
+    from oracle import mlp_oracle as M
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 3.14159], np.float32)
+    r = M.bf16_round(x)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6 and r[3] == -2.5
+    assert abs(r[4] - 3.140625) < 1e-12
