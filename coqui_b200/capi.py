@@ -34,7 +34,9 @@ SYMBOLS = [
     "coqui_b200_mlp_last_error", "coqui_b200_mlp_num_params", "coqui_b200_mlp_set_params",
     "coqui_b200_mlp_get_params", "coqui_b200_mlp_forward", "coqui_b200_mlp_gradient",
     "coqui_b200_mlp_train", "coqui_b200_mlp_extrapolate", "coqui_b200_scgw_set_mlp",
-    "coqui_b200_scgw_sigma_diag_w",
+    "coqui_b200_scgw_sigma_diag_w", "coqui_b200_batch_create", "coqui_b200_batch_destroy",
+    "coqui_b200_batch_last_error", "coqui_b200_batch_set_ir", "coqui_b200_batch_set_thc",
+    "coqui_b200_batch_gw_iteration", "coqui_b200_batch_last_ms",
 ]
 
 
@@ -112,6 +114,16 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_mlp_extrapolate.argtypes = [P, P, I64, D, P]
     lib.coqui_b200_scgw_set_mlp.argtypes = [P, P, ctypes.c_int, D]
     lib.coqui_b200_scgw_sigma_diag_w.argtypes = [P, P]
+    lib.coqui_b200_batch_create.argtypes = [ctypes.POINTER(P), I64, P, P, I64, I64, ctypes.c_int]
+    lib.coqui_b200_batch_destroy.argtypes = [P]
+    lib.coqui_b200_batch_destroy.restype = None
+    lib.coqui_b200_batch_last_error.argtypes = [P]
+    lib.coqui_b200_batch_last_error.restype = ctypes.c_char_p
+    lib.coqui_b200_batch_set_ir.argtypes = [P, P, P, P]
+    lib.coqui_b200_batch_set_thc.argtypes = [P, I64, P, P]
+    lib.coqui_b200_batch_gw_iteration.argtypes = [P, P, P]
+    lib.coqui_b200_batch_last_ms.argtypes = [P]
+    lib.coqui_b200_batch_last_ms.restype = D
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -449,3 +461,61 @@ class Mlp:
         self._check(self.lib.coqui_b200_mlp_train(self.h, _ptr(X, "X"), _ptr(T, "T"), X.shape[0],
                                                   batch, epochs, float(lr), seed, _ptr(hist, "h")))
         return hist
+
+
+class Batch:
+    """Uneven batch of Gamma-only molecules run with fused launches (mixed precision)."""
+
+    def __init__(self, nb, Np, nt_f, nw_b, device=0):
+        self.lib = load()
+        self.nb = [int(v) for v in nb]
+        self.Np = [int(v) for v in Np]
+        self.nt, self.nw_b = nt_f, nw_b
+        a = np.ascontiguousarray(self.nb, np.int64)
+        b = np.ascontiguousarray(self.Np, np.int64)
+        self.h = ctypes.c_void_p()
+        rc = self.lib.coqui_b200_batch_create(ctypes.byref(self.h), len(self.nb), _ptr(a, "nb"),
+                                              _ptr(b, "Np"), nt_f, nw_b, device)
+        if rc != OK:
+            raise CoquiB200Error(rc, "coqui_b200_batch_create failed")
+
+    def close(self):
+        if self.h:
+            self.lib.coqui_b200_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != OK:
+            raise CoquiB200Error(rc, self.lib.coqui_b200_batch_last_error(self.h).decode())
+
+    def set_ir(self, ft):
+        nt, nw = self.nt, self.nw_b
+        Twt = _c128(ft.Twt_bb, (nw, nt), "Twt_bb")
+        Ttw = _c128(ft.Ttw_bb, (nt, nw), "Ttw_bb")
+        x = np.ascontiguousarray(ft.tau_mesh_x, np.float64)
+        self._check(self.lib.coqui_b200_batch_set_ir(self.h, _ptr(Twt, "Twt"), _ptr(Ttw, "Ttw"),
+                                                     _ptr(x, "tau")))
+
+    def set_thc(self, m, X, V):
+        X = _c128(X, (self.Np[m], self.nb[m]), "X")
+        V = _c128(V, (self.Np[m], self.Np[m]), "V")
+        self._check(self.lib.coqui_b200_batch_set_thc(self.h, int(m), _ptr(X, "X"), _ptr(V, "V")))
+
+    def gw_iteration(self, G_list, sigma_out=None):
+        """G_list[m] (nt, nb_m, nb_m) complex128 -> list of Sigma (nt, nb_m, nb_m)."""
+        Gs = [_c128(G, (self.nt, n, n), "G") for G, n in zip(G_list, self.nb)]
+        Ss = sigma_out if sigma_out is not None else [np.empty_like(G) for G in Gs]
+        gp = (ctypes.c_void_p * len(Gs))(*[G.ctypes.data for G in Gs])
+        sp = (ctypes.c_void_p * len(Ss))(*[S.ctypes.data for S in Ss])
+        self._check(self.lib.coqui_b200_batch_gw_iteration(self.h, gp, sp))
+        return Ss
+
+    def last_ms(self):
+        """Device time of the last gw_iteration (CUDA events), ms."""
+        return float(self.lib.coqui_b200_batch_last_ms(self.h))

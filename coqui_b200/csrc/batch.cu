@@ -1,0 +1,467 @@
+// Uneven batch of independent Gamma-only molecules (one k-point each, different orbital and
+// interpolating-point counts): one GW iteration for all of them with fused launches.
+//
+// Per molecule m the path is the one of the single-system context with nk = 1 (no k <-> R
+// transform): G_PQ = X G X^H (thc_solver_comm.hpp:363-429), Pi = -2 G_PQ(t) o conj(G_PQ(beta-t))
+// (rpa_pi.icc:156-162), tau -> iW (IAFT.icc:49-73), Dyson in Hermitian form, iW -> tau,
+// Sigma_PQ = -G_PQ o W (thc_gw.icc:161-167), Sigma_ab = X^H Sigma X (thc_solver_comm.hpp:516-569).
+// Fusion across molecules:
+//   * every [tau][column] array concatenates the molecules' Np_m^2 columns, so the Hadamard
+//     products and the IR transforms are single launches over all molecules;
+//   * the projections and the Dyson products are grouped tensor-core GEMMs (one launch, one
+//     group per molecule, batched over tau or iW);
+//   * the FP64 factorisations of all (m, iW) problems are one grouped launch.
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include <cusolverDn.h>
+
+#include "chol.cuh"
+#include "dyson.cuh"
+#include "kernels.cuh"
+#include "tc_gemm.cuh"
+
+namespace cq {
+namespace {
+
+// Gt[m][t] = G[m][t]^T as complex64 for all molecules; offsets/edges from the molecule table
+__global__ void k_transpose_grouped(const double2* __restrict__ G, float2* __restrict__ Gt,
+                                    const int64_t* __restrict__ off, const int64_t* __restrict__ nb,
+                                    int nmol, int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nmol - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (off[mid] <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    const int64_t n = nb[lo], loc = i - off[lo], mat = loc / (n * n), e = loc % (n * n);
+    const double2 v = G[i];
+    Gt[off[lo] + mat * n * n + (e % n) * n + e / n] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+struct HermProblem {
+  const float2* DH;
+  const float2* F;
+  float2* E;
+  int64_t n;
+};
+
+// E = DH + DH^H + F (F lower triangle only) for problems of different sizes; 32 x 32 tiles over
+// the largest edge, tiles outside a problem exit at once
+__global__ void k_herm_sum_grouped(const HermProblem* __restrict__ probs) {
+  __shared__ float2 tile[32][33];
+  __shared__ float2 ftile[32][33];
+  const HermProblem pr = probs[blockIdx.z];
+  const int64_t n = pr.n;
+  const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
+  if (i0 >= n || j0 >= n) return;
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t r = j0 + ty, c = i0 + threadIdx.x;
+    const bool in = r < n && c < n;
+    tile[ty][threadIdx.x] = in ? pr.DH[r * n + c] : make_float2(0.f, 0.f);
+    ftile[ty][threadIdx.x] = (in && r >= c) ? pr.F[r * n + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t i = i0 + ty, j = j0 + threadIdx.x;
+    if (i < n && j < n) {
+      const float2 a = pr.DH[i * n + j];
+      const float2 b = tile[threadIdx.x][ty];  // DH[j][i]
+      float2 fv;
+      if (i >= j) {
+        fv = pr.F[i * n + j];
+      } else {
+        const float2 t = ftile[threadIdx.x][ty];
+        fv = make_float2(t.x, -t.y);
+      }
+      pr.E[i * n + j] = make_float2(a.x + b.x + fv.x, a.y - b.y + fv.y);
+    }
+  }
+}
+
+#define CQ_SOLVER_CHECK(expr)                                                                   \
+  do {                                                                                          \
+    cusolverStatus_t _s = (expr);                                                               \
+    if (_s != CUSOLVER_STATUS_SUCCESS)                                                          \
+      throw cq::Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
+  } while (0)
+
+}  // namespace
+}  // namespace cq
+
+using cq::DevBuf;
+
+struct coqui_b200_batch {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  cusolverDnHandle_t sol = nullptr;
+  std::string err;
+  int64_t nmol = 0, nt = 0, nth = 0, nwb = 0, nwh = 0, nmax = 0;
+  std::vector<int64_t> nb, Np;
+  std::vector<int64_t> offPQ, offX, offG, offL, offD;  // element offsets per molecule
+  int64_t cols = 0, nX = 0, nG = 0, nL = 0, nD = 0;
+  std::vector<char> have_thc;
+  bool have_ir = false;
+  std::vector<double2> Twt_pos, Ttw_pos;
+  DevBuf<double> dTwtR, dTtwR;
+  DevBuf<float4> Xs, XTs, Ls, LHs;
+  DevBuf<double2> G, Sig, Ltmp, LHtmp;
+  DevBuf<float2> Gt, T, UT, Sab, cache, PW;
+  DevBuf<float2> T1, Mb, Zb;
+  DevBuf<double2> Ab;
+  DevBuf<int64_t> dofG, dnb;
+  DevBuf<unsigned char> gtab, ctab, htab;
+  DevBuf<int> info;
+  DevBuf<double> ld;
+  DevBuf<double2> tr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+};
+
+namespace {
+
+using Batch = coqui_b200_batch;
+
+template <typename F> int bguarded(Batch* b, F&& f) {
+  if (!b) return COQUI_B200_EINVAL;
+  try {
+    CQ_CHECK_CUDA(cudaSetDevice(b->dev));
+    f();
+    if (b->st) CQ_CHECK_CUDA(cudaStreamSynchronize(b->st));
+    if (cq::tc_take_error())
+      throw cq::Error(COQUI_B200_ETIMEDOUT, "a tensor-core kernel gave up a bounded wait");
+    b->err.clear();
+    return COQUI_B200_OK;
+  } catch (const cq::Error& e) {
+    b->err = e.what();
+    if (b->st) (void)cudaStreamSynchronize(b->st);
+    return e.code;
+  } catch (const std::exception& e) {
+    b->err = e.what();
+    if (b->st) (void)cudaStreamSynchronize(b->st);
+    return COQUI_B200_EINVAL;
+  }
+}
+
+cq::TcGroup group(const void* A, bool as, bool ca, int64_t lda, int64_t sA, const void* B, bool bs,
+                  bool cb, int64_t ldb, int64_t sB, float2* C, int64_t ldc, int64_t sC, int64_t M,
+                  int64_t N, int64_t K, int64_t batch, cq::TcStructure st = cq::TcStructure{}) {
+  cq::TcGroup g;
+  g.A = A;
+  g.a_split = as;
+  g.conj_a = ca;
+  g.lda = lda;
+  g.sA = sA;
+  g.Bt = B;
+  g.b_split = bs;
+  g.conj_b = cb;
+  g.ldb = ldb;
+  g.sB = sB;
+  g.C = C;
+  g.ldc = ldc;
+  g.sC = sC;
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  g.batch = batch;
+  g.st = st;
+  return g;
+}
+
+// one GW iteration for all molecules; G in b->G, Sigma (complex128) into b->Sig
+void batch_gw(Batch* b) {
+  const cudaStream_t s = b->st;
+  const int64_t nt = b->nt, nth = b->nth, nwh = b->nwh, cols = b->cols;
+  // ---- G_PQ(t) = X G(t) X^H for every molecule and t (two grouped products) ----
+  cq::k_transpose_grouped<<<cq::grid_for(b->nG, 256), 256, 0, s>>>(b->G.p, b->Gt.p, b->dofG.p,
+                                                                   b->dnb.p, (int)b->nmol, b->nG);
+  cq::count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+  std::vector<cq::TcGroup> g1, g2;
+  for (int64_t m = 0; m < b->nmol; ++m) {
+    const int64_t nb = b->nb[m], Np = b->Np[m];
+    float2* Tm = b->T.p + b->offX[m] * nt;  // (nt, Np, nb)
+    g1.push_back(group(b->Xs.p + b->offX[m], true, false, nb, 0, b->Gt.p + b->offG[m], false, false,
+                       nb, nb * nb, Tm, nb, Np * nb, Np, nb, nb, nt));
+    g2.push_back(group(Tm, false, false, nb, Np * nb, b->Xs.p + b->offX[m], true, true, nb, 0,
+                       b->cache.p + b->offPQ[m], Np, cols, Np, Np, nb, nt));
+  }
+  cq::tc_cgemm_grouped(g1, b->gtab, s);
+  cq::tc_cgemm_grouped(g2, b->gtab, s);
+  // ---- Pi(t) over all columns (nk = 1: no k <-> R transform) ----
+  const cq::KGrid g0{1, 1, 1};
+  for (int64_t it = 0; it < nth; ++it)
+    cq::launch_pi_fused<float>(b->cache.p + it * cols, b->cache.p + (nt - 1 - it) * cols,
+                               b->PW.p + it * cols, cols, g0, -2.0, s);
+  cq::launch_ir_transform_real<float>(b->PW.p, cols, (int)nth, (int)nwh, b->dTwtR.p, s);
+  // ---- Dyson per (m, iW): M = L^H Pi L, I - M = C C^H, W = L (D + D^H + D^H D) L^H ----
+  std::vector<cq::TcGroup> p1, p2;
+  for (int64_t m = 0; m < b->nmol; ++m) {
+    const int64_t Np = b->Np[m], NN = Np * Np;
+    cq::TcStructure s1;
+    s1.a_upper = true;
+    p1.push_back(group(b->LHs.p + b->offL[m], true, false, Np, 0, b->PW.p + b->offPQ[m], false, true,
+                       Np, cols, b->T1.p + b->offD[m], Np, NN, Np, Np, Np, nwh, s1));
+    cq::TcStructure s2;
+    s2.b_lower = true;
+    s2.lower_only = true;
+    p2.push_back(group(b->T1.p + b->offD[m], false, false, Np, NN, b->LHs.p + b->offL[m], true, true,
+                       Np, 0, b->Mb.p + b->offD[m], Np, NN, Np, Np, Np, nwh, s2));
+  }
+  cq::tc_cgemm_grouped(p1, b->gtab, s);
+  cq::tc_cgemm_grouped(p2, b->gtab, s);
+  std::vector<cq::CholProblem> cp;
+  for (int64_t m = 0; m < b->nmol; ++m)
+    for (int64_t w = 0; w < nwh; ++w) {
+      const int64_t Np = b->Np[m], o = b->offD[m] + w * Np * Np;
+      cp.push_back(cq::CholProblem{b->Mb.p + o, b->Ab.p + o, b->Zb.p + o, Np});
+    }
+  const int64_t nprob = (int64_t)cp.size();
+  b->info.ensure(nprob);
+  b->ld.ensure(nprob);
+  b->tr.ensure(nprob);
+  cq::launch_chol_inv_grouped(cp, b->ctab, b->ld.p, b->tr.p, b->info.p, s);
+  std::vector<cq::TcGroup> f, t4, t5;
+  std::vector<cq::HermProblem> hp;
+  for (int64_t m = 0; m < b->nmol; ++m) {
+    const int64_t Np = b->Np[m], NN = Np * Np;
+    float2* Z = b->Zb.p + b->offD[m];
+    float2* F = b->T1.p + b->offD[m];
+    float2* E = b->Mb.p + b->offD[m];
+    cq::TcStructure s3;
+    s3.a_upper = true;
+    s3.b_lower = true;
+    s3.lower_only = true;
+    f.push_back(group(Z, false, false, Np, NN, Z, false, true, Np, NN, F, Np, NN, Np, Np, Np, nwh, s3));
+    for (int64_t w = 0; w < nwh; ++w)
+      hp.push_back(cq::HermProblem{Z + w * NN, F + w * NN, E + w * NN, Np});
+    cq::TcStructure s4;
+    s4.a_lower = true;
+    t4.push_back(group(b->Ls.p + b->offL[m], true, false, Np, 0, E, false, true, Np, NN, F, Np, NN,
+                       Np, Np, Np, nwh, s4));
+    cq::TcStructure s5;
+    s5.b_upper = true;
+    t5.push_back(group(F, false, false, Np, NN, b->Ls.p + b->offL[m], true, true, Np, 0,
+                       b->PW.p + b->offPQ[m], Np, cols, Np, Np, Np, nwh, s5));
+  }
+  cq::tc_cgemm_grouped(f, b->gtab, s);
+  CQ_REQUIRE((int64_t)hp.size() <= 65535, COQUI_B200_EINVAL, "too many Dyson problems");
+  b->htab.ensure(hp.size() * sizeof(cq::HermProblem));
+  CQ_CHECK_CUDA(cudaMemcpyAsync(b->htab.p, hp.data(), hp.size() * sizeof(cq::HermProblem),
+                                cudaMemcpyHostToDevice, s));
+  const unsigned tiles = (unsigned)((b->nmax + 31) / 32);
+  cq::k_herm_sum_grouped<<<dim3(tiles, tiles, (unsigned)hp.size()), dim3(32, 8), 0, s>>>(
+      (const cq::HermProblem*)b->htab.p);
+  cq::count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+  cq::tc_cgemm_grouped(t4, b->gtab, s);
+  cq::tc_cgemm_grouped(t5, b->gtab, s);
+  cq::launch_ir_transform_real<float>(b->PW.p, cols, (int)nwh, (int)nth, b->dTtwR.p, s);
+  // ---- Sigma_PQ(t) = -G_PQ(t) o W(t) in place in the cache (both halves), then X^H S X ----
+  for (int64_t it = 0; it < nth; ++it) {
+    const bool minus = it < nt / 2;
+    float2* gp = b->cache.p + it * cols;
+    float2* gn = minus ? b->cache.p + (nt - 1 - it) * cols : nullptr;
+    cq::launch_sigma_fused<float>(gp, gn, b->PW.p + it * cols, gp, gn, cols, g0, s);
+  }
+  std::vector<cq::TcGroup> a1, a2;
+  for (int64_t m = 0; m < b->nmol; ++m) {
+    const int64_t nb = b->nb[m], Np = b->Np[m];
+    float2* U = b->UT.p + b->offX[m] * nt;  // (nt, nb, Np)
+    a1.push_back(group(b->XTs.p + b->offX[m], true, false, Np, 0, b->cache.p + b->offPQ[m], false,
+                       false, Np, cols, U, Np, nb * Np, nb, Np, Np, nt));
+    a2.push_back(group(b->XTs.p + b->offX[m], true, true, Np, 0, U, false, false, Np, nb * Np,
+                       b->Sab.p + b->offG[m], nb, nb * nb, nb, nb, Np, nt));
+  }
+  cq::tc_cgemm_grouped(a1, b->gtab, s);
+  cq::tc_cgemm_grouped(a2, b->gtab, s);
+  cq::launch_to_c128<float>(b->Sab.p, b->Sig.p, b->nG, s);
+  // factorisation status
+  std::vector<int> info(nprob);
+  CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), b->info.p, nprob * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CQ_CHECK_CUDA(cudaStreamSynchronize(s));
+  for (int64_t i = 0; i < nprob; ++i)
+    CQ_REQUIRE(info[i] == 0, COQUI_B200_ENOTHPD,
+               "I - L^H Pi L is not positive definite (problem " + std::to_string(i) + ")");
+}
+
+}  // namespace
+
+extern "C" {
+
+int coqui_b200_batch_create(coqui_b200_batch** out, int64_t nmol, const int64_t* nb,
+                            const int64_t* Np, int64_t nt_f, int64_t nw_b, int device) {
+  if (!out || nmol < 1 || !nb || !Np || nt_f < 2 || nw_b < 1) return COQUI_B200_EINVAL;
+  *out = nullptr;
+  for (int64_t m = 0; m < nmol; ++m)
+    if (nb[m] < 1 || Np[m] < 1) return COQUI_B200_EINVAL;
+  auto* b = new (std::nothrow) coqui_b200_batch();
+  if (!b) return COQUI_B200_ENOMEM;
+  b->dev = device;
+  int rc = bguarded(b, [&] {
+    CQ_CHECK_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+    CQ_CHECK_CUDA(cudaEventCreate(&b->ev0));
+    CQ_CHECK_CUDA(cudaEventCreate(&b->ev1));
+    if (cusolverDnCreate(&b->sol) != CUSOLVER_STATUS_SUCCESS)
+      throw cq::Error(COQUI_B200_ECUDA, "cusolverDnCreate failed");
+    CQ_SOLVER_CHECK(cusolverDnSetStream(b->sol, b->st));
+    b->nmol = nmol;
+    b->nt = nt_f;
+    b->nth = (nt_f + 1) / 2;
+    b->nwb = nw_b;
+    b->nwh = (nw_b + 1) / 2;
+    b->nb.assign(nb, nb + nmol);
+    b->Np.assign(Np, Np + nmol);
+    b->have_thc.assign(nmol, 0);
+    for (int64_t m = 0; m < nmol; ++m) {
+      b->offPQ.push_back(b->cols);
+      b->offX.push_back(b->nX);
+      b->offG.push_back(b->nG);
+      b->offL.push_back(b->nL);
+      b->offD.push_back(b->nD);
+      b->cols += Np[m] * Np[m];
+      b->nX += Np[m] * nb[m];
+      b->nG += nt_f * nb[m] * nb[m];
+      b->nL += Np[m] * Np[m];
+      b->nD += b->nwh * Np[m] * Np[m];
+      b->nmax = std::max(b->nmax, Np[m]);
+    }
+    const int64_t nrow = std::max(b->nth, b->nwh);
+    b->Xs.ensure(b->nX);
+    b->XTs.ensure(b->nX);
+    b->Ls.ensure(b->nL);
+    b->LHs.ensure(b->nL);
+    b->G.ensure(b->nG);
+    b->Sig.ensure(b->nG);
+    b->Gt.ensure(b->nG);
+    b->Sab.ensure(b->nG);
+    b->T.ensure(b->nX * nt_f);
+    b->UT.ensure(b->nX * nt_f);
+    b->cache.ensure(nt_f * b->cols);
+    b->PW.ensure(nrow * b->cols);
+    b->T1.ensure(b->nD);
+    b->Mb.ensure(b->nD);
+    b->Zb.ensure(b->nD);
+    b->Ab.ensure(b->nD);
+    std::vector<int64_t> offs(b->offG);
+    b->dofG.ensure(nmol);
+    b->dnb.ensure(nmol);
+    CQ_CHECK_CUDA(cudaMemcpyAsync(b->dofG.p, offs.data(), nmol * sizeof(int64_t),
+                                  cudaMemcpyHostToDevice, b->st));
+    CQ_CHECK_CUDA(cudaMemcpyAsync(b->dnb.p, b->nb.data(), nmol * sizeof(int64_t),
+                                  cudaMemcpyHostToDevice, b->st));
+  });
+  if (rc != COQUI_B200_OK) {
+    coqui_b200_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return COQUI_B200_OK;
+}
+
+void coqui_b200_batch_destroy(coqui_b200_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->dev);
+  if (b->st) cudaStreamSynchronize(b->st);
+  cudaStream_t st = b->st;
+  cusolverDnHandle_t sol = b->sol;
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+  if (sol) cusolverDnDestroy(sol);
+  if (st) cudaStreamDestroy(st);
+}
+
+double coqui_b200_batch_last_ms(const coqui_b200_batch* b) { return b ? b->last_ms : 0.0; }
+
+const char* coqui_b200_batch_last_error(const coqui_b200_batch* b) {
+  return b ? b->err.c_str() : "";
+}
+
+int coqui_b200_batch_set_ir(coqui_b200_batch* b, const double* Twt_bb, const double* Ttw_bb,
+                            const double* tau_mesh_x) {
+  return bguarded(b, [&] {
+    CQ_REQUIRE(Twt_bb && Ttw_bb && tau_mesh_x, COQUI_B200_EINVAL, "null IR table");
+    const int64_t nt = b->nt;
+    for (int64_t it = 0; it < nt; ++it)
+      CQ_REQUIRE(std::abs(std::abs(tau_mesh_x[it]) - std::abs(tau_mesh_x[nt - it - 1])) <= 1e-6,
+                 COQUI_B200_EPHSYM, "IAFT grid is not compatible with particle-hole symmetry");
+    cq::ph_symmetric_matrices(Twt_bb, Ttw_bb, nt, b->nwb, b->Twt_pos, b->Ttw_pos);
+    double re = 0, im = 0;
+    for (const auto* v : {&b->Twt_pos, &b->Ttw_pos})
+      for (const double2& z : *v) {
+        re = std::max(re, std::abs(z.x));
+        im = std::max(im, std::abs(z.y));
+      }
+    CQ_REQUIRE(im <= 1e-12 * re, COQUI_B200_EUNSUPPORTED,
+               "the batched path needs real particle-hole symmetric IR matrices");
+    std::vector<double> a(b->Twt_pos.size()), c(b->Ttw_pos.size());
+    for (size_t i = 0; i < a.size(); ++i) a[i] = b->Twt_pos[i].x;
+    for (size_t i = 0; i < c.size(); ++i) c[i] = b->Ttw_pos[i].x;
+    b->dTwtR.ensure(a.size());
+    b->dTtwR.ensure(c.size());
+    CQ_CHECK_CUDA(cudaMemcpyAsync(b->dTwtR.p, a.data(), a.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, b->st));
+    CQ_CHECK_CUDA(cudaMemcpyAsync(b->dTtwR.p, c.data(), c.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, b->st));
+    CQ_CHECK_CUDA(cudaStreamSynchronize(b->st));
+    b->have_ir = true;
+  });
+}
+
+int coqui_b200_batch_set_thc(coqui_b200_batch* b, int64_t m, const double* X_Pa, const double* V_PQ) {
+  return bguarded(b, [&] {
+    CQ_REQUIRE(m >= 0 && m < b->nmol && X_Pa && V_PQ, COQUI_B200_EINVAL, "bad arguments");
+    const int64_t Np = b->Np[m], nb = b->nb[m];
+    DevBuf<double2> X, L, LH;
+    X.ensure(Np * nb);
+    L.ensure(Np * Np);
+    LH.ensure(Np * Np);
+    CQ_CHECK_CUDA(cudaMemcpyAsync(X.p, X_Pa, Np * nb * sizeof(double2), cudaMemcpyHostToDevice, b->st));
+    CQ_CHECK_CUDA(cudaMemcpyAsync(L.p, V_PQ, Np * Np * sizeof(double2), cudaMemcpyHostToDevice, b->st));
+    const int info = cq::cholesky_lower_batched(b->sol, L.p, Np, 1, b->st);
+    CQ_REQUIRE(info == 0, COQUI_B200_ENOTHPD, "Coulomb matrix V is not positive definite");
+    cq::launch_zero_upper_and_adjoint(L.p, LH.p, Np, 1, b->st);
+    cq::to_split(X.p, b->Xs.p + b->offX[m], Np, nb, 1, false, b->st);
+    cq::to_split(X.p, b->XTs.p + b->offX[m], Np, nb, 1, true, b->st);
+    cq::to_split(L.p, b->Ls.p + b->offL[m], Np, Np, 1, false, b->st);
+    cq::to_split(LH.p, b->LHs.p + b->offL[m], Np, Np, 1, false, b->st);
+    CQ_CHECK_CUDA(cudaStreamSynchronize(b->st));
+    b->have_thc[m] = 1;
+  });
+}
+
+int coqui_b200_batch_gw_iteration(coqui_b200_batch* b, const double* const* G_list,
+                                  double* const* Sigma_list) {
+  return bguarded(b, [&] {
+    CQ_REQUIRE(b->have_ir, COQUI_B200_EINVAL, "batch_set_ir not called");
+    for (int64_t m = 0; m < b->nmol; ++m)
+      CQ_REQUIRE(b->have_thc[m], COQUI_B200_EINVAL, "batch_set_thc not called for every molecule");
+    CQ_REQUIRE(G_list, COQUI_B200_EINVAL, "null G list");
+    for (int64_t m = 0; m < b->nmol; ++m) {
+      CQ_REQUIRE(G_list[m], COQUI_B200_EINVAL, "null G");
+      CQ_CHECK_CUDA(cudaMemcpyAsync(b->G.p + b->offG[m], G_list[m],
+                                    b->nt * b->nb[m] * b->nb[m] * sizeof(double2),
+                                    cudaMemcpyHostToDevice, b->st));
+    }
+    CQ_CHECK_CUDA(cudaEventRecord(b->ev0, b->st));
+    batch_gw(b);
+    CQ_CHECK_CUDA(cudaEventRecord(b->ev1, b->st));
+    CQ_CHECK_CUDA(cudaEventSynchronize(b->ev1));
+    float ms = 0;
+    CQ_CHECK_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    b->last_ms = ms;
+    if (Sigma_list)
+      for (int64_t m = 0; m < b->nmol; ++m)
+        if (Sigma_list[m])
+          CQ_CHECK_CUDA(cudaMemcpyAsync(Sigma_list[m], b->Sig.p + b->offG[m],
+                                        b->nt * b->nb[m] * b->nb[m] * sizeof(double2),
+                                        cudaMemcpyDeviceToHost, b->st));
+  });
+}
+
+}  // extern "C"

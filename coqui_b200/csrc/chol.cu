@@ -226,13 +226,13 @@ __device__ void invert_lower(const double2* S, double2* Sinv, int n) {
 
 // inv_group: the inverse is formed within diagonal groups of inv_group blocks only (the
 // whole matrix when inv_group >= nblk); the tensor-core levels fill in the rest.
+// One problem: M, A (n x n), results at logdet/trace/info[0].
 template <bool INV>
-__global__ void __launch_bounds__(CT, 4) k_chol_inv(const float2* __restrict__ Mall,
-                                                    double2* __restrict__ Aall,
-                                                    double* __restrict__ logdet,
-                                                    double2* __restrict__ trace,
-                                                    int* __restrict__ info, int64_t n,
-                                                    int inv_group) {
+__device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
+                                                 double2* __restrict__ A,
+                                                 double* __restrict__ logdet,
+                                                 double2* __restrict__ trace,
+                                                 int* __restrict__ info, int64_t n, int inv_group) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* S0 = reinterpret_cast<double2*>(smem_raw);
   double2* S1 = S0 + CB * PITCH;
@@ -240,9 +240,6 @@ __global__ void __launch_bounds__(CT, 4) k_chol_inv(const float2* __restrict__ M
   __shared__ double s_ld;
   __shared__ int s_bad;
   __shared__ double s_red[2][CT];
-  const int64_t p = blockIdx.x;
-  const float2* M = Mall + p * n * n;
-  double2* A = Aall + p * n * n;
   const int nblk = (int)((n + CB - 1) / CB);
   const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
 
@@ -378,9 +375,60 @@ __global__ void __launch_bounds__(CT, 4) k_chol_inv(const float2* __restrict__ M
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    logdet[p] = 2.0 * s_ld;
-    trace[p] = make_double2(s_red[0][0], s_red[1][0]);
-    info[p] = s_bad;
+    *logdet = 2.0 * s_ld;
+    *trace = make_double2(s_red[0][0], s_red[1][0]);
+    *info = s_bad;
+  }
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(CT, 4) k_chol_inv(const float2* __restrict__ Mall,
+                                                    double2* __restrict__ Aall,
+                                                    double* __restrict__ logdet,
+                                                    double2* __restrict__ trace,
+                                                    int* __restrict__ info, int64_t n,
+                                                    int inv_group) {
+  const int64_t p = blockIdx.x;
+  chol_inv_problem<INV>(Mall + p * n * n, Aall + p * n * n, logdet + p, trace + p, info + p, n,
+                        inv_group);
+}
+
+// Problems of different sizes in one launch (one CTA each).
+__global__ void __launch_bounds__(CT, 4) k_chol_inv_grouped(const CholProblem* __restrict__ probs,
+                                                            double* __restrict__ logdet,
+                                                            double2* __restrict__ trace,
+                                                            int* __restrict__ info) {
+  const CholProblem pr = probs[blockIdx.x];
+  chol_inv_problem<true>(pr.M, pr.A, logdet + blockIdx.x, trace + blockIdx.x, info + blockIdx.x,
+                         pr.n, 1 << 30);
+}
+
+// grouped A = I - M (lower) and Z = X^H - I, blockIdx.y = problem
+__global__ void k_chol_prep_grouped(const CholProblem* __restrict__ probs) {
+  const CholProblem pr = probs[blockIdx.y];
+  const int64_t n = pr.n, total = n * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / n, c = e % n;
+    if (c <= r) {
+      const float2 m = pr.M[e];
+      pr.A[e] = make_double2((r == c ? 1.0 : 0.0) - (double)m.x, -(double)m.y);
+    }
+  }
+}
+
+__global__ void k_chol_final_grouped(const CholProblem* __restrict__ probs) {
+  const CholProblem pr = probs[blockIdx.y];
+  const int64_t n = pr.n, total = n * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / n, c = e % n;
+    float2 z = make_float2(0.f, 0.f);
+    if (c >= r) {
+      const double2 a = pr.A[e];
+      z = make_float2((float)(a.x - (r == c ? 1.0 : 0.0)), (float)a.y);
+    }
+    pr.Z[e] = z;
   }
 }
 
@@ -559,6 +607,36 @@ void launch_block_adjoint(const float2* Z, float2* Zl, int64_t Np, int64_t r0, i
              "block_adjoint: bad block");
   const dim3 g((unsigned)((b1 + 31) / 32), (unsigned)((b + 31) / 32), (unsigned)nprob);
   k_block_adjoint<<<g, dim3(32, 8), 0, s>>>(Z, Zl, Np, r0, r1, b, b1);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,
+                             double* logdet, double2* trace, int* info, cudaStream_t s) {
+  if (probs.empty()) return;
+  const int64_t np = (int64_t)probs.size();
+  CQ_REQUIRE(np <= 65535, COQUI_B200_EINVAL, "chol grouped: at most 65535 problems per launch");
+  table.ensure(np * sizeof(CholProblem));
+  CQ_CHECK_CUDA(cudaMemcpyAsync(table.p, probs.data(), np * sizeof(CholProblem),
+                                cudaMemcpyHostToDevice, s));
+  const CholProblem* t = (const CholProblem*)table.p;
+  int64_t nmax = 0;
+  for (const auto& p : probs) nmax = std::max(nmax, p.n);
+  const unsigned gx = (unsigned)std::min<int64_t>((nmax * nmax + 255) / 256, 1024);
+  k_chol_prep_grouped<<<dim3(gx, (unsigned)np), 256, 0, s>>>(t);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+  const size_t smem = (size_t)3 * CB * PITCH * sizeof(double2);
+  static bool set = false;
+  if (!set) {
+    CQ_CHECK_CUDA(cudaFuncSetAttribute(k_chol_inv_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    set = true;
+  }
+  k_chol_inv_grouped<<<(unsigned)np, CT, smem, s>>>(t, logdet, trace, info);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+  k_chol_final_grouped<<<dim3(gx, (unsigned)np), 256, 0, s>>>(t);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
 }

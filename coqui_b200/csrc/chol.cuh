@@ -12,6 +12,20 @@ namespace cq {
 void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, double2* trace,
                      int* info, int64_t Np, int64_t nprob, cudaStream_t s);
 
+// One problem of a grouped factorisation: M (n x n complex64, lower triangle read), A (n x n
+// FP64 workspace, C and C^{-H} on return), Z (n x n complex64, C^{-H} - I written).
+struct CholProblem {
+  const float2* M;
+  double2* A;
+  float2* Z;
+  int64_t n;
+};
+
+// launch_chol_inv with Z for problems of different sizes in one launch per step (prep,
+// factorisation + full FP64 inverse, Z); results per problem in table order.
+void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,
+                             double* logdet, double2* trace, int* info, cudaStream_t s);
+
 // Diagonal group edge of the FP64 inverse when the tensor cores form the off-group blocks.
 constexpr int64_t kInvGroup = 128;
 

@@ -790,31 +790,9 @@ int coqui_b200_set_ir(coqui_b200_ctx* c, const double* Twt_bb, const double* Ttw
                  "IAFT grid is not compatible with particle-hole symmetry");
     }
     auto at = [](const double* p, int64_t i) { return make_double2(p[2 * i], p[2 * i + 1]); };
-    // IAFT.icc:61-70 (tau -> w) and :116-125 (w -> tau); nt_b() == nt_f (IAFT.hpp:167-169)
-    c->Twt_pos.assign(nwh * nth, make_double2(0, 0));
-    for (int64_t n = 0; n < nwh; ++n)
-      for (int64_t it = 0; it < nth; ++it) {
-        const int64_t iw = nwb / 2 + n, imt = nt - it - 1;
-        double2 v = at(Twt_bb, iw * nt + it);
-        if (it != imt) {
-          const double2 u = at(Twt_bb, iw * nt + imt);
-          v.x += u.x;
-          v.y += u.y;
-        }
-        c->Twt_pos[n * nth + it] = v;
-      }
-    c->Ttw_pos.assign(nth * nwh, make_double2(0, 0));
-    for (int64_t it = 0; it < nth; ++it)
-      for (int64_t n = 0; n < nwh; ++n) {
-        const int64_t iw = nwb / 2 + n, imw = nwb / 2 - n;
-        double2 v = at(Ttw_bb, it * nwb + iw);
-        if (iw != imw) {
-          const double2 u = at(Ttw_bb, it * nwb + imw);
-          v.x += u.x;
-          v.y += u.y;
-        }
-        c->Ttw_pos[it * nwh + n] = v;
-      }
+    (void)nth;
+    (void)nwh;
+    cq::ph_symmetric_matrices(Twt_bb, Ttw_bb, nt, nwb, c->Twt_pos, c->Ttw_pos);
     c->Ttw_bb.resize(nt * nwb);
     for (int64_t i = 0; i < nt * nwb; ++i) c->Ttw_bb[i] = at(Ttw_bb, i);
     c->T_beta.resize(nt);

@@ -902,4 +902,34 @@ CQ_GEMM_INST(float2, double2, double2, double)
 CQ_GEMM_INST(double2, float2, double2, double)
 CQ_GEMM_INST(double2, double2, double2, double)
 
+void ph_symmetric_matrices(const double* Twt_bb, const double* Ttw_bb, int64_t nt, int64_t nwb,
+                           std::vector<double2>& Twt_pos, std::vector<double2>& Ttw_pos) {
+  const int64_t nth = (nt + 1) / 2, nwh = (nwb + 1) / 2;
+  auto at = [](const double* p, int64_t i) { return make_double2(p[2 * i], p[2 * i + 1]); };
+  Twt_pos.assign(nwh * nth, make_double2(0, 0));
+  for (int64_t n = 0; n < nwh; ++n)
+    for (int64_t it = 0; it < nth; ++it) {
+      const int64_t iw = nwb / 2 + n, imt = nt - it - 1;
+      double2 v = at(Twt_bb, iw * nt + it);
+      if (it != imt) {
+        const double2 u = at(Twt_bb, iw * nt + imt);
+        v.x += u.x;
+        v.y += u.y;
+      }
+      Twt_pos[n * nth + it] = v;
+    }
+  Ttw_pos.assign(nth * nwh, make_double2(0, 0));
+  for (int64_t it = 0; it < nth; ++it)
+    for (int64_t n = 0; n < nwh; ++n) {
+      const int64_t iw = nwb / 2 + n, imw = nwb / 2 - n;
+      double2 v = at(Ttw_bb, it * nwb + iw);
+      if (iw != imw) {
+        const double2 u = at(Ttw_bb, it * nwb + imw);
+        v.x += u.x;
+        v.y += u.y;
+      }
+      Ttw_pos[it * nwh + n] = v;
+    }
+}
+
 }  // namespace cq

@@ -87,4 +87,10 @@ struct GemmDesc {
 template <typename TA, typename TB, typename TC, typename Acc>
 void launch_gemm_simt(const GemmDesc& d, const TA* A, const TB* B, TC* C, cudaStream_t s);
 
+// Particle-hole symmetric IR matrices (IAFT.icc:61-70 tau -> w, :116-125 w -> tau; nt_b() is
+// nt_f, IAFT.hpp:167-169) from the bosonic tables Twt_bb (nwb, nt), Ttw_bb (nt, nwb) given as
+// (re, im) pairs: Twt_pos (nwh, nth), Ttw_pos (nth, nwh).
+void ph_symmetric_matrices(const double* Twt_bb, const double* Ttw_bb, int64_t nt, int64_t nwb,
+                           std::vector<double2>& Twt_pos, std::vector<double2>& Ttw_pos);
+
 }  // namespace cq

@@ -278,19 +278,18 @@ template <class Cfg, bool A64, bool B64> struct Staging {
   }
 };
 
+// One output tile (rows m0.., columns n0.. of problem bz) of the split-TF32 product.
 template <int BNC, int NP, int ST, bool A64, bool B64>
-__global__ void __launch_bounds__(NP + 32, (NP == 128 ? 2 : 1)) k_tc_cgemm(TcParams p) {
+__device__ __forceinline__ void tc_tile(const TcParams& p, int64_t bz, int64_t m0, int64_t n0,
+                                        unsigned char* smem_raw) {
   using Cfg = TileCfg<BNC, NP, ST>;
   constexpr int kStages = ST;
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * Cfg::STAGE);
   // bars[0..ST) full, bars[ST..2ST) empty, bars[2ST] accumulator ready, then the TMEM base
   uint64_t* acc_bar = bars + 2 * kStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t bz = blockIdx.z;
-  const int64_t m0 = (int64_t)blockIdx.y * kBM, n0 = (int64_t)blockIdx.x * BNC;
   if (p.lower_only && n0 > m0 + kBM - 1) return;  // tile strictly above the diagonal
 
   // K blocks (16 complex each) that can be nonzero for this tile
@@ -447,6 +446,47 @@ __global__ void __launch_bounds__(NP + 32, (NP == 128 ? 2 : 1)) k_tc_cgemm(TcPar
                  "r"((uint32_t)Cfg::TMEM_COLS)
                  : "memory");
   }
+}
+
+template <int BNC, int NP, int ST, bool A64, bool B64>
+__global__ void __launch_bounds__(NP + 32, (NP == 128 ? 2 : 1))
+    k_tc_cgemm(const __grid_constant__ TcParams p) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  tc_tile<BNC, NP, ST, A64, B64>(p, blockIdx.z, (int64_t)blockIdx.y * kBM, (int64_t)blockIdx.x * BNC,
+                                 smem_raw);
+}
+
+// Grouped form: one launch over several problems of different shapes and strides (each group
+// a batched product); the flattened tile index picks the group by binary search.
+struct TcGroupDev {
+  TcParams p;
+  int64_t tiles_n, tiles_m, tile_begin;
+};
+
+template <int BNC, int NP, int ST, bool A64, bool B64>
+__global__ void __launch_bounds__(NP + 32, (NP == 128 ? 2 : 1))
+    k_tc_cgemm_grouped(const TcGroupDev* __restrict__ groups, int ngroups) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ TcParams sp;
+  __shared__ int64_t s_bz, s_m0, s_n0;
+  if (threadIdx.x == 0) {
+    const int64_t t = blockIdx.x;
+    int lo = 0, hi = ngroups - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (groups[mid].tile_begin <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const TcGroupDev& g = groups[lo];
+    const int64_t local = t - g.tile_begin, per_b = g.tiles_n * g.tiles_m;
+    const int64_t r = local % per_b;
+    sp = g.p;
+    s_bz = local / per_b;
+    s_m0 = (r / g.tiles_n) * kBM;
+    s_n0 = (r % g.tiles_n) * BNC;
+  }
+  __syncthreads();
+  tc_tile<BNC, NP, ST, A64, B64>(sp, s_bz, s_m0, s_n0, smem_raw);
 }
 
 template <int BNC, int NP, int ST, bool A64, bool B64>
@@ -649,6 +689,107 @@ void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, i
   k_c64_to_c128<<<grid_for(t, 256), 256, 0, s>>>(Sab, out, t);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+namespace {
+TcParams make_params(const TcGroup& g) {
+  TcParams p;
+  p.A = g.A;
+  p.Bt = g.Bt;
+  p.C = g.C;
+  p.M = g.M;
+  p.N = g.N;
+  p.K = g.K;
+  p.lda = g.lda;
+  p.ldb = g.ldb;
+  p.ldc = g.ldc;
+  p.sA = g.sA;
+  p.sB = g.sB;
+  p.sC = g.sC;
+  p.a64 = g.a_split;
+  p.b64 = g.b_split;
+  p.conj_a = g.conj_a;
+  p.conj_b = g.conj_b;
+  p.a_upper = g.st.a_upper;
+  p.a_lower = g.st.a_lower;
+  p.b_lower = g.st.b_lower;
+  p.b_upper = g.st.b_upper;
+  p.lower_only = g.st.lower_only;
+  p.a_ident = g.st.a_ident;
+  p.b_ident = g.st.b_ident;
+  p.a_mod = g.st.a_mod;
+  p.a_q0 = g.st.a_q0;
+  p.b_mod = g.st.b_mod;
+  p.b_q0 = g.st.b_q0;
+  return p;
+}
+
+template <int BNC, int NP, int ST, bool A64, bool B64>
+void launch_grouped(const std::vector<TcGroup>& gs, DevBuf<unsigned char>& table, cudaStream_t s) {
+  using Cfg = TileCfg<BNC, NP, ST>;
+  auto fn = k_tc_cgemm_grouped<BNC, NP, ST, A64, B64>;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    CQ_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+    attr_set[dev] = true;
+  }
+  std::vector<TcGroupDev> h;
+  int64_t tiles = 0;
+  for (const TcGroup& g : gs) {
+    TcGroupDev d;
+    d.p = make_params(g);
+    d.tiles_n = (g.N + BNC - 1) / BNC;
+    d.tiles_m = (g.M + kBM - 1) / kBM;
+    d.tile_begin = tiles;
+    tiles += d.tiles_n * d.tiles_m * g.batch;
+    h.push_back(d);
+  }
+  CQ_REQUIRE(tiles <= 2147483647, COQUI_B200_EINVAL, "tc_cgemm_grouped: too many tiles");
+  table.ensure(h.size() * sizeof(TcGroupDev));
+  CQ_CHECK_CUDA(cudaMemcpyAsync(table.p, h.data(), h.size() * sizeof(TcGroupDev),
+                                cudaMemcpyHostToDevice, s));
+  fn<<<(unsigned)tiles, Cfg::THREADS, Cfg::SMEM, s>>>((const TcGroupDev*)table.p, (int)h.size());
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+template <bool A64, bool B64>
+void grouped_dispatch(const std::vector<TcGroup>& gs, DevBuf<unsigned char>& table, cudaStream_t s) {
+  int64_t maxK = 0, maxN = 0;
+  for (const TcGroup& g : gs) {
+    maxK = std::max(maxK, g.K);
+    maxN = std::max(maxN, g.N);
+  }
+  if (maxK <= 64) {
+    if (maxN >= 128) launch_grouped<128, 128, 1, A64, B64>(gs, table, s);
+    else if (maxN > 32) launch_grouped<64, 128, 1, A64, B64>(gs, table, s);
+    else launch_grouped<32, 128, 1, A64, B64>(gs, table, s);
+  } else {
+    if (maxN >= 128) launch_grouped<128, 256, 2, A64, B64>(gs, table, s);
+    else if (maxN > 32) launch_grouped<64, 256, 2, A64, B64>(gs, table, s);
+    else launch_grouped<32, 256, 2, A64, B64>(gs, table, s);
+  }
+}
+}  // namespace
+
+void tc_cgemm_grouped(const std::vector<TcGroup>& groups, DevBuf<unsigned char>& table,
+                      cudaStream_t s) {
+  if (groups.empty()) return;
+  const bool a64 = groups[0].a_split, b64 = groups[0].b_split;
+  for (const TcGroup& g : groups) {
+    CQ_REQUIRE(g.a_split == a64 && g.b_split == b64, COQUI_B200_EINVAL,
+               "tc_cgemm_grouped: all groups need the same operand formats");
+    CQ_REQUIRE(g.M > 0 && g.N > 0 && g.K > 0 && g.batch > 0, COQUI_B200_EINVAL,
+               "tc_cgemm_grouped: empty group");
+    CQ_REQUIRE(!(g.st.a_ident && g.a_split) && !(g.st.b_ident && g.b_split), COQUI_B200_EINVAL,
+               "tc_cgemm_grouped: identity shift needs a complex64 operand");
+  }
+  if (a64 && b64) grouped_dispatch<true, true>(groups, table, s);
+  else if (a64) grouped_dispatch<true, false>(groups, table, s);
+  else if (b64) grouped_dispatch<false, true>(groups, table, s);
+  else grouped_dispatch<false, false>(groups, table, s);
 }
 
 }  // namespace cq

@@ -60,6 +60,25 @@ void tc_cgemm_nt(const void* A, bool a_split, bool conj_a, int64_t lda, int64_t 
                  int64_t sC, int64_t M, int64_t N, int64_t K, int64_t batch, cudaStream_t s,
                  const TcStructure& st = TcStructure{});
 
+// One group of a grouped product: a batched "NT" product as tc_cgemm_nt describes.
+struct TcGroup {
+  const void* A = nullptr;
+  bool a_split = false, conj_a = false;
+  int64_t lda = 0, sA = 0;
+  const void* Bt = nullptr;
+  bool b_split = false, conj_b = false;
+  int64_t ldb = 0, sB = 0;
+  float2* C = nullptr;
+  int64_t ldc = 0, sC = 0;
+  int64_t M = 0, N = 0, K = 0, batch = 1;
+  TcStructure st;
+};
+
+// All groups in one launch (same operand formats; the tile configuration follows the largest
+// K and N).  table is the device copy of the group descriptors.
+void tc_cgemm_grouped(const std::vector<TcGroup>& groups, DevBuf<unsigned char>& table,
+                      cudaStream_t s);
+
 // Returns (and clears) the device flag set when a bounded wait inside a tensor-core kernel
 // gave up (nonzero = a kernel timed out).
 int tc_take_error();

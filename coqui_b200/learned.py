@@ -107,3 +107,60 @@ def train(X, T, width=256, epochs=20, batch=4096, lr=1e-3, seed=0):
     net = capi.Mlp(4, width, 2, seed=seed)
     loss = net.train(X, T, batch=batch, epochs=epochs, lr=lr, seed=seed)
     return net, loss
+
+
+def report(n_train=64, n_test=4, grid=3, nb=48, nocc=24, Np=384, epochs=20, tol=1e-9, seed=0,
+           mode=capi.FP64):
+    """Config-5 style study: train on n_train seeded systems' plain-loop trajectories, then
+    compare plain damping, damping + network and DIIS on n_test held-out systems run to
+    |dE| < tol and residual < tol; for each run also the first iteration whose total energy is
+    within 1e-6 Ha of the converged one.  Returns a dict of the measurements."""
+    from .iaft import IAFT
+    from .synthetic import make_system
+    ft = IAFT(1000.0, 10.0, "low")
+    t0 = time.perf_counter()
+    trajs = [trajectory(make_system(grid, nb, nocc, Np, seed=1000 + i), ft) for i in range(n_train)]
+    t_traj = time.perf_counter() - t0
+    X, T = dataset(trajs, seed=seed)
+    t0 = time.perf_counter()
+    net, loss = train(X, T, epochs=epochs, seed=seed)
+    t_train = time.perf_counter() - t0
+    runs = []
+    for i in range(n_test):
+        s = make_system(grid, nb, nocc, Np, seed=5000 + i)
+        c = make_context(s, ft, mode)
+        G0 = s.G0(ft)
+        row = {}
+        for name, kw in (("damping", dict()), ("damping+mlp", dict(mlp=net)),
+                         ("diis", dict(alg="diis", mixing=0.2))):
+            r = run_loop(c, G0, tol_e=tol, tol_r=tol, **kw)
+            e = [h["e_tot"] for h in r["history"]]
+            evals = np.cumsum([h["evaluations"] for h in r["history"]])
+            first = next(i for i in range(len(e)) if all(abs(x - e[-1]) < 1e-6 for x in e[i:]))
+            row[name] = dict(iterations=r["iterations"], evaluations=r["evaluations"],
+                             wall_s=r["wall_s"], e_tot=r["e_tot"], learned_steps=r["learned_steps"],
+                             withdrawn=r["withdrawn"], iterations_to_1e6=first + 1,
+                             evaluations_to_1e6=int(evals[first]),
+                             residuals=[h["residual"] for h in r["history"]])
+        runs.append(row)
+        c.close()
+    net.close()
+    return dict(config=dict(grid=grid, nb=nb, nocc=nocc, Np=Np, n_train=n_train, n_test=n_test,
+                            tol=tol, mixing=0.7, mode="fp64" if mode == capi.FP64 else "mixed"),
+                trajectories_s=t_traj, train_s=t_train, samples=int(X.shape[0]),
+                loss_first=float(loss[0]), loss_last=float(loss[-1]), runs=runs)
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="learned self-energy update study")
+    ap.add_argument("--train", type=int, default=64)
+    ap.add_argument("--test", type=int, default=4)
+    ap.add_argument("--grid", type=int, default=3)
+    ap.add_argument("--nb", type=int, default=48)
+    ap.add_argument("--nocc", type=int, default=24)
+    ap.add_argument("--Np", type=int, default=384)
+    ap.add_argument("--epochs", type=int, default=20)
+    a = ap.parse_args()
+    print(json.dumps(report(a.train, a.test, a.grid, a.nb, a.nocc, a.Np, a.epochs), indent=1))

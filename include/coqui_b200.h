@@ -209,6 +209,33 @@ COQUI_B200_API int coqui_b200_mlp_train(coqui_b200_mlp* mlp, const float* X, con
                                         int64_t n_samples, int64_t batch, int64_t epochs,
                                         double lr, uint64_t seed, float* loss_history);
 
+/* ---- uneven batch of independent Gamma-only molecules (one k-point each, their own nb and Np,
+   shared IR grid) with fused launches: grouped tensor-core GEMMs, one grouped FP64
+   factorisation launch, Hadamard products and IR transforms over all molecules' columns.
+   No counterpart in the reference, which runs one system per process; the per-molecule path
+   is the single-system context above with nk = 1.  Mixed precision only. ---- */
+typedef struct coqui_b200_batch coqui_b200_batch;
+
+COQUI_B200_API int coqui_b200_batch_create(coqui_b200_batch** batch, int64_t nmol,
+                                           const int64_t* nb, const int64_t* Np, int64_t nt_f,
+                                           int64_t nw_b, int device);
+COQUI_B200_API void coqui_b200_batch_destroy(coqui_b200_batch* batch);
+COQUI_B200_API const char* coqui_b200_batch_last_error(const coqui_b200_batch* batch);
+/* Device time (CUDA events on the batch's stream) of the last batch GW iteration, ms. */
+COQUI_B200_API double coqui_b200_batch_last_ms(const coqui_b200_batch* batch);
+/* Shared bosonic IR tables as for coqui_b200_set_ir (Twt_bb (nw_b, nt_f), Ttw_bb (nt_f, nw_b),
+   tau_mesh_x (nt_f)). */
+COQUI_B200_API int coqui_b200_batch_set_ir(coqui_b200_batch* batch, const double* Twt_bb,
+                                           const double* Ttw_bb, const double* tau_mesh_x);
+/* THC data of molecule m: X_Pa (Np, nb), V_PQ (Np, Np) complex128. */
+COQUI_B200_API int coqui_b200_batch_set_thc(coqui_b200_batch* batch, int64_t m, const double* X_Pa,
+                                            const double* V_PQ);
+/* One GW iteration (update_w + evaluate) of every molecule: G_list[m] (nt_f, nb_m, nb_m) in,
+   Sigma_list[m] (nt_f, nb_m, nb_m) out (the list or entries may be NULL). */
+COQUI_B200_API int coqui_b200_batch_gw_iteration(coqui_b200_batch* batch,
+                                                 const double* const* G_list,
+                                                 double* const* Sigma_list);
+
 /* Building blocks (same layouts as the reference's arguments). */
 COQUI_B200_API int coqui_b200_primary_to_aux(coqui_b200_ctx* ctx, int64_t n_tau, const double* O_tskab,
                               double* O_tskPQ);
