@@ -36,7 +36,8 @@ SYMBOLS = [
     "coqui_b200_mlp_train", "coqui_b200_mlp_extrapolate", "coqui_b200_scgw_set_mlp",
     "coqui_b200_scgw_sigma_diag_w", "coqui_b200_batch_create", "coqui_b200_batch_destroy",
     "coqui_b200_batch_last_error", "coqui_b200_batch_set_ir", "coqui_b200_batch_set_thc",
-    "coqui_b200_batch_gw_iteration", "coqui_b200_batch_last_ms",
+    "coqui_b200_batch_gw_iteration", "coqui_b200_batch_last_ms", "coqui_b200_set_autotune",
+    "coqui_b200_tuned_shapes",
 ]
 
 
@@ -124,6 +125,10 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_batch_gw_iteration.argtypes = [P, P, P]
     lib.coqui_b200_batch_last_ms.argtypes = [P]
     lib.coqui_b200_batch_last_ms.restype = D
+    lib.coqui_b200_set_autotune.argtypes = [ctypes.c_int]
+    lib.coqui_b200_set_autotune.restype = None
+    lib.coqui_b200_tuned_shapes.argtypes = []
+    lib.coqui_b200_tuned_shapes.restype = I64
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -519,3 +524,12 @@ class Batch:
     def last_ms(self):
         """Device time of the last gw_iteration (CUDA events), ms."""
         return float(self.lib.coqui_b200_batch_last_ms(self.h))
+
+
+def set_autotune(on: bool):
+    """Tile-shape autotuner of the tensor-core GEMMs (process-wide)."""
+    load().coqui_b200_set_autotune(1 if on else 0)
+
+
+def tuned_shapes() -> int:
+    return int(load().coqui_b200_tuned_shapes())

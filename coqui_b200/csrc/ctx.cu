@@ -1591,4 +1591,8 @@ int coqui_b200_gm_energy(coqui_b200_ctx* c, const double* G_tskij, const double*
   });
 }
 
+void coqui_b200_set_autotune(int on) { cq::tc_set_autotune(on); }
+
+int64_t coqui_b200_tuned_shapes(void) { return cq::tc_tuned_shapes(); }
+
 }  // extern "C"

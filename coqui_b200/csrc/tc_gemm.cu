@@ -13,11 +13,15 @@
 //
 // CTA tile: 128 rows x BNC complex columns (UMMA M = 128, N = 2 BNC), 16 complex (32 real)
 // of K per pipeline stage = one 128-byte swizzle row.  Warps 0-7 stage operands (global ->
-// registers, one stage ahead -> split -> swizzled st.shared) and then drain TMEM through a
+// registers, two stages ahead -> split -> swizzled st.shared) and then drain TMEM through a
 // shared-memory transpose into coalesced rows; warp 8 allocates TMEM and one of its lanes
 // issues the MMAs.  Known triangular structure of A or B trims each tile's K range.  Waits
 // are bounded by a 2 s global-timer budget that sets an error flag instead of hanging.
+#include <atomic>
 #include <cstdint>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -519,23 +523,81 @@ void launch_tc(const TcParams& p, int64_t batch, cudaStream_t s) {
   }
 }
 
+// Tile configurations: (BNC, producer threads, stages).  Every configuration forms the same
+// products in the same K order, so the results are identical and only the speed differs.
+constexpr int kNumCfg = 6;
+
+template <bool A64, bool B64>
+void launch_cfg(int cfg, const TcParams& p, int64_t batch, cudaStream_t s) {
+  switch (cfg) {
+    case 0: launch_tc<32, 128, 1, A64, B64>(p, batch, s); break;
+    case 1: launch_tc<64, 128, 1, A64, B64>(p, batch, s); break;
+    case 2: launch_tc<128, 128, 1, A64, B64>(p, batch, s); break;
+    case 3: launch_tc<32, 256, 2, A64, B64>(p, batch, s); break;
+    case 4: launch_tc<64, 256, 2, A64, B64>(p, batch, s); break;
+    default: launch_tc<128, 256, 2, A64, B64>(p, batch, s); break;
+  }
+}
+
+// Default choice: short K gets one stage and four producer warps (several CTAs per SM), long
+// K two stages and eight producer warps; the tile width follows N.
+int heuristic_cfg(const TcParams& p) {
+  const int w = p.N >= 128 ? 2 : (p.N > 32 ? 1 : 0);
+  return (p.K <= 64 ? 0 : 3) + w;
+}
+
+// Autotuner: the first product of each shape class runs every configuration once (timed with
+// CUDA events on the launching stream) and the fastest is kept for the class.
+std::atomic<int> g_autotune{-1};  // -1: not yet read from COQUI_B200_AUTOTUNE (default on)
+std::mutex g_tune_mu;
+std::map<std::vector<int64_t>, int> g_tuned;
+
+bool autotune_on() {
+  int v = g_autotune.load();
+  if (v < 0) {
+    const char* e = std::getenv("COQUI_B200_AUTOTUNE");
+    v = (e && e[0] == '0') ? 0 : 1;
+    g_autotune.store(v);
+  }
+  return v == 1;
+}
+
 template <bool A64, bool B64>
 void dispatch_n(const TcParams& p, int64_t batch, cudaStream_t s) {
-  if (p.K <= 64) {  // short K: one stage, four producer warps, several CTAs per SM
-    if (p.N >= 128)
-      launch_tc<128, 128, 1, A64, B64>(p, batch, s);
-    else if (p.N > 32)
-      launch_tc<64, 128, 1, A64, B64>(p, batch, s);
-    else
-      launch_tc<32, 128, 1, A64, B64>(p, batch, s);
-  } else {
-    if (p.N >= 128)
-      launch_tc<128, 256, 2, A64, B64>(p, batch, s);
-    else if (p.N > 32)
-      launch_tc<64, 256, 2, A64, B64>(p, batch, s);
-    else
-      launch_tc<32, 256, 2, A64, B64>(p, batch, s);
+  if (!autotune_on()) return launch_cfg<A64, B64>(heuristic_cfg(p), p, batch, s);
+  int64_t bb = 1;
+  while (bb < batch) bb <<= 1;  // batch class: next power of two
+  const std::vector<int64_t> key = {p.M, p.N, p.K, bb, A64, B64, p.conj_a, p.conj_b, p.a_upper,
+                                    p.a_lower, p.b_lower, p.b_upper, p.lower_only};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return launch_cfg<A64, B64>(it->second, p, batch, s);
   }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CQ_CHECK_CUDA(cudaStreamIsCapturing(s, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return launch_cfg<A64, B64>(heuristic_cfg(p), p, batch, s);
+  cudaEvent_t ev[kNumCfg + 1];
+  for (auto& e : ev) CQ_CHECK_CUDA(cudaEventCreate(&e));
+  CQ_CHECK_CUDA(cudaEventRecord(ev[0], s));
+  for (int c = 0; c < kNumCfg; ++c) {
+    launch_cfg<A64, B64>(c, p, batch, s);
+    CQ_CHECK_CUDA(cudaEventRecord(ev[c + 1], s));
+  }
+  CQ_CHECK_CUDA(cudaEventSynchronize(ev[kNumCfg]));
+  int best = heuristic_cfg(p);
+  float best_ms = 1e30f;
+  for (int c = 0; c < kNumCfg; ++c) {
+    float ms = 0;
+    CQ_CHECK_CUDA(cudaEventElapsedTime(&ms, ev[c], ev[c + 1]));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[key] = best;
 }
 
 }  // namespace
@@ -790,6 +852,13 @@ void tc_cgemm_grouped(const std::vector<TcGroup>& groups, DevBuf<unsigned char>&
   else if (a64) grouped_dispatch<true, false>(groups, table, s);
   else if (b64) grouped_dispatch<false, true>(groups, table, s);
   else grouped_dispatch<false, false>(groups, table, s);
+}
+
+void tc_set_autotune(int on) { g_autotune.store(on ? 1 : 0); }
+
+int64_t tc_tuned_shapes() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return (int64_t)g_tuned.size();
 }
 
 }  // namespace cq

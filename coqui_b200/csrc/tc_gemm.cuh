@@ -79,6 +79,11 @@ struct TcGroup {
 void tc_cgemm_grouped(const std::vector<TcGroup>& groups, DevBuf<unsigned char>& table,
                       cudaStream_t s);
 
+// Tile-configuration autotuner of tc_cgemm_nt (default on; COQUI_B200_AUTOTUNE=0 or
+// tc_set_autotune(0) selects the built-in heuristic) and the number of tuned shape classes.
+void tc_set_autotune(int on);
+int64_t tc_tuned_shapes();
+
 // Returns (and clears) the device flag set when a bounded wait inside a tensor-core kernel
 // gave up (nonzero = a kernel timed out).
 int tc_take_error();

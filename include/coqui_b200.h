@@ -255,6 +255,13 @@ COQUI_B200_API int coqui_b200_set_profiling(coqui_b200_ctx* ctx, int on);
 COQUI_B200_API int coqui_b200_kernel_stats(const coqui_b200_ctx* ctx, char* names, int name_len,
                                            double* ms, int64_t* launches, int n);
 
+/* Tile-shape autotuner of the tensor-core GEMMs (process-wide, on by default; the environment
+   variable COQUI_B200_AUTOTUNE=0 starts with it off): the first product of each shape class
+   runs every tile configuration once and keeps the fastest (all configurations give identical
+   results).  coqui_b200_tuned_shapes returns the number of tuned classes. */
+COQUI_B200_API void coqui_b200_set_autotune(int on);
+COQUI_B200_API int64_t coqui_b200_tuned_shapes(void);
+
 /* Number of kernels this library launched since the context was created. */
 COQUI_B200_API int64_t coqui_b200_kernel_launches(const coqui_b200_ctx* ctx);
 

@@ -185,3 +185,16 @@ def test_errors_are_codes_not_aborts(base):
     c.set_thc(s.X, s.V)
     W, _ = c.update_w(base.G)
     assert maxabs(W, base.dW) < 1e-6
+
+
+def test_autotuned_tiles_give_identical_results(base):
+    """Every tile configuration forms the same products in the same K order: the tuned and
+    the heuristic choice agree bit for bit."""
+    capi.set_autotune(False)
+    c = base.ctx(capi.MIXED)
+    S0, _ = c.gw_iteration(base.G)
+    capi.set_autotune(True)
+    S1, _ = c.gw_iteration(base.G)
+    assert capi.tuned_shapes() > 0
+    assert np.array_equal(S0, S1)
+    c.close()
