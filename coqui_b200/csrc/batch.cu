@@ -241,10 +241,12 @@ void batch_gw(Batch* b) {
       hp.push_back(cq::HermProblem{Z + w * NN, F + w * NN, E + w * NN, Np});
     cq::TcStructure s4;
     s4.a_lower = true;
+    s4.lower_only = true;  // W is Hermitian: its lower triangle needs T only down there
     t4.push_back(group(b->Ls.p + b->offL[m], true, false, Np, 0, E, false, true, Np, NN, F, Np, NN,
                        Np, Np, Np, nwh, s4));
     cq::TcStructure s5;
     s5.b_upper = true;
+    s5.lower_only = true;
     t5.push_back(group(F, false, false, Np, NN, b->Ls.p + b->offL[m], true, true, Np, 0,
                        b->PW.p + b->offPQ[m], Np, cols, Np, Np, Np, nwh, s5));
   }
@@ -260,6 +262,8 @@ void batch_gw(Batch* b) {
   CQ_CHECK_CUDA(cudaGetLastError());
   cq::tc_cgemm_grouped(t4, b->gtab, s);
   cq::tc_cgemm_grouped(t5, b->gtab, s);
+  for (int64_t m = 0; m < b->nmol; ++m)  // upper triangle of W from the lower one
+    cq::launch_mirror_upper(b->PW.p + b->offPQ[m], b->Np[m], nwh, s, cols);
   cq::launch_ir_transform_real<float>(b->PW.p, cols, (int)nwh, (int)nth, b->dTtwR.p, s);
   // ---- Sigma_PQ(t) = -G_PQ(t) o W(t) in place in the cache (both halves), then X^H S X ----
   for (int64_t it = 0; it < nth; ++it) {

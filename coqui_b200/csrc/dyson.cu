@@ -76,6 +76,35 @@ __global__ void k_herm_sum(const float2* __restrict__ DH, const float2* __restri
   }
 }
 
+// Hermitian completion: A[i][j] = conj(A[j][i]) for j > i (32 x 32 tiles on or above the
+// diagonal, the lower tile read through shared memory)
+__global__ void k_mirror_upper(float2* __restrict__ A, int64_t n, int64_t stride) {
+  __shared__ float2 tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
+  if (j0 < i0) return;
+  float2* a = A + (int64_t)blockIdx.z * stride;
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {  // lower tile (j0.., i0..)
+    const int64_t r = j0 + ty, c = i0 + threadIdx.x;
+    tile[ty][threadIdx.x] = (r < n && c < n) ? a[r * n + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t i = i0 + ty, j = j0 + threadIdx.x;
+    if (i < n && j < n && j > i) {
+      const float2 v = tile[threadIdx.x][ty];  // A[j][i]
+      a[i * n + j] = make_float2(v.x, -v.y);
+    }
+  }
+}
+
+void launch_mirror_upper(float2* A, int64_t n, int64_t nbatch, cudaStream_t s, int64_t stride) {
+  CQ_REQUIRE(nbatch <= 65535, COQUI_B200_EINVAL, "mirror: too many problems per launch");
+  const unsigned t = (unsigned)((n + 31) / 32);
+  k_mirror_upper<<<dim3(t, t, (unsigned)nbatch), dim3(32, 8), 0, s>>>(A, n, stride > 0 ? stride : n * n);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
 void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t nbatch,
                                    cudaStream_t s) {
   const int64_t total = Np * Np * nbatch;
@@ -296,19 +325,24 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         dim3 hb(32, 8), hg((unsigned)((Np + 31) / 32), (unsigned)((Np + 31) / 32), (unsigned)nb);
         k_herm_sum<<<hg, hb, 0, s>>>(Z, F, E, Np);
         count_launch();
+        // W is Hermitian: its lower triangle W_ij (j <= i) = sum_{k <= j} T_ik conj(L_jk) needs
+        // T = L E only on and below the diagonal tiles, and the upper triangle is its mirror.
         // T = L E  (E Hermitian: B(k, n) = conj(E[n][k]))
         TcStructure s4;
         s4.a_lower = true;  // L lower
+        s4.lower_only = true;
         s4.a_mod = nq;
         s4.a_q0 = q0;
         tc_cgemm_nt(Ls, true, false, Np, NN, E, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s4);
         // W = T L^H  (B(k, n) = conj(L[n][k])), written over Pi
         TcStructure s5;
         s5.b_upper = true;  // B(k, n) = conj(L[n][k]) vanishes for k > n
+        s5.lower_only = true;
         s5.b_mod = nq;
         s5.b_q0 = q0;
         tc_cgemm_nt(F, false, false, Np, NN, Ls, true, true, Np, NN, (float2*)Pi, Np, NN, Np, Np,
                     Np, nb, s, s5);
+        launch_mirror_upper((float2*)Pi, Np, nb, s);
       } else if (a.want_w) {
         // Y = C^{-1} L^H: column-major Y^T C^T = (L^H)^T  (right, upper)
         CQ_CHECK_CUDA(cudaMemcpyAsync(Y, LH, nb * NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));

@@ -24,6 +24,10 @@ int cholesky_lower_batched(cusolverDnHandle_t sol, double2* A, int64_t Np, int64
                            cudaStream_t s);
 
 // Zero the strict upper triangle of L and write LH = L^H (row-major), batched.
+// A[i][j] = conj(A[j][i]) for j > i, nbatch n x n complex64 matrices `stride` elements apart
+// (0: n * n).
+void launch_mirror_upper(float2* A, int64_t n, int64_t nbatch, cudaStream_t s, int64_t stride = 0);
+
 void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t nbatch,
                                    cudaStream_t s);
 
