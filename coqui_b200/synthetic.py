@@ -116,6 +116,8 @@ WORKLOADS = {
     "g0w0_k4_nb64_np512": dict(n=4, nb=64, nocc=24, Np=512, beta=1000.0, lam=1e4, prec="low"),
     # same orbitals / N_mu on a 2x2x2 grid: the small case used for kernel profiles
     "g0w0_k2_nb64_np512": dict(n=2, nb=64, nocc=24, Np=512, beta=1000.0, lam=1e4, prec="low"),
+    # 64 k-points at a smaller N_mu: the case used for profiles of the k <-> R kernels
+    "g0w0_k4_nb48_np384": dict(n=4, nb=48, nocc=24, Np=384, beta=1000.0, lam=1e4, prec="low"),
     "rpa_gw_k6_nb96_np1024": dict(n=6, nb=96, nocc=48, Np=1024, beta=1000.0, lam=1e5, prec="low"),
     "scgw_k3_nb48_np384": dict(n=3, nb=48, nocc=24, Np=384, beta=1000.0, lam=1e4, prec="low"),
 }
