@@ -90,6 +90,15 @@ struct coqui_b200_ctx {
   DevBuf<unsigned char> Gcache;
   bool gcache_valid = false;
 
+  // Dyson results per (iW, q) problem on the device
+  DevBuf<int> dinfo;
+  DevBuf<double> dlogdet;
+  DevBuf<double2> dtrace;
+  // CUDA graph of the resident-G GW iteration (captured on the first of consecutive calls)
+  bool capturing = false;
+  cudaGraphExec_t gexec = nullptr;
+  int64_t calls = 0, graph_call = -2, graph_launches = 0;
+
   // self-consistent loop: fermionic IR grid, mean field, iteration state
   bool have_irf = false, have_mf = false;
   int64_t nwf = 0;
@@ -135,6 +144,7 @@ struct coqui_b200_ctx {
   size_t elem() const { return mode == COQUI_B200_FP64 ? sizeof(double2) : sizeof(float2); }
 
   void mark(const char* name) {
+    if (capturing) return;  // the phases of a captured iteration are not recorded
     cudaEvent_t e;
     CQ_CHECK_CUDA(cudaEventCreate(&e));
     CQ_CHECK_CUDA(cudaEventRecord(e, st));
@@ -172,6 +182,7 @@ void settle(Ctx* c) {
 
 template <typename F> int guarded(Ctx* c, F&& f) {
   if (!c) return COQUI_B200_EINVAL;
+  ++c->calls;  // a captured iteration graph is replayed only by directly consecutive calls
   try {
     CQ_CHECK_CUDA(cudaSetDevice(c->dev));
     f();
@@ -673,6 +684,7 @@ std::pair<double, double> diis_device(Ctx* c, double2* FS, int64_t it) {
   return {cF, cS};
 }
 
+
 // =======================================================================================
 // ABI
 // =======================================================================================
@@ -731,6 +743,7 @@ void coqui_b200_destroy(coqui_b200_ctx* c) {
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
   if (c->cs) cudaStreamSynchronize(c->cs);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
   for (auto* b : {&c->X, &c->V, &c->L, &c->LH, &c->chi, &c->G, &c->Sig, &c->Tproj, &c->stage,
                   &c->dTwt, &c->dTtw, &c->eps, &c->Gx})
     b->release();
@@ -1000,6 +1013,14 @@ void dyson_all(Ctx* c, bool want_w, bool want_e, std::vector<double>* logdet,
   a.mixed = (c->mode == COQUI_B200_MIXED);
   a.PW = c->PW.p;
   a.prof = &c->prof;
+  const int64_t nprob = c->nwh * c->nq;
+  c->dinfo.ensure(nprob);
+  c->dlogdet.ensure(nprob);
+  c->dtrace.ensure(nprob);
+  a.info = c->dinfo.p;
+  a.logdet = c->dlogdet.p;
+  a.trace = c->dtrace.p;
+  a.defer_check = c->capturing;
   std::vector<double> ld;
   std::vector<double2> t;
   cq::dyson_run(a, c->blas, c->sol, c->dyn, c->st, want_e ? &ld : nullptr, want_e ? &t : nullptr);
@@ -1152,6 +1173,52 @@ void sigma_device(Ctx* c, double* host_out) {
   c->w_in_R = false;
 }
 
+
+// One GW iteration of the resident G as a CUDA graph (update_w + Sigma, no host transfers).
+void gw_iteration_graph(Ctx* c) {
+  c->begin_timing();
+  const bool replay = c->gexec && c->graph_call == c->calls - 1;
+  if (!replay) {
+    if (c->gexec) {
+      cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+    }
+    c->g_pipelined = false;  // the resident G is complete on the device
+    const int64_t l0 = cq::launches_total();
+    CQ_CHECK_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+    c->capturing = true;
+    cudaGraph_t g = nullptr;
+    try {
+      update_w_device(c);
+      sigma_device(c, nullptr);
+    } catch (...) {
+      c->capturing = false;
+      if (cudaStreamEndCapture(c->st, &g) == cudaSuccess && g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    c->capturing = false;
+    CQ_CHECK_CUDA(cudaStreamEndCapture(c->st, &g));
+    c->graph_launches = cq::launches_total() - l0;
+    const cudaError_t e = cudaGraphInstantiate(&c->gexec, g, 0);
+    cudaGraphDestroy(g);
+    CQ_CHECK_CUDA(e);
+  } else {
+    cq::count_launch(c->graph_launches);  // the replay launches the captured kernels again
+  }
+  CQ_CHECK_CUDA(cudaGraphLaunch(c->gexec, c->st));
+  c->mark("GW_ITERATION_GRAPH");
+  c->graph_call = c->calls;
+  // factorisation status of every (iW, q) problem of this iteration
+  const int64_t nprob = c->nwh * c->nq;
+  std::vector<int> info(nprob);
+  CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), c->dinfo.p, nprob * sizeof(int), cudaMemcpyDeviceToHost,
+                                c->st));
+  CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+  for (int64_t i = 0; i < nprob; ++i)
+    CQ_REQUIRE(info[i] == 0, COQUI_B200_ENOTHPD, "I - L^H Pi L is not positive definite");
+  c->end_timing();
+}
 }  // namespace
 
 int coqui_b200_update_w(coqui_b200_ctx* c, const double* G_tskij, double* dW_qtPQ,
@@ -1209,6 +1276,13 @@ int coqui_b200_gw_iteration(coqui_b200_ctx* c, const double* G_tskij, double* Si
                             double* eps_inv_head) {
   return guarded(c, [&] {
     require_ready(c, true, true, true);
+    // resident G, no host outputs: the device work of the iteration runs as one CUDA graph,
+    // captured on the first of a run of such calls and replayed by the following ones
+    if (!G_tskij && !Sigma_tskij && !eps_inv_head && c->mode == COQUI_B200_MIXED &&
+        !c->prof.on && c->g_resident) {
+      gw_iteration_graph(c);
+      return;
+    }
     c->begin_timing();
     upload_G(c, G_tskij);
     c->mark("h2d_G");

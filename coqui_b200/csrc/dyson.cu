@@ -185,8 +185,12 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
     hA[i] = A + i * NN;
     hY[i] = Y ? Y + i * NN : nullptr;
   }
-  CQ_CHECK_CUDA(cudaMemcpyAsync(dptrA, hA.data(), nbq * sizeof(void*), cudaMemcpyHostToDevice, s));
-  CQ_CHECK_CUDA(cudaMemcpyAsync(dptrY, hY.data(), nbq * sizeof(void*), cudaMemcpyHostToDevice, s));
+  if (!a.mixed) {  // pointer arrays of the cuSOLVER / cuBLAS batched calls (FP64 form)
+    CQ_CHECK_CUDA(cudaMemcpyAsync(dptrA, hA.data(), nbq * sizeof(void*), cudaMemcpyHostToDevice, s));
+    CQ_CHECK_CUDA(cudaMemcpyAsync(dptrY, hY.data(), nbq * sizeof(void*), cudaMemcpyHostToDevice, s));
+  }
+  CQ_REQUIRE(!a.mixed || (a.info && a.logdet && a.trace), COQUI_B200_EINVAL,
+             "dyson_run: result arrays missing");
 
   if (a.want_e) {
     logdet->assign(nw * nq, 0.0);
@@ -257,19 +261,18 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       if (a.mixed) {
         Prof::Scope sc(a.prof, "dyson_chol_inv");
         if (tc_inverse)
-          launch_chol_group_inv((const float2*)Mb, A, dld, dtr, dinfo, Np, nb, s);
+          launch_chol_group_inv((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0, Np,
+                                nb, s);
         else
-          launch_chol_inv((const float2*)Mb, A, a.want_w ? (float2*)Y : nullptr, dld, dtr, dinfo,
-                          Np, nb, s);
+          launch_chol_inv((const float2*)Mb, A, a.want_w ? (float2*)Y : nullptr, a.logdet + p0,
+                          a.trace + p0, a.info + p0, Np, nb, s);
       } else {
         Prof::Scope sc(a.prof, "dyson_potrf");
         potrf_ptrs(sol, dptrA, Np, dinfo, nb);
       }
-      CQ_CHECK_CUDA(cudaMemcpyAsync(info_h.data(), dinfo, nb * sizeof(int), cudaMemcpyDeviceToHost, s));
-      if (a.want_e && a.mixed) {
-        CQ_CHECK_CUDA(cudaMemcpyAsync(ld_h.data(), dld, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CQ_CHECK_CUDA(cudaMemcpyAsync(tr_h.data(), dtr, nb * sizeof(double2), cudaMemcpyDeviceToHost, s));
-      } else if (a.want_e) {
+      if (!a.mixed)
+        CQ_CHECK_CUDA(cudaMemcpyAsync(info_h.data(), dinfo, nb * sizeof(int), cudaMemcpyDeviceToHost, s));
+      if (a.want_e && !a.mixed) {
         Prof::Scope sc(a.prof, "rpa_logdet");
         if (a.mixed)
           launch_logdet_trace<float>(A, (const float2*)Mb, dld, dtr, Np, nb, s);
@@ -365,6 +368,7 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
                                             (int)Np, NN, (int)nb));
         }
       }
+      if (a.mixed) continue;  // results stay on the device until all chunks ran
       CQ_CHECK_CUDA(cudaStreamSynchronize(s));
       for (int64_t i = 0; i < nb; ++i) {
         if (info_h[i] != 0)
@@ -377,6 +381,22 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         }
       }
     }
+  }
+  if (a.mixed && !a.defer_check) {
+    std::vector<int> info(nprob);
+    CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), a.info, nprob * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (a.want_e) {
+      CQ_CHECK_CUDA(cudaMemcpyAsync(logdet->data(), a.logdet, nprob * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+      CQ_CHECK_CUDA(cudaMemcpyAsync(trace->data(), a.trace, nprob * sizeof(double2),
+                                    cudaMemcpyDeviceToHost, s));
+    }
+    CQ_CHECK_CUDA(cudaStreamSynchronize(s));
+    for (int64_t i = 0; i < nprob; ++i)
+      if (info[i] != 0)
+        throw Error(COQUI_B200_ENOTHPD, "I - L^H Pi L is not positive definite at (w=" +
+                                            std::to_string(i / nq) + ", q=" + std::to_string(i % nq) +
+                                            ")");
   }
 }
 

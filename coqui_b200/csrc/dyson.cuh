@@ -5,7 +5,8 @@
 // Here the Hermitian form of the same quantities is used:
 //   V = L L^H (once per q),  M = L^H Pi L,  I - M = C C^H  (FP64 Cholesky),
 //   Tr(Pi V) = Tr M,  ln det(I - Pi V) = 2 sum_i ln C_ii,
-//   W = L (I - M)^{-1} L^H - V = Y^H Y - V  with  Y = C^{-1} L^H.
+//   W = L [(I - M)^{-1} - I] L^H = L (D + D^H + D^H D) L^H,  D = C^{-1} - I  (mixed form),
+//   W = Y^H Y - V,  Y = C^{-1} L^H  (FP64 form).
 #pragma once
 
 #include <cublas_v2.h>
@@ -23,11 +24,11 @@ namespace cq {
 int cholesky_lower_batched(cusolverDnHandle_t sol, double2* A, int64_t Np, int64_t nbatch,
                            cudaStream_t s);
 
-// Zero the strict upper triangle of L and write LH = L^H (row-major), batched.
 // A[i][j] = conj(A[j][i]) for j > i, nbatch n x n complex64 matrices `stride` elements apart
 // (0: n * n).
 void launch_mirror_upper(float2* A, int64_t n, int64_t nbatch, cudaStream_t s, int64_t stride = 0);
 
+// Zero the strict upper triangle of L and write LH = L^H (row-major), batched.
 void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t nbatch,
                                    cudaStream_t s);
 
@@ -41,6 +42,13 @@ struct DysonArgs {
   bool want_w = true, want_e = false, mixed = true;
   unsigned char* PW = nullptr;  // (nw, nq, Np, Np): Pi(iW) in, W(iW) out (if want_w)
   Prof* prof = nullptr;
+  // mixed form: per-problem results on the device (nw * nq entries, n * nq + q); with
+  // defer_check the host neither waits nor checks (the caller reads `info` later, e.g. after
+  // replaying a captured graph)
+  int* info = nullptr;
+  double* logdet = nullptr;
+  double2* trace = nullptr;
+  bool defer_check = false;
 };
 
 // Runs every (iW, q) problem; fills logdet / trace (indexed n * nq + q) if want_e.

@@ -685,6 +685,25 @@ __global__ void k_transpose_c64(const double2* __restrict__ in, float2* __restri
   }
 }
 
+// out[b] = in[b]^T, (rows x cols) complex64 blocks; 32 x 32 tiles through shared memory
+__global__ void k_transpose_f2(const float2* __restrict__ in, float2* __restrict__ out,
+                               int64_t rows, int64_t cols) {
+  __shared__ float2 tile[32][33];
+  const int64_t b = blockIdx.z;
+  const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+  const float2* src = in + b * rows * cols;
+  float2* dst = out + b * rows * cols;
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t r = r0 + ty, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[ty][threadIdx.x] = src[r * cols + c];
+  }
+  __syncthreads();
+  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
+    const int64_t c = c0 + ty, r = r0 + threadIdx.x;  // out row c, column r
+    if (r < rows && c < cols) dst[c * rows + r] = tile[threadIdx.x][ty];
+  }
+}
+
 __global__ void k_c64_to_c128(const float2* __restrict__ in, double2* __restrict__ out,
                               int64_t total) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
@@ -739,11 +758,21 @@ void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, i
   op.tmp.ensure((size_t)nbatch * Np * nb * sizeof(float2) + (size_t)nbatch * nb * nb * sizeof(float2));
   float2* UT = (float2*)op.tmp.p;
   float2* Sab = UT + nbatch * Np * nb;
+  // U = S X (Np x nb, K = Np) with the Np rows on the 128-row tiles, then U^T (the big product
+  // would waste half of every tile with the nb rows of U^T = X^T S^T on them)
+  op.tmp2.ensure((size_t)nbatch * Np * nb * sizeof(float2));
+  float2* U = (float2*)op.tmp2.p;
+  TcStructure sb;
+  sb.b_mod = nk;
+  tc_cgemm_nt(Sk, false, false, Np, Np * Np, XTs, true, false, Np, nb * Np, U, nb, Np * nb, Np,
+              nb, Np, nbatch, s, sb);
+  CQ_REQUIRE(nbatch <= 65535, COQUI_B200_EINVAL, "a2p: too many problems per launch");
+  k_transpose_f2<<<dim3((unsigned)((nb + 31) / 32), (unsigned)((Np + 31) / 32), (unsigned)nbatch),
+                   dim3(32, 8), 0, s>>>(U, UT, Np, nb);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
   TcStructure sx;
   sx.a_mod = nk;
-  // U^T = X^T S^T (nb x Np, K = Np): A = X^T, Bt = S
-  tc_cgemm_nt(XTs, true, false, Np, nb * Np, Sk, false, false, Np, Np * Np, UT, Np, nb * Np, nb,
-              Np, Np, nbatch, s, sx);
   // Sigma_ab = X^H U (nb x nb, K = Np): A(a, P) = conj(X^T[a][P]), Bt = U^T
   tc_cgemm_nt(XTs, true, true, Np, nb * Np, UT, false, false, Np, nb * Np, Sab, nb, nb * nb, nb,
               nb, Np, nbatch, s, sx);

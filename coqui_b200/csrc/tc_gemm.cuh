@@ -10,10 +10,11 @@ struct TcOperand {
   const double2* X = nullptr;
   int64_t nk = 0, Np = 0, nb = 0;
   DevBuf<unsigned char> packed;  // pre-split X (nk, Np, nb) then X^T (nk, nb, Np)
-  DevBuf<unsigned char> tmp;     // per-call intermediates
+  DevBuf<unsigned char> tmp, tmp2;  // per-call intermediates
   void release() {
     packed.release();
     tmp.release();
+    tmp2.release();
   }
 };
 
