@@ -135,10 +135,11 @@ def algorithmic_work(w, s, ft):
         "sigma_fused": ("hbm", 5 * nk * ncol * 8, None),
         "dft_w": ("hbm", 2 * nth * nk * ncol * 8, None),
         "ir_transform": ("hbm", (nth + nwh) * nk * ncol * 8, None),
-        # M = L^H Pi L with L triangular and M Hermitian: 3/4 of two dense products
-        "dyson_M_gemm": ("tensor", None, 0.75 * 8 * n3 * P),
-        # F = D^H D (1/6), T = L E (1/2), W = T L^H (1/2)
-        "dyson_W_gemm": ("tensor", None, (1 / 6 + 0.5 + 0.5) * 8 * n3 * P),
+        # M = L^H Pi L: P1 = L^H Pi (L^H triangular, Np^3 / 2) and the lower triangle of
+        # L^H P1^H (Np^3 / 6) complex multiply-adds
+        "dyson_M_gemm": ("tensor", None, (0.5 + 1 / 6) * 8 * n3 * P),
+        # lower triangles of F = D^H D (1/6), T = L E (1/3) and W = T L^H (1/6)
+        "dyson_W_gemm": ("tensor", None, (1 / 6 + 1 / 3 + 1 / 6) * 8 * n3 * P),
         # FP64 Cholesky (Np^3 / 6 complex multiply-adds) + inverse of the 128 x 128 diagonal
         # groups (Np 128^2 / 6); the whole inverse (Np^3 / 6) when Np <= 128
         "dyson_chol_inv": ("fp64", None, 8 * (n3 / 6 + (Np * min(Np, 128) ** 2) / 6) * P),

@@ -206,11 +206,11 @@ void batch_gw(Batch* b) {
     s1.a_upper = true;
     p1.push_back(group(b->LHs.p + b->offL[m], true, false, Np, 0, b->PW.p + b->offPQ[m], false, true,
                        Np, cols, b->T1.p + b->offD[m], Np, NN, Np, Np, Np, nwh, s1));
-    cq::TcStructure s2;
-    s2.b_lower = true;
+    cq::TcStructure s2;  // M = L^H (P1)^H, P1 = L^H Pi (Pi Hermitian)
+    s2.a_upper = true;
     s2.lower_only = true;
-    p2.push_back(group(b->T1.p + b->offD[m], false, false, Np, NN, b->LHs.p + b->offL[m], true, true,
-                       Np, 0, b->Mb.p + b->offD[m], Np, NN, Np, Np, Np, nwh, s2));
+    p2.push_back(group(b->LHs.p + b->offL[m], true, false, Np, 0, b->T1.p + b->offD[m], false, true,
+                       Np, NN, b->Mb.p + b->offD[m], Np, NN, Np, Np, Np, nwh, s2));
   }
   cq::tc_cgemm_grouped(p1, b->gtab, s);
   cq::tc_cgemm_grouped(p2, b->gtab, s);

@@ -232,13 +232,14 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         s1.a_q0 = q0;
         tc_cgemm_nt(LHs, true, false, Np, NN, Pi, false, true, Np, NN, (float2*)T1, Np, NN, Np,
                     Np, Np, nb, s, s1);
-        // M = P1 L  (B(k, n) = L[k][n] = conj(LH[n][k]))
+        // M = L^H Q with Q = Pi L = P1^H (Pi Hermitian): B(k, n) = Q[k][n] = conj(P1[n][k]).
+        // With L^H upper the lower triangle of M needs k >= i only (Np^3 / 6 products).
         TcStructure s2;
-        s2.b_lower = true;     // L lower triangular
-        s2.b_mod = nq;
-        s2.b_q0 = q0;
+        s2.a_upper = true;     // L^H upper triangular
+        s2.a_mod = nq;
+        s2.a_q0 = q0;
         s2.lower_only = true;  // M Hermitian: the Cholesky reads the lower triangle
-        tc_cgemm_nt(T1, false, false, Np, NN, LHs, true, true, Np, NN, (float2*)Mb, Np, NN, Np, Np,
+        tc_cgemm_nt(LHs, true, false, Np, NN, T1, false, true, Np, NN, (float2*)Mb, Np, NN, Np, Np,
                     Np, nb, s, s2);
       } else {
         // row-major C = A B  ->  column-major C^T = B^T A^T
