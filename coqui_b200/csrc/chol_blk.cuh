@@ -1,0 +1,370 @@
+// Blocked FP64 Cholesky / log-determinant / triangular inverse of one problem per CTA.
+// Included once per block size inside a namespace that defines
+//   CB (block edge), CT (threads, (CB / 4)^2), TW (thread grid edge, CB / 4),
+//   PITCH (shared-memory row pitch in double2, CB + 1), MINB (CTAs per SM for the launch bounds)
+// and the complex helpers cmul_, cmulc_, conj_.  (No include guard: it is meant to be
+// included more than once.)
+// smem tile <- global block (rows r0.., cols c0..) of an ld x ld row-major matrix, rb x cb valid
+__device__ __forceinline__ void load_blk(double2* S, const double2* G, int64_t ld, int64_t r0,
+                                         int64_t c0, int rb, int cb) {
+  double2 v[CB * CB / CT];
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {  // all loads in flight before the smem stores
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;
+    v[u] = (r < rb && c < cb) ? G[(r0 + r) * ld + c0 + c] : make_double2(0, 0);
+  }
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    S[(i / CB) * PITCH + i % CB] = v[u];
+  }
+}
+// smem tile <- conj transpose of a global block: S[r][c] = conj(G[c0 + c][r0 + r])... given as
+// (the block stored at rows gr0, cols gc0 with gr x gc valid) -> S = G_blk^H
+__device__ __forceinline__ void load_blk_adj(double2* S, const double2* G, int64_t ld, int64_t gr0,
+                                             int64_t gc0, int gr, int gc) {
+  double2 v[CB * CB / CT];
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;  // S[c][r] = conj(G[gr0 + r][gc0 + c])
+    v[u] = (r < gr && c < gc) ? conj_(G[(gr0 + r) * ld + gc0 + c]) : make_double2(0, 0);
+  }
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    S[(i % CB) * PITCH + i / CB] = v[u];
+  }
+}
+// S (lower triangular part) <- adjoint of the upper triangle of a global diagonal block:
+// S[r][c] = conj(G[r0 + c][r0 + r]) for r >= c, 0 above
+__device__ __forceinline__ void load_blk_adjU(double2* S, const double2* G, int64_t ld, int64_t r0,
+                                              int nb) {
+  double2 v[CB * CB / CT];
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;  // v = conj(G[r0 + r][r0 + c]) feeds S[c][r], c >= r
+    v[u] = (r < nb && c < nb && c >= r) ? conj_(G[(r0 + r) * ld + r0 + c]) : make_double2(0, 0);
+  }
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    S[(i % CB) * PITCH + i / CB] = v[u];
+  }
+}
+// upper triangle of a global diagonal block <- adjoint of the lower-triangular S:
+// G[r0 + c][r0 + r] = conj(S[r][c]) for r >= c
+__device__ __forceinline__ void store_blk_adjU(const double2* S, double2* G, int64_t ld, int64_t r0,
+                                               int nb) {
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;
+    if (r < nb && c < nb && r >= c) G[(r0 + c) * ld + r0 + r] = conj_(S[r * PITCH + c]);
+  }
+}
+__device__ __forceinline__ void store_blk(const double2* S, double2* G, int64_t ld, int64_t r0,
+                                          int64_t c0, int rb, int cb) {
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;
+    if (r < rb && c < cb) G[(r0 + r) * ld + c0 + c] = S[r * PITCH + c];
+  }
+}
+
+// acc[i][j] (rows ty + TW i, cols tx + TW j) += sum_k X[r][k] * Y'[k][c] over k < K, where
+// Y'(k, c) = conj(Y[c][k]) if ADJ_Y (product with Y^H) else Y[k][c].
+template <bool ADJ_Y>
+__device__ __forceinline__ void mma_tile(const double2* X, const double2* Y, int K,
+                                         double2 (&acc)[4][4]) {
+  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
+  for (int k = 0; k < K; ++k) {
+    double2 a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = X[(ty + TW * i) * PITCH + k];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      b[j] = ADJ_Y ? conj_(Y[(tx + TW * j) * PITCH + k]) : Y[k * PITCH + tx + TW * j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        acc[i][j].x = fma(a[i].x, b[j].x, fma(-a[i].y, b[j].y, acc[i][j].x));
+        acc[i][j].y = fma(a[i].x, b[j].y, fma(a[i].y, b[j].x, acc[i][j].y));
+      }
+  }
+}
+
+// acc[i][j] -= sum_k X[r][k] conj(Y[c][k])  (A - X Y^H)
+__device__ __forceinline__ void mma_tile_sub(const double2* X, const double2* Y, int K,
+                                             double2 (&acc)[4][4]) {
+  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
+  for (int k = 0; k < K; ++k) {
+    double2 a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a[i] = X[(ty + TW * i) * PITCH + k];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = Y[(tx + TW * j) * PITCH + k];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        // a * conj(b) = (ax bx + ay by) + i (ay bx - ax by)
+        acc[i][j].x = fma(-a[i].x, b[j].x, fma(-a[i].y, b[j].y, acc[i][j].x));
+        acc[i][j].y = fma(-a[i].y, b[j].x, fma(a[i].x, b[j].y, acc[i][j].y));
+      }
+  }
+}
+
+__device__ __forceinline__ void zero_acc(double2 (&acc)[4][4]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0, 0);
+}
+
+// In-place Cholesky of the lower triangle of S (n x n); adds sum ln C_ii to *ld_acc
+// (thread 0) and sets *bad if a pivot is not positive.  One barrier per column: column c is
+// used unscaled (times 1/d_c) in its rank-1 update and scaled during the next column's step.
+__device__ void factor_diag(double2* S, int n, double* ld_acc, int* bad) {
+  double prev_inv = 1.0, prev_d = 1.0;
+  for (int c = 0; c < n; ++c) {
+    __syncthreads();
+    double d = S[c * PITCH + c].x;
+    const bool good = d > 0.0;
+    d = good ? sqrt(d) : 1.0;
+    const double inv = 1.0 / d;
+    if (c > 0) {  // finish column c - 1: diagonal and scaled entries below it
+      if (threadIdx.x == 0) S[(c - 1) * PITCH + c - 1] = make_double2(prev_d, 0.0);
+      for (int r = c + threadIdx.x; r < n; r += CT) {
+        S[r * PITCH + c - 1].x *= prev_inv;
+        S[r * PITCH + c - 1].y *= prev_inv;
+      }
+    }
+    const int m = n - c - 1;
+    const double inv2 = inv * inv;
+    for (int idx = threadIdx.x; idx < m * m; idx += CT) {
+      const int r = c + 1 + idx / m, s = c + 1 + idx % m;
+      if (s <= r) {
+        const double2 u = cmulc_(S[r * PITCH + c], S[s * PITCH + c]);
+        S[r * PITCH + s].x -= u.x * inv2;
+        S[r * PITCH + s].y -= u.y * inv2;
+      }
+    }
+    if (threadIdx.x == 0) {
+      if (!good) *bad = 1;
+      *ld_acc += log(d);
+    }
+    prev_inv = inv;
+    prev_d = d;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) S[(n - 1) * PITCH + n - 1] = make_double2(prev_d, 0.0);
+  __syncthreads();
+}
+
+// Sinv = inverse of the lower-triangular S (n x n): forward substitution with one column
+// per group of CT / CB lanes of a warp (partial dot products reduced by shuffles).
+__device__ void invert_lower(const double2* S, double2* Sinv, int n) {
+  constexpr int LPC = CT / CB;  // lanes per column
+  for (int i = threadIdx.x; i < CB * CB; i += CT) Sinv[(i / CB) * PITCH + i % CB] = make_double2(0, 0);
+  __syncthreads();
+  const int c = threadIdx.x / LPC, sub = threadIdx.x % LPC;
+  const bool col = c < n;
+  if (col && sub == 0) Sinv[c * PITCH + c] = make_double2(1.0 / S[c * PITCH + c].x, 0.0);
+  __syncwarp();
+  for (int r = 1; r < n; ++r) {
+    double ax = 0, ay = 0;
+    if (col && r > c)
+      for (int k = c + sub; k < r; k += LPC) {
+        const double2 u = cmul_(S[r * PITCH + k], Sinv[k * PITCH + c]);
+        ax += u.x;
+        ay += u.y;
+      }
+#pragma unroll
+    for (int off = LPC / 2; off > 0; off >>= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, off);
+      ay += __shfl_xor_sync(0xffffffffu, ay, off);
+    }
+    if (col && r > c && sub == 0) {
+      const double inv = -1.0 / S[r * PITCH + r].x;
+      Sinv[r * PITCH + c] = make_double2(ax * inv, ay * inv);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+}
+
+// inv_group: the inverse is formed within diagonal groups of inv_group blocks only (the
+// whole matrix when inv_group >= nblk); the tensor-core levels fill in the rest.
+// One problem: M, A (n x n), results at logdet/trace/info[0].
+template <bool INV>
+__device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
+                                                 double2* __restrict__ A,
+                                                 double* __restrict__ logdet,
+                                                 double2* __restrict__ trace,
+                                                 int* __restrict__ info, int64_t n, int inv_group) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // two staging blocks: the diagonal block and its inverse, then (panel) a panel block and the
+  // inverse, (trailing update) the two panel blocks, (inverse) C_ik and X_kj
+  double2* S0 = reinterpret_cast<double2*>(smem_raw);
+  double2* S1 = S0 + CB * PITCH;
+  __shared__ double s_ld;
+  __shared__ int s_bad;
+  __shared__ double s_red[2][CT];
+  const int nblk = (int)((n + CB - 1) / CB);
+  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
+
+  if (threadIdx.x == 0) {
+    s_ld = 0.0;
+    s_bad = 0;
+  }
+  // trace of M (A = I - M was set up by k_chol_prep)
+  double tr = 0, ti = 0;
+  for (int64_t i = threadIdx.x; i < n; i += CT) {
+    const float2 m = M[i * n + i];
+    tr += m.x;
+    ti += m.y;
+  }
+  s_red[0][threadIdx.x] = tr;
+  s_red[1][threadIdx.x] = ti;
+  __syncthreads();
+
+  for (int j = 0; j < nblk; ++j) {
+    const int64_t j0 = (int64_t)j * CB;
+    const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+    // 1. diagonal block: factor and invert
+    load_blk(S0, A, n, j0, j0, jb, jb);
+    __syncthreads();
+    factor_diag(S0, jb, &s_ld, &s_bad);
+    invert_lower(S0, S1, jb);
+    // C_jj is not needed again; the upper triangle of the diagonal block keeps C_jj^{-H}
+    if (INV) store_blk_adjU(S1, A, n, j0, jb);
+    __syncthreads();
+    // 2. panel: L_ib = A_ib C_jj^{-H}
+    for (int ib = j + 1; ib < nblk; ++ib) {
+      const int64_t i0 = (int64_t)ib * CB;
+      const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+      load_blk(S0, A, n, i0, j0, rb, jb);
+      __syncthreads();
+      double2 acc[4][4];
+      zero_acc(acc);
+      mma_tile<true>(S0, S1, jb, acc);
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int r = ty + TW * i, c = tx + TW * jj;
+          if (r < rb && c < jb) A[(i0 + r) * n + j0 + c] = acc[i][jj];
+        }
+      __syncthreads();
+    }
+    // 3. trailing update of the lower triangle: A_ik -= L_ij L_kj^H
+    for (int kb = j + 1; kb < nblk; ++kb) {
+      const int64_t k0 = (int64_t)kb * CB;
+      const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
+      load_blk(S1, A, n, k0, j0, kbsz, jb);
+      for (int ib = kb; ib < nblk; ++ib) {
+        const int64_t i0 = (int64_t)ib * CB;
+        const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+        load_blk(S0, A, n, i0, j0, rb, jb);
+        __syncthreads();
+        double2 acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)  // start from the current A block (loads in flight early)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int r = ty + TW * i, c = tx + TW * jj;
+            acc[i][jj] = (r < rb && c < kbsz && (ib > kb || c <= r)) ? A[(i0 + r) * n + k0 + c]
+                                                                      : make_double2(0, 0);
+          }
+        mma_tile_sub(S0, S1, jb, acc);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int r = ty + TW * i, c = tx + TW * jj;
+            if (r < rb && c < kbsz && (ib > kb || c <= r)) A[(i0 + r) * n + k0 + c] = acc[i][jj];
+          }
+        __syncthreads();
+      }
+    }
+  }
+
+  if (INV) {
+    // X = C^{-1} block column by block column, X^H kept in the upper triangle of A
+    for (int j = 0; j < nblk; ++j) {
+      const int64_t j0 = (int64_t)j * CB;
+      const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+      const int gend = min(nblk, (j / inv_group + 1) * inv_group);
+      for (int ib = j + 1; ib < gend; ++ib) {
+        const int64_t i0 = (int64_t)ib * CB;
+        const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+        double2 acc[4][4];
+        zero_acc(acc);
+        for (int kb = j; kb < ib; ++kb) {
+          const int64_t k0 = (int64_t)kb * CB;
+          const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
+          load_blk(S1, A, n, i0, k0, rb, kbsz);  // C_ik (strictly lower block)
+          if (kb == j)
+            load_blk_adjU(S0, A, n, j0, jb);  // X_jj
+          else
+            load_blk_adj(S0, A, n, j0, k0, jb, kbsz);  // X_kj = (A_jk)^H
+          __syncthreads();
+          mma_tile<false>(S1, S0, kbsz, acc);
+          __syncthreads();
+        }
+        // X_ij = -C_ii^{-1} acc
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) S1[(ty + TW * i) * PITCH + tx + TW * jj] = acc[i][jj];
+        load_blk_adjU(S0, A, n, i0, rb);  // C_ii^{-1}
+        __syncthreads();
+        zero_acc(acc);
+        mma_tile<false>(S0, S1, rb, acc);
+        __syncthreads();
+        // A[j0 + c][i0 + r] = conj(X_ij[r][c]) = -conj(acc[r][c])
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const int r = ty + TW * i, c = tx + TW * jj;
+            if (r < rb && c < jb) A[(j0 + c) * n + i0 + r] = make_double2(-acc[i][jj].x, acc[i][jj].y);
+          }
+        __syncthreads();
+      }
+    }
+  }
+
+  // reductions
+  for (int w = CT / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s_red[0][threadIdx.x] += s_red[0][threadIdx.x + w];
+      s_red[1][threadIdx.x] += s_red[1][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *logdet = 2.0 * s_ld;
+    *trace = make_double2(s_red[0][0], s_red[1][0]);
+    *info = s_bad;
+  }
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(CT, MINB) k_chol_inv(const float2* __restrict__ Mall,
+                                                    double2* __restrict__ Aall,
+                                                    double* __restrict__ logdet,
+                                                    double2* __restrict__ trace,
+                                                    int* __restrict__ info, int64_t n,
+                                                    int inv_group) {
+  const int64_t p = blockIdx.x;
+  chol_inv_problem<INV>(Mall + p * n * n, Aall + p * n * n, logdet + p, trace + p, info + p, n,
+                        inv_group);
+}
+
