@@ -330,6 +330,15 @@ def run_ours(args, rank, world, local):
                 if kind == "tensor":
                     g["frac_of_bf16"] = g["achieved_TFLOPs"] / bf16
         groups[name] = g
+    # DRAM bytes of the screened-interaction products per (q, iW) problem from the committed
+    # ncu summary (measured on a smaller case; the traffic grows with the problem count)
+    w_bytes_per_problem = None
+    try:
+        for ln in open(os.path.join(ROOT, "profiles", "dram_traffic_g0w0_k2_nb64_np512.md")):
+            if ln.startswith("bytes_per_problem:"):
+                w_bytes_per_problem = float(ln.split(":")[1])
+    except OSError:
+        pass
     roof = None
     cand = [(g["ms_per_step"], k) for k, g in groups.items() if g["bound"] in ("hbm", "tensor")
             and ("achieved_GBps" in g or "achieved_TFLOPs" in g)]
@@ -343,9 +352,14 @@ def run_ours(args, rank, world, local):
                     "unit": "GB/s", "frac": g["achieved_GBps"] / hbm, "traffic": None,
                     "avg_launch_ms": per_ms, "peak_source": peak_src + " HBM copy"}
         else:
+            traffic = None
+            if name == "dyson_W_gemm" and w_bytes_per_problem and s.Np == 512:
+                traffic = w_bytes_per_problem * s.nk * ft.nw_half
             roof = {"kernel": name, "bound": "tensor", "achieved": g["achieved_TFLOPs"],
                     "peak": bf16, "unit": "TFLOP/s", "frac": g["achieved_TFLOPs"] / bf16,
-                    "traffic": None, "avg_launch_ms": per_ms,
+                    "traffic": traffic, "traffic_note": "DRAM bytes per step (ncu, scaled from the "
+                    "200-problem case by the problem count)" if traffic else None,
+                    "avg_launch_ms": per_ms,
                     "peak_source": peak_src + " dense bf16 cuBLAS; split-TF32 complex products "
                                    "issue 3 TF32 MMAs at half the bf16 rate per counted flop"}
 

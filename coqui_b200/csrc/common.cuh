@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cuComplex.h>
 #include <stdint.h>
 
@@ -113,6 +114,7 @@ struct Prof {
     cudaEvent_t a = nullptr;
     Scope(Prof* pr, const char* n) : p(pr && pr->on ? pr : nullptr), name(n) {
       if (p) {
+        nvtxRangePushA(n);  // profilers can select the group's kernels by this range
         cudaEventCreate(&a);
         cudaEventRecord(a, p->st);
       }
@@ -120,6 +122,7 @@ struct Prof {
     Scope(const Scope&) = delete;
     ~Scope() {
       if (!p) return;
+      nvtxRangePop();
       cudaEvent_t b;
       cudaEventCreate(&b);
       cudaEventRecord(b, p->st);
