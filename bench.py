@@ -50,6 +50,18 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(vals, world, device="cuda"):
+    """Element-wise maximum of per-rank timings over the process group (identity for one rank):
+    the replicas' step time is that of the slowest rank."""
+    if world <= 1:
+        return [float(v) for v in vals]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 class Clocks:
     """Samples nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -298,11 +310,7 @@ def run_ours(args, rank, world, local):
         c64.close()
 
     # max over ranks
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([t_step, t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step, t_e2e = float(tt[0]), float(tt[1])
+    t_step, t_e2e = max_over_ranks([t_step, t_e2e], world)
 
     # per-group achieved rates and the roofline of the dominant HBM- or tensor-bound group
     work = algorithmic_work(w, s, ft)

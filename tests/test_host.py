@@ -78,3 +78,36 @@ def test_bf16_rounding_ties_to_even():
     r = M.bf16_round(x)
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6 and r[3] == -2.5
     assert abs(r[4] - 3.140625) < 1e-12
+
+
+def test_oracle_commutator_diis_converges_faster_than_damping():
+    from coqui_b200.synthetic import make_system
+    from oracle import thc_oracle as O
+    s = make_system(2, 8, 4, 32, seed=5)
+    ft = O.IAFT(1000.0, 10.0, "low")
+    H0, S, F = s.mean_field()
+    G0 = s.G0(ft)
+    runs = {}
+    for alg, mix in (("damping", 0.7), ("diis", 0.2)):
+        hist, _, _ = O.scgw_loop(G0, s.X, s.V, H0, S, F, 0.0, ft, s.kpts, s.lattv, s.kp_grid,
+                                 30, 1e-9, alg=alg, mixing=mix, diis_start=3)
+        runs[alg] = hist
+    assert len(runs["diis"]) < len(runs["damping"])
+    assert abs(runs["diis"][-1]["e_tot"] - runs["damping"][-1]["e_tot"]) < 1e-8
+
+
+def test_learned_features_of_a_geometric_sequence():
+    from coqui_b200 import learned
+    rho = np.array([0.3, 0.5 * np.exp(0.2j)])
+    s_inf = np.array([1.0 + 1j, -2.0])
+    d = np.array([0.1, 0.05j])
+    hist = np.array([s_inf - d * rho ** j / (1 - rho) for j in range(4)])
+    X, d1, valid = learned.features(hist)
+    assert valid.all()
+    np.testing.assert_allclose(X[:, 0] + 1j * X[:, 1], rho, rtol=1e-6)  # q1 = d1 / d2
+    np.testing.assert_allclose(X[:, 2] + 1j * X[:, 3], rho, rtol=1e-6)  # q2 = d2 / d3
+    # the target of a geometric sequence is rho / (1 - rho) in units of the last step
+    tgt = (s_inf - hist[3]) / d1
+    np.testing.assert_allclose(tgt, rho / (1 - rho), rtol=1e-12)
+    Xd, Td = learned.dataset([np.concatenate([hist, s_inf[None]])], max_samples=10)
+    assert Xd.shape == (2, 4) and Td.shape == (2, 2)
