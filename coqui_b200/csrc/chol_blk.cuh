@@ -89,12 +89,21 @@ __device__ __forceinline__ void mma_tile(const double2* X, const double2* Y, int
     for (int j = 0; j < 4; ++j)
       b[j] = ADJ_Y ? conj_(Y[(tx + TW * j) * PITCH + k]) : Y[k * PITCH + tx + TW * j];
 #pragma unroll
+    for (int i = 0; i < 4; ++i)  // four passes of 16 independent FMAs (no back-to-back
+#pragma unroll                   // dependency inside a complex multiply-add)
+      for (int j = 0; j < 4; ++j) acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
+#pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        acc[i][j].x = fma(a[i].x, b[j].x, fma(-a[i].y, b[j].y, acc[i][j].x));
-        acc[i][j].y = fma(a[i].x, b[j].y, fma(a[i].y, b[j].x, acc[i][j].y));
-      }
+      for (int j = 0; j < 4; ++j) acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
   }
 }
 
@@ -111,11 +120,21 @@ __device__ __forceinline__ void mma_tile_sub(const double2* X, const double2* Y,
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        // a * conj(b) = (ax bx + ay by) + i (ay bx - ax by)
-        acc[i][j].x = fma(-a[i].x, b[j].x, fma(-a[i].y, b[j].y, acc[i][j].x));
-        acc[i][j].y = fma(-a[i].y, b[j].x, fma(a[i].x, b[j].y, acc[i][j].y));
-      }
+      for (int j = 0; j < 4; ++j) acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
+    // a * conj(b) = (ax bx + ay by) + i (ay bx - ax by), subtracted; four passes of 16
+    // independent FMAs
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j].x = fma(-a[i].x, b[j].x, acc[i][j].x);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j].y = fma(-a[i].y, b[j].x, acc[i][j].y);
   }
 }
 
