@@ -200,6 +200,105 @@ __device__ __forceinline__ void store_tile(const C* A, C* dst, int nk, int64_t n
   }
 }
 
+// Compile-time line length for a runtime DFT dimension n (1..8).
+template <typename F> __device__ __forceinline__ void with_n(int n, F&& f) {
+  switch (n) {
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 3: f(std::integral_constant<int, 3>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 5: f(std::integral_constant<int, 5>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 7: f(std::integral_constant<int, 7>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    default: break;  // rejected on the host
+  }
+}
+
+// One in-shared-memory DFT dimension (the middle one, stride n2) of a tile.
+template <typename C, int TILE, int NC>
+__device__ __forceinline__ void mid_pass(C* A, int n1, int n2, int nk, int sign) {
+  if constexpr (NC > 0) {
+    if constexpr (NC > 1) dft_dim_n<C, TILE, NC>(A, NC, NC * NC * NC, sign);
+  } else {
+    dft_dim<C, TILE>(A, n1, n2, nk, sign);
+  }
+}
+
+// Global rows (k, ncol apart) -> DFT along the innermost dimension (length N, stride 1 in k)
+// in registers -> shared tile A[k][TILE]: the load and the first DFT pass in one sweep.
+template <typename C, int TILE, int N>
+__device__ __forceinline__ void load_dft_inner(C* A, const C* __restrict__ src, int nk,
+                                               int64_t ncol, int64_t col0, int sign) {
+  const int lines = nk / N;
+  for (int i = threadIdx.x; i < lines * TILE; i += blockDim.x) {
+    const int c = i % TILE, line = i / TILE;
+    const int64_t col = col0 + c;
+    C x[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      x[m].x = 0;
+      x[m].y = 0;
+      if (col < ncol) x[m] = src[(int64_t)(line * N + m) * ncol + col];
+    }
+    dft_line<C, N>(x, sign);
+#pragma unroll
+    for (int m = 0; m < N; ++m) A[(line * N + m) * TILE + c] = x[m];
+  }
+}
+
+// Shared tile -> DFT along the innermost dimension in registers -> global rows: the last DFT
+// pass and the store in one sweep.
+template <typename C, int TILE, int N>
+__device__ __forceinline__ void dft_inner_store(const C* A, C* dst, int nk, int64_t ncol,
+                                                int64_t col0, int sign) {
+  const int lines = nk / N;
+  for (int i = threadIdx.x; i < lines * TILE; i += blockDim.x) {
+    const int c = i % TILE, line = i / TILE;
+    const int64_t col = col0 + c;
+    C x[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) x[m] = A[(line * N + m) * TILE + c];
+    dft_line<C, N>(x, sign);
+    if (col < ncol) {
+#pragma unroll
+      for (int m = 0; m < N; ++m) dst[(int64_t)(line * N + m) * ncol + col] = x[m];
+    }
+  }
+}
+
+// The outermost dimension (length N, stride `stride` = n1 n2): forward DFT of the A (and B)
+// lines, op(a, b, k_inner, c) on them in registers, inverse DFT of A (and, if inv_b, B), back to
+// shared memory: the last forward pass, the pointwise product and the first inverse pass in
+// one sweep.
+template <typename C, int TILE, int N, typename Op>
+__device__ __forceinline__ void outer_pointwise(C* A, C* B, bool inv_b, int stride, Op&& op) {
+  for (int i = threadIdx.x; i < stride * TILE; i += blockDim.x) {
+    const int c = i % TILE, inner = i / TILE;
+    C a[N], b[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) a[m] = A[(inner + m * stride) * TILE + c];
+    if (B) {
+#pragma unroll
+      for (int m = 0; m < N; ++m) b[m] = B[(inner + m * stride) * TILE + c];
+      dft_line<C, N>(b, -1);
+    }
+    dft_line<C, N>(a, -1);
+    op(a, b, inner, c);
+    dft_line<C, N>(a, +1);
+#pragma unroll
+    for (int m = 0; m < N; ++m) A[(inner + m * stride) * TILE + c] = a[m];
+    if (B && inv_b) {
+      dft_line<C, N>(b, +1);
+#pragma unroll
+      for (int m = 0; m < N; ++m) B[(inner + m * stride) * TILE + c] = b[m];
+    }
+  }
+}
+
+// Pi(t) columns: Pi = f_qR[ scale Gp(R) o conj(Gn(R)) ] with G(R) = f_Rk G(k), four shared-
+// memory sweeps per tile (load + innermost DFT, middle DFT, outermost DFT + product + inverse,
+// middle inverse, innermost inverse + store).
 template <typename R, int TILE, int NC>
 __global__ void __launch_bounds__(256) k_pi_fused(const cplx_t<R>* __restrict__ Gp,
                                                   const cplx_t<R>* __restrict__ Gn,
@@ -214,18 +313,33 @@ __global__ void __launch_bounds__(256) k_pi_fused(const cplx_t<R>* __restrict__ 
   const int64_t ntiles = (ncol + TILE - 1) / TILE;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t col0 = t * TILE;
-    load_tile<C, TILE>(A, Gp, nk, ncol, col0);
-    load_tile<C, TILE>(B, Gn, nk, ncol, col0);
+    with_n(n2, [&](auto N2) {
+      load_dft_inner<C, TILE, decltype(N2)::value>(A, Gp, nk, ncol, col0, -1);
+      load_dft_inner<C, TILE, decltype(N2)::value>(B, Gn, nk, ncol, col0, -1);
+    });
     __syncthreads();
-    dft3c<C, TILE, NC>(A, B, n0, n1, n2, -1);
-    for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) A[i] = cscale(cmulc(A[i], B[i]), scale);
+    mid_pass<C, TILE, NC>(A, n1, n2, nk, -1);
+    mid_pass<C, TILE, NC>(B, n1, n2, nk, -1);
     __syncthreads();
-    dft3c<C, TILE, NC>(A, (C*)nullptr, n0, n1, n2, +1);
-    store_tile<C, TILE>(A, Pi, nk, ncol, col0);
+    with_n(n0, [&](auto N0) {
+      constexpr int N = decltype(N0)::value;
+      outer_pointwise<C, TILE, N>(A, B, false, n1 * n2, [&](C (&a)[N], C (&b)[N], int, int) {
+#pragma unroll
+        for (int m = 0; m < N; ++m) a[m] = cscale(cmulc(a[m], b[m]), scale);
+      });
+    });
+    __syncthreads();
+    mid_pass<C, TILE, NC>(A, n1, n2, nk, +1);
+    __syncthreads();
+    with_n(n2, [&](auto N2) {
+      dft_inner_store<C, TILE, decltype(N2)::value>(A, Pi, nk, ncol, col0, +1);
+    });
     __syncthreads();
   }
 }
 
+// Sigma(t) columns (both halves): S = f_kR[ -(f_Rk G) o W_R ] (scale = -1/nk), W_R read from
+// global memory inside the outermost-dimension sweep.  In place (S may alias G).
 template <typename R, int TILE, int NC>
 __global__ void __launch_bounds__(256) k_sigma_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gm,
                                                      const cplx_t<R>* __restrict__ WR,
@@ -237,25 +351,44 @@ __global__ void __launch_bounds__(256) k_sigma_fused(const cplx_t<R>* Gp, const 
   const int nk = n0 * n1 * n2;
   C* A = reinterpret_cast<C*>(smem_raw);
   C* B = A + nk * TILE;
-  C* Wt = B + nk * TILE;
   const bool has_m = (Gm != nullptr);
   const int64_t ntiles = (ncol + TILE - 1) / TILE;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t col0 = t * TILE;
-    load_tile<C, TILE>(A, Gp, nk, ncol, col0);
-    if (has_m) load_tile<C, TILE>(B, Gm, nk, ncol, col0);
-    load_tile<C, TILE>(Wt, WR, nk, ncol, col0);
+    with_n(n2, [&](auto N2) {
+      load_dft_inner<C, TILE, decltype(N2)::value>(A, Gp, nk, ncol, col0, -1);
+      if (has_m) load_dft_inner<C, TILE, decltype(N2)::value>(B, Gm, nk, ncol, col0, -1);
+    });
     __syncthreads();
-    dft3c<C, TILE, NC>(A, has_m ? B : (C*)nullptr, n0, n1, n2, -1);
-    for (int i = threadIdx.x; i < nk * TILE; i += blockDim.x) {
-      const C w = cscale(Wt[i], scale);
-      A[i] = cmul(A[i], w);
-      if (has_m) B[i] = cmul(B[i], w);
-    }
+    mid_pass<C, TILE, NC>(A, n1, n2, nk, -1);
+    if (has_m) mid_pass<C, TILE, NC>(B, n1, n2, nk, -1);
     __syncthreads();
-    dft3c<C, TILE, NC>(A, has_m ? B : (C*)nullptr, n0, n1, n2, +1);
-    store_tile<C, TILE>(A, Sp, nk, ncol, col0);
-    if (has_m) store_tile<C, TILE>(B, Sm, nk, ncol, col0);
+    const int stride = n1 * n2;
+    with_n(n0, [&](auto N0) {
+      constexpr int N = decltype(N0)::value;
+      outer_pointwise<C, TILE, N>(A, has_m ? B : nullptr, true, stride,
+                                  [&](C (&a)[N], C (&b)[N], int inner, int c) {
+        const int64_t col = col0 + c;
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+          C w;
+          w.x = 0;
+          w.y = 0;
+          if (col < ncol) w = WR[(int64_t)(inner + m * stride) * ncol + col];
+          w = cscale(w, scale);
+          a[m] = cmul(a[m], w);
+          if (has_m) b[m] = cmul(b[m], w);
+        }
+      });
+    });
+    __syncthreads();
+    mid_pass<C, TILE, NC>(A, n1, n2, nk, +1);
+    if (has_m) mid_pass<C, TILE, NC>(B, n1, n2, nk, +1);
+    __syncthreads();
+    with_n(n2, [&](auto N2) {
+      dft_inner_store<C, TILE, decltype(N2)::value>(A, Sp, nk, ncol, col0, +1);
+      if (has_m) dft_inner_store<C, TILE, decltype(N2)::value>(B, Sm, nk, ncol, col0, +1);
+    });
     __syncthreads();
   }
 }
@@ -347,7 +480,7 @@ void launch_sigma_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gm, const cplx_t<R
   // Sigma = f_kR [ -(f_Rk G) * W_R ]; f_Rk carries 1/nk
   const R scale = (R)(-1.0 / (double)nk);
   const int tile = pick_tile<R>(nk);
-  const size_t smem = (size_t)3 * nk * tile * sizeof(cplx_t<R>);
+  const size_t smem = (size_t)2 * nk * tile * sizeof(cplx_t<R>);
   const int64_t ntiles = (ncol + tile - 1) / tile;
   const unsigned grid = (unsigned)std::min<int64_t>(ntiles, 148 * 16);
   if (tile == 32) {
