@@ -286,7 +286,7 @@ def run_ours(args, rank, world, local):
     # RPA energy time (resident G) and E_c
     ctx.rpa_energy(Gh)
     rpa = []
-    for _ in range(max(1, args.steps // 2)):
+    for _ in range(max(1, args.steps)):
         e_c = ctx.rpa_energy(None)
         rpa.append(total_ms(ctx))
     t_rpa = float(np.mean(rpa))
