@@ -108,7 +108,7 @@ struct coqui_b200_batch {
   bool have_ir = false;
   std::vector<double2> Twt_pos, Ttw_pos;
   DevBuf<double> dTwtR, dTtwR;
-  DevBuf<float4> Xs, XTs, Ls, LHs;
+  DevBuf<float2> Xs, XTs, Ls, LHs;  // complex64 tensor-core operands
   DevBuf<double2> G, Sig, Ltmp, LHtmp;
   DevBuf<float2> Gt, T, UT, Sab, cache, PW;
   DevBuf<float2> T1, Mb, Zb;
@@ -185,9 +185,9 @@ void batch_gw(Batch* b) {
   for (int64_t m = 0; m < b->nmol; ++m) {
     const int64_t nb = b->nb[m], Np = b->Np[m];
     float2* Tm = b->T.p + b->offX[m] * nt;  // (nt, Np, nb)
-    g1.push_back(group(b->Xs.p + b->offX[m], true, false, nb, 0, b->Gt.p + b->offG[m], false, false,
+    g1.push_back(group(b->Xs.p + b->offX[m], false, false, nb, 0, b->Gt.p + b->offG[m], false, false,
                        nb, nb * nb, Tm, nb, Np * nb, Np, nb, nb, nt));
-    g2.push_back(group(Tm, false, false, nb, Np * nb, b->Xs.p + b->offX[m], true, true, nb, 0,
+    g2.push_back(group(Tm, false, false, nb, Np * nb, b->Xs.p + b->offX[m], false, true, nb, 0,
                        b->cache.p + b->offPQ[m], Np, cols, Np, Np, nb, nt));
   }
   cq::tc_cgemm_grouped(g1, b->gtab, s);
@@ -204,12 +204,12 @@ void batch_gw(Batch* b) {
     const int64_t Np = b->Np[m], NN = Np * Np;
     cq::TcStructure s1;
     s1.a_upper = true;
-    p1.push_back(group(b->LHs.p + b->offL[m], true, false, Np, 0, b->PW.p + b->offPQ[m], false, true,
+    p1.push_back(group(b->LHs.p + b->offL[m], false, false, Np, 0, b->PW.p + b->offPQ[m], false, true,
                        Np, cols, b->T1.p + b->offD[m], Np, NN, Np, Np, Np, nwh, s1));
     cq::TcStructure s2;  // M = L^H (P1)^H, P1 = L^H Pi (Pi Hermitian)
     s2.a_upper = true;
     s2.lower_only = true;
-    p2.push_back(group(b->LHs.p + b->offL[m], true, false, Np, 0, b->T1.p + b->offD[m], false, true,
+    p2.push_back(group(b->LHs.p + b->offL[m], false, false, Np, 0, b->T1.p + b->offD[m], false, true,
                        Np, NN, b->Mb.p + b->offD[m], Np, NN, Np, Np, Np, nwh, s2));
   }
   cq::tc_cgemm_grouped(p1, b->gtab, s);
@@ -242,12 +242,12 @@ void batch_gw(Batch* b) {
     cq::TcStructure s4;
     s4.a_lower = true;
     s4.lower_only = true;  // W is Hermitian: its lower triangle needs T only down there
-    t4.push_back(group(b->Ls.p + b->offL[m], true, false, Np, 0, E, false, true, Np, NN, F, Np, NN,
+    t4.push_back(group(b->Ls.p + b->offL[m], false, false, Np, 0, E, false, true, Np, NN, F, Np, NN,
                        Np, Np, Np, nwh, s4));
     cq::TcStructure s5;
     s5.b_upper = true;
     s5.lower_only = true;
-    t5.push_back(group(F, false, false, Np, NN, b->Ls.p + b->offL[m], true, true, Np, 0,
+    t5.push_back(group(F, false, false, Np, NN, b->Ls.p + b->offL[m], false, true, Np, 0,
                        b->PW.p + b->offPQ[m], Np, cols, Np, Np, Np, nwh, s5));
   }
   cq::tc_cgemm_grouped(f, b->gtab, s);
@@ -276,9 +276,9 @@ void batch_gw(Batch* b) {
   for (int64_t m = 0; m < b->nmol; ++m) {
     const int64_t nb = b->nb[m], Np = b->Np[m];
     float2* U = b->UT.p + b->offX[m] * nt;  // (nt, nb, Np)
-    a1.push_back(group(b->XTs.p + b->offX[m], true, false, Np, 0, b->cache.p + b->offPQ[m], false,
+    a1.push_back(group(b->XTs.p + b->offX[m], false, false, Np, 0, b->cache.p + b->offPQ[m], false,
                        false, Np, cols, U, Np, nb * Np, nb, Np, Np, nt));
-    a2.push_back(group(b->XTs.p + b->offX[m], true, true, Np, 0, U, false, false, Np, nb * Np,
+    a2.push_back(group(b->XTs.p + b->offX[m], false, true, Np, 0, U, false, false, Np, nb * Np,
                        b->Sab.p + b->offG[m], nb, nb * nb, nb, nb, Np, nt));
   }
   cq::tc_cgemm_grouped(a1, b->gtab, s);
@@ -430,10 +430,10 @@ int coqui_b200_batch_set_thc(coqui_b200_batch* b, int64_t m, const double* X_Pa,
     const int info = cq::cholesky_lower_batched(b->sol, L.p, Np, 1, b->st);
     CQ_REQUIRE(info == 0, COQUI_B200_ENOTHPD, "Coulomb matrix V is not positive definite");
     cq::launch_zero_upper_and_adjoint(L.p, LH.p, Np, 1, b->st);
-    cq::to_split(X.p, b->Xs.p + b->offX[m], Np, nb, 1, false, b->st);
-    cq::to_split(X.p, b->XTs.p + b->offX[m], Np, nb, 1, true, b->st);
-    cq::to_split(L.p, b->Ls.p + b->offL[m], Np, Np, 1, false, b->st);
-    cq::to_split(LH.p, b->LHs.p + b->offL[m], Np, Np, 1, false, b->st);
+    cq::to_c64(X.p, b->Xs.p + b->offX[m], Np, nb, 1, false, b->st);
+    cq::to_c64(X.p, b->XTs.p + b->offX[m], Np, nb, 1, true, b->st);
+    cq::to_c64(L.p, b->Ls.p + b->offL[m], Np, Np, 1, false, b->st);
+    cq::to_c64(LH.p, b->LHs.p + b->offL[m], Np, Np, 1, false, b->st);
     CQ_CHECK_CUDA(cudaStreamSynchronize(b->st));
     b->have_thc[m] = 1;
   });

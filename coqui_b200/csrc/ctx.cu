@@ -81,7 +81,7 @@ struct coqui_b200_ctx {
   DevBuf<double2> eps;
   DevBuf<unsigned char> Gp, Gn, PW;  // storage precision, bytes
   DevBuf<unsigned char> dyn;         // Dyson scratch
-  DevBuf<float4> Ls, LHs;            // pre-split L, L^H for the tensor-core Dyson products
+  DevBuf<float2> Lc, LHc;            // complex64 L, L^H for the tensor-core Dyson products
   cq::TcOperand Xtc;                 // packed X for the tensor-core projections
   DevBuf<double2> Gx;                // primary_to_aux staging (the resident G stays intact)
 
@@ -758,8 +758,8 @@ void coqui_b200_destroy(coqui_b200_ctx* c) {
   c->Gn.release();
   c->PW.release();
   c->dyn.release();
-  c->Ls.release();
-  c->LHs.release();
+  c->Lc.release();
+  c->LHc.release();
   c->Xtc.release();
   for (auto& m : c->marks) cudaEventDestroy(m.second);
   if (c->sol) cusolverDnDestroy(c->sol);
@@ -907,10 +907,10 @@ int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_
     cq::launch_zero_upper_and_adjoint(c->L.p, c->LH.p, Np, nk, c->st);
     if (c->mode == COQUI_B200_MIXED) {
       cq::tc_pack_X(c->Xtc, c->X.p, nk, Np, nb, c->st);
-      c->Ls.ensure((size_t)nk * Np * Np);
-      c->LHs.ensure((size_t)nk * Np * Np);
-      cq::to_split(c->L.p, c->Ls.p, Np, Np, nk, false, c->st);
-      cq::to_split(c->LH.p, c->LHs.p, Np, Np, nk, false, c->st);
+      c->Lc.ensure((size_t)nk * Np * Np);
+      c->LHc.ensure((size_t)nk * Np * Np);
+      cq::to_c64(c->L.p, c->Lc.p, Np, Np, nk, false, c->st);
+      cq::to_c64(c->LH.p, c->LHc.p, Np, Np, nk, false, c->st);
     }
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->have_thc = true;
@@ -1006,8 +1006,8 @@ void dyson_all(Ctx* c, bool want_w, bool want_e, std::vector<double>* logdet,
   a.L = c->L.p;
   a.LH = c->LH.p;
   a.V = c->V.p;
-  a.Ls = c->Ls.p;
-  a.LHs = c->LHs.p;
+  a.Lc = c->Lc.p;
+  a.LHc = c->LHc.p;
   a.want_w = want_w;
   a.want_e = want_e;
   a.mixed = (c->mode == COQUI_B200_MIXED);

@@ -218,8 +218,8 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       // the mixed form addresses the per-q factors periodically from their bases
       const double2* L = a.L + q0 * NN;
       const double2* LH = a.LH + q0 * NN;
-      const float4* Ls = a.Ls;    // mixed form: pre-split factors, addressed periodically in q
-      const float4* LHs = a.LHs;
+      const float2* Lc = a.Lc;    // mixed form: complex64 factors, addressed periodically in q
+      const float2* LHc = a.LHc;
       const double2* V = a.V + q0 * NN;
       // M = L^H (Pi L)
       {
@@ -230,7 +230,7 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         s1.a_upper = true;  // L^H upper triangular
         s1.a_mod = nq;
         s1.a_q0 = q0;
-        tc_cgemm_nt(LHs, true, false, Np, NN, Pi, false, true, Np, NN, (float2*)T1, Np, NN, Np,
+        tc_cgemm_nt(LHc, false, false, Np, NN, Pi, false, true, Np, NN, (float2*)T1, Np, NN, Np,
                     Np, Np, nb, s, s1);
         // M = L^H Q with Q = Pi L = P1^H (Pi Hermitian): B(k, n) = Q[k][n] = conj(P1[n][k]).
         // With L^H upper the lower triangle of M needs k >= i only (Np^3 / 6 products).
@@ -239,7 +239,7 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         s2.a_mod = nq;
         s2.a_q0 = q0;
         s2.lower_only = true;  // M Hermitian: the Cholesky reads the lower triangle
-        tc_cgemm_nt(LHs, true, false, Np, NN, T1, false, true, Np, NN, (float2*)Mb, Np, NN, Np, Np,
+        tc_cgemm_nt(LHc, false, false, Np, NN, T1, false, true, Np, NN, (float2*)Mb, Np, NN, Np, Np,
                     Np, nb, s, s2);
       } else {
         // row-major C = A B  ->  column-major C^T = B^T A^T
@@ -337,14 +337,14 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         s4.lower_only = true;
         s4.a_mod = nq;
         s4.a_q0 = q0;
-        tc_cgemm_nt(Ls, true, false, Np, NN, E, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s4);
+        tc_cgemm_nt(Lc, false, false, Np, NN, E, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s4);
         // W = T L^H  (B(k, n) = conj(L[n][k])), written over Pi
         TcStructure s5;
         s5.b_upper = true;  // B(k, n) = conj(L[n][k]) vanishes for k > n
         s5.lower_only = true;
         s5.b_mod = nq;
         s5.b_q0 = q0;
-        tc_cgemm_nt(F, false, false, Np, NN, Ls, true, true, Np, NN, (float2*)Pi, Np, NN, Np, Np,
+        tc_cgemm_nt(F, false, false, Np, NN, Lc, false, true, Np, NN, (float2*)Pi, Np, NN, Np, Np,
                     Np, nb, s, s5);
         launch_mirror_upper((float2*)Pi, Np, nb, s);
       } else if (a.want_w) {

@@ -37,8 +37,8 @@ struct DysonArgs {
   const double2* L = nullptr;   // (nq, Np, Np) lower Cholesky factors of V
   const double2* LH = nullptr;  // (nq, Np, Np) L^H
   const double2* V = nullptr;   // (nq, Np, Np)
-  const float4* Ls = nullptr;   // mixed form: L and L^H in the pre-split tensor-core format
-  const float4* LHs = nullptr;
+  const float2* Lc = nullptr;   // mixed form: L and L^H as complex64 tensor-core operands
+  const float2* LHc = nullptr;
   bool want_w = true, want_e = false, mixed = true;
   unsigned char* PW = nullptr;  // (nw, nq, Np, Np): Pi(iW) in, W(iW) out (if want_w)
   Prof* prof = nullptr;

@@ -33,6 +33,13 @@ namespace {
 
 __device__ int g_tc_error = 0;
 
+// Whether every row of an operand starts 16-byte aligned at even K: a complex64 operand needs
+// an aligned base and even row and batch strides; pre-split values are 16 bytes each.
+int rows_aligned(const void* X, bool split, int64_t ld, int64_t sX) {
+  if ((reinterpret_cast<uintptr_t>(X) & 15) != 0) return 0;
+  return split ? 1 : (ld % 2 == 0 && sX % 2 == 0);
+}
+
 constexpr int kBM = 128;
 constexpr int kBKR = 32;  // real K per stage (128 bytes of fp32)
 // BNC complex columns per tile; NP producer threads (warps 0..NP/32-1 stage operands, then
@@ -74,6 +81,8 @@ struct TcParams {
   int conj_a, conj_b;
   int a_upper, a_lower, b_lower, b_upper, lower_only;
   int a_ident, b_ident;  // operand + identity (complex64 operands only)
+  // every row of the operand starts 16-byte aligned at even K (vector loads allowed)
+  int a_al, b_al;
   // periodic batch index (0 = off): operand batch = (q0 + b) % mod, for per-q operands
   int64_t a_mod, a_q0, b_mod, b_q0;
 };
@@ -96,28 +105,35 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("{ .reg .b64 st; mbarrier.arrive.shared::cta.b64 st, [%0]; }" ::"r"(bar) : "memory");
 }
 
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
 // Bounded wait for the phase with the given parity; returns false (and flags) on timeout.
+// The clock is read only after a first failed attempt and then every 16 attempts.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = global_ns();
-  while (true) {
-    uint32_t done;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (global_ns() - t0 > 2000000000ull) {
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 15u) == 0 && global_ns() - t0 > 2000000000ull) {
       atomicExch(&g_tc_error, 1);
       return false;
     }
   }
 }
 
+// Rounds to TF32 (10 explicit mantissa bits), to nearest with ties away from zero, as integer
+// arithmetic on the magnitude bits (two ALU operations, no conversion unit): a finite input
+// gives its TF32 value with the low 13 bits cleared.
 __device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
+  return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
 }
 
 // split x into TF32 hi + lo (hi = rna(x), lo = rna(x - hi))
@@ -165,17 +181,18 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 template <bool C128> struct Pair;
 template <> struct Pair<false> {
   float4 v;
-  __device__ __forceinline__ void load(const void* base, int64_t off, int64_t k, int64_t kmax,
-                                       bool row_ok) {
-    const float2* p = reinterpret_cast<const float2*>(base) + off;
-    if (row_ok && k + 1 < kmax && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
-      v = __ldg(reinterpret_cast<const float4*>(p));
-    } else {
-      float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
-      if (row_ok && k < kmax) a = __ldg(p);
-      if (row_ok && k + 1 < kmax) b = __ldg(p + 1);
-      v = make_float4(a.x, a.y, b.x, b.y);
-    }
+  static constexpr int kBytes = 8;  // per complex value
+  // both values inside K and the address 16-byte aligned
+  __device__ __forceinline__ void load_fast(const unsigned char* p, bool row_ok) {
+    v = row_ok ? __ldg(reinterpret_cast<const float4*>(p)) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __device__ __forceinline__ void load_edge(const unsigned char* base, int64_t k, int64_t kmax,
+                                            bool row_ok) {
+    const float2* p = reinterpret_cast<const float2*>(base);
+    float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+    if (row_ok && k < kmax) a = __ldg(p);
+    if (row_ok && k + 1 < kmax) b = __ldg(p + 1);
+    v = make_float4(a.x, a.y, b.x, b.y);
   }
   __device__ __forceinline__ void get(float (&x)[4]) const {
     x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
@@ -189,9 +206,19 @@ template <> struct Pair<false> {
 // Pre-split operand: one float4 (hi.re, hi.im, lo.re, lo.im) per complex value, hi/lo TF32.
 template <> struct Pair<true> {
   float4 a, b;
-  __device__ __forceinline__ void load(const void* base, int64_t off, int64_t k, int64_t kmax,
-                                       bool row_ok) {
-    const float4* p = reinterpret_cast<const float4*>(base) + off;
+  static constexpr int kBytes = 16;  // per complex value
+  __device__ __forceinline__ void load_fast(const unsigned char* base, bool row_ok) {
+    const float4* p = reinterpret_cast<const float4*>(base);
+    a = make_float4(0.f, 0.f, 0.f, 0.f);
+    b = a;
+    if (row_ok) {
+      a = __ldg(p);
+      b = __ldg(p + 1);
+    }
+  }
+  __device__ __forceinline__ void load_edge(const unsigned char* base, int64_t k, int64_t kmax,
+                                            bool row_ok) {
+    const float4* p = reinterpret_cast<const float4*>(base);
     a = make_float4(0.f, 0.f, 0.f, 0.f);
     b = a;
     if (row_ok && k < kmax) a = __ldg(p);
@@ -199,53 +226,95 @@ template <> struct Pair<true> {
   }
   __device__ __forceinline__ void add_one(int) {}  // not used: rejected on the host
 };
+
+// The operand rows one producer thread stages, fixed for a tile: chunk j of the thread lies
+// in row row0 + j * (producer threads / 8) at complex column 2 * (thread % 8) of the K block.
+struct OpRows {
+  const unsigned char* base;  // chunk 0 at k = 0
+  int64_t step;               // bytes from one chunk's row to the next chunk's
+  int64_t row0;               // operand row of chunk 0
+  uint32_t ok;                // bit j: chunk j's row lies inside the operand
+};
+
+template <int NCH, int NP>
+__device__ __forceinline__ OpRows op_rows(const void* X, int64_t ld, int64_t sX, int64_t bidx,
+                                          int64_t rows, int64_t r0, int es) {
+  OpRows o;
+  const int t = threadIdx.x;
+  o.row0 = r0 + (t >> 3);
+  o.step = (int64_t)(NP / 8) * ld * es;
+  o.base = reinterpret_cast<const unsigned char*>(X) + (bidx * sX + o.row0 * ld + 2 * (t & 7)) * es;
+  o.ok = 0;
+#pragma unroll
+  for (int j = 0; j < NCH; ++j)
+    if (o.row0 + j * (NP / 8) < rows) o.ok |= 1u << j;
+  return o;
+}
+
 template <class Cfg, bool A64, bool B64> struct Staging {
   Pair<A64> a[Cfg::A_CHUNKS];
   Pair<B64> b[Cfg::B_CHUNKS];
+  static constexpr int RSTEP = Cfg::NPROD / 8;  // rows between a thread's chunks
 
-  __device__ __forceinline__ void load(const TcParams& p, int64_t bz, int64_t m0, int64_t n0,
+  // the K block of 16 complex columns starting at k0c
+  __device__ __forceinline__ void load(const TcParams& p, const OpRows& ra, const OpRows& rb,
                                        int64_t k0c) {
-    const int t = threadIdx.x;
-    const int64_t ba = p.a_mod ? (p.a_q0 + bz) % p.a_mod : bz;
-    const int64_t bb = p.b_mod ? (p.b_q0 + bz) % p.b_mod : bz;
+    const int64_t k = k0c + 2 * (threadIdx.x & 7);
+    const bool inner = k0c + 16 <= p.K;  // uniform over the CTA
+    const int64_t offa = k0c * Pair<A64>::kBytes, offb = k0c * Pair<B64>::kBytes;
+    if (inner && p.a_al) {
 #pragma unroll
-    for (int j = 0; j < Cfg::A_CHUNKS; ++j) {
-      const int i = t + j * Cfg::NPROD;
-      const int r = i >> 3, c = i & 7;
-      const int64_t m = m0 + r, k = k0c + 2 * c;
-      a[j].load(p.A, ba * p.sA + m * p.lda + k, k, p.K, m < p.M);
-      if (p.a_ident && m < p.M) {
+      for (int j = 0; j < Cfg::A_CHUNKS; ++j)
+        a[j].load_fast(ra.base + j * ra.step + offa, (ra.ok >> j) & 1u);
+    } else {
+#pragma unroll
+      for (int j = 0; j < Cfg::A_CHUNKS; ++j)
+        a[j].load_edge(ra.base + j * ra.step + offa, k, p.K, (ra.ok >> j) & 1u);
+    }
+    if (p.a_ident) {
+#pragma unroll
+      for (int j = 0; j < Cfg::A_CHUNKS; ++j) {
+        const int64_t m = ra.row0 + j * RSTEP;
+        if (!((ra.ok >> j) & 1u)) continue;
         if (m == k && k < p.K) a[j].add_one(0);
         if (m == k + 1 && k + 1 < p.K) a[j].add_one(1);
       }
     }
+    if (inner && p.b_al) {
 #pragma unroll
-    for (int j = 0; j < Cfg::B_CHUNKS; ++j) {
-      const int i = t + j * Cfg::NPROD;
-      const int r = i >> 3, c = i & 7;
-      const int64_t n = n0 + r, k = k0c + 2 * c;
-      b[j].load(p.Bt, bb * p.sB + n * p.ldb + k, k, p.K, n < p.N);
-      if (p.b_ident && n < p.N) {
+      for (int j = 0; j < Cfg::B_CHUNKS; ++j)
+        b[j].load_fast(rb.base + j * rb.step + offb, (rb.ok >> j) & 1u);
+    } else {
+#pragma unroll
+      for (int j = 0; j < Cfg::B_CHUNKS; ++j)
+        b[j].load_edge(rb.base + j * rb.step + offb, k, p.K, (rb.ok >> j) & 1u);
+    }
+    if (p.b_ident) {
+#pragma unroll
+      for (int j = 0; j < Cfg::B_CHUNKS; ++j) {
+        const int64_t n = rb.row0 + j * RSTEP;
+        if (!((rb.ok >> j) & 1u)) continue;
         if (n == k && k < p.K) b[j].add_one(0);
         if (n == k + 1 && k + 1 < p.K) b[j].add_one(1);
       }
     }
   }
 
-  // hi/lo TF32 words of the two complex values of a chunk: (re0, im0, re1, im1)
+  // hi/lo TF32 words of the two complex values of a chunk: (re0, im0, re1, im1); sgn is the
+  // sign bit applied to the imaginary parts (conjugation)
   template <bool SPLIT>
-  __device__ __forceinline__ static void words(const Pair<SPLIT>& q, float sgn, uint32_t (&h)[4],
+  __device__ __forceinline__ static void words(const Pair<SPLIT>& q, uint32_t sgn, uint32_t (&h)[4],
                                                uint32_t (&l)[4]) {
     if constexpr (SPLIT) {
-      h[0] = __float_as_uint(q.a.x); h[1] = __float_as_uint(sgn * q.a.y);
-      h[2] = __float_as_uint(q.b.x); h[3] = __float_as_uint(sgn * q.b.y);
-      l[0] = __float_as_uint(q.a.z); l[1] = __float_as_uint(sgn * q.a.w);
-      l[2] = __float_as_uint(q.b.z); l[3] = __float_as_uint(sgn * q.b.w);
+      h[0] = __float_as_uint(q.a.x); h[1] = __float_as_uint(q.a.y) ^ sgn;
+      h[2] = __float_as_uint(q.b.x); h[3] = __float_as_uint(q.b.y) ^ sgn;
+      l[0] = __float_as_uint(q.a.z); l[1] = __float_as_uint(q.a.w) ^ sgn;
+      l[2] = __float_as_uint(q.b.z); l[3] = __float_as_uint(q.b.w) ^ sgn;
     } else {
       float v[4];
       q.get(v);
-      v[1] *= sgn;
-      v[3] *= sgn;
+      v[1] = __uint_as_float(__float_as_uint(v[1]) ^ sgn);
+      v[3] = __uint_as_float(__float_as_uint(v[3]) ^ sgn);
 #pragma unroll
       for (int j = 0; j < 4; ++j) split2(v[j], h[j], l[j]);
     }
@@ -254,7 +323,8 @@ template <class Cfg, bool A64, bool B64> struct Staging {
   __device__ __forceinline__ void store(const TcParams& p, uint32_t sA_hi, uint32_t sA_lo,
                                         uint32_t sB_hi, uint32_t sB_lo) const {
     const int t = threadIdx.x;
-    const float ca = p.conj_a ? -1.f : 1.f, cb = p.conj_b ? -1.f : 1.f;
+    constexpr uint32_t SGN = 0x80000000u;
+    const uint32_t ca = p.conj_a ? SGN : 0u, cb = p.conj_b ? SGN : 0u;
 #pragma unroll
     for (int j = 0; j < Cfg::A_CHUNKS; ++j) {
       const int i = t + j * Cfg::NPROD;
@@ -265,7 +335,6 @@ template <class Cfg, bool A64, bool B64> struct Staging {
       st_shared_v4(sA_hi + off, h[0], h[1], h[2], h[3]);
       st_shared_v4(sA_lo + off, l[0], l[1], l[2], l[3]);
     }
-    constexpr uint32_t SGN = 0x80000000u;
 #pragma unroll
     for (int j = 0; j < Cfg::B_CHUNKS; ++j) {
       const int i = t + j * Cfg::NPROD;
@@ -306,7 +375,7 @@ __device__ __forceinline__ void tc_tile(const TcParams& p, int64_t bz, int64_t m
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(smem_u32(&bars[s]), Cfg::NPROD);
+      mbar_init(smem_u32(&bars[s]), Cfg::NPW);  // one arrival per producer warp
       mbar_init(smem_u32(&bars[kStages + s]), 1);
     }
     mbar_init(smem_u32(acc_bar), 1);
@@ -331,6 +400,10 @@ __device__ __forceinline__ void tc_tile(const TcParams& p, int64_t bz, int64_t m
     // loads have two stage times to arrive before its split values go to shared memory.
     // Short K (four producer warps, twice the values per thread): one set, one stage ahead.
     constexpr int kAhead = (NP == 256) ? 2 : 1;
+    const int64_t ba = p.a_mod ? (p.a_q0 + bz) % p.a_mod : bz;
+    const int64_t bb = p.b_mod ? (p.b_q0 + bz) % p.b_mod : bz;
+    const OpRows ra = op_rows<Cfg::A_CHUNKS, NP>(p.A, p.lda, p.sA, ba, p.M, m0, Pair<A64>::kBytes);
+    const OpRows rb = op_rows<Cfg::B_CHUNKS, NP>(p.Bt, p.ldb, p.sB, bb, p.N, n0, Pair<B64>::kBytes);
     auto step = [&](Staging<Cfg, A64, B64>& st, int it) -> bool {
       const int s = it % kStages;
       const uint32_t ph = (uint32_t)(it / kStages) & 1u;
@@ -339,22 +412,25 @@ __device__ __forceinline__ void tc_tile(const TcParams& p, int64_t bz, int64_t m
       const uint32_t a_hi = smem_u32(sp), a_lo = a_hi + Cfg::A_PLANE;
       const uint32_t b_hi = a_lo + Cfg::A_PLANE, b_lo = b_hi + Cfg::B_PLANE;
       st.store(p, a_hi, a_lo, b_hi, b_lo);
+      // each thread's stores become visible to the tensor core (async proxy); the warp's
+      // lanes are ordered by the warp barrier and one lane arrives for the warp
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(smem_u32(&bars[s]));
-      if (it + kAhead < nkb) st.load(p, bz, m0, n0, (int64_t)(kb_lo + it + kAhead) * 16);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&bars[s]));
+      if (it + kAhead < nkb) st.load(p, ra, rb, (int64_t)(kb_lo + it + kAhead) * 16);
       return true;
     };
     if constexpr (kAhead == 2) {
       Staging<Cfg, A64, B64> st0, st1;
-      if (nkb > 0) st0.load(p, bz, m0, n0, (int64_t)kb_lo * 16);
-      if (nkb > 1) st1.load(p, bz, m0, n0, (int64_t)(kb_lo + 1) * 16);
+      if (nkb > 0) st0.load(p, ra, rb, (int64_t)kb_lo * 16);
+      if (nkb > 1) st1.load(p, ra, rb, (int64_t)(kb_lo + 1) * 16);
       for (int it = 0; it < nkb; it += 2) {
         if (!step(st0, it)) { ok = false; break; }
         if (it + 1 < nkb && !step(st1, it + 1)) { ok = false; break; }
       }
     } else {
       Staging<Cfg, A64, B64> st0;
-      if (nkb > 0) st0.load(p, bz, m0, n0, (int64_t)kb_lo * 16);
+      if (nkb > 0) st0.load(p, ra, rb, (int64_t)kb_lo * 16);
       for (int it = 0; it < nkb; ++it)
         if (!step(st0, it)) { ok = false; break; }
     }
@@ -634,6 +710,8 @@ void tc_cgemm_nt(const void* A, bool a_split, bool conj_a, int64_t lda, int64_t 
              "tc_cgemm: identity shift needs a complex64 operand");
   p.a_ident = st.a_ident;
   p.b_ident = st.b_ident;
+  p.a_al = rows_aligned(A, a_c128, lda, sA);
+  p.b_al = rows_aligned(Bt, b_c128, ldb, sB);
   p.a_mod = st.a_mod;
   p.a_q0 = st.a_q0;
   p.b_mod = st.b_mod;
@@ -671,6 +749,21 @@ __global__ void k_to_split(const double2* __restrict__ in, float4* __restrict__ 
     }
     out[o] = make_float4(__uint_as_float(hr), __uint_as_float(hi), __uint_as_float(lr),
                          __uint_as_float(li));
+  }
+}
+
+// out = in as complex64; if transpose, the (rows x cols) blocks are written transposed
+__global__ void k_to_c64(const double2* __restrict__ in, float2* __restrict__ out, int64_t rows,
+                         int64_t cols, int64_t total, int transpose) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 x = in[i];
+    int64_t o = i;
+    if (transpose) {
+      const int64_t b = i / (rows * cols), e = i % (rows * cols);
+      o = b * rows * cols + (e % cols) * rows + e / cols;
+    }
+    out[o] = make_float2((float)x.x, (float)x.y);
   }
 }
 
@@ -719,21 +812,29 @@ void to_split(const double2* in, float4* out, int64_t rows, int64_t cols, int64_
   CQ_CHECK_CUDA(cudaGetLastError());
 }
 
+void to_c64(const double2* in, float2* out, int64_t rows, int64_t cols, int64_t batch,
+            bool transpose, cudaStream_t s) {
+  const int64_t total = rows * cols * batch;
+  k_to_c64<<<grid_for(total, 256), 256, 0, s>>>(in, out, rows, cols, total, transpose ? 1 : 0);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
 void tc_pack_X(TcOperand& op, const double2* X, int64_t nk, int64_t Np, int64_t nb,
                cudaStream_t s) {
   op.X = X;
   op.nk = nk;
   op.Np = Np;
   op.nb = nb;
-  op.packed.ensure((size_t)nk * Np * nb * sizeof(float4) * 2);
-  float4* Xs = (float4*)op.packed.p;
-  to_split(X, Xs, Np, nb, nk, false, s);                 // X   (nk, Np, nb)
-  to_split(X, Xs + nk * Np * nb, Np, nb, nk, true, s);   // X^T (nk, nb, Np)
+  op.packed.ensure((size_t)nk * Np * nb * sizeof(float2) * 2);
+  float2* Xc = (float2*)op.packed.p;
+  to_c64(X, Xc, Np, nb, nk, false, s);                 // X   (nk, Np, nb)
+  to_c64(X, Xc + nk * Np * nb, Np, nb, nk, true, s);   // X^T (nk, nb, Np)
 }
 
 void tc_project_p2a(TcOperand& op, const double2* Gk, float2* out, int64_t nk, int64_t Np,
                     int64_t nb, int64_t nbatch, cudaStream_t s) {
-  const float4* Xs = (const float4*)op.packed.p;
+  const float2* Xs = (const float2*)op.packed.p;
   op.tmp.ensure((size_t)nbatch * Np * nb * sizeof(float2) + (size_t)nbatch * nb * nb * sizeof(float2));
   float2* T = (float2*)op.tmp.p;
   float2* Gt = T + nbatch * Np * nb;
@@ -745,16 +846,16 @@ void tc_project_p2a(TcOperand& op, const double2* Gk, float2* out, int64_t nk, i
   sx_a.a_mod = nk;
   sx_b.b_mod = nk;
   // T = X G  (Np x nb, K = nb): Bt[j][i] = G[i][j]
-  tc_cgemm_nt(Xs, true, false, nb, Np * nb, Gt, false, false, nb, nb * nb, T, nb, Np * nb, Np,
+  tc_cgemm_nt(Xs, false, false, nb, Np * nb, Gt, false, false, nb, nb * nb, T, nb, Np * nb, Np,
               nb, nb, nbatch, s, sx_a);
   // out = T X^H: B(k=b, n=Q) = conj(X[Q][b])
-  tc_cgemm_nt(T, false, false, nb, Np * nb, Xs, true, true, nb, Np * nb, out, Np, Np * Np, Np,
+  tc_cgemm_nt(T, false, false, nb, Np * nb, Xs, false, true, nb, Np * nb, out, Np, Np * Np, Np,
               Np, nb, nbatch, s, sx_b);
 }
 
 void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, int64_t Np,
                     int64_t nb, int64_t nbatch, cudaStream_t s) {
-  const float4* XTs = (const float4*)op.packed.p + nk * Np * nb;
+  const float2* XTs = (const float2*)op.packed.p + nk * Np * nb;
   op.tmp.ensure((size_t)nbatch * Np * nb * sizeof(float2) + (size_t)nbatch * nb * nb * sizeof(float2));
   float2* UT = (float2*)op.tmp.p;
   float2* Sab = UT + nbatch * Np * nb;
@@ -764,7 +865,7 @@ void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, i
   float2* U = (float2*)op.tmp2.p;
   TcStructure sb;
   sb.b_mod = nk;
-  tc_cgemm_nt(Sk, false, false, Np, Np * Np, XTs, true, false, Np, nb * Np, U, nb, Np * nb, Np,
+  tc_cgemm_nt(Sk, false, false, Np, Np * Np, XTs, false, false, Np, nb * Np, U, nb, Np * nb, Np,
               nb, Np, nbatch, s, sb);
   CQ_REQUIRE(nbatch <= 65535, COQUI_B200_EINVAL, "a2p: too many problems per launch");
   k_transpose_f2<<<dim3((unsigned)((nb + 31) / 32), (unsigned)((Np + 31) / 32), (unsigned)nbatch),
@@ -774,7 +875,7 @@ void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, i
   TcStructure sx;
   sx.a_mod = nk;
   // Sigma_ab = X^H U (nb x nb, K = Np): A(a, P) = conj(X^T[a][P]), Bt = U^T
-  tc_cgemm_nt(XTs, true, true, Np, nb * Np, UT, false, false, Np, nb * Np, Sab, nb, nb * nb, nb,
+  tc_cgemm_nt(XTs, false, true, Np, nb * Np, UT, false, false, Np, nb * Np, Sab, nb, nb * nb, nb,
               nb, Np, nbatch, s, sx);
   const int64_t t = nbatch * nb * nb;
   k_c64_to_c128<<<grid_for(t, 256), 256, 0, s>>>(Sab, out, t);
@@ -808,6 +909,8 @@ TcParams make_params(const TcGroup& g) {
   p.lower_only = g.st.lower_only;
   p.a_ident = g.st.a_ident;
   p.b_ident = g.st.b_ident;
+  p.a_al = rows_aligned(g.A, g.a_split, g.lda, g.sA);
+  p.b_al = rows_aligned(g.Bt, g.b_split, g.ldb, g.sB);
   p.a_mod = g.st.a_mod;
   p.a_q0 = g.st.a_q0;
   p.b_mod = g.st.b_mod;

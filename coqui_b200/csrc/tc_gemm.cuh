@@ -9,7 +9,7 @@ namespace cq {
 struct TcOperand {
   const double2* X = nullptr;
   int64_t nk = 0, Np = 0, nb = 0;
-  DevBuf<unsigned char> packed;  // pre-split X (nk, Np, nb) then X^T (nk, nb, Np)
+  DevBuf<unsigned char> packed;  // complex64 X (nk, Np, nb) then X^T (nk, nb, Np)
   DevBuf<unsigned char> tmp, tmp2;  // per-call intermediates
   void release() {
     packed.release();
@@ -36,6 +36,11 @@ void tc_project_a2p(TcOperand& op, const float2* Sk, double2* out, int64_t nk, i
 // in: nbatch blocks of (rows x cols) complex128; transpose writes each block transposed.
 void to_split(const double2* in, float4* out, int64_t rows, int64_t cols, int64_t batch,
               bool transpose, cudaStream_t s);
+// Complex64 copy of nbatch (rows x cols) complex128 blocks (transposed if asked).  The GEMM
+// splits complex64 operands while staging them; the copy reads half the bytes of the
+// pre-split format per K block, which is what bounds the long-K products.
+void to_c64(const double2* in, float2* out, int64_t rows, int64_t cols, int64_t batch,
+            bool transpose, cudaStream_t s);
 
 // Split-TF32 tensor-core GEMM, "NT" form:
 //   C[b](m, n) = sum_k opA(A[b])(m, k) * opB(Bt[b])(n, k)
