@@ -37,7 +37,7 @@ SYMBOLS = [
     "coqui_b200_scgw_sigma_diag_w", "coqui_b200_batch_create", "coqui_b200_batch_destroy",
     "coqui_b200_batch_last_error", "coqui_b200_batch_set_ir", "coqui_b200_batch_set_thc",
     "coqui_b200_batch_gw_iteration", "coqui_b200_batch_last_ms", "coqui_b200_set_autotune",
-    "coqui_b200_tuned_shapes",
+    "coqui_b200_tuned_shapes", "coqui_b200_set_tile_config", "coqui_b200_num_tile_configs",
 ]
 
 
@@ -129,6 +129,10 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_set_autotune.restype = None
     lib.coqui_b200_tuned_shapes.argtypes = []
     lib.coqui_b200_tuned_shapes.restype = I64
+    lib.coqui_b200_set_tile_config.argtypes = [ctypes.c_int]
+    lib.coqui_b200_set_tile_config.restype = ctypes.c_int
+    lib.coqui_b200_num_tile_configs.argtypes = []
+    lib.coqui_b200_num_tile_configs.restype = ctypes.c_int
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -533,3 +537,13 @@ def set_autotune(on: bool):
 
 def tuned_shapes() -> int:
     return int(load().coqui_b200_tuned_shapes())
+
+
+def set_tile_config(cfg: int):
+    """Pins every tensor-core GEMM to tile configuration cfg (-1: autotuner / heuristic)."""
+    if load().coqui_b200_set_tile_config(int(cfg)) != OK:
+        raise ValueError(f"tile configuration {cfg} outside -1 .. {num_tile_configs() - 1}")
+
+
+def num_tile_configs() -> int:
+    return int(load().coqui_b200_num_tile_configs())

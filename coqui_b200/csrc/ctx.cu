@@ -1669,4 +1669,10 @@ void coqui_b200_set_autotune(int on) { cq::tc_set_autotune(on); }
 
 int64_t coqui_b200_tuned_shapes(void) { return cq::tc_tuned_shapes(); }
 
+int coqui_b200_set_tile_config(int cfg) {
+  return cq::tc_set_forced_cfg(cfg) ? COQUI_B200_OK : COQUI_B200_EINVAL;
+}
+
+int coqui_b200_num_tile_configs(void) { return cq::tc_num_cfgs(); }
+
 }  // extern "C"

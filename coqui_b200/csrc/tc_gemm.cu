@@ -638,8 +638,12 @@ bool autotune_on() {
   return v == 1;
 }
 
+std::atomic<int> g_forced_cfg{-1};
+
 template <bool A64, bool B64>
 void dispatch_n(const TcParams& p, int64_t batch, cudaStream_t s) {
+  const int forced = g_forced_cfg.load();
+  if (forced >= 0) return launch_cfg<A64, B64>(forced, p, batch, s);
   if (!autotune_on()) return launch_cfg<A64, B64>(heuristic_cfg(p), p, batch, s);
   int64_t bb = 1;
   while (bb < batch) bb <<= 1;  // batch class: next power of two
@@ -987,6 +991,14 @@ void tc_cgemm_grouped(const std::vector<TcGroup>& groups, DevBuf<unsigned char>&
 }
 
 void tc_set_autotune(int on) { g_autotune.store(on ? 1 : 0); }
+
+bool tc_set_forced_cfg(int cfg) {
+  if (cfg < -1 || cfg >= kNumCfg) return false;
+  g_forced_cfg.store(cfg);
+  return true;
+}
+
+int tc_num_cfgs() { return kNumCfg; }
 
 int64_t tc_tuned_shapes() {
   std::lock_guard<std::mutex> lk(g_tune_mu);

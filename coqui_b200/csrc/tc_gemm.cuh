@@ -89,6 +89,9 @@ void tc_cgemm_grouped(const std::vector<TcGroup>& groups, DevBuf<unsigned char>&
 // tc_set_autotune(0) selects the built-in heuristic) and the number of tuned shape classes.
 void tc_set_autotune(int on);
 int64_t tc_tuned_shapes();
+// Pins the tile configuration (-1: autotuner / heuristic); false for an unknown index.
+bool tc_set_forced_cfg(int cfg);
+int tc_num_cfgs();
 
 // Returns (and clears) the device flag set when a bounded wait inside a tensor-core kernel
 // gave up (nonzero = a kernel timed out).

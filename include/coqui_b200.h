@@ -262,6 +262,12 @@ COQUI_B200_API int coqui_b200_kernel_stats(const coqui_b200_ctx* ctx, char* name
 COQUI_B200_API void coqui_b200_set_autotune(int on);
 COQUI_B200_API int64_t coqui_b200_tuned_shapes(void);
 
+/* Pins every tensor-core GEMM to one tile configuration (0 .. coqui_b200_num_tile_configs()-1;
+   -1 returns to the autotuner or heuristic), process-wide, for reproducible timing and for
+   checking that the configurations agree.  Returns COQUI_B200_EINVAL for other values. */
+COQUI_B200_API int coqui_b200_set_tile_config(int cfg);
+COQUI_B200_API int coqui_b200_num_tile_configs(void);
+
 /* Number of kernels this library launched since the context was created. */
 COQUI_B200_API int64_t coqui_b200_kernel_launches(const coqui_b200_ctx* ctx);
 

@@ -51,3 +51,14 @@ def test_bad_dims_rejected_without_device(lib):
 def test_null_context_is_an_error(lib):
     assert lib.coqui_b200_set_thc(None, None, None) == -1
     assert lib.coqui_b200_kernel_launches(None) == 0
+
+
+def test_tile_configuration_pinning_validates_its_argument(lib):
+    n = capi.num_tile_configs()
+    assert n >= 6
+    with pytest.raises(ValueError):
+        capi.set_tile_config(n)
+    with pytest.raises(ValueError):
+        capi.set_tile_config(-2)
+    capi.set_tile_config(n - 1)
+    capi.set_tile_config(-1)

@@ -187,6 +187,26 @@ def test_errors_are_codes_not_aborts(base):
     assert maxabs(W, base.dW) < 1e-6
 
 
+def test_every_tile_configuration_gives_identical_results(base):
+    """Four or eight producer warps, one or two stages, 32 to 128 columns: each configuration
+    forms the same products in the same K order, so a whole GW iteration agrees bit for bit
+    whichever configuration every GEMM is pinned to."""
+    c = base.ctx(capi.MIXED)
+    ref = None
+    try:
+        for cfg in range(capi.num_tile_configs()):
+            capi.set_tile_config(cfg)
+            S, _ = c.gw_iteration(base.G)
+            if ref is None:
+                ref = S
+                assert maxabs(S, base.Sigma) < 1e-6
+            else:
+                assert np.array_equal(S, ref), f"tile configuration {cfg}"
+    finally:
+        capi.set_tile_config(-1)
+        c.close()
+
+
 def test_autotuned_tiles_give_identical_results(base):
     """Every tile configuration forms the same products in the same K order: the tuned and
     the heuristic choice agree bit for bit."""
