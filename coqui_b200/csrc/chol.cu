@@ -7,9 +7,11 @@
 // Right-looking blocked algorithm (chol_blk.cuh): the diagonal block is factored and
 // inverted in shared memory, the panel below is L_ib = A_ib C_jj^{-H}, the trailing lower
 // triangle gets A_ik -= L_ij L_kj^H.  The inverse is formed block column by block column:
-// X_ij = -C_ii^{-1} sum_{k=j}^{i-1} C_ik X_kj.  Block products use 4 x 4 register tiles per
-// thread, operands staged in shared memory.  A = I - M is set up and D^H written out by
-// separate element-wise kernels.
+// X_ij = -C_ii^{-1} sum_{k=j}^{i-1} C_ik X_kj.  The 32 x 32 block products run on the FP64
+// tensor cores (mma.sync m8n8k4, four real products per complex one; each of the two warps
+// holds a 16 x 32 accumulator as 8 x 8 fragments), operands staged in shared memory; the
+// CUDA-core FMA form (4 x 4 register tiles) is kept behind CHOL_FMA for comparison.  A = I - M
+// is set up and D^H written out by separate element-wise kernels.
 #include <cstdint>
 
 #include "chol.cuh"
@@ -32,7 +34,15 @@ __device__ __forceinline__ double2 conj_(double2 a) { return make_double2(a.x, -
 // overlap the others' FP64 arithmetic.  (64 x 64 blocks halve the block traffic per flop but
 // leave one problem per SM; measured slower.)
 namespace b32 {
-constexpr int CB = 32, CT = 64, TW = 8, PITCH = CB + 1, MINB = 6;
+#ifdef CHOL_FMA
+constexpr bool DMMA = false;
+#else
+constexpr bool DMMA = true;
+#endif
+constexpr int CB = 32, RT = 4, CTT = 4, TWR = CB / RT, TWC = CB / CTT, CT = TWR * TWC,
+              PITCH = CB + 1, MINB = 6;
+constexpr int AR = DMMA ? 2 : RT, AC = DMMA ? 8 : CTT;
+static_assert(!DMMA || (CB == 32 && CT == 64), "DMMA tiles: 32-blocks, two warps");
 #include "chol_blk.cuh"
 }  // namespace b32
 

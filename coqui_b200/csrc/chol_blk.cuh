@@ -1,7 +1,9 @@
 // Blocked FP64 Cholesky / log-determinant / triangular inverse of one problem per CTA.
 // Included once per block size inside a namespace that defines
-//   CB (block edge), CT (threads, (CB / 4)^2), TW (thread grid edge, CB / 4),
-//   PITCH (shared-memory row pitch in double2, CB + 1), MINB (CTAs per SM for the launch bounds)
+//   CB (block edge), CT (threads), PITCH (shared-memory row pitch in double2, CB + 1), MINB
+//   (CTAs per SM for the launch bounds), DMMA (block products on the FP64 tensor cores; needs
+//   CB = 32 and CT = 64), AR x AC (a thread's accumulator tile: 2 x 8 for DMMA, else RT x CTT
+//   with the thread grid TWR = CB / RT by TWC = CB / CTT, CT = TWR * TWC)
 // and the complex helpers cmul_, cmulc_, conj_.  (No include guard: it is meant to be
 // included more than once.)
 // smem tile <- global block (rows r0.., cols c0..) of an ld x ld row-major matrix, rb x cb valid
@@ -75,74 +77,114 @@ __device__ __forceinline__ void store_blk(const double2* S, double2* G, int64_t 
   }
 }
 
-// acc[i][j] (rows ty + TW i, cols tx + TW j) += sum_k X[r][k] * Y'[k][c] over k < K, where
-// Y'(k, c) = conj(Y[c][k]) if ADJ_Y (product with Y^H) else Y[k][c].
+// Register tile of a 32 x 32 block product: acc[i][j] is the element (acc_row(i, j),
+// acc_col(i, j)).  FMA form: thread (ty, tx) of the TWR x TWC grid holds rows ty + TWR i and
+// columns tx + TWC j.  DMMA form (FP64 tensor-core mma.sync m8n8k4, DMMA = true, two warps):
+// warp w holds the 8 x 8 tiles of tile rows 2w, 2w + 1 and all four tile columns; lane l
+// holds elements (8 (2w + i) + l / 4, 8 (j / 2) + 2 (l % 4) + j % 2) of the accumulator
+// fragments.
+__device__ __forceinline__ int acc_row(int i, int j) {
+  if constexpr (DMMA) return 8 * (2 * (int)(threadIdx.x >> 5) + i) + (int)((threadIdx.x & 31) >> 2);
+  else return (int)(threadIdx.x / TWC) + TWR * i;
+}
+__device__ __forceinline__ int acc_col(int i, int j) {
+  if constexpr (DMMA) return 8 * (j >> 1) + 2 * (int)(threadIdx.x & 3) + (j & 1);
+  else return (int)(threadIdx.x % TWC) + TWC * j;
+}
+
+// D (8 x 8, two values per lane) += A (8 x 4, one per lane) * B (4 x 8, one per lane), FP64
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// acc += sign * sum_k X[r][k] * Y'(k, c) over k < K, with Y'(k, c) = conj(Y[c][k]) if ADJ_Y
+// (product with Y^H) else Y[k][c]; sign = -1 if SUB.  The DMMA form runs K up to a multiple of
+// four: the staging tiles hold zeros beyond their valid extent.
+template <bool ADJ_Y, bool SUB>
+__device__ __forceinline__ void block_mma(const double2* X, const double2* Y, int K,
+                                          double2 (&acc)[AR][AC]) {
+  if constexpr (DMMA) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, g = l >> 2, q = l & 3;
+    const double sg = SUB ? -1.0 : 1.0;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const int k = k0 + q;
+      double2 x[AR], y[4];
+#pragma unroll
+      for (int i = 0; i < AR; ++i) x[i] = X[(8 * (2 * w + i) + g) * PITCH + k];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) y[t] = ADJ_Y ? Y[(8 * t + g) * PITCH + k] : Y[k * PITCH + 8 * t + g];
+#pragma unroll
+      for (int i = 0; i < AR; ++i) {
+        const double xr = sg * x[i].x, xi = sg * x[i].y;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          double2& c0 = acc[i][2 * t];
+          double2& c1 = acc[i][2 * t + 1];
+          if (ADJ_Y) {  // x conj(y) = (xr yr + xi yi) + i (xi yr - xr yi)
+            dmma(c0.x, c1.x, xr, y[t].x);
+            dmma(c0.x, c1.x, xi, y[t].y);
+            dmma(c0.y, c1.y, xi, y[t].x);
+            dmma(c0.y, c1.y, -xr, y[t].y);
+          } else {      // x y = (xr yr - xi yi) + i (xr yi + xi yr)
+            dmma(c0.x, c1.x, xr, y[t].x);
+            dmma(c0.x, c1.x, -xi, y[t].y);
+            dmma(c0.y, c1.y, xr, y[t].y);
+            dmma(c0.y, c1.y, xi, y[t].x);
+          }
+        }
+      }
+    }
+  } else {
+    const int tx = threadIdx.x % TWC, ty = threadIdx.x / TWC;
+    for (int k = 0; k < K; ++k) {
+      double2 a[AR], b[AC];
+#pragma unroll
+      for (int i = 0; i < AR; ++i) {
+        a[i] = X[(ty + TWR * i) * PITCH + k];
+        if (SUB) a[i] = make_double2(-a[i].x, -a[i].y);
+      }
+#pragma unroll
+      for (int j = 0; j < AC; ++j)
+        b[j] = ADJ_Y ? conj_(Y[(tx + TWC * j) * PITCH + k]) : Y[k * PITCH + tx + TWC * j];
+#pragma unroll
+      for (int i = 0; i < AR; ++i)  // four passes of AR * AC independent FMAs (no back-to-back
+#pragma unroll                   // dependency inside a complex multiply-add)
+        for (int j = 0; j < AC; ++j) acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int j = 0; j < AC; ++j) acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int j = 0; j < AC; ++j) acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int j = 0; j < AC; ++j) acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
+    }
+  }
+}
+
 template <bool ADJ_Y>
 __device__ __forceinline__ void mma_tile(const double2* X, const double2* Y, int K,
-                                         double2 (&acc)[4][4]) {
-  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
-  for (int k = 0; k < K; ++k) {
-    double2 a[4], b[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = X[(ty + TW * i) * PITCH + k];
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      b[j] = ADJ_Y ? conj_(Y[(tx + TW * j) * PITCH + k]) : Y[k * PITCH + tx + TW * j];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)  // four passes of 16 independent FMAs (no back-to-back
-#pragma unroll                   // dependency inside a complex multiply-add)
-      for (int j = 0; j < 4; ++j) acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
-  }
+                                         double2 (&acc)[AR][AC]) {
+  block_mma<ADJ_Y, false>(X, Y, K, acc);
 }
 
-// acc[i][j] -= sum_k X[r][k] conj(Y[c][k])  (A - X Y^H)
+// acc -= sum_k X[r][k] conj(Y[c][k])  (A - X Y^H)
 __device__ __forceinline__ void mma_tile_sub(const double2* X, const double2* Y, int K,
-                                             double2 (&acc)[4][4]) {
-  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
-  for (int k = 0; k < K; ++k) {
-    double2 a[4], b[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = X[(ty + TW * i) * PITCH + k];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) b[j] = Y[(tx + TW * j) * PITCH + k];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
-    // a * conj(b) = (ax bx + ay by) + i (ay bx - ax by), subtracted; four passes of 16
-    // independent FMAs
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j].x = fma(-a[i].x, b[j].x, acc[i][j].x);
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j].y = fma(-a[i].y, b[j].x, acc[i][j].y);
-  }
+                                             double2 (&acc)[AR][AC]) {
+  block_mma<true, true>(X, Y, K, acc);
 }
 
-__device__ __forceinline__ void zero_acc(double2 (&acc)[4][4]) {
+__device__ __forceinline__ void zero_acc(double2 (&acc)[AR][AC]) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < AR; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0, 0);
+    for (int j = 0; j < AC; ++j) acc[i][j] = make_double2(0, 0);
 }
 
 // In-place Cholesky of the lower triangle of S (n x n); adds sum ln C_ii to *ld_acc
@@ -235,7 +277,6 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
   __shared__ int s_bad;
   __shared__ double s_red[2][CT];
   const int nblk = (int)((n + CB - 1) / CB);
-  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
 
   if (threadIdx.x == 0) {
     s_ld = 0.0;
@@ -269,15 +310,15 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
       const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
       load_blk(S0, A, n, i0, j0, rb, jb);
       __syncthreads();
-      double2 acc[4][4];
+      double2 acc[AR][AC];
       zero_acc(acc);
       mma_tile<true>(S0, S1, jb, acc);
       __syncthreads();
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < AR; ++i)
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          const int r = ty + TW * i, c = tx + TW * jj;
+        for (int jj = 0; jj < AC; ++jj) {
+          const int r = acc_row(i, jj), c = acc_col(i, jj);
           if (r < rb && c < jb) A[(i0 + r) * n + j0 + c] = acc[i][jj];
         }
       __syncthreads();
@@ -292,21 +333,21 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
         const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
         load_blk(S0, A, n, i0, j0, rb, jb);
         __syncthreads();
-        double2 acc[4][4];
+        double2 acc[AR][AC];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)  // start from the current A block (loads in flight early)
+        for (int i = 0; i < AR; ++i)  // start from the current A block (loads in flight early)
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) {
-            const int r = ty + TW * i, c = tx + TW * jj;
+          for (int jj = 0; jj < AC; ++jj) {
+            const int r = acc_row(i, jj), c = acc_col(i, jj);
             acc[i][jj] = (r < rb && c < kbsz && (ib > kb || c <= r)) ? A[(i0 + r) * n + k0 + c]
                                                                       : make_double2(0, 0);
           }
         mma_tile_sub(S0, S1, jb, acc);
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < AR; ++i)
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) {
-            const int r = ty + TW * i, c = tx + TW * jj;
+          for (int jj = 0; jj < AC; ++jj) {
+            const int r = acc_row(i, jj), c = acc_col(i, jj);
             if (r < rb && c < kbsz && (ib > kb || c <= r)) A[(i0 + r) * n + k0 + c] = acc[i][jj];
           }
         __syncthreads();
@@ -323,7 +364,7 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
       for (int ib = j + 1; ib < gend; ++ib) {
         const int64_t i0 = (int64_t)ib * CB;
         const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
-        double2 acc[4][4];
+        double2 acc[AR][AC];
         zero_acc(acc);
         for (int kb = j; kb < ib; ++kb) {
           const int64_t k0 = (int64_t)kb * CB;
@@ -339,9 +380,9 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
         }
         // X_ij = -C_ii^{-1} acc
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < AR; ++i)
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) S1[(ty + TW * i) * PITCH + tx + TW * jj] = acc[i][jj];
+          for (int jj = 0; jj < AC; ++jj) S1[acc_row(i, jj) * PITCH + acc_col(i, jj)] = acc[i][jj];
         load_blk_adjU(S0, A, n, i0, rb);  // C_ii^{-1}
         __syncthreads();
         zero_acc(acc);
@@ -349,10 +390,10 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
         __syncthreads();
         // A[j0 + c][i0 + r] = conj(X_ij[r][c]) = -conj(acc[r][c])
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < AR; ++i)
 #pragma unroll
-          for (int jj = 0; jj < 4; ++jj) {
-            const int r = ty + TW * i, c = tx + TW * jj;
+          for (int jj = 0; jj < AC; ++jj) {
+            const int r = acc_row(i, jj), c = acc_col(i, jj);
             if (r < rb && c < jb) A[(j0 + c) * n + i0 + r] = make_double2(-acc[i][jj].x, acc[i][jj].y);
           }
         __syncthreads();
