@@ -111,7 +111,7 @@ struct coqui_b200_batch {
   DevBuf<float2> Xs, XTs, Ls, LHs;  // complex64 tensor-core operands
   DevBuf<double2> G, Sig, Ltmp, LHtmp;
   DevBuf<float2> Gt, T, UT, Sab, cache, PW;
-  DevBuf<float2> T1, Mb, Zb;
+  DevBuf<float2> T1, Mb, Zb, Zl;
   DevBuf<double2> Ab;
   DevBuf<int64_t> dofG, dnb;
   DevBuf<unsigned char> gtab, ctab, htab;
@@ -224,7 +224,50 @@ void batch_gw(Batch* b) {
   b->info.ensure(nprob);
   b->ld.ensure(nprob);
   b->tr.ensure(nprob);
-  cq::launch_chol_inv_grouped(cp, b->ctab, b->ld.p, b->tr.p, b->info.p, s);
+  // FP64 factorisation with the inverse inside the kInvGroup diagonal groups only; the
+  // off-group blocks of U = C^{-H} come from tensor-core doubling levels, as in the one-system
+  // Dyson solve: per level bl and pair of diagonal blocks (r0: bl, r1: b1)
+  //   S = U00 (-C10)^H,  U01 = S U11
+  // grouped over every molecule large enough for the level.  Z = U - I, Zl = U^H - I where a
+  // later level needs it, Zc = -C off the groups (in T1), S in Mb.
+  cq::launch_chol_inv_grouped(cp, b->ctab, b->ld.p, b->tr.p, b->info.p, s, true);
+  for (int64_t m = 0; m < b->nmol; ++m)
+    cq::launch_chol_split(b->Ab.p + b->offD[m], b->Zb.p + b->offD[m], b->Zl.p + b->offD[m],
+                          b->T1.p + b->offD[m], b->Np[m], nwh, s);
+  for (int64_t bl = cq::kInvGroup; bl < b->nmax; bl *= 2) {
+    struct Adj {
+      int64_t m, r0, r1, b1;
+    };
+    std::vector<cq::TcGroup> l1, l2;
+    std::vector<Adj> adj;
+    for (int64_t m = 0; m < b->nmol; ++m) {
+      const int64_t Np = b->Np[m], NN = Np * Np;
+      if (Np <= bl) continue;
+      float2* Z = b->Zb.p + b->offD[m];
+      float2* Zl = b->Zl.p + b->offD[m];
+      float2* Zc = b->T1.p + b->offD[m];
+      float2* S = b->Mb.p + b->offD[m];
+      for (int64_t r0 = 0; r0 + bl < Np; r0 += 2 * bl) {
+        const int64_t r1 = r0 + bl, b1 = std::min(bl, Np - r1);
+        cq::TcStructure t1;  // S = (Z + I)_00 (-C10)^H, A upper
+        t1.a_upper = true;
+        t1.a_ident = true;
+        l1.push_back(group(Z + r0 * Np + r0, false, false, Np, NN, Zc + r1 * Np + r0, false, true,
+                           Np, NN, S + r0 * Np + r1, Np, NN, bl, b1, bl, nwh, t1));
+        cq::TcStructure t2;  // U01 = S U11, U11(k, n) = conj(Zl[n][k]) + delta
+        t2.b_upper = true;
+        t2.b_ident = true;
+        l2.push_back(group(S + r0 * Np + r1, false, false, Np, NN, Zl + r1 * Np + r1, false, true,
+                           Np, NN, Z + r0 * Np + r1, Np, NN, bl, b1, b1, nwh, t2));
+        if (2 * bl < Np) adj.push_back(Adj{m, r0, r1, b1});
+      }
+    }
+    cq::tc_cgemm_grouped(l1, b->gtab, s);
+    cq::tc_cgemm_grouped(l2, b->gtab, s);
+    for (const Adj& a : adj)
+      cq::launch_block_adjoint(b->Zb.p + b->offD[a.m], b->Zl.p + b->offD[a.m], b->Np[a.m], a.r0,
+                               a.r1, bl, a.b1, nwh, s);
+  }
   std::vector<cq::TcGroup> f, t4, t5;
   std::vector<cq::HermProblem> hp;
   for (int64_t m = 0; m < b->nmol; ++m) {
@@ -350,6 +393,7 @@ int coqui_b200_batch_create(coqui_b200_batch** out, int64_t nmol, const int64_t*
     b->T1.ensure(b->nD);
     b->Mb.ensure(b->nD);
     b->Zb.ensure(b->nD);
+    b->Zl.ensure(b->nD);
     b->Ab.ensure(b->nD);
     std::vector<int64_t> offs(b->offG);
     b->dofG.ensure(nmol);

@@ -50,10 +50,11 @@ static_assert(!DMMA || (CB == 32 && CT == 64), "DMMA tiles: 32-blocks, two warps
 __global__ void __launch_bounds__(b32::CT, b32::MINB) k_chol_inv_grouped(const CholProblem* __restrict__ probs,
                                                                  double* __restrict__ logdet,
                                                                  double2* __restrict__ trace,
-                                                                 int* __restrict__ info) {
+                                                                 int* __restrict__ info,
+                                                                 int inv_group) {
   const CholProblem pr = probs[blockIdx.x];
   b32::chol_inv_problem<true>(pr.M, pr.A, logdet + blockIdx.x, trace + blockIdx.x,
-                              info + blockIdx.x, pr.n, 1 << 30);
+                              info + blockIdx.x, pr.n, inv_group);
 }
 
 // k_chol_inv<INV> of the block size chosen for n; the inverse is formed within diagonal groups
@@ -258,7 +259,8 @@ void launch_block_adjoint(const float2* Z, float2* Zl, int64_t Np, int64_t r0, i
 }
 
 void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,
-                             double* logdet, double2* trace, int* info, cudaStream_t s) {
+                             double* logdet, double2* trace, int* info, cudaStream_t s,
+                             bool group_inverse) {
   if (probs.empty()) return;
   const int64_t np = (int64_t)probs.size();
   CQ_REQUIRE(np <= 65535, COQUI_B200_EINVAL, "chol grouped: at most 65535 problems per launch");
@@ -279,9 +281,11 @@ void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsig
                                        (int)smem));
     set = true;
   }
-  k_chol_inv_grouped<<<(unsigned)np, b32::CT, smem, s>>>(t, logdet, trace, info);
+  const int inv_group = group_inverse ? (int)(kInvGroup / b32::CB) : (1 << 30);
+  k_chol_inv_grouped<<<(unsigned)np, b32::CT, smem, s>>>(t, logdet, trace, info, inv_group);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
+  if (group_inverse) return;
   k_chol_final_grouped<<<dim3(gx, (unsigned)np), 256, 0, s>>>(t);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());

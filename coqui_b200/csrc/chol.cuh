@@ -21,13 +21,17 @@ struct CholProblem {
   int64_t n;
 };
 
-// launch_chol_inv with Z for problems of different sizes in one launch per step (prep,
-// factorisation + full FP64 inverse, Z); results per problem in table order.
-void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,
-                             double* logdet, double2* trace, int* info, cudaStream_t s);
-
 // Diagonal group edge of the FP64 inverse when the tensor cores form the off-group blocks.
 constexpr int64_t kInvGroup = 128;
+
+// launch_chol_inv with Z for problems of different sizes in one launch per step (prep,
+// factorisation + full FP64 inverse, Z); results per problem in table order.  With
+// group_inverse the inverse is formed only inside the kInvGroup diagonal groups (as
+// launch_chol_group_inv) and Z is not written: launch_chol_split and the tensor-core levels
+// take over.
+void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,
+                             double* logdet, double2* trace, int* info, cudaStream_t s,
+                             bool group_inverse = false);
 
 // As launch_chol_inv without Z, but the inverse U = C^{-H} is formed only inside the
 // kInvGroup x kInvGroup diagonal groups (upper triangle of A there).

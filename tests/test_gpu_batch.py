@@ -10,7 +10,8 @@ from oracle import thc_oracle as O
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [(8, 48), (12, 72), (6, 36), (16, 150), (10, 260)]  # (orbitals, interpolating points)
+# (orbitals, interpolating points): one to three tensor-core inverse levels above Np = 128
+SIZES = [(8, 48), (12, 72), (6, 36), (16, 150), (10, 260), (20, 540)]
 
 
 @pytest.fixture(scope="module")
