@@ -230,7 +230,12 @@ void batch_gw(Batch* b) {
   //   S = U00 (-C10)^H,  U01 = S U11
   // grouped over every molecule large enough for the level.  Z = U - I, Zl = U^H - I where a
   // later level needs it, Zc = -C off the groups (in T1), S in Mb.
-  cq::launch_chol_inv_grouped(cp, b->ctab, b->ld.p, b->tr.p, b->info.p, s, true);
+  std::vector<int64_t> sizes;
+  for (const auto& c : cp) sizes.push_back(c.n);
+  if (cq::chol_prefer_tiled(sizes))  // the largest molecules spread over many CTAs each
+    cq::launch_chol_tiled(cp, b->ctab, b->ld.p, b->tr.p, b->info.p, s);
+  else
+    cq::launch_chol_inv_grouped(cp, b->ctab, b->ld.p, b->tr.p, b->info.p, s, true);
   for (int64_t m = 0; m < b->nmol; ++m)
     cq::launch_chol_split(b->Ab.p + b->offD[m], b->Zb.p + b->offD[m], b->Zl.p + b->offD[m],
                           b->T1.p + b->offD[m], b->Np[m], nwh, s);

@@ -12,7 +12,10 @@
 // holds a 16 x 32 accumulator as 8 x 8 fragments), operands staged in shared memory; the
 // CUDA-core FMA form (4 x 4 register tiles) is kept behind CHOL_FMA for comparison.  A = I - M
 // is set up and D^H written out by separate element-wise kernels.
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include "chol.cuh"
 
@@ -55,6 +58,132 @@ __global__ void __launch_bounds__(b32::CT, b32::MINB) k_chol_inv_grouped(const C
   const CholProblem pr = probs[blockIdx.x];
   b32::chol_inv_problem<true>(pr.M, pr.A, logdet + blockIdx.x, trace + blockIdx.x,
                               info + blockIdx.x, pr.n, inv_group);
+}
+
+// ---- tiled factorisation (several CTAs per problem) ----
+// Problems come in runs of equal size; a problem's matrices are taken from the table, or
+// (table == nullptr, one run) at base + p * stride.
+constexpr int kMaxRuns = 64;
+struct TiledRuns {
+  int nrun;
+  int64_t n[kMaxRuns];
+  int first[kMaxRuns];
+  int count[kMaxRuns];
+  const float2* M0;
+  double2* A0;
+  int64_t stride;
+};
+constexpr int kTiledG = (int)(kInvGroup / b32::CB);  // blocks per diagonal inverse group
+
+// work items of one launch: kind 0 diagonal block j (one per problem), 1 panel blocks below
+// it, 2 trailing blocks (i, k) with j < k <= i, 3 inverse columns (all columns that have a
+// block below them in their group; j is not used)
+__host__ __device__ inline int64_t tiled_items(int kind, int64_t nblk, int j) {
+  const int64_t m = nblk - j - 1;
+  switch (kind) {
+    case 0: return nblk > j ? 1 : 0;
+    case 1: return m > 0 ? m : 0;
+    case 2: return m > 0 ? m * (m + 1) / 2 : 0;
+    default: return nblk - (nblk + kTiledG - 1) / kTiledG;
+  }
+}
+
+__global__ void __launch_bounds__(b32::CT, b32::MINB)
+    k_chol_tiled(const CholProblem* __restrict__ probs, const __grid_constant__ TiledRuns R, int kind,
+                 int j, double* __restrict__ logdet, int* __restrict__ info) {
+  int64_t idx = blockIdx.x, local = 0, nblk = 0;
+  int p = -1;
+  for (int r = 0; r < R.nrun; ++r) {
+    const int64_t nb = (R.n[r] + b32::CB - 1) / b32::CB;
+    const int64_t per = tiled_items(kind, nb, j), tot = per * R.count[r];
+    if (idx < tot) {
+      p = R.first[r] + (int)(idx / per);
+      local = idx % per;
+      nblk = nb;
+      break;
+    }
+    idx -= tot;
+  }
+  if (p < 0) return;  // uniform over the CTA
+  double2* A = probs ? probs[p].A : R.A0 + p * R.stride;
+  const int64_t n = probs ? probs[p].n : R.n[0];
+  if (kind == 0) {
+    b32::tiled_diag(A, n, j, logdet + p, info + p);
+  } else if (kind == 1) {
+    b32::tiled_panel(A, n, j, j + 1 + (int)local);
+  } else if (kind == 2) {  // local -> (i', k'), 0 <= k' <= i'
+    int64_t a = (int64_t)((sqrt(8.0 * (double)local + 1.0) - 1.0) * 0.5);
+    while ((a + 1) * (a + 2) / 2 <= local) ++a;
+    while (a * (a + 1) / 2 > local) --a;
+    const int64_t b = local - a * (a + 1) / 2;
+    b32::tiled_update(A, n, j, j + 1 + (int)a, j + 1 + (int)b);
+  } else {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* S0 = reinterpret_cast<double2*>(smem_raw);
+    double2* S1 = S0 + b32::CB * b32::PITCH;
+    const int jj = (int)(local + local / (kTiledG - 1));
+    b32::inverse_column(A, n, jj, (int)min(nblk, (int64_t)(jj / kTiledG + 1) * kTiledG), S0, S1);
+  }
+}
+
+// trace = sum_i M_ii, logdet = 0, info = 0 per problem
+__global__ void k_tiled_init(const CholProblem* __restrict__ probs, const __grid_constant__ TiledRuns R,
+                             double* __restrict__ logdet, double2* __restrict__ trace,
+                             int* __restrict__ info) {
+  __shared__ double red[2][256];
+  const int p = blockIdx.x;
+  const float2* M = probs ? probs[p].M : R.M0 + p * R.stride;
+  const int64_t n = probs ? probs[p].n : R.n[0];
+  double tr = 0, ti = 0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const float2 m = M[i * n + i];
+    tr += m.x;
+    ti += m.y;
+  }
+  red[0][threadIdx.x] = tr;
+  red[1][threadIdx.x] = ti;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + w];
+      red[1][threadIdx.x] += red[1][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    trace[p] = make_double2(red[0][0], red[1][0]);
+    logdet[p] = 0.0;
+    info[p] = 0;
+  }
+}
+
+void run_tiled(const CholProblem* t, const TiledRuns& R, int64_t np, double* logdet, double2* trace,
+               int* info, cudaStream_t s) {
+  k_tiled_init<<<(unsigned)np, 256, 0, s>>>(t, R, logdet, trace, info);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+  const size_t smem = (size_t)2 * b32::CB * b32::PITCH * sizeof(double2);
+  static bool set = false;
+  if (!set) {
+    CQ_CHECK_CUDA(cudaFuncSetAttribute(k_chol_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    set = true;
+  }
+  int64_t maxblk = 0;
+  for (int r = 0; r < R.nrun; ++r) maxblk = std::max<int64_t>(maxblk, (R.n[r] + b32::CB - 1) / b32::CB);
+  auto go = [&](int kind, int j) {
+    int64_t grid = 0;
+    for (int r = 0; r < R.nrun; ++r)
+      grid += tiled_items(kind, (R.n[r] + b32::CB - 1) / b32::CB, j) * R.count[r];
+    if (grid == 0) return;
+    CQ_REQUIRE(grid <= 2147483647, COQUI_B200_EINVAL, "tiled Cholesky: too many blocks");
+    k_chol_tiled<<<(unsigned)grid, b32::CT, smem, s>>>(t, R, kind, j, logdet, info);
+    count_launch();
+    CQ_CHECK_CUDA(cudaGetLastError());
+  };
+  for (int j = 0; j < maxblk; ++j)
+    for (int kind = 0; kind < 3; ++kind) go(kind, j);
+  go(3, 0);
 }
 
 // k_chol_inv<INV> of the block size chosen for n; the inverse is formed within diagonal groups
@@ -256,6 +385,69 @@ void launch_block_adjoint(const float2* Z, float2* Zl, int64_t Np, int64_t r0, i
   k_block_adjoint<<<g, dim3(32, 8), 0, s>>>(Z, Zl, Np, r0, r1, b, b1);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+bool chol_prefer_tiled(const std::vector<int64_t>& sizes) {
+  // one CTA per problem: the makespan is at least the largest problem's time; spreading each
+  // problem over many CTAs pays when the whole set would otherwise finish sooner than that
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  double total = 0, mx = 0;
+  for (int64_t n : sizes) {
+    const double c = (double)n * n * n;
+    total += c;
+    mx = std::max(mx, c);
+  }
+  const int64_t nmax = sizes.empty() ? 0 : *std::max_element(sizes.begin(), sizes.end());
+  return nmax >= 4 * b32::CB && total / ((double)sms * b32::MINB) < mx;
+}
+
+void launch_chol_tiled_strided(const float2* M, double2* A, double* logdet, double2* trace,
+                               int* info, int64_t Np, int64_t nprob, cudaStream_t s) {
+  const int64_t total = Np * Np * nprob;
+  k_chol_prep<<<grid_for(total, 256), 256, 0, s>>>(M, A, Np, total);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+  CQ_REQUIRE(nprob <= 2147483647, COQUI_B200_EINVAL, "tiled Cholesky: too many problems");
+  TiledRuns R{};
+  R.nrun = 1;
+  R.n[0] = Np;
+  R.first[0] = 0;
+  R.count[0] = (int)nprob;
+  R.M0 = M;
+  R.A0 = A;
+  R.stride = Np * Np;
+  run_tiled(nullptr, R, nprob, logdet, trace, info, s);
+}
+
+void launch_chol_tiled(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,
+                       double* logdet, double2* trace, int* info, cudaStream_t s) {
+  if (probs.empty()) return;
+  const int64_t np = (int64_t)probs.size();
+  TiledRuns R{};
+  for (int64_t p = 0; p < np; ++p) {
+    if (R.nrun > 0 && R.n[R.nrun - 1] == probs[p].n) {
+      ++R.count[R.nrun - 1];
+      continue;
+    }
+    CQ_REQUIRE(R.nrun < kMaxRuns, COQUI_B200_EINVAL, "tiled Cholesky: too many problem sizes");
+    R.n[R.nrun] = probs[p].n;
+    R.first[R.nrun] = (int)p;
+    R.count[R.nrun] = 1;
+    ++R.nrun;
+  }
+  table.ensure(np * sizeof(CholProblem));
+  CQ_CHECK_CUDA(cudaMemcpyAsync(table.p, probs.data(), np * sizeof(CholProblem),
+                                cudaMemcpyHostToDevice, s));
+  const CholProblem* t = (const CholProblem*)table.p;
+  int64_t nmax = 0;
+  for (const auto& p : probs) nmax = std::max(nmax, p.n);
+  const unsigned gx = (unsigned)std::min<int64_t>((nmax * nmax + 255) / 256, 1024);
+  k_chol_prep_grouped<<<dim3(gx, (unsigned)np), 256, 0, s>>>(t);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+  run_tiled(t, R, np, logdet, trace, info, s);
 }
 
 void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,

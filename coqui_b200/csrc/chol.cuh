@@ -33,6 +33,20 @@ void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsig
                              double* logdet, double2* trace, int* info, cudaStream_t s,
                              bool group_inverse = false);
 
+// The same results as launch_chol_inv_grouped(..., group_inverse = true) with each problem
+// spread over many CTAs: one launch per phase of every block column (the diagonal block; the
+// panel blocks below it; the trailing blocks), then one for the group inverse.  Problems of
+// equal size must be consecutive (at most 64 runs).  For sets whose largest problem would
+// otherwise set the finishing time (few problems, or a few much larger than the rest).
+void launch_chol_tiled(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,
+                       double* logdet, double2* trace, int* info, cudaStream_t s);
+// launch_chol_group_inv through the tiled path (problems at M + p Np^2, A + p Np^2)
+void launch_chol_tiled_strided(const float2* M, double2* A, double* logdet, double2* trace,
+                               int* info, int64_t Np, int64_t nprob, cudaStream_t s);
+// Whether the tiled path finishes sooner for problems of these sizes (one CTA per problem
+// leaves the GPU mostly idle while the largest problem finishes).
+bool chol_prefer_tiled(const std::vector<int64_t>& sizes);
+
 // As launch_chol_inv without Z, but the inverse U = C^{-H} is formed only inside the
 // kInvGroup x kInvGroup diagonal groups (upper triangle of A there).
 void launch_chol_group_inv(const float2* M, double2* A, double* logdet, double2* trace, int* info,

@@ -259,6 +259,134 @@ __device__ void invert_lower(const double2* S, double2* Sinv, int n) {
   __syncthreads();
 }
 
+// Column j of X = C^{-1} below the diagonal within its diagonal group (blocks j+1 .. gend-1):
+//   X_ij = -C_ii^{-1} sum_{k=j}^{i-1} C_ik X_kj,
+// with C_ik in the lower triangle of A, C_ii^{-H} in the upper triangle of the diagonal
+// blocks; X_ij is kept as its adjoint in the upper block (j, i).  Columns are independent.
+__device__ void inverse_column(double2* A, int64_t n, int j, int gend, double2* S0, double2* S1) {
+  const int64_t j0 = (int64_t)j * CB;
+  const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+  for (int ib = j + 1; ib < gend; ++ib) {
+    const int64_t i0 = (int64_t)ib * CB;
+    const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+    double2 acc[AR][AC];
+    zero_acc(acc);
+    for (int kb = j; kb < ib; ++kb) {
+      const int64_t k0 = (int64_t)kb * CB;
+      const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
+      load_blk(S1, A, n, i0, k0, rb, kbsz);  // C_ik (strictly lower block)
+      if (kb == j)
+        load_blk_adjU(S0, A, n, j0, jb);  // X_jj
+      else
+        load_blk_adj(S0, A, n, j0, k0, jb, kbsz);  // X_kj = (A_jk)^H
+      __syncthreads();
+      mma_tile<false>(S1, S0, kbsz, acc);
+      __syncthreads();
+    }
+    // X_ij = -C_ii^{-1} acc
+#pragma unroll
+    for (int i = 0; i < AR; ++i)
+#pragma unroll
+      for (int jj = 0; jj < AC; ++jj) S1[acc_row(i, jj) * PITCH + acc_col(i, jj)] = acc[i][jj];
+    load_blk_adjU(S0, A, n, i0, rb);  // C_ii^{-1}
+    __syncthreads();
+    zero_acc(acc);
+    mma_tile<false>(S0, S1, rb, acc);
+    __syncthreads();
+    // A[j0 + c][i0 + r] = conj(X_ij[r][c]) = -conj(acc[r][c])
+#pragma unroll
+    for (int i = 0; i < AR; ++i)
+#pragma unroll
+      for (int jj = 0; jj < AC; ++jj) {
+        const int r = acc_row(i, jj), c = acc_col(i, jj);
+        if (r < rb && c < jb) A[(j0 + c) * n + i0 + r] = make_double2(-acc[i][jj].x, acc[i][jj].y);
+      }
+    __syncthreads();
+  }
+}
+
+// ---- tiled factorisation: one problem spread over many CTAs, one launch per phase of each
+// block column j (diagonal block; panel blocks; trailing blocks), then the group inverse ----
+
+// diagonal block j: factor and invert in shared memory, C_jj^{-H} into the upper triangle,
+// ln det contribution added to *logdet, *info set for a non-positive pivot
+__device__ void tiled_diag(double2* A, int64_t n, int j, double* logdet, int* info) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* S0 = reinterpret_cast<double2*>(smem_raw);
+  double2* S1 = S0 + CB * PITCH;
+  __shared__ double s_ld;
+  __shared__ int s_bad;
+  if (threadIdx.x == 0) {
+    s_ld = 0.0;
+    s_bad = 0;
+  }
+  const int64_t j0 = (int64_t)j * CB;
+  const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+  load_blk(S0, A, n, j0, j0, jb, jb);
+  __syncthreads();
+  factor_diag(S0, jb, &s_ld, &s_bad);
+  invert_lower(S0, S1, jb);
+  store_blk_adjU(S1, A, n, j0, jb);
+  if (threadIdx.x == 0) {
+    *logdet += 2.0 * s_ld;
+    if (s_bad) *info = 1;
+  }
+}
+
+// panel block (i, j), i > j: L_ij = A_ij C_jj^{-H}
+__device__ void tiled_panel(double2* A, int64_t n, int j, int ib) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* S0 = reinterpret_cast<double2*>(smem_raw);
+  double2* S1 = S0 + CB * PITCH;
+  const int64_t j0 = (int64_t)j * CB, i0 = (int64_t)ib * CB;
+  const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+  const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+  load_blk(S0, A, n, i0, j0, rb, jb);
+  load_blk_adjU(S1, A, n, j0, jb);  // C_jj^{-1}
+  __syncthreads();
+  double2 acc[AR][AC];
+  zero_acc(acc);
+  mma_tile<true>(S0, S1, jb, acc);
+#pragma unroll
+  for (int i = 0; i < AR; ++i)
+#pragma unroll
+    for (int jj = 0; jj < AC; ++jj) {
+      const int r = acc_row(i, jj), c = acc_col(i, jj);
+      if (r < rb && c < jb) A[(i0 + r) * n + j0 + c] = acc[i][jj];
+    }
+}
+
+// trailing block (i, k), j < k <= i: A_ik -= L_ij L_kj^H (lower triangle only when i == k)
+__device__ void tiled_update(double2* A, int64_t n, int j, int ib, int kb) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* S0 = reinterpret_cast<double2*>(smem_raw);
+  double2* S1 = S0 + CB * PITCH;
+  const int64_t j0 = (int64_t)j * CB, i0 = (int64_t)ib * CB, k0 = (int64_t)kb * CB;
+  const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+  const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+  const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
+  load_blk(S0, A, n, i0, j0, rb, jb);
+  load_blk(S1, A, n, k0, j0, kbsz, jb);
+  double2 acc[AR][AC];
+#pragma unroll
+  for (int i = 0; i < AR; ++i)
+#pragma unroll
+    for (int jj = 0; jj < AC; ++jj) {
+      const int r = acc_row(i, jj), c = acc_col(i, jj);
+      acc[i][jj] = (r < rb && c < kbsz && (ib > kb || c <= r)) ? A[(i0 + r) * n + k0 + c]
+                                                               : make_double2(0, 0);
+    }
+  __syncthreads();
+  mma_tile_sub(S0, S1, jb, acc);
+#pragma unroll
+  for (int i = 0; i < AR; ++i)
+#pragma unroll
+    for (int jj = 0; jj < AC; ++jj) {
+      const int r = acc_row(i, jj), c = acc_col(i, jj);
+      if (r < rb && c < kbsz && (ib > kb || c <= r)) A[(i0 + r) * n + k0 + c] = acc[i][jj];
+    }
+}
+
 // inv_group: the inverse is formed within diagonal groups of inv_group blocks only (the
 // whole matrix when inv_group >= nblk); the tensor-core levels fill in the rest.
 // One problem: M, A (n x n), results at logdet/trace/info[0].
@@ -357,48 +485,8 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
 
   if (INV) {
     // X = C^{-1} block column by block column, X^H kept in the upper triangle of A
-    for (int j = 0; j < nblk; ++j) {
-      const int64_t j0 = (int64_t)j * CB;
-      const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
-      const int gend = min(nblk, (j / inv_group + 1) * inv_group);
-      for (int ib = j + 1; ib < gend; ++ib) {
-        const int64_t i0 = (int64_t)ib * CB;
-        const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
-        double2 acc[AR][AC];
-        zero_acc(acc);
-        for (int kb = j; kb < ib; ++kb) {
-          const int64_t k0 = (int64_t)kb * CB;
-          const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
-          load_blk(S1, A, n, i0, k0, rb, kbsz);  // C_ik (strictly lower block)
-          if (kb == j)
-            load_blk_adjU(S0, A, n, j0, jb);  // X_jj
-          else
-            load_blk_adj(S0, A, n, j0, k0, jb, kbsz);  // X_kj = (A_jk)^H
-          __syncthreads();
-          mma_tile<false>(S1, S0, kbsz, acc);
-          __syncthreads();
-        }
-        // X_ij = -C_ii^{-1} acc
-#pragma unroll
-        for (int i = 0; i < AR; ++i)
-#pragma unroll
-          for (int jj = 0; jj < AC; ++jj) S1[acc_row(i, jj) * PITCH + acc_col(i, jj)] = acc[i][jj];
-        load_blk_adjU(S0, A, n, i0, rb);  // C_ii^{-1}
-        __syncthreads();
-        zero_acc(acc);
-        mma_tile<false>(S0, S1, rb, acc);
-        __syncthreads();
-        // A[j0 + c][i0 + r] = conj(X_ij[r][c]) = -conj(acc[r][c])
-#pragma unroll
-        for (int i = 0; i < AR; ++i)
-#pragma unroll
-          for (int jj = 0; jj < AC; ++jj) {
-            const int r = acc_row(i, jj), c = acc_col(i, jj);
-            if (r < rb && c < jb) A[(j0 + c) * n + i0 + r] = make_double2(-acc[i][jj].x, acc[i][jj].y);
-          }
-        __syncthreads();
-      }
-    }
+    for (int j = 0; j < nblk; ++j)
+      inverse_column(A, n, j, min(nblk, (j / inv_group + 1) * inv_group), S0, S1);
   }
 
   // reductions

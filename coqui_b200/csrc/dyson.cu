@@ -261,7 +261,10 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       const bool tc_inverse = a.mixed && a.want_w && Np > kInvGroup;
       if (a.mixed) {
         Prof::Scope sc(a.prof, "dyson_chol_inv");
-        if (tc_inverse)
+        if (tc_inverse && chol_prefer_tiled(std::vector<int64_t>((size_t)nb, Np)))
+          launch_chol_tiled_strided((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0,
+                                    Np, nb, s);  // few large problems: many CTAs per problem
+        else if (tc_inverse)
           launch_chol_group_inv((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0, Np,
                                 nb, s);
         else
