@@ -321,6 +321,8 @@ def run_ours(args, rank, world, local):
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     bf16 = peaks.get("bf16_tflops", 1590.0)
+    # FP64 (CUDA-core FMA and DMMA alike): 64 multiply-adds per clock per SM, nominal clock
+    fp64_nom = 148 * 64 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     peak_src = "measured" if peaks else "fallback"
     groups = {}
     for name, (ms_tot, n) in stats.items():
@@ -337,6 +339,8 @@ def run_ours(args, rank, world, local):
                 g["achieved_TFLOPs"] = amount / (ms_it * 1e-3) / 1e12
                 if kind == "tensor":
                     g["frac_of_bf16"] = g["achieved_TFLOPs"] / bf16
+                elif kind == "fp64":
+                    g["frac_of_fp64_nominal"] = g["achieved_TFLOPs"] / fp64_nom
         groups[name] = g
     # DRAM bytes of the screened-interaction products per (q, iW) problem from the committed
     # ncu summary (measured on a smaller case; the traffic grows with the problem count)
