@@ -11,7 +11,8 @@
 // tensor cores (mma.sync m8n8k4, four real products per complex one; each of the two warps
 // holds a 16 x 32 accumulator as 8 x 8 fragments), operands staged in shared memory; the
 // CUDA-core FMA form (4 x 4 register tiles) is kept behind CHOL_FMA for comparison.  A = I - M
-// is set up and D^H written out by separate element-wise kernels.
+// is read from M in the first block column (A holds only FP64 blocks written by the
+// factorisation); D^H is written out by a separate element-wise kernel.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -106,17 +107,18 @@ __global__ void __launch_bounds__(b32::CT, b32::MINB)
   }
   if (p < 0) return;  // uniform over the CTA
   double2* A = probs ? probs[p].A : R.A0 + p * R.stride;
+  const float2* M = probs ? probs[p].M : R.M0 + p * R.stride;
   const int64_t n = probs ? probs[p].n : R.n[0];
   if (kind == 0) {
-    b32::tiled_diag(A, n, j, logdet + p, info + p);
+    b32::tiled_diag(M, A, n, j, logdet + p, info + p);
   } else if (kind == 1) {
-    b32::tiled_panel(A, n, j, j + 1 + (int)local);
+    b32::tiled_panel(M, A, n, j, j + 1 + (int)local);
   } else if (kind == 2) {  // local -> (i', k'), 0 <= k' <= i'
     int64_t a = (int64_t)((sqrt(8.0 * (double)local + 1.0) - 1.0) * 0.5);
     while ((a + 1) * (a + 2) / 2 <= local) ++a;
     while (a * (a + 1) / 2 > local) --a;
     const int64_t b = local - a * (a + 1) / 2;
-    b32::tiled_update(A, n, j, j + 1 + (int)a, j + 1 + (int)b);
+    b32::tiled_update(M, A, n, j, j + 1 + (int)a, j + 1 + (int)b);
   } else {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* S0 = reinterpret_cast<double2*>(smem_raw);
@@ -202,20 +204,7 @@ void launch_factor(const float2* M, double2* A, double* logdet, double2* trace, 
   go(b32::k_chol_inv<INV>, b32::CB, b32::CT, b32::PITCH);
 }
 
-// grouped A = I - M (lower) and Z = X^H - I, blockIdx.y = problem
-__global__ void k_chol_prep_grouped(const CholProblem* __restrict__ probs) {
-  const CholProblem pr = probs[blockIdx.y];
-  const int64_t n = pr.n, total = n * n;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = e / n, c = e % n;
-    if (c <= r) {
-      const float2 m = pr.M[e];
-      pr.A[e] = make_double2((r == c ? 1.0 : 0.0) - (double)m.x, -(double)m.y);
-    }
-  }
-}
-
+// grouped Z = X^H - I, blockIdx.y = problem
 __global__ void k_chol_final_grouped(const CholProblem* __restrict__ probs) {
   const CholProblem pr = probs[blockIdx.y];
   const int64_t n = pr.n, total = n * n;
@@ -228,19 +217,6 @@ __global__ void k_chol_final_grouped(const CholProblem* __restrict__ probs) {
       z = make_float2((float)(a.x - (r == c ? 1.0 : 0.0)), (float)a.y);
     }
     pr.Z[e] = z;
-  }
-}
-
-// A = I - M on the lower triangle of every problem (FP64)
-__global__ void k_chol_prep(const float2* __restrict__ M, double2* __restrict__ A, int64_t n,
-                            int64_t total) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = i % (n * n), r = e / n, c = e % n;
-    if (c <= r) {
-      const float2 m = M[i];
-      A[i] = make_double2((r == c ? 1.0 : 0.0) - (double)m.x, -(double)m.y);
-    }
   }
 }
 
@@ -345,9 +321,6 @@ __global__ void k_block_adjoint(const float2* __restrict__ Zall, float2* __restr
 void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, double2* trace,
                      int* info, int64_t Np, int64_t nprob, cudaStream_t s) {
   const int64_t total = Np * Np * nprob;
-  k_chol_prep<<<grid_for(total, 256), 256, 0, s>>>(M, A, Np, total);
-  count_launch();
-  CQ_CHECK_CUDA(cudaGetLastError());
   const int64_t all = (int64_t)1 << 40;  // inverse over the whole matrix
   if (Z) {
     launch_factor<true>(M, A, logdet, trace, info, Np, nprob, all, s);
@@ -361,10 +334,6 @@ void launch_chol_inv(const float2* M, double2* A, float2* Z, double* logdet, dou
 
 void launch_chol_group_inv(const float2* M, double2* A, double* logdet, double2* trace, int* info,
                            int64_t Np, int64_t nprob, cudaStream_t s) {
-  const int64_t total = Np * Np * nprob;
-  k_chol_prep<<<grid_for(total, 256), 256, 0, s>>>(M, A, Np, total);
-  count_launch();
-  CQ_CHECK_CUDA(cudaGetLastError());
   launch_factor<true>(M, A, logdet, trace, info, Np, nprob, kInvGroup, s);
 }
 
@@ -405,10 +374,6 @@ bool chol_prefer_tiled(const std::vector<int64_t>& sizes) {
 
 void launch_chol_tiled_strided(const float2* M, double2* A, double* logdet, double2* trace,
                                int* info, int64_t Np, int64_t nprob, cudaStream_t s) {
-  const int64_t total = Np * Np * nprob;
-  k_chol_prep<<<grid_for(total, 256), 256, 0, s>>>(M, A, Np, total);
-  count_launch();
-  CQ_CHECK_CUDA(cudaGetLastError());
   CQ_REQUIRE(nprob <= 2147483647, COQUI_B200_EINVAL, "tiled Cholesky: too many problems");
   TiledRuns R{};
   R.nrun = 1;
@@ -440,14 +405,7 @@ void launch_chol_tiled(const std::vector<CholProblem>& probs, DevBuf<unsigned ch
   table.ensure(np * sizeof(CholProblem));
   CQ_CHECK_CUDA(cudaMemcpyAsync(table.p, probs.data(), np * sizeof(CholProblem),
                                 cudaMemcpyHostToDevice, s));
-  const CholProblem* t = (const CholProblem*)table.p;
-  int64_t nmax = 0;
-  for (const auto& p : probs) nmax = std::max(nmax, p.n);
-  const unsigned gx = (unsigned)std::min<int64_t>((nmax * nmax + 255) / 256, 1024);
-  k_chol_prep_grouped<<<dim3(gx, (unsigned)np), 256, 0, s>>>(t);
-  count_launch();
-  CQ_CHECK_CUDA(cudaGetLastError());
-  run_tiled(t, R, np, logdet, trace, info, s);
+  run_tiled((const CholProblem*)table.p, R, np, logdet, trace, info, s);
 }
 
 void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,
@@ -463,9 +421,6 @@ void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsig
   int64_t nmax = 0;
   for (const auto& p : probs) nmax = std::max(nmax, p.n);
   const unsigned gx = (unsigned)std::min<int64_t>((nmax * nmax + 255) / 256, 1024);
-  k_chol_prep_grouped<<<dim3(gx, (unsigned)np), 256, 0, s>>>(t);
-  count_launch();
-  CQ_CHECK_CUDA(cudaGetLastError());
   const size_t smem = (size_t)2 * b32::CB * b32::PITCH * sizeof(double2);
   static bool set = false;
   if (!set) {

@@ -22,6 +22,27 @@ __device__ __forceinline__ void load_blk(double2* S, const double2* G, int64_t l
     S[(i / CB) * PITCH + i % CB] = v[u];
   }
 }
+// element (r, c) of I - M (M complex64, n x n row-major) in FP64
+__device__ __forceinline__ double2 i_minus_m(const float2* M, int64_t n, int64_t r, int64_t c) {
+  const float2 m = M[r * n + c];
+  return make_double2((r == c ? 1.0 : 0.0) - (double)m.x, -(double)m.y);
+}
+// smem tile <- block of I - M (the first block column's reads: A = I - M is not stored)
+__device__ __forceinline__ void load_blk_im(double2* S, const float2* M, int64_t n, int64_t r0,
+                                            int64_t c0, int rb, int cb) {
+  double2 v[CB * CB / CT];
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    const int r = i / CB, c = i % CB;
+    v[u] = (r < rb && c < cb) ? i_minus_m(M, n, r0 + r, c0 + c) : make_double2(0, 0);
+  }
+#pragma unroll
+  for (int u = 0; u < CB * CB / CT; ++u) {
+    const int i = threadIdx.x + u * CT;
+    S[(i / CB) * PITCH + i % CB] = v[u];
+  }
+}
 // smem tile <- conj transpose of a global block: S[r][c] = conj(G[c0 + c][r0 + r])... given as
 // (the block stored at rows gr0, cols gc0 with gr x gc valid) -> S = G_blk^H
 __device__ __forceinline__ void load_blk_adj(double2* S, const double2* G, int64_t ld, int64_t gr0,
@@ -187,6 +208,33 @@ __device__ __forceinline__ void zero_acc(double2 (&acc)[AR][AC]) {
     for (int j = 0; j < AC; ++j) acc[i][j] = make_double2(0, 0);
 }
 
+// acc <- block (i0.., k0..) of A, or of I - M (from_m, the first block column), restricted
+// to rb x kbsz and, unless off_diag, to the lower triangle; the source is chosen once for the
+// whole tile so that all its loads are issued back to back
+__device__ __forceinline__ void acc_init(double2 (&acc)[AR][AC], const double2* A, const float2* M,
+                                         bool from_m, int64_t n, int64_t i0, int64_t k0, int rb,
+                                         int kbsz, bool off_diag) {
+  if (from_m) {
+#pragma unroll
+    for (int i = 0; i < AR; ++i)
+#pragma unroll
+      for (int jj = 0; jj < AC; ++jj) {
+        const int r = acc_row(i, jj), c = acc_col(i, jj);
+        acc[i][jj] = (r < rb && c < kbsz && (off_diag || c <= r)) ? i_minus_m(M, n, i0 + r, k0 + c)
+                                                                  : make_double2(0, 0);
+      }
+  } else {
+#pragma unroll
+    for (int i = 0; i < AR; ++i)
+#pragma unroll
+      for (int jj = 0; jj < AC; ++jj) {
+        const int r = acc_row(i, jj), c = acc_col(i, jj);
+        acc[i][jj] = (r < rb && c < kbsz && (off_diag || c <= r)) ? A[(i0 + r) * n + k0 + c]
+                                                                  : make_double2(0, 0);
+      }
+  }
+}
+
 // In-place Cholesky of the lower triangle of S (n x n); adds sum ln C_ii to *ld_acc
 // (thread 0) and sets *bad if a pivot is not positive.  One barrier per column: column c is
 // used unscaled (times 1/d_c) in its rank-1 update and scaled during the next column's step.
@@ -310,7 +358,8 @@ __device__ void inverse_column(double2* A, int64_t n, int j, int gend, double2* 
 
 // diagonal block j: factor and invert in shared memory, C_jj^{-H} into the upper triangle,
 // ln det contribution added to *logdet, *info set for a non-positive pivot
-__device__ void tiled_diag(double2* A, int64_t n, int j, double* logdet, int* info) {
+__device__ void tiled_diag(const float2* M, double2* A, int64_t n, int j, double* logdet,
+                           int* info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* S0 = reinterpret_cast<double2*>(smem_raw);
   double2* S1 = S0 + CB * PITCH;
@@ -322,7 +371,10 @@ __device__ void tiled_diag(double2* A, int64_t n, int j, double* logdet, int* in
   }
   const int64_t j0 = (int64_t)j * CB;
   const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
-  load_blk(S0, A, n, j0, j0, jb, jb);
+  if (j == 0)
+    load_blk_im(S0, M, n, j0, j0, jb, jb);
+  else
+    load_blk(S0, A, n, j0, j0, jb, jb);
   __syncthreads();
   factor_diag(S0, jb, &s_ld, &s_bad);
   invert_lower(S0, S1, jb);
@@ -334,14 +386,17 @@ __device__ void tiled_diag(double2* A, int64_t n, int j, double* logdet, int* in
 }
 
 // panel block (i, j), i > j: L_ij = A_ij C_jj^{-H}
-__device__ void tiled_panel(double2* A, int64_t n, int j, int ib) {
+__device__ void tiled_panel(const float2* M, double2* A, int64_t n, int j, int ib) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* S0 = reinterpret_cast<double2*>(smem_raw);
   double2* S1 = S0 + CB * PITCH;
   const int64_t j0 = (int64_t)j * CB, i0 = (int64_t)ib * CB;
   const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
   const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
-  load_blk(S0, A, n, i0, j0, rb, jb);
+  if (j == 0)
+    load_blk_im(S0, M, n, i0, j0, rb, jb);
+  else
+    load_blk(S0, A, n, i0, j0, rb, jb);
   load_blk_adjU(S1, A, n, j0, jb);  // C_jj^{-1}
   __syncthreads();
   double2 acc[AR][AC];
@@ -357,7 +412,7 @@ __device__ void tiled_panel(double2* A, int64_t n, int j, int ib) {
 }
 
 // trailing block (i, k), j < k <= i: A_ik -= L_ij L_kj^H (lower triangle only when i == k)
-__device__ void tiled_update(double2* A, int64_t n, int j, int ib, int kb) {
+__device__ void tiled_update(const float2* M, double2* A, int64_t n, int j, int ib, int kb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* S0 = reinterpret_cast<double2*>(smem_raw);
   double2* S1 = S0 + CB * PITCH;
@@ -368,14 +423,7 @@ __device__ void tiled_update(double2* A, int64_t n, int j, int ib, int kb) {
   load_blk(S0, A, n, i0, j0, rb, jb);
   load_blk(S1, A, n, k0, j0, kbsz, jb);
   double2 acc[AR][AC];
-#pragma unroll
-  for (int i = 0; i < AR; ++i)
-#pragma unroll
-    for (int jj = 0; jj < AC; ++jj) {
-      const int r = acc_row(i, jj), c = acc_col(i, jj);
-      acc[i][jj] = (r < rb && c < kbsz && (ib > kb || c <= r)) ? A[(i0 + r) * n + k0 + c]
-                                                               : make_double2(0, 0);
-    }
+  acc_init(acc, A, M, j == 0, n, i0, k0, rb, kbsz, ib > kb);
   __syncthreads();
   mma_tile_sub(S0, S1, jb, acc);
 #pragma unroll
@@ -410,7 +458,8 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
     s_ld = 0.0;
     s_bad = 0;
   }
-  // trace of M (A = I - M was set up by k_chol_prep)
+  // trace of M; A = I - M is read from M in block column 0 (every lower block of A is written
+  // there: the panel and the trailing update of column 0)
   double tr = 0, ti = 0;
   for (int64_t i = threadIdx.x; i < n; i += CT) {
     const float2 m = M[i * n + i];
@@ -425,7 +474,10 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
     const int64_t j0 = (int64_t)j * CB;
     const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
     // 1. diagonal block: factor and invert
-    load_blk(S0, A, n, j0, j0, jb, jb);
+    if (j == 0)
+      load_blk_im(S0, M, n, j0, j0, jb, jb);
+    else
+      load_blk(S0, A, n, j0, j0, jb, jb);
     __syncthreads();
     factor_diag(S0, jb, &s_ld, &s_bad);
     invert_lower(S0, S1, jb);
@@ -436,7 +488,10 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
     for (int ib = j + 1; ib < nblk; ++ib) {
       const int64_t i0 = (int64_t)ib * CB;
       const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
-      load_blk(S0, A, n, i0, j0, rb, jb);
+      if (j == 0)
+        load_blk_im(S0, M, n, i0, j0, rb, jb);
+      else
+        load_blk(S0, A, n, i0, j0, rb, jb);
       __syncthreads();
       double2 acc[AR][AC];
       zero_acc(acc);
@@ -462,14 +517,7 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
         load_blk(S0, A, n, i0, j0, rb, jb);
         __syncthreads();
         double2 acc[AR][AC];
-#pragma unroll
-        for (int i = 0; i < AR; ++i)  // start from the current A block (loads in flight early)
-#pragma unroll
-          for (int jj = 0; jj < AC; ++jj) {
-            const int r = acc_row(i, jj), c = acc_col(i, jj);
-            acc[i][jj] = (r < rb && c < kbsz && (ib > kb || c <= r)) ? A[(i0 + r) * n + k0 + c]
-                                                                      : make_double2(0, 0);
-          }
+        acc_init(acc, A, M, j == 0, n, i0, k0, rb, kbsz, ib > kb);  // loads in flight early
         mma_tile_sub(S0, S1, jb, acc);
 #pragma unroll
         for (int i = 0; i < AR; ++i)
