@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <vector>
 
 #include "chol.cuh"
@@ -357,6 +358,11 @@ void launch_block_adjoint(const float2* Z, float2* Zl, int64_t Np, int64_t r0, i
 }
 
 bool chol_prefer_tiled(const std::vector<int64_t>& sizes) {
+  // COQUI_B200_CHOL_TILED=1 / 0 forces the choice (for problems above one inverse group)
+  const char* force = std::getenv("COQUI_B200_CHOL_TILED");
+  const int64_t nmax0 = sizes.empty() ? 0 : *std::max_element(sizes.begin(), sizes.end());
+  if (force && (force[0] == '0' || force[0] == '1'))
+    return force[0] == '1' && nmax0 >= 4 * b32::CB;
   // one CTA per problem: the makespan is at least the largest problem's time; spreading each
   // problem over many CTAs pays when the whole set would otherwise finish sooner than that
   int dev = 0, sms = 148;

@@ -44,7 +44,8 @@ void launch_chol_tiled(const std::vector<CholProblem>& probs, DevBuf<unsigned ch
 void launch_chol_tiled_strided(const float2* M, double2* A, double* logdet, double2* trace,
                                int* info, int64_t Np, int64_t nprob, cudaStream_t s);
 // Whether the tiled path finishes sooner for problems of these sizes (one CTA per problem
-// leaves the GPU mostly idle while the largest problem finishes).
+// leaves the GPU mostly idle while the largest problem finishes); the environment variable
+// COQUI_B200_CHOL_TILED=1 or 0 forces the choice.
 bool chol_prefer_tiled(const std::vector<int64_t>& sizes);
 
 // As launch_chol_inv without Z, but the inverse U = C^{-H} is formed only inside the
