@@ -373,7 +373,10 @@ def run_ours(args, rank, world, local):
                     "200-problem case by the problem count)" if traffic else None,
                     "avg_launch_ms": per_ms,
                     "peak_source": peak_src + " dense bf16 cuBLAS; split-TF32 complex products "
-                                   "issue 3 TF32 MMAs at half the bf16 rate per counted flop"}
+                                   "issue 3 TF32 MMAs at half the bf16 rate per counted flop",
+                    # the rate the split form can reach at that peak: peak / 6 per counted flop
+                    "split_tf32_ceiling": bf16 / 6.0,
+                    "frac_of_split_tf32_ceiling": g["achieved_TFLOPs"] / (bf16 / 6.0)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
