@@ -108,3 +108,22 @@ def test_resident_iteration_graph_matches_direct_launches(case):
     S_graph = c.eval_sigma(None)
     assert np.array_equal(S_graph, S_direct)
     c.close()
+
+
+def test_graph_capture_of_tiled_factorisation_and_tensor_core_inverse():
+    """Np = 300 with one q: a few large Dyson problems take the tiled factorisation and the
+    tensor-core inverse levels; both are captured in the resident-G graph and replay to the
+    directly launched result."""
+    s = make_system(1, 16, 8, 300, seed=7, gamma_only=True)
+    ft = O.IAFT(1000.0, 10.0, "low")
+    G = s.G0(ft)
+    c = capi.Context(s.nk, s.nb, s.Np, ft.nt_f, ft.nw_b, s.kp_grid, mode=capi.MIXED)
+    c.set_ir(ProductIAFT(1000.0, 10.0, "low"))
+    c.set_kmesh(s.kpts, s.lattv, s.chi_bar)
+    c.set_thc(s.X, s.V)
+    S_direct, _ = c.gw_iteration(G)
+    c.gw_iteration(None, want_sigma=False)  # capture + launch
+    c.gw_iteration(None, want_sigma=False)  # replay
+    assert [name for name, _ in c.timings()] == ["GW_ITERATION_GRAPH"]
+    assert np.array_equal(c.eval_sigma(None), S_direct)
+    c.close()
