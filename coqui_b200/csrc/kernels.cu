@@ -452,12 +452,51 @@ static int cubic_edge(KGrid g) {
     default: { constexpr int NCV = 0; __VA_ARGS__; } break; \
   }
 
+// One k-point (Gamma-only): every DFT is the identity and the column kernels reduce to
+// element-wise products; these stream the arrays at full width instead of staging 32-column
+// tiles through shared memory.
+template <typename R>
+__global__ void __launch_bounds__(256) k_pi_gamma(const cplx_t<R>* __restrict__ Gp,
+                                                  const cplx_t<R>* __restrict__ Gn,
+                                                  cplx_t<R>* __restrict__ Pi, int64_t n, R scale) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    Pi[i] = cscale(cmulc(Gp[i], Gn[i]), scale);
+}
+template <typename R>
+__global__ void __launch_bounds__(256) k_sigma_gamma(const cplx_t<R>* Gp, const cplx_t<R>* Gm,
+                                                     const cplx_t<R>* __restrict__ WR,
+                                                     cplx_t<R>* Sp, cplx_t<R>* Sm, int64_t n,
+                                                     R scale) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const cplx_t<R> w = cscale(WR[i], scale);
+    Sp[i] = cmul(Gp[i], w);
+    if (Gm) Sm[i] = cmul(Gm[i], w);
+  }
+}
+template <typename R>
+__global__ void __launch_bounds__(256) k_scale_batch(cplx_t<R>* buf, int64_t ncol, int64_t nbatch,
+                                                     int64_t bstride, R scale) {
+  const int64_t n = ncol * nbatch;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    cplx_t<R>* p = buf + (i / ncol) * bstride + i % ncol;
+    *p = cscale(*p, scale);
+  }
+}
+
 template <typename R>
 void launch_pi_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gn, cplx_t<R>* Pi, int64_t ncol,
                      KGrid g, double sp, cudaStream_t s) {
   check_grid(g);
   const int nk = g.nk();
   const R scale = (R)(sp / ((double)nk * (double)nk));
+  if (nk == 1) {
+    k_pi_gamma<R><<<grid_for(ncol, 256), 256, 0, s>>>(Gp, Gn, Pi, ncol, scale);
+    CQ_LAUNCHED();
+    return;
+  }
   const int tile = pick_tile<R>(nk);
   const size_t smem = (size_t)2 * nk * tile * sizeof(cplx_t<R>);
   const int64_t ntiles = (ncol + tile - 1) / tile;
@@ -479,6 +518,11 @@ void launch_sigma_fused(const cplx_t<R>* Gp, const cplx_t<R>* Gm, const cplx_t<R
   const int nk = g.nk();
   // Sigma = f_kR [ -(f_Rk G) * W_R ]; f_Rk carries 1/nk
   const R scale = (R)(-1.0 / (double)nk);
+  if (nk == 1) {
+    k_sigma_gamma<R><<<grid_for(ncol, 256), 256, 0, s>>>(Gp, Gm, WR, Sp, Sm, ncol, scale);
+    CQ_LAUNCHED();
+    return;
+  }
   const int tile = pick_tile<R>(nk);
   const size_t smem = (size_t)2 * nk * tile * sizeof(cplx_t<R>);
   const int64_t ntiles = (ncol + tile - 1) / tile;
@@ -500,6 +544,14 @@ void launch_dft_plain(cplx_t<R>* buf, int64_t ncol, KGrid g, int sign, double sc
                       int64_t nbatch, int64_t bstride, cudaStream_t s) {
   check_grid(g);
   const int nk = g.nk();
+  if (nk == 1) {  // a length-1 DFT: only the scale
+    if (scale != 1.0) {
+      k_scale_batch<R><<<grid_for(ncol * nbatch, 256), 256, 0, s>>>(buf, ncol, nbatch, bstride,
+                                                                     (R)scale);
+      CQ_LAUNCHED();
+    }
+    return;
+  }
   const int tile = pick_tile<R>(nk);
   const size_t smem = (size_t)nk * tile * sizeof(cplx_t<R>);
   const int64_t ntiles = (ncol + tile - 1) / tile * nbatch;
