@@ -408,10 +408,20 @@ void launch_chol_tiled(const std::vector<CholProblem>& probs, DevBuf<unsigned ch
     R.count[R.nrun] = 1;
     ++R.nrun;
   }
+  // largest problems first within every launch (the work items are decoded run by run)
+  std::vector<int> ord(R.nrun);
+  for (int r = 0; r < R.nrun; ++r) ord[r] = r;
+  std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return R.n[x] > R.n[y]; });
+  TiledRuns S = R;
+  for (int r = 0; r < R.nrun; ++r) {
+    S.n[r] = R.n[ord[r]];
+    S.first[r] = R.first[ord[r]];
+    S.count[r] = R.count[ord[r]];
+  }
   table.ensure(np * sizeof(CholProblem));
   CQ_CHECK_CUDA(cudaMemcpyAsync(table.p, probs.data(), np * sizeof(CholProblem),
                                 cudaMemcpyHostToDevice, s));
-  run_tiled((const CholProblem*)table.p, R, np, logdet, trace, info, s);
+  run_tiled((const CholProblem*)table.p, S, np, logdet, trace, info, s);
 }
 
 void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsigned char>& table,

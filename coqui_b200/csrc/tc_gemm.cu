@@ -17,6 +17,7 @@
 // shared-memory transpose into coalesced rows; warp 8 allocates TMEM and one of its lanes
 // issues the MMAs.  Known triangular structure of A or B trims each tile's K range.  Waits
 // are bounded by a 2 s global-timer budget that sets an error flag instead of hanging.
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstdlib>
@@ -984,10 +985,15 @@ void tc_cgemm_grouped(const std::vector<TcGroup>& groups, DevBuf<unsigned char>&
     CQ_REQUIRE(!(g.st.a_ident && g.a_split) && !(g.st.b_ident && g.b_split), COQUI_B200_EINVAL,
                "tc_cgemm_grouped: identity shift needs a complex64 operand");
   }
-  if (a64 && b64) grouped_dispatch<true, true>(groups, table, s);
-  else if (a64) grouped_dispatch<true, false>(groups, table, s);
-  else if (b64) grouped_dispatch<false, true>(groups, table, s);
-  else grouped_dispatch<false, false>(groups, table, s);
+  // longest tiles first: CTAs start in tile order, so the groups with the longest K (the
+  // largest problems) must not be left for the tail of the launch
+  std::vector<TcGroup> order(groups);
+  std::stable_sort(order.begin(), order.end(),
+                   [](const TcGroup& x, const TcGroup& y) { return x.K > y.K; });
+  if (a64 && b64) grouped_dispatch<true, true>(order, table, s);
+  else if (a64) grouped_dispatch<true, false>(order, table, s);
+  else if (b64) grouped_dispatch<false, true>(order, table, s);
+  else grouped_dispatch<false, false>(order, table, s);
 }
 
 void tc_set_autotune(int on) { g_autotune.store(on ? 1 : 0); }
