@@ -96,6 +96,8 @@ struct coqui_b200_ctx {
   DevBuf<double2> dtrace;
   // CUDA graph of the resident-G GW iteration (captured on the first of consecutive calls)
   bool capturing = false;
+  // the Dyson step leaves its per-problem status on the device (checked after the iteration)
+  bool defer_dyson_check = false;
   cudaGraphExec_t gexec = nullptr;
   int64_t calls = 0, graph_call = -2, graph_launches = 0;
 
@@ -1020,7 +1022,7 @@ void dyson_all(Ctx* c, bool want_w, bool want_e, std::vector<double>* logdet,
   a.info = c->dinfo.p;
   a.logdet = c->dlogdet.p;
   a.trace = c->dtrace.p;
-  a.defer_check = c->capturing;
+  a.defer_check = c->capturing || c->defer_dyson_check;
   std::vector<double> ld;
   std::vector<double2> t;
   cq::dyson_run(a, c->blas, c->sol, c->dyn, c->st, want_e ? &ld : nullptr, want_e ? &t : nullptr);
@@ -1175,6 +1177,17 @@ void sigma_device(Ctx* c, double* host_out) {
 
 
 // One GW iteration of the resident G as a CUDA graph (update_w + Sigma, no host transfers).
+// status of every (iW, q) factorisation of the last Dyson step, left on the device
+void check_dyson_status(Ctx* c) {
+  const int64_t nprob = c->nwh * c->nq;
+  std::vector<int> info(nprob);
+  CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), c->dinfo.p, nprob * sizeof(int), cudaMemcpyDeviceToHost,
+                                c->st));
+  CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+  for (int64_t i = 0; i < nprob; ++i)
+    CQ_REQUIRE(info[i] == 0, COQUI_B200_ENOTHPD, "I - L^H Pi L is not positive definite");
+}
+
 void gw_iteration_graph(Ctx* c) {
   c->begin_timing();
   const bool replay = c->gexec && c->graph_call == c->calls - 1;
@@ -1209,14 +1222,7 @@ void gw_iteration_graph(Ctx* c) {
   CQ_CHECK_CUDA(cudaGraphLaunch(c->gexec, c->st));
   c->mark("GW_ITERATION_GRAPH");
   c->graph_call = c->calls;
-  // factorisation status of every (iW, q) problem of this iteration
-  const int64_t nprob = c->nwh * c->nq;
-  std::vector<int> info(nprob);
-  CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), c->dinfo.p, nprob * sizeof(int), cudaMemcpyDeviceToHost,
-                                c->st));
-  CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
-  for (int64_t i = 0; i < nprob; ++i)
-    CQ_REQUIRE(info[i] == 0, COQUI_B200_ENOTHPD, "I - L^H Pi L is not positive definite");
+  check_dyson_status(c);  // factorisation status of every (iW, q) problem of this iteration
   c->end_timing();
 }
 }  // namespace
@@ -1286,12 +1292,23 @@ int coqui_b200_gw_iteration(coqui_b200_ctx* c, const double* G_tskij, double* Si
     c->begin_timing();
     upload_G(c, G_tskij);
     c->mark("h2d_G");
-    update_w_device(c);
-    if (eps_inv_head) {
-      eps_head(c, eps_inv_head);
-      c->mark("EPS_INV_HEAD");
+    // mixed form: no host round trip between the Dyson step and the self-energy; the
+    // factorisation status is checked once the iteration has run
+    const bool defer = (c->mode == COQUI_B200_MIXED);
+    c->defer_dyson_check = defer;
+    try {
+      update_w_device(c);
+      if (eps_inv_head) {
+        eps_head(c, eps_inv_head);
+        c->mark("EPS_INV_HEAD");
+      }
+      sigma_device(c, Sigma_tskij);
+    } catch (...) {
+      c->defer_dyson_check = false;
+      throw;
     }
-    sigma_device(c, Sigma_tskij);
+    c->defer_dyson_check = false;
+    if (defer) check_dyson_status(c);
     c->end_timing();
   });
 }
