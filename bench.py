@@ -274,12 +274,13 @@ def run_ours(args, rank, world, local):
     Gh[...] = G
     Sh = torch.empty(G.shape, dtype=torch.complex128, pin_memory=True).numpy()
     ctx.gw_iteration(Gh, sigma_out=Sh)
-    e2e, e2e_w = [], []
+    e2e, e2e_wall = [], []
     with Clocks(local) as clk_e2e:
         for _ in range(args.steps):
-            ctx.gw_iteration(Gh, sigma_out=Sh)
+            t0 = time.perf_counter()
+            ctx.gw_iteration(Gh, sigma_out=Sh)  # returns with Sigma in Sh
+            e2e_wall.append((time.perf_counter() - t0) * 1e3)
             e2e.append(total_ms(ctx))
-            e2e_w.append(dict(ctx.timings()).get("EVALUATE_W", 0.0))
     t_e2e = float(np.mean(e2e))
     e2e_phases = dict(ctx.timings())
 
@@ -404,7 +405,8 @@ def run_ours(args, rank, world, local):
         "phases_ms": phases,
         "steps_ms": [round(t, 3) for t in times],
         "e2e_steps_ms": [round(t, 3) for t in e2e],
-        "e2e_evaluate_w_ms": [round(t, 3) for t in e2e_w],
+        # wall clock of each public-API call (host G in, Sigma out, returns after the copy)
+        "e2e_wall_steps_ms": [round(t, 3) for t in e2e_wall],
         "e2e_clocks": clk_e2e.summary(),
         "e2e_phases_ms": e2e_phases,
         "rpa_phases_ms": rpa_phases,

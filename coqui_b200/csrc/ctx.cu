@@ -96,6 +96,9 @@ struct coqui_b200_ctx {
   DevBuf<double2> dtrace;
   // CUDA graph of the resident-G GW iteration (captured on the first of consecutive calls)
   bool capturing = false;
+  // host buffers baked into the captured graph (nullptr: resident G / Sigma left on the device)
+  const double* graph_g = nullptr;
+  double* graph_s = nullptr;
   // the Dyson step leaves its per-problem status on the device (checked after the iteration)
   bool defer_dyson_check = false;
   cudaGraphExec_t gexec = nullptr;
@@ -1023,6 +1026,7 @@ void dyson_all(Ctx* c, bool want_w, bool want_e, std::vector<double>* logdet,
   a.logdet = c->dlogdet.p;
   a.trace = c->dtrace.p;
   a.defer_check = c->capturing || c->defer_dyson_check;
+  a.keep_scratch = c->capturing;
   std::vector<double> ld;
   std::vector<double2> t;
   cq::dyson_run(a, c->blas, c->sol, c->dyn, c->st, want_e ? &ld : nullptr, want_e ? &t : nullptr);
@@ -1188,9 +1192,13 @@ void check_dyson_status(Ctx* c) {
     CQ_REQUIRE(info[i] == 0, COQUI_B200_ENOTHPD, "I - L^H Pi L is not positive definite");
 }
 
-void gw_iteration_graph(Ctx* c) {
+// G_host / S_host: page-locked host buffers copied in / out inside the graph (chunked on the
+// copy stream as in the directly launched path), or nullptr for the resident G and a Sigma
+// left on the device.  The graph is replayed by the next call with the same buffers.
+void gw_iteration_graph(Ctx* c, const double* G_host, double* S_host) {
   c->begin_timing();
-  const bool replay = c->gexec && c->graph_call == c->calls - 1;
+  const bool replay = c->gexec && c->graph_call == c->calls - 1 && c->graph_g == G_host &&
+                      c->graph_s == S_host;
   if (!replay) {
     if (c->gexec) {
       cudaGraphExecDestroy(c->gexec);
@@ -1202,8 +1210,9 @@ void gw_iteration_graph(Ctx* c) {
     c->capturing = true;
     cudaGraph_t g = nullptr;
     try {
+      if (G_host) upload_G(c, G_host);
       update_w_device(c);
-      sigma_device(c, nullptr);
+      sigma_device(c, S_host);
     } catch (...) {
       c->capturing = false;
       if (cudaStreamEndCapture(c->st, &g) == cudaSuccess && g) cudaGraphDestroy(g);
@@ -1216,6 +1225,8 @@ void gw_iteration_graph(Ctx* c) {
     const cudaError_t e = cudaGraphInstantiate(&c->gexec, g, 0);
     cudaGraphDestroy(g);
     CQ_CHECK_CUDA(e);
+    c->graph_g = G_host;
+    c->graph_s = S_host;
   } else {
     cq::count_launch(c->graph_launches);  // the replay launches the captured kernels again
   }
@@ -1282,11 +1293,13 @@ int coqui_b200_gw_iteration(coqui_b200_ctx* c, const double* G_tskij, double* Si
                             double* eps_inv_head) {
   return guarded(c, [&] {
     require_ready(c, true, true, true);
-    // resident G, no host outputs: the device work of the iteration runs as one CUDA graph,
-    // captured on the first of a run of such calls and replayed by the following ones
-    if (!G_tskij && !Sigma_tskij && !eps_inv_head && c->mode == COQUI_B200_MIXED &&
-        !c->prof.on && c->g_resident) {
-      gw_iteration_graph(c);
+    // resident G or page-locked host buffers, no eps head: the iteration (the copies included)
+    // runs as one CUDA graph, captured on the first of a run of such calls with the same
+    // buffers and replayed by the following ones
+    // page-locked host buffers: the copies join the graph
+    if (!eps_inv_head && c->mode == COQUI_B200_MIXED && !c->prof.on &&
+        (G_tskij ? is_pinned(G_tskij) : c->g_resident) && (!Sigma_tskij || is_pinned(Sigma_tskij))) {
+      gw_iteration_graph(c, G_tskij, Sigma_tskij);
       return;
     }
     c->begin_timing();

@@ -159,6 +159,9 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
     size_t fr = 0, tot = 0;
     CQ_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
     budget = std::max(scratch.n, (size_t)(0.6 * (double)(fr + scratch.n)));
+    // while a graph is captured the scratch keeps its size (no device allocation or free
+    // inside the capture) when it holds at least one problem
+    if (a.keep_scratch && scratch.n >= per + 1024) budget = scratch.n - 1024;
   }
   const int64_t nprob = nw * nq;
   const int64_t nbq = a.mixed ? std::max<int64_t>(1, std::min<int64_t>(nprob, (int64_t)(budget / per)))

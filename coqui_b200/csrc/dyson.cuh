@@ -41,6 +41,7 @@ struct DysonArgs {
   const float2* LHc = nullptr;
   bool want_w = true, want_e = false, mixed = true;
   unsigned char* PW = nullptr;  // (nw, nq, Np, Np): Pi(iW) in, W(iW) out (if want_w)
+  bool keep_scratch = false;    // use the scratch as it is (a CUDA graph is being captured)
   Prof* prof = nullptr;
   // mixed form: per-problem results on the device (nw * nq entries, n * nq + q); with
   // defer_check the host neither waits nor checks (the caller reads `info` later, e.g. after
