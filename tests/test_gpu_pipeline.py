@@ -127,3 +127,25 @@ def test_graph_capture_of_tiled_factorisation_and_tensor_core_inverse():
     assert [name for name, _ in c.timings()] == ["GW_ITERATION_GRAPH"]
     assert np.array_equal(c.eval_sigma(None), S_direct)
     c.close()
+
+
+def test_pinned_host_buffer_iteration_runs_as_a_graph(case):
+    """gw_iteration with page-locked G in and Sigma out runs as one graph with its copies:
+    replayed for the same buffers, captured again for new ones, always the directly launched
+    result (pageable buffers take the direct path)."""
+    import torch
+    c = make_ctx(case, capi.MIXED)
+    S_direct, _ = c.gw_iteration(np.ascontiguousarray(case["G"]))  # pageable: direct path
+    assert "GW_ITERATION_GRAPH" not in [name for name, _ in c.timings()]
+    outs = []
+    for _ in range(2):
+        G_p = torch.from_numpy(np.ascontiguousarray(case["G"])).pin_memory()
+        S_p = torch.zeros(G_p.shape, dtype=torch.complex128).pin_memory()
+        for _ in range(2):  # capture + launch, then replay
+            S_p.zero_()
+            c.gw_iteration(G_p.numpy(), sigma_out=S_p.numpy())
+            assert [name for name, _ in c.timings()] == ["GW_ITERATION_GRAPH"]
+            outs.append(S_p.numpy().copy())
+    for S in outs:
+        assert np.array_equal(S, S_direct)
+    c.close()
