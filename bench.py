@@ -71,8 +71,35 @@ class Clocks:
 
     def __init__(self, device):
         self.device, self.rows, self.stop = device, [], threading.Event()
+        self.nvml = None
+        try:  # in-process NVML reads: one sample costs microseconds, not a process start
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            p = torch.cuda.get_device_properties(device)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            self.nvml = (pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus))
+        except Exception:
+            self.nvml = None
+
+    def _nvml_row(self):
+        nv, h = self.nvml
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        flags = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        return ([str(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                 str(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
+                 str(nv.nvmlDeviceGetPowerUsage(h) / 1000.0)]
+                + ["Active" if bits & f else "Not Active" for f in flags])
 
     def _run(self):
+        while self.nvml is not None and not self.stop.is_set():
+            try:
+                self.rows.append(self._nvml_row())
+            except Exception:
+                self.nvml = None
+                break
+            self.stop.wait(0.01)
         while not self.stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
