@@ -29,6 +29,7 @@ SYMBOLS = [
     "coqui_b200_kernel_launches", "coqui_b200_gw_iteration", "coqui_b200_set_profiling",
     "coqui_b200_kernel_stats", "coqui_b200_primary_to_aux_noalloc",
     "coqui_b200_set_ir_fermi", "coqui_b200_set_mean_field", "coqui_b200_set_iter_alg",
+    "coqui_b200_hf_evaluate", "coqui_b200_scgw_set_hf",
     "coqui_b200_scgw_iteration", "coqui_b200_get_scgw_state", "coqui_b200_dyson_g",
     "coqui_b200_gm_energy", "coqui_b200_mlp_create", "coqui_b200_mlp_destroy",
     "coqui_b200_mlp_last_error", "coqui_b200_mlp_num_params", "coqui_b200_mlp_set_params",
@@ -95,6 +96,8 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_set_ir_fermi.argtypes = [P, P, P, P, I64, D]
     lib.coqui_b200_set_mean_field.argtypes = [P, P, P, P, D]
     lib.coqui_b200_set_iter_alg.argtypes = [P, ctypes.c_int, D, I64, I64]
+    lib.coqui_b200_hf_evaluate.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, D, P]
+    lib.coqui_b200_scgw_set_hf.argtypes = [P, ctypes.c_int, ctypes.c_int, D]
     lib.coqui_b200_scgw_iteration.argtypes = [P, P, I64, P]
     lib.coqui_b200_get_scgw_state.argtypes = [P, P, P, P]
     lib.coqui_b200_dyson_g.argtypes = [P, P, P, P]
@@ -152,6 +155,9 @@ def _c128(a, shape, name):
     if tuple(a.shape) != tuple(shape):
         raise ValueError(f"{name} has shape {a.shape}, expected {tuple(shape)}")
     return a
+
+
+_DIV = {"ignore_g0": 0, "gygi": 1}
 
 
 class Context:
@@ -214,6 +220,24 @@ class Context:
         a = {"damping": 0, "diis": 1}[alg]
         self._check(self.lib.coqui_b200_set_iter_alg(self.h, a, float(mixing), int(max_subsp),
                                                      int(diis_start)))
+
+    def hf_evaluate(self, Dm, S=None, hartree=True, exchange=True, div="ignore_g0",
+                    madelung=0.0):
+        """THC Hartree-Fock F = J + K of the density matrix Dm (1, nk, nb, nb); div "gygi"
+        adds -madelung S Dm S to the exchange."""
+        sh = (1, self.nk, self.nb, self.nb)
+        Dm = _c128(Dm, sh, "Dm")
+        S = None if S is None else _c128(S, sh, "S")
+        F = np.empty(sh, np.complex128)
+        self._check(self.lib.coqui_b200_hf_evaluate(
+            self.h, _ptr(Dm, "Dm"), _ptr(S, "S"), int(bool(hartree)), int(bool(exchange)),
+            _DIV[div], float(madelung), _ptr(F, "F")))
+        return F
+
+    def set_hf(self, enable=True, div="ignore_g0", madelung=0.0):
+        """Re-evaluate F = J + K from the density matrix at the start of every scGW iteration."""
+        self._check(self.lib.coqui_b200_scgw_set_hf(self.h, int(bool(enable)), _DIV[div],
+                                                    float(madelung)))
 
     def scgw_iteration(self, it, G=None):
         """One self-consistent GW iteration; G (iteration 1) uploads the starting G."""

@@ -119,6 +119,14 @@ struct coqui_b200_ctx {
   DevBuf<int> ginfo;
   DevBuf<double> red;
   DevBuf<double2> trc;
+  // THC Hartree-Fock: bare V(q) transformed to R in storage precision (built on first use),
+  // scratch, and whether the loop re-evaluates F = J + K from the density matrix
+  DevBuf<double2> VR;
+  bool vr_valid = false;
+  DevBuf<double2> hfd, hfs, hff, hfv, hft, hfp;
+  bool hf_on = false;
+  int hf_div = 0;
+  double hf_madelung = 0;
   int iter_alg = 0;                        // 0 damping, 1 commutator DIIS
   double mixing = 0.7;
   int64_t max_subsp = 5, diis_start = 5;
@@ -244,21 +252,40 @@ void require_ready(Ctx* c, bool thc, bool ir, bool k) {
 
 // ntau consecutive G slices (ntau, nk, nb, nb) complex128 on the device -> out (ntau, nk,
 // Np, Np) in storage precision.  The tensor-core form batches all ntau * nk problems.
+void p2a_fp64(Ctx* c, const double2* Gk, double2* out, int64_t ntau) {
+  const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
+  c->Tproj.ensure((size_t)nk * Np * nb);
+  for (int64_t t = 0; t < ntau; ++t) {
+    const double2* G = Gk + t * nk * nb * nb;
+    double2* O = out + t * nk * Np * Np;
+    // T = X G  (Np x nb)
+    zgemm_rm(c, 'N', 'N', Np, nb, nb, make_double2(1, 0), c->X.p, nb, Np * nb, G, nb, nb * nb,
+             make_double2(0, 0), c->Tproj.p, nb, Np * nb, nk);
+    // O = T X^H  (Np x Np)
+    zgemm_rm(c, 'N', 'C', Np, Np, nb, make_double2(1, 0), c->Tproj.p, nb, Np * nb, c->X.p, nb,
+             Np * nb, make_double2(0, 0), O, Np, Np * Np, nk);
+  }
+}
+void a2p_fp64(Ctx* c, const double2* Sk, double2* out, int64_t ntau) {
+  const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
+  c->Tproj.ensure((size_t)nk * Np * nb);
+  for (int64_t t = 0; t < ntau; ++t) {
+    const double2* S = Sk + t * nk * Np * Np;
+    double2* O = out + t * nk * nb * nb;
+    // T = X^H S  (nb x Np)
+    zgemm_rm(c, 'C', 'N', nb, Np, Np, make_double2(1, 0), c->X.p, nb, Np * nb, S, Np, Np * Np,
+             make_double2(0, 0), c->Tproj.p, Np, Np * nb, nk);
+    // O = T X  (nb x nb)
+    zgemm_rm(c, 'N', 'N', nb, nb, Np, make_double2(1, 0), c->Tproj.p, Np, Np * nb, c->X.p, nb,
+             Np * nb, make_double2(0, 0), O, nb, nb * nb, nk);
+  }
+}
+
 void project_p2a(Ctx* c, const double2* Gk, void* out, int64_t ntau = 1) {
   cq::Prof::Scope sc(&c->prof, "proj_p2a");
   const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
   if (c->mode == COQUI_B200_FP64) {
-    c->Tproj.ensure((size_t)nk * Np * nb);
-    for (int64_t t = 0; t < ntau; ++t) {
-      const double2* G = Gk + t * nk * nb * nb;
-      double2* O = (double2*)out + t * nk * Np * Np;
-      // T = X G  (Np x nb)
-      zgemm_rm(c, 'N', 'N', Np, nb, nb, make_double2(1, 0), c->X.p, nb, Np * nb, G, nb, nb * nb,
-               make_double2(0, 0), c->Tproj.p, nb, Np * nb, nk);
-      // O = T X^H  (Np x Np)
-      zgemm_rm(c, 'N', 'C', Np, Np, nb, make_double2(1, 0), c->Tproj.p, nb, Np * nb, c->X.p, nb,
-               Np * nb, make_double2(0, 0), O, Np, Np * Np, nk);
-    }
+    p2a_fp64(c, Gk, (double2*)out, ntau);
   } else {
     cq::tc_project_p2a(c->Xtc, Gk, (float2*)out, nk, Np, nb, ntau * nk, c->st);
   }
@@ -269,17 +296,7 @@ void project_a2p(Ctx* c, const void* Sk, double2* out, int64_t ntau = 1) {
   cq::Prof::Scope sc(&c->prof, "proj_a2p");
   const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
   if (c->mode == COQUI_B200_FP64) {
-    c->Tproj.ensure((size_t)nk * Np * nb);
-    for (int64_t t = 0; t < ntau; ++t) {
-      const double2* S = (const double2*)Sk + t * nk * Np * Np;
-      double2* O = out + t * nk * nb * nb;
-      // T = X^H S  (nb x Np)
-      zgemm_rm(c, 'C', 'N', nb, Np, Np, make_double2(1, 0), c->X.p, nb, Np * nb, S, Np, Np * Np,
-               make_double2(0, 0), c->Tproj.p, Np, Np * nb, nk);
-      // O = T X  (nb x nb)
-      zgemm_rm(c, 'N', 'N', nb, nb, Np, make_double2(1, 0), c->Tproj.p, Np, Np * nb, c->X.p, nb,
-               Np * nb, make_double2(0, 0), O, nb, nb * nb, nk);
-    }
+    a2p_fp64(c, (const double2*)Sk, out, ntau);
   } else {
     cq::tc_project_a2p(c->Xtc, (const float2*)Sk, out, nk, Np, nb, ntau * nk, c->st);
   }
@@ -469,6 +486,18 @@ void require_scgw(Ctx* c) {
   CQ_REQUIRE(c->have_mf, COQUI_B200_EINVAL, "set_mean_field not called");
 }
 
+// c->Dm <- -G(beta^-) of the resident G (IAFT.icc:226-238, simple_dyson.cpp:119-121), made
+// Hermitian (scf_driver.cpp:140-143)
+void dm_from_g(Ctx* c) {
+  const int64_t ncol = c->nk * c->nb * c->nb;
+  c->Dm.ensure(ncol);
+  c->trc.ensure(c->nt);
+  upload(c, c->trc.p, c->T_beta.data(), c->nt * sizeof(double2));
+  zgemm_rm(c, 'N', 'N', 1, ncol, c->nt, make_double2(-1, 0), c->trc.p, c->nt, 0, c->G.p, ncol, 0,
+           make_double2(0, 0), c->Dm.p, ncol, 0, 1);
+  cq::hermitize_c128(c->Dm.p, c->nb, c->nk, c->st);
+}
+
 // simple_dyson.cpp:66-123 with the hermitization of scf_driver.cpp:140-143: c->G <- G(tau)
 // from Sigma(tau) (device, (nt, nk, nb, nb)), c->Dm <- -G(beta^-).
 void dyson_g_device(Ctx* c, const double2* Sig) {
@@ -484,12 +513,7 @@ void dyson_g_device(Ctx* c, const double2* Sig) {
                          nw, nk, nb, c->st);
   cq::invert_batched(c->Xw.p, nb, nw * nk, c->ginfo.p, c->blas, c->st);
   w_to_tau_ff(c, c->Xw.p, c->G.p, ncol);
-  // Dm = -sum_t T_beta(t) G(t)  (IAFT.icc:226-238, simple_dyson.cpp:119-121)
-  c->trc.ensure(c->nt);
-  upload(c, c->trc.p, c->T_beta.data(), c->nt * sizeof(double2));
-  zgemm_rm(c, 'N', 'N', 1, ncol, c->nt, make_double2(-1, 0), c->trc.p, c->nt, 0, c->G.p, ncol, 0,
-           make_double2(0, 0), c->Dm.p, ncol, 0, 1);
-  cq::hermitize_c128(c->Dm.p, nb, nk, c->st);
+  dm_from_g(c);
   cq::hermitize_c128(c->G.p, nb, c->nt * nk, c->st);
   std::vector<int> info(nw * nk);
   CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), c->ginfo.p, info.size() * sizeof(int),
@@ -891,6 +915,7 @@ int coqui_b200_set_kmesh(coqui_b200_ctx* c, const double* kpts, const double* la
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->have_k = true;
     c->gcache_valid = false;
+    c->vr_valid = false;
   });
 }
 
@@ -921,6 +946,7 @@ int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_
     c->have_thc = true;
     c->gcache_valid = false;
     c->w_valid = false;
+    c->vr_valid = false;
   });
 }
 
@@ -1179,6 +1205,65 @@ void sigma_device(Ctx* c, double* host_out) {
   c->w_in_R = false;
 }
 
+
+// ---------------------------------------------------------------------------------------
+// THC Hartree-Fock: hf_t::evaluate for q-independent THC without symmetry (thc_hf.cpp:21-60
+// -> thc_hf.icc:17-272, npol = 1) and HF_K_correction (hf_t.cpp:45-84).
+// ---------------------------------------------------------------------------------------
+
+// V(R) = f_Rq V(q) (thc_hf.icc:143-152) in FP64, built once per set_thc
+void ensure_v_R(Ctx* c) {
+  if (c->vr_valid) return;
+  const int64_t nk = c->nk, ncol = c->Np * c->Np;
+  c->VR.ensure((size_t)nk * ncol);
+  CQ_CHECK_CUDA(cudaMemcpyAsync(c->VR.p, c->V.p, (size_t)nk * ncol * sizeof(double2),
+                                cudaMemcpyDeviceToDevice, c->st));
+  cq::launch_dft_plain<double>(c->VR.p, ncol, c->g, -1, 1.0 / (double)nk, 1, nk * ncol, c->st);
+  c->vr_valid = true;
+}
+
+// F (device, (nk, nb, nb)) <- J + K [- madelung S Dm S] of the density matrix Dm (device), in
+// FP64 in both precision modes (one slice of the self-energy's work; F enters every G(i w)).
+// K_PQ(R) = -D_PQ(R) V_PQ(R) takes the self-energy's route (projection, fused k -> R, product,
+// R -> k, back-projection) with D(k) = X Dm X^H in place of G(tau) and V(R) in place of W(R).
+// J: rho_Q = (2/nk) sum_k (X Dm X^H)_QQ (the R = 0 diagonal of thc_hf.icc:184-190),
+// J = V(q=0) rho (:194-196), F += X^H diag(J) X.
+void hf_device(Ctx* c, const double2* Dm, const double2* S, bool hartree, bool exchange, int div,
+               double madelung, double2* F) {
+  cq::Prof::Scope sc(&c->prof, "hf");
+  const int64_t nk = c->nk, nb = c->nb, Np = c->Np, ncol = Np * Np;
+  const int64_t nF = nk * nb * nb;
+  if (exchange) {
+    ensure_v_R(c);
+    c->hfp.ensure((size_t)nk * ncol);
+    p2a_fp64(c, Dm, c->hfp.p, 1);
+    cq::launch_sigma_fused<double>(c->hfp.p, nullptr, c->VR.p, c->hfp.p, nullptr, ncol, c->g,
+                                   c->st);
+    a2p_fp64(c, c->hfp.p, F, 1);
+  } else {
+    CQ_CHECK_CUDA(cudaMemsetAsync(F, 0, nF * sizeof(double2), c->st));
+  }
+  if (hartree) {
+    c->Tproj.ensure((size_t)nk * Np * nb);
+    c->hfv.ensure(2 * Np);
+    const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
+    zgemm_rm(c, 'N', 'N', Np, nb, nb, one, c->X.p, nb, Np * nb, Dm, nb, nb * nb, zero,
+             c->Tproj.p, nb, Np * nb, nk);
+    cq::aux_diag(c->Tproj.p, c->X.p, c->hfv.p, nk, Np, nb, 2.0 / (double)nk, c->st);
+    zgemm_rm(c, 'N', 'N', Np, 1, Np, one, c->V.p, Np, 0, c->hfv.p, 1, 0, zero, c->hfv.p + Np, 1,
+             0, 1);
+    cq::scale_rows(c->X.p, c->hfv.p + Np, c->Tproj.p, nk, Np, nb, c->st);
+    zgemm_rm(c, 'C', 'N', nb, nb, Np, one, c->X.p, nb, Np * nb, c->Tproj.p, nb, Np * nb, one, F,
+             nb, nb * nb, nk);
+  }
+  if (exchange && div == 1) {
+    c->hft.ensure(nF);
+    zgemm_rm(c, 'N', 'N', nb, nb, nb, make_double2(1, 0), S, nb, nb * nb, Dm, nb, nb * nb,
+             make_double2(0, 0), c->hft.p, nb, nb * nb, nk);
+    zgemm_rm(c, 'N', 'N', nb, nb, nb, make_double2(-madelung, 0), c->hft.p, nb, nb * nb, S, nb,
+             nb * nb, make_double2(1, 0), F, nb, nb * nb, nk);
+  }
+}
 
 // One GW iteration of the resident G as a CUDA graph (update_w + Sigma, no host transfers).
 // status of every (iW, q) factorisation of the last Dyson step, left on the device
@@ -1506,6 +1591,45 @@ int coqui_b200_set_iter_alg(coqui_b200_ctx* c, int alg, double mixing, int64_t m
   });
 }
 
+int coqui_b200_hf_evaluate(coqui_b200_ctx* c, const double* Dm_skij, const double* S_skij,
+                           int hartree, int exchange, int div_treatment, double madelung,
+                           double* F_skij) {
+  return guarded(c, [&] {
+    require_ready(c, true, false, true);
+    CQ_REQUIRE(Dm_skij && F_skij, COQUI_B200_EINVAL, "null density or Fock matrix");
+    CQ_REQUIRE(div_treatment == 0 || div_treatment == 1, COQUI_B200_EINVAL,
+               "div_treatment must be 0 (ignore_g0) or 1 (gygi)");
+    const bool gygi = exchange && div_treatment == 1;
+    CQ_REQUIRE(!gygi || S_skij, COQUI_B200_EINVAL, "gygi needs the overlap matrix");
+    const int64_t n = c->nk * c->nb * c->nb;
+    c->begin_timing();
+    c->hfd.ensure(n);
+    c->hff.ensure(n);
+    upload(c, c->hfd.p, Dm_skij, n * sizeof(double2));
+    if (gygi) {
+      c->hfs.ensure(n);
+      upload(c, c->hfs.p, S_skij, n * sizeof(double2));
+    }
+    c->mark("h2d_Dm");
+    hf_device(c, c->hfd.p, gygi ? c->hfs.p : nullptr, hartree != 0, exchange != 0,
+              div_treatment, madelung, c->hff.p);
+    c->mark("HF");
+    download(c, F_skij, c->hff.p, n * sizeof(double2));
+    c->mark("d2h_F");
+    c->end_timing();
+  });
+}
+
+int coqui_b200_scgw_set_hf(coqui_b200_ctx* c, int enable, int div_treatment, double madelung) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(div_treatment == 0 || div_treatment == 1, COQUI_B200_EINVAL,
+               "div_treatment must be 0 (ignore_g0) or 1 (gygi)");
+    c->hf_on = enable != 0;
+    c->hf_div = div_treatment;
+    c->hf_madelung = madelung;
+  });
+}
+
 int coqui_b200_scgw_iteration(coqui_b200_ctx* c, const double* G_tskij, int64_t it, double* stats) {
   return guarded(c, [&] {
     require_scgw(c);
@@ -1515,11 +1639,19 @@ int coqui_b200_scgw_iteration(coqui_b200_ctx* c, const double* G_tskij, int64_t 
                "iteration > 1 without a previous iteration");
     c->begin_timing();
     upload_G(c, G_tskij);
+    // the DIIS copy and the density matrix below read all of G: a page-locked G that is
+    // still arriving in chunks on the copy stream must have landed first
+    for (int64_t i = 0; i < n_tau_chunks(c); ++i) wait_G_chunk(c, i);
     c->mark("h2d_G");
     if (c->iter_alg == 1) {  // the residual of this step is taken with the incoming G
       c->Gin.ensure(nS);
       CQ_CHECK_CUDA(cudaMemcpyAsync(c->Gin.p, c->G.p, nS * sizeof(double2),
                                     cudaMemcpyDeviceToDevice, c->st));
+    }
+    if (c->hf_on) {  // scf_driver.cpp:94-114: F = J + K of the current density matrix
+      if (it == 1) dm_from_g(c);
+      hf_device(c, c->Dm.p, c->Sov.p, true, true, c->hf_div, c->hf_madelung, c->F.p);
+      c->mark("HF");
     }
     update_w_device(c);
     sigma_device(c, nullptr);

@@ -251,7 +251,55 @@ __global__ void __launch_bounds__(256) k_dotc(const double2* __restrict__ a,
   }
 }
 
+// rho[Q] = scale sum_k sum_b T[k, Q, b] conj(X[k, Q, b]): one warp per Q, FP64
+__global__ void __launch_bounds__(256) k_aux_diag(const double2* __restrict__ T,
+                                                  const double2* __restrict__ X,
+                                                  double2* __restrict__ rho, int64_t nk,
+                                                  int64_t Np, int64_t nb, double scale) {
+  const int64_t Q = (int64_t)blockIdx.x * 8 + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (Q >= Np) return;
+  double sr = 0, si = 0;
+  for (int64_t k = 0; k < nk; ++k) {
+    const double2* t = T + (k * Np + Q) * nb;
+    const double2* x = X + (k * Np + Q) * nb;
+    for (int64_t b = lane; b < nb; b += 32) {
+      const double2 a = t[b], y = x[b];
+      sr += a.x * y.x + a.y * y.y;
+      si += a.y * y.x - a.x * y.y;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sr += __shfl_down_sync(0xffffffffu, sr, o);
+    si += __shfl_down_sync(0xffffffffu, si, o);
+  }
+  if (lane == 0) rho[Q] = make_double2(scale * sr, scale * si);
+}
+
+// Y[k, P, b] = d[P] X[k, P, b]
+__global__ void k_scale_rows(const double2* __restrict__ X, const double2* __restrict__ d,
+                             double2* __restrict__ Y, int64_t nk, int64_t Np, int64_t nb) {
+  const int64_t n = nk * Np * nb;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    Y[i] = cmul2(d[(i / nb) % Np], X[i]);
+}
+
 }  // namespace
+
+void aux_diag(const double2* T, const double2* X, double2* rho, int64_t nk, int64_t Np,
+              int64_t nb, double scale, cudaStream_t s) {
+  k_aux_diag<<<(unsigned)((Np + 7) / 8), 256, 0, s>>>(T, X, rho, nk, Np, nb, scale);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+void scale_rows(const double2* X, const double2* d, double2* Y, int64_t nk, int64_t Np,
+                int64_t nb, cudaStream_t s) {
+  k_scale_rows<<<grid_for(nk * Np * nb, 256), 256, 0, s>>>(X, d, Y, nk, Np, nb);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
 
 void hermitize_c128(double2* A, int64_t nb, int64_t nmat, cudaStream_t s) {
   const int64_t n = nb * nb * nmat;

@@ -46,6 +46,13 @@ std::complex<double> dotc(const double2* a, const double2* b, int64_t n, DevBuf<
 void extract_diag(const double2* A, double2* out, int64_t nb, int64_t nmat, cudaStream_t s);
 void add_diag(double2* A, const double2* d, int64_t nb, int64_t nmat, cudaStream_t s);
 
+// Hartree pieces of THC Hartree-Fock (FP64): rho[Q] = scale sum_k sum_b T[k,Q,b] conj(X[k,Q,b])
+// for T = X Dm per k (the diagonal of X Dm X^H summed over k), and Y[k,P,b] = d[P] X[k,P,b].
+void aux_diag(const double2* T, const double2* X, double2* rho, int64_t nk, int64_t Np,
+              int64_t nb, double scale, cudaStream_t s);
+void scale_rows(const double2* X, const double2* d, double2* Y, int64_t nk, int64_t Np,
+                int64_t nb, cudaStream_t s);
+
 // Eigen-decomposition of a small real symmetric matrix by cyclic Jacobi rotations (host):
 // A (n x n, row-major) -> ev (n), U (n x n, row-major, column k = eigenvector k).
 void sym_eigen(const std::vector<double>& A, int64_t n, std::vector<double>& ev,

@@ -10,6 +10,7 @@ CoQui tree):
 * :class:`scr_coulomb_t` has ``update_w``, ``eval_Pi_qdep``, ``tau_to_w``, ``w_to_tau``,
   ``dyson_W_in_place`` (``src/methods/scr_coulomb/scr_coulomb_t.h``).
 * :class:`gw_t` has ``evaluate`` and ``rpa_energy`` (``src/methods/GW/gw_t.h:55-75``).
+* :class:`hf_t` has the THC ``evaluate`` (``src/methods/HF/hf_t.h:52-56``).
 
 Every call runs on the GPU through :mod:`coqui_b200.capi`; the reference's fatal
 ``utils::check`` failures surface as :class:`coqui_b200.capi.CoquiB200Error`.
@@ -35,6 +36,7 @@ class THCData:
     lattv: np.ndarray  # (3, 3) rows = lattice vectors
     kp_grid: tuple
     chi_bar: Optional[np.ndarray] = None  # (nq, Np) basis_bar_head
+    madelung: float = 0.0  # MF::madelung(), used by the gygi exchange correction
 
     @property
     def Np(self):
@@ -77,6 +79,20 @@ def context_for(thc: THCData, ft: IAFT, mode: int = capi.MIXED, device: int = 0)
         ctx.set_kmesh(thc.kpts, thc.lattv, thc.chi_bar)
         ctx.set_thc(thc.X, thc.V)
         _ctx_cache[key] = ctx
+    return ctx
+
+
+def hf_context_for(thc: THCData, mode: int = capi.MIXED, device: int = 0) -> capi.Context:
+    """A context holding thc: any context of the same (thc, mode, device), else one without
+    imaginary-time grids (Hartree-Fock needs none)."""
+    for (t, _, m, d), ctx in _ctx_cache.items():
+        if t == id(thc) and m == mode and d == device:
+            return ctx
+    key = (id(thc), None, mode, device)
+    ctx = capi.Context(thc.nkpts, thc.nbnd, thc.Np, 2, 1, thc.kp_grid, mode=mode, device=device)
+    ctx.set_kmesh(thc.kpts, thc.lattv, thc.chi_bar)
+    ctx.set_thc(thc.X, thc.V)
+    _ctx_cache[key] = ctx
     return ctx
 
 
@@ -147,3 +163,27 @@ class gw_t:
     def rpa_energy(self, G_tskij, thc: THCData) -> float:
         """thc_rpa.cpp:22 / thc_rpa.icc:21-181."""
         return context_for(thc, self.ft, self.mode).rpa_energy(G_tskij)
+
+
+class hf_t:
+    """THC Hartree-Fock (hf_t.h:40-60; thc_hf.cpp:21-60 -> thc_hf.icc:17-272 for q-independent
+    THC without symmetry; HF_K_correction hf_t.cpp:45-84).
+
+    As the reference constructor (hf_t.cpp:31-37), a treatment other than "ignore_g0" or
+    "gygi" becomes "gygi"."""
+
+    def __init__(self, div_treatment: str = "gygi", mode: int = capi.MIXED):
+        if div_treatment not in DIV_TREATMENTS:
+            raise ValueError(f"unknown div_treatment {div_treatment}")
+        self.div_treatment = div_treatment if div_treatment in ("ignore_g0", "gygi") else "gygi"
+        self.mode = mode
+
+    def evaluate(self, sF_skij, Dm_skij, thc: THCData, S_skij, hartree: bool = True,
+                 exchange: bool = True):
+        """Overwrites sF_skij (ns, nk, nb, nb) with J + K of the density matrix Dm_skij; the
+        gygi treatment adds -madelung S Dm S (thc.madelung) to the exchange."""
+        ctx = hf_context_for(thc, self.mode)
+        F = ctx.hf_evaluate(Dm_skij, S_skij, hartree, exchange, self.div_treatment,
+                            thc.madelung)
+        sF_skij[...] = F.reshape(np.shape(sF_skij))
+        return sF_skij

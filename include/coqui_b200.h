@@ -123,8 +123,19 @@ COQUI_B200_API int coqui_b200_rpa_energy(coqui_b200_ctx* ctx, const double* G_ts
 COQUI_B200_API int coqui_b200_gw_iteration(coqui_b200_ctx* ctx, const double* G_tskij,
                                            double* Sigma_tskij, double* eps_inv_head);
 
-/* ---- self-consistent GW loop (scf_loop, src/methods/SCF/scf_driver.cpp:90-173, for GW with
-   hf = nullptr and a constant chemical potential) ---- */
+/* ---- THC Hartree-Fock (hf_t::evaluate, src/methods/HF/thc_hf.cpp:21-60 ->
+   thc_hf.icc:17-272 for q-independent THC without symmetry; hf_t.cpp:45-84) ---- */
+
+/* F_skij (ns, nk, nb, nb) complex128, overwritten, = J (hartree != 0) + K (exchange != 0) of the
+   density matrix Dm_skij (ns, nk, nb, nb) with the context's X and V.  div_treatment 0 =
+   ignore_g0, 1 = gygi: K also gets -madelung S Dm S (S_skij needed then; may be NULL
+   otherwise).  Needs set_thc and set_kmesh. */
+COQUI_B200_API int coqui_b200_hf_evaluate(coqui_b200_ctx* ctx, const double* Dm_skij,
+                                          const double* S_skij, int hartree, int exchange,
+                                          int div_treatment, double madelung, double* F_skij);
+
+/* ---- self-consistent GW loop (scf_loop, src/methods/SCF/scf_driver.cpp:90-173, for GW with a
+   constant chemical potential; hf = nullptr unless coqui_b200_scgw_set_hf enables it) ---- */
 
 /* Fermionic IR tables, rescaled by beta as in ir_driver.hpp:68-73: Twt_ff (nw_f, nt_f) and
    Ttw_ff (nt_f, nw_f) complex128, wn_mesh_f (nw_f) Matsubara integers (omega_n = pi wn / beta,
@@ -133,8 +144,9 @@ COQUI_B200_API int coqui_b200_set_ir_fermi(coqui_b200_ctx* ctx, const double* Tw
                                            const double* Ttw_ff, const int64_t* wn_mesh_f,
                                            int64_t nw_f, double beta);
 
-/* Mean field of the loop: H0_skij, S_skij, F_skij (ns, nk, nb, nb) complex128 (F without H0,
-   kept fixed as with hf = nullptr) and the chemical potential mu. */
+/* Mean field of the loop: H0_skij, S_skij, F_skij (ns, nk, nb, nb) complex128 (F without H0;
+   kept fixed as with hf = nullptr unless coqui_b200_scgw_set_hf enables it) and the chemical
+   potential mu. */
 COQUI_B200_API int coqui_b200_set_mean_field(coqui_b200_ctx* ctx, const double* H0_skij,
                                              const double* S_skij, const double* F_skij, double mu);
 
@@ -144,7 +156,13 @@ COQUI_B200_API int coqui_b200_set_mean_field(coqui_b200_ctx* ctx, const double* 
 COQUI_B200_API int coqui_b200_set_iter_alg(coqui_b200_ctx* ctx, int alg, double mixing,
                                            int64_t max_subsp, int64_t diis_start);
 
-/* One loop iteration it (>= 1): update_w, Sigma, hermitize, damping/DIIS, Dyson for G
+/* enable != 0: every iteration first re-evaluates F = J + K (+ the gygi term with the
+   mean-field overlap) from the density matrix, as scf_loop does with an hf solver
+   (scf_driver.cpp:94-114); iteration 1 takes Dm = -G(beta^-) of the starting G. */
+COQUI_B200_API int coqui_b200_scgw_set_hf(coqui_b200_ctx* ctx, int enable, int div_treatment,
+                                          double madelung);
+
+/* One loop iteration it (>= 1): [HF,] update_w, Sigma, hermitize, damping/DIIS, Dyson for G
    (simple_dyson.cpp:11-123, G stays resident for the next iteration), energies.
    G_tskij != NULL uploads the starting G (iteration 1).  stats[8] = max|dF|, max|dSigma|,
    e_1e, e_hf, e_corr (Galitskii-Migdal, scf_common.cpp:87-136), the residual

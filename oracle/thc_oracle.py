@@ -323,6 +323,63 @@ def eval_Sigma_all_Rspace(G_tskij, dW_qtPQ, X_skPa, kpts, lattv, kp_grid) -> np.
 
 
 # ----------------------------------------------------------------------------------------
+# THC Hartree-Fock (static part of the self-consistent loop)
+# ----------------------------------------------------------------------------------------
+def thc_hf(Dm_skij, X_skPa, V_qPQ, kpts, lattv, kp_grid, S_skij=None, hartree=True,
+           exchange=True, div="ignore_g0", madelung=0.0) -> np.ndarray:
+    """hf_t::evaluate for q-independent THC without symmetry (thc_hf.cpp:21-60 ->
+    thc_hf.icc:17-272 with npol = 1) and HF_K_correction (hf_t.cpp:45-84).
+
+    F_skij = J + K, overwritten (thc_hf.icc:35):
+      D_PQ(k) = X^k Dm^k X^kH (:164), D(R) = f_Rk D(k) (:170-180);
+      J_P = sum_Q V^{q=0}_PQ rho_Q, rho_Q = factor sum_s D_QQ(s, R=0), factor 2 for one spin
+      (:182-209), added on the diagonal of F_PQ at every k;
+      K_PQ(R) = -D_PQ(R) V_PQ(R), V(R) = f_Rq V(q) (:143-152, :213-218), F_PQ(k) += f_kR K(R)
+      (:220-231);
+      F_ab = conj(X_Pa) F_PQ X_Qb (:238-241);
+      gygi: F += -madelung S Dm S (hf_t.cpp:72-80); ignore_g0 adds nothing.
+    """
+    ns, nk, nb, _ = Dm_skij.shape
+    Np = X_skPa.shape[2]
+    F = np.zeros((ns, nk, nb, nb), np.complex128)
+    if not hartree and not exchange:
+        return F
+    Dp = primary_to_aux(Dm_skij, X_skPa)  # (ns, nk, Np, Np)
+    f_Rk = k_to_R_coefficients(kpts, lattv, kp_grid)
+    f_kR = R_to_k_coefficients(kpts, lattv, kp_grid)
+    if nk != 1:
+        Dp = np.einsum("Rk,skx->sRx", f_Rk, Dp.reshape(ns, nk, -1)).reshape(Dp.shape)
+    F_PQ = np.zeros((ns, nk, Np, Np), np.complex128)
+    if hartree:
+        factor = 2.0 if ns == 1 else 1.0
+        rho = factor * np.einsum("spp->p", Dp[:, 0])  # R = 0 (first R point)
+        J = V_qPQ[0] @ rho  # q = 0 (Gamma, first q point)
+        idx = np.arange(Np)
+        F_PQ[:, :, idx, idx] += J
+    if exchange:
+        U = V_qPQ.reshape(V_qPQ.shape[0], -1)
+        U_R = (f_Rk @ U) if nk != 1 else U
+        K_R = -(Dp * U_R.reshape(nk, Np, Np)[None])
+        if nk != 1:
+            K_R = np.einsum("kR,sRx->skx", f_kR, K_R.reshape(ns, nk, -1)).reshape(K_R.shape)
+        F_PQ += K_R
+    F = aux_to_primary(F_PQ, X_skPa)
+    if exchange and div == "gygi":
+        if S_skij is None:
+            raise ValueError("gygi needs the overlap matrix")
+        F += -madelung * (S_skij @ Dm_skij @ S_skij)
+    elif div not in ("ignore_g0", "gygi"):
+        raise ValueError("div must be ignore_g0 or gygi")
+    return F
+
+
+def dm_from_G(G_tskij, ft: IAFT):
+    """Dm = -G(beta^-) (IAFT.icc:226-238 as used at simple_dyson.cpp:119-121), made
+    Hermitian as the loop does (scf_driver.cpp:140-143)."""
+    return hermitize(-ft.tau_to_beta(G_tskij))
+
+
+# ----------------------------------------------------------------------------------------
 # RPA correlation energy
 # ----------------------------------------------------------------------------------------
 def rpa_energy_from_Pi_w(Pi_wqPQ, V_qPQ, ft: IAFT, nk: int, q_weight=None) -> float:
@@ -536,17 +593,24 @@ def damp_pair(F, Sigma, F_prev, Sigma_prev, mixing):
 
 def scgw_loop(G0_tskij, X_skPa, V_qPQ, H0_skij, S_skij, F_skij, mu, ft: IAFT, kpts, lattv,
               kp_grid, niter, conv_tol, alg="damping", mixing=0.7, max_subsp_size=5,
-              diis_start=5):
-    """scf_loop (scf_driver.cpp:90-173) for GW with hf = nullptr and a constant mu: update_w,
-    evaluate, hermitize, solve_iterative, Dyson, energies; stops when max|dF| and max|dSigma|
-    are below conv_tol.  Returns the per-iteration records and the final (G, Sigma)."""
+              diis_start=5, hf=None):
+    """scf_loop (scf_driver.cpp:90-173) for GW with a constant mu: [hf,] update_w, evaluate,
+    hermitize, solve_iterative, Dyson, energies; stops when max|dF| and max|dSigma| are below
+    conv_tol.  hf = None is hf = nullptr (F stays the mean-field Fock matrix until damped);
+    hf = dict(div=..., madelung=...) re-evaluates F = J + K from the current density matrix at
+    the start of every iteration (scf_driver.cpp:94-114), the first from Dm = -G0(beta^-).
+    Returns the per-iteration records and the final (G, Sigma)."""
     nk = kpts.shape[0]
     w = np.full(nk, 1.0 / nk)
     G, F = G0_tskij.copy(), F_skij.copy()
+    Dm = dm_from_G(G0_tskij, ft) if hf is not None else None
     F_prev = Sigma_prev = None
     diis = CommutatorDIIS(mixing, max_subsp_size, diis_start) if alg == "diis" else None
     hist = []
     for it in range(1, niter + 1):
+        if hf is not None:
+            F = thc_hf(Dm, X_skPa, V_qPQ, kpts, lattv, kp_grid, S_skij, True, True,
+                       hf.get("div", "ignore_g0"), hf.get("madelung", 0.0))
         dW, _, _ = update_w(G, X_skPa, V_qPQ, ft, kpts, lattv, kp_grid)
         Sigma = eval_Sigma_all_Rspace(G, dW, X_skPa, kpts, lattv, kp_grid)
         F, Sigma = hermitize(F), hermitize(Sigma)

@@ -86,3 +86,60 @@ def test_damp_and_hermitize():
     assert diff == pytest.approx(np.abs(0.7 * a).max())
     hh = O.hermitize(a)
     np.testing.assert_allclose(hh, hh.conj().T)
+
+
+def _random_dm(rng, nk, nb):
+    A = rng.standard_normal((1, nk, nb, nb)) + 1j * rng.standard_normal((1, nk, nb, nb))
+    return 0.25 * (A + np.conj(np.swapaxes(A, -1, -2)))
+
+
+def test_hf_equals_k_convolution():
+    """thc_hf's R-space exchange equals K(k) = -(1/nk) sum_q D(k-q) o V(q) and its Hartree
+    term J_P = sum_Q V(0)_PQ (2/nk) sum_k D_QQ(k) (no DFT involved)."""
+    s = make_system((2, 1, 3), 5, 2, 12, seed=7)
+    n0, n1, n2 = s.kp_grid
+    nk, Np = s.nk, s.Np
+    Dm = _random_dm(np.random.default_rng(2), nk, s.nb)
+    F = O.thc_hf(Dm, s.X, s.V, s.kpts, s.lattv, s.kp_grid)
+    D = O.primary_to_aux(Dm, s.X)[0]
+    ijl = [(i, j, l) for i in range(n0) for j in range(n1) for l in range(n2)]
+    minus = lambda a, b: (((a[0] - b[0]) % n0) * n1 + (a[1] - b[1]) % n1) * n2 + (a[2] - b[2]) % n2
+    rho = 2.0 / nk * np.einsum("kpp->p", D)
+    J = s.V[0] @ rho
+    Fp = np.zeros((nk, Np, Np), np.complex128)
+    for k in range(nk):
+        for q in range(nk):
+            Fp[k] -= D[minus(ijl[k], ijl[q])] * s.V[q] / nk
+        Fp[k] += np.diag(J)
+    ref = O.aux_to_primary(Fp[None], s.X)
+    np.testing.assert_allclose(F, ref, atol=1e-12)
+
+
+def test_hf_gamma_equals_four_index_contraction():
+    """At one k-point J_ab = 2 sum_cd (ab|dc) D_cd and K_ab = -sum_cd (ac|db) D_cd with the
+    THC integrals (ab|cd) = sum_PQ conj(X_Pa) X_Pb V_PQ conj(X_Qc) X_Qd."""
+    s = make_system(1, 6, 3, 10, seed=4)
+    Dm = _random_dm(np.random.default_rng(3), 1, s.nb)
+    X, V = s.X[0, 0], s.V[0]
+    eri = np.einsum("Pa,Pb,PQ,Qc,Qd->abcd", np.conj(X), X, V, np.conj(X), X)
+    J = 2.0 * np.einsum("abdc,cd->ab", eri, Dm[0, 0])
+    K = -np.einsum("acdb,cd->ab", eri, Dm[0, 0])
+    args = (s.X, s.V, s.kpts, s.lattv, s.kp_grid)
+    np.testing.assert_allclose(O.thc_hf(Dm, *args, hartree=True, exchange=False)[0, 0], J,
+                               atol=1e-12)
+    np.testing.assert_allclose(O.thc_hf(Dm, *args, hartree=False, exchange=True)[0, 0], K,
+                               atol=1e-12)
+
+
+def test_hf_gygi_correction(small):
+    """HF_K_correction (hf_t.cpp:72-80): gygi adds -madelung S Dm S to the exchange only."""
+    s, _ = small
+    rng = np.random.default_rng(5)
+    Dm = _random_dm(rng, s.nk, s.nb)
+    S = np.eye(s.nb)[None, None] + 0.1 * _random_dm(rng, s.nk, s.nb)
+    args = (s.X, s.V, s.kpts, s.lattv, s.kp_grid, S)
+    F0 = O.thc_hf(Dm, *args)
+    F1 = O.thc_hf(Dm, *args, div="gygi", madelung=0.37)
+    np.testing.assert_allclose(F1 - F0, -0.37 * S @ Dm @ S, atol=1e-13)
+    J1 = O.thc_hf(Dm, *args, exchange=False, div="gygi", madelung=0.37)
+    np.testing.assert_allclose(J1, O.thc_hf(Dm, *args, exchange=False), atol=0)
