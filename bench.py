@@ -320,6 +320,28 @@ def run_ours(args, rank, world, local):
     t_rpa = float(np.mean(rpa))
     rpa_phases = dict(ctx.timings())
 
+    # THC Hartree-Fock F = J + K (gygi) of the density matrix of G, FP64 in both precision
+    # modes: the device phase and the public call with the host Dm in and F out
+    Dm = -np.tensordot(ft.T_beta_t_ff, G, axes=(0, 0))
+    Dm = np.ascontiguousarray(0.5 * (Dm + np.conj(np.swapaxes(Dm, -1, -2))))
+    S_ov = np.ascontiguousarray(np.broadcast_to(np.eye(s.nb, dtype=np.complex128), Dm.shape))
+    hf_dev, hf_e2e, hf_wall = [], [], []
+    l0 = ctx.kernel_launches()
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        F_hf = ctx.hf_evaluate(Dm, S_ov, True, True, "gygi", 0.5)
+        wall = (time.perf_counter() - t0) * 1e3
+        if i >= args.warmup:
+            hf_dev.append(dict(ctx.timings())["HF"])
+            hf_e2e.append(total_ms(ctx))
+            hf_wall.append(wall)
+    hf = {"what": "THC Hartree-Fock J + K with the gygi term (hf_t::evaluate), FP64",
+          "ms": float(np.mean(hf_dev)), "e2e_ms": float(np.mean(hf_e2e)),
+          "e2e_wall_ms": float(np.mean(hf_wall)),
+          "gpu_launches": int((ctx.kernel_launches() - l0) // (args.warmup + args.steps)),
+          "h2d_bytes": int(Dm.nbytes + S_ov.nbytes),
+          "d2h_bytes": int(F_hf.nbytes)}
+
     fp64 = None
     if not args.no_fp64:
         c64 = make_ctx(s, ft, capi.FP64)
@@ -413,6 +435,13 @@ def run_ours(args, rank, world, local):
                "sample": "FP64 numpy/OpenBLAS oracle: 1 tau of Pi and Sigma, 1/8 of one IR "
                          "transform, 2 (q,W) LU Dyson solves; extrapolated to one iteration",
                "parts_ms": {k: v * 1e3 for k, v in parts.items()}}
+        # the oracle's Hartree-Fock on the same density matrix: time and full-size parity
+        from oracle import thc_oracle as O
+        t0 = time.perf_counter()
+        F_ref = O.thc_hf(Dm, s.X, s.V, s.kpts, s.lattv, s.kp_grid, S_ov, True, True, "gygi", 0.5)
+        hf["cpu_oracle_ms"] = (time.perf_counter() - t0) * 1e3
+        hf["max_abs_dF_vs_oracle"] = float(np.abs(F_hf - F_ref).max())
+        hf["max_abs_F"] = float(np.abs(F_ref).max())
 
     gbytes = G.nbytes
     line = {
@@ -428,6 +457,7 @@ def run_ours(args, rank, world, local):
                 "d2h_bytes_per_step": gbytes},
         "gpu_launches": int(launches),
         "rpa_energy_ms": t_rpa, "E_c": e_c,
+        "hartree_fock": hf,
         "fp64_form": fp64,
         "phases_ms": phases,
         "steps_ms": [round(t, 3) for t in times],
