@@ -29,7 +29,7 @@ SYMBOLS = [
     "coqui_b200_kernel_launches", "coqui_b200_gw_iteration", "coqui_b200_set_profiling",
     "coqui_b200_kernel_stats", "coqui_b200_primary_to_aux_noalloc",
     "coqui_b200_set_ir_fermi", "coqui_b200_set_mean_field", "coqui_b200_set_iter_alg",
-    "coqui_b200_hf_evaluate", "coqui_b200_scgw_set_hf",
+    "coqui_b200_hf_evaluate", "coqui_b200_scgw_set_hf", "coqui_b200_set_div_treatment",
     "coqui_b200_scgw_iteration", "coqui_b200_get_scgw_state", "coqui_b200_dyson_g",
     "coqui_b200_gm_energy", "coqui_b200_mlp_create", "coqui_b200_mlp_destroy",
     "coqui_b200_mlp_last_error", "coqui_b200_mlp_num_params", "coqui_b200_mlp_set_params",
@@ -98,6 +98,7 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_set_iter_alg.argtypes = [P, ctypes.c_int, D, I64, I64]
     lib.coqui_b200_hf_evaluate.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, D, P]
     lib.coqui_b200_scgw_set_hf.argtypes = [P, ctypes.c_int, ctypes.c_int, D]
+    lib.coqui_b200_set_div_treatment.argtypes = [P, ctypes.c_int, D, P]
     lib.coqui_b200_scgw_iteration.argtypes = [P, P, I64, P]
     lib.coqui_b200_get_scgw_state.argtypes = [P, P, P, P]
     lib.coqui_b200_dyson_g.argtypes = [P, P, P, P]
@@ -158,6 +159,7 @@ def _c128(a, shape, name):
 
 
 _DIV = {"ignore_g0": 0, "gygi": 1}
+_DIV_ALL = {"ignore_g0": 0, "gygi": 1, "gygi_extrplt": 2, "gygi_extrplt_2d": 3}
 
 
 class Context:
@@ -233,6 +235,13 @@ class Context:
             self.h, _ptr(Dm, "Dm"), _ptr(S, "S"), int(bool(hartree)), int(bool(exchange)),
             _DIV[div], float(madelung), _ptr(F, "F")))
         return F
+
+    def set_div_treatment(self, div="ignore_g0", madelung=0.0, chi_head=None):
+        """q -> 0 treatment of the eps^-1 head and of Sigma; chi_head (Np) is basis_head at
+        q = 0, needed by the gygi corrections of Sigma."""
+        chi = None if chi_head is None else _c128(chi_head, (self.Np,), "chi_head")
+        self._check(self.lib.coqui_b200_set_div_treatment(self.h, _DIV_ALL[div], float(madelung),
+                                                          _ptr(chi, "chi_head")))
 
     def set_hf(self, enable=True, div="ignore_g0", madelung=0.0):
         """Re-evaluate F = J + K from the density matrix at the start of every scGW iteration."""

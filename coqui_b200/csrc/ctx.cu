@@ -15,6 +15,7 @@
 #include <complex>
 #include <cstring>
 #include <memory>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -119,8 +120,21 @@ struct coqui_b200_ctx {
   DevBuf<int> ginfo;
   DevBuf<double> red;
   DevBuf<double2> trc;
-  // THC Hartree-Fock: bare V(q) transformed to R in storage precision (built on first use),
-  // scratch, and whether the loop re-evaluates F = J + K from the density matrix
+  // long-wavelength treatment (div_treatment_e): 0 ignore_g0, 1 gygi, 2 gygi_extrplt,
+  // 3 gygi_extrplt_2d; the madelung constant; conj(basis_head) at q = 0 (device)
+  int div = 0;
+  double madelung = 0;
+  std::vector<double> qnorm, qz;   // |q| (as the reference forms it) and q_z per q-point
+  DevBuf<double2> chi0c, Tdiv, divY;
+  bool tdiv_valid = false;
+  // eps^-1 head per (tau, q) of the current W (host, (nth, nq)) and the selected head (nth)
+  std::vector<double2> eps_raw, head_h;
+  bool eps_raw_valid = false;
+  DevBuf<double> divf;
+  DevBuf<const double2*> divp;     // pointer arrays of the batched correction products
+  std::vector<const double2*> divp_h;
+  // THC Hartree-Fock: bare V(q) transformed to R in FP64 (built on first use), scratch, and
+  // whether the loop re-evaluates F = J + K from the density matrix
   DevBuf<double2> VR;
   bool vr_valid = false;
   DevBuf<double2> hfd, hfs, hff, hfv, hft, hfp;
@@ -231,6 +245,19 @@ void zgemm_rm(Ctx* c, char opA, char opB, int64_t M, int64_t N, int64_t K, doubl
       (int)ldb, sB, reinterpret_cast<const cuDoubleComplex*>(A), (int)lda, sA,
       reinterpret_cast<const cuDoubleComplex*>(&beta), reinterpret_cast<cuDoubleComplex*>(C),
       (int)ldc, sC, (int)batch));
+}
+
+// The same with per-problem operand pointers (device arrays of batch pointers each).
+void zgemm_rm_ptrs(Ctx* c, char opA, char opB, int64_t M, int64_t N, int64_t K, double2 alpha,
+                   const double2* const* A, int64_t lda, const double2* const* B, int64_t ldb,
+                   double2 beta, double2* const* C, int64_t ldc, int64_t batch) {
+  CQ_CHECK_BLAS(cublasZgemmBatched(
+      c->blas, blas_op(opB), blas_op(opA), (int)N, (int)M, (int)K,
+      reinterpret_cast<const cuDoubleComplex*>(&alpha),
+      reinterpret_cast<const cuDoubleComplex* const*>(B), (int)ldb,
+      reinterpret_cast<const cuDoubleComplex* const*>(A), (int)lda,
+      reinterpret_cast<const cuDoubleComplex*>(&beta), reinterpret_cast<cuDoubleComplex* const*>(C),
+      (int)ldc, (int)batch));
 }
 
 void upload(Ctx* c, void* dst, const void* src, size_t bytes) {
@@ -889,19 +916,27 @@ int coqui_b200_set_kmesh(coqui_b200_ctx* c, const double* kpts, const double* la
                    "k-points are not a Gamma-centred grid in lexicographic order");
       }
     }
-    // dielectric-head prefactors (g0_div_utils.hpp:196-207) and smallest |q|
+    // dielectric-head prefactors (g0_div_utils.hpp:196-207) and the q of the reported head:
+    // the first smallest nonzero |q| (find_smallest_qabs, g0_div_utils.hpp:263-282; q = 0
+    // itself has a vanishing prefactor), q = 0 for a single q-point
     const double* a = lattv;
     const double vol = std::abs(a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
                                 a[2] * (a[3] * a[7] - a[4] * a[6]));
     const double fpi = 4.0 * 3.14159265358979323846;
     c->head_fac.resize(nk);
-    double best = 1e300;
+    double best = -1;
+    c->q_smallest = 0;
+    c->qnorm.resize(nk);
+    c->qz.resize(nk);
     for (int64_t q = 0; q < nk; ++q) {
       const double q2 = kpts[3 * q] * kpts[3 * q] + kpts[3 * q + 1] * kpts[3 * q + 1] +
                         kpts[3 * q + 2] * kpts[3 * q + 2];
       c->head_fac[q] = q2 / fpi * vol;
-      if (q2 < best) {
-        best = q2;
+      const double norm = std::sqrt(q2);
+      c->qnorm[q] = norm;
+      c->qz[q] = kpts[3 * q + 2];
+      if (nk > 1 && norm > 0.0 && (best < 0 || norm < best)) {
+        best = norm;
         c->q_smallest = q;
       }
     }
@@ -916,6 +951,7 @@ int coqui_b200_set_kmesh(coqui_b200_ctx* c, const double* kpts, const double* la
     c->have_k = true;
     c->gcache_valid = false;
     c->vr_valid = false;
+    c->eps_raw_valid = false;
   });
 }
 
@@ -947,6 +983,8 @@ int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_
     c->gcache_valid = false;
     c->w_valid = false;
     c->vr_valid = false;
+    c->tdiv_valid = false;
+    c->eps_raw_valid = false;
   });
 }
 
@@ -1071,10 +1109,18 @@ void update_w_device(Ctx* c) {
   c->mark("IMAG_FT_WtoT");
   c->w_valid = true;
   c->w_in_R = false;
+  c->eps_raw_valid = false;
 }
 
-void eps_head(Ctx* c, double* out) {
+// the treatment in effect: with one q-point every treatment is ignore_g0
+// (g0_div_utils.hpp:68-72, thc_gw.icc:454-458)
+bool div_active(const Ctx* c) { return c->div != 0 && c->nq > 1; }
+
+// eps^-1 head per (tau, q) of the current W, which must be in q-space (eval_eps_inv_q,
+// g0_div_utils.hpp:180-214) -> c->eps_raw (nth, nq)
+void eps_raw_heads(Ctx* c) {
   cq::Prof::Scope sc(&c->prof, "eps_head");
+  CQ_REQUIRE(!c->w_in_R, COQUI_B200_EINVAL, "eps head: W is not in q-space");
   c->eps.ensure((size_t)c->nth * c->nq);
   if (c->mode == COQUI_B200_FP64)
     cq::launch_eps_head<double>((double2*)c->PW.p, c->chi.p, c->fac.p, c->eps.p, c->nth, c->nq,
@@ -1082,13 +1128,131 @@ void eps_head(Ctx* c, double* out) {
   else
     cq::launch_eps_head<float>((float2*)c->PW.p, c->chi.p, c->fac.p, c->eps.p, c->nth, c->nq,
                                c->Np, c->st);
-  std::vector<double2> h((size_t)c->nth * c->nq);
-  download(c, h.data(), c->eps.p, h.size() * sizeof(double2));
+  c->eps_raw.resize((size_t)c->nth * c->nq);
+  download(c, c->eps_raw.data(), c->eps.p, c->eps_raw.size() * sizeof(double2));
   CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
-  for (int64_t t = 0; t < c->nth; ++t) {
-    out[2 * t] = h[t * c->nq + c->q_smallest].x;
-    out[2 * t + 1] = h[t * c->nq + c->q_smallest].y;
+  c->eps_raw_valid = true;
+}
+
+// eps_inv_head_t (g0_div_utils.hpp:55-111): c->head_h (nth) from c->eps_raw.  ignore_g0 and
+// gygi: the first smallest nonzero |q|.  gygi_extrplt(_2d): through the q with
+// 0 < |q| <= 0.8 (q_z = 0 for _2d; distinct |q| only, filter_qpts :26-42), per bosonic
+// frequency (tau_to_w_PHsym), the least-squares quadratic in |q| extrapolated to q = 0
+// (extrapolate_to_q0 :284-311), back with w_to_tau_PHsym; the first such q alone when fewer
+// than 3.
+void select_head(Ctx* c) {
+  const int64_t nth = c->nth, nq = c->nq, nwh = c->nwh;
+  const std::vector<double2>& eps = c->eps_raw;
+  c->head_h.assign(nth, make_double2(0, 0));
+  const int div = nq == 1 ? 0 : c->div;
+  int64_t col = c->q_smallest;
+  if (div >= 2) {
+    std::vector<int64_t> idx;
+    std::set<double> seen;
+    for (int64_t q = 0; q < nq; ++q) {
+      const double n = c->qnorm[q];
+      if (n > 0.0 && n <= 0.8 && (div != 3 || c->qz[q] == 0.0) && seen.insert(n).second)
+        idx.push_back(q);
+    }
+    CQ_REQUIRE(!idx.empty(), COQUI_B200_EINVAL,
+               "gygi_extrplt: no q-point with 0 < |q| <= 0.8 for the extrapolation");
+    if (idx.size() >= 3) {
+      using cd = std::complex<double>;
+      const size_t m = idx.size();
+      // normal equations of A(i, j) = |q_i|^j, j = 0..2
+      double a[3][3] = {};
+      for (size_t i = 0; i < m; ++i) {
+        const double Q = c->qnorm[idx[i]], p[3] = {1.0, Q, Q * Q};
+        for (int j = 0; j < 3; ++j)
+          for (int l = 0; l < 3; ++l) a[j][l] += p[j] * p[l];
+      }
+      // first row of (A^T A)^{-1} (cofactors of the symmetric 3 x 3)
+      const double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+      const double c01 = a[0][2] * a[2][1] - a[0][1] * a[2][2];
+      const double c02 = a[0][1] * a[1][2] - a[0][2] * a[1][1];
+      const double det = a[0][0] * c00 + a[1][0] * c01 + a[2][0] * c02;
+      CQ_REQUIRE(det != 0.0, COQUI_B200_EINVAL, "gygi_extrplt: singular fit");
+      const double r0[3] = {c00 / det, c01 / det, c02 / det};
+      std::vector<cd> e0(nwh);
+      for (int64_t n = 0; n < nwh; ++n) {
+        cd atb[3] = {};
+        for (size_t i = 0; i < m; ++i) {
+          cd ew = 0;
+          for (int64_t t = 0; t < nth; ++t) {
+            const double2 T = c->Twt_pos[n * nth + t], e = eps[t * nq + idx[i]];
+            ew += cd(T.x, T.y) * cd(e.x, e.y);
+          }
+          const double Q = c->qnorm[idx[i]], p[3] = {1.0, Q, Q * Q};
+          for (int j = 0; j < 3; ++j) atb[j] += p[j] * ew;
+        }
+        e0[n] = r0[0] * atb[0] + r0[1] * atb[1] + r0[2] * atb[2];
+      }
+      for (int64_t t = 0; t < nth; ++t) {
+        cd h = 0;
+        for (int64_t n = 0; n < nwh; ++n) {
+          const double2 T = c->Ttw_pos[t * nwh + n];
+          h += cd(T.x, T.y) * e0[n];
+        }
+        c->head_h[t] = make_double2(h.real(), h.imag());
+      }
+      return;
+    }
+    col = idx[0];
   }
+  for (int64_t t = 0; t < nth; ++t) c->head_h[t] = eps[t * nq + col];
+}
+
+// the eps^-1 head of the current W (nth complex values as (re, im) into out, if not null)
+void eps_head(Ctx* c, double* out) {
+  if (!c->eps_raw_valid) eps_raw_heads(c);
+  select_head(c);
+  if (out)
+    for (int64_t t = 0; t < c->nth; ++t) {
+      out[2 * t] = c->head_h[t].x;
+      out[2 * t + 1] = c->head_h[t].y;
+    }
+}
+
+// gw_t::Sigma_div_correction (thc_gw.icc:446-526) on the device Sigma (FP64), for the gygi
+// treatments: Sigma(t, k) += -madelung Re head(t_pos) T^k G(t, k) T^kH with
+// T^k = X^kH diag(conj chi_head) X^k, t_pos = t below nt_half, else nt - 1 - t.
+void sigma_div_correction(Ctx* c) {
+  cq::Prof::Scope sc(&c->prof, "sigma_div");
+  const int64_t nk = c->nk, nb = c->nb, Np = c->Np, nt = c->nt, nth = c->nth, per = nb * nb;
+  const int64_t nprob = nt * nk;
+  if (!c->tdiv_valid) {
+    c->Tdiv.ensure(nk * per);
+    c->Tproj.ensure((size_t)nk * Np * nb);
+    cq::scale_rows(c->X.p, c->chi0c.p, c->Tproj.p, nk, Np, nb, c->st);
+    zgemm_rm(c, 'C', 'N', nb, nb, Np, make_double2(1, 0), c->X.p, nb, Np * nb, c->Tproj.p, nb,
+             Np * nb, make_double2(0, 0), c->Tdiv.p, nb, per, nk);
+    c->tdiv_valid = true;
+  }
+  std::vector<double> f(nt);
+  for (int64_t t = 0; t < nt; ++t) f[t] = -c->madelung * c->head_h[t < nth ? t : nt - t - 1].x;
+  c->divf.ensure(nt);
+  upload(c, c->divf.p, f.data(), nt * sizeof(double));
+  c->divY.ensure(nprob * per);
+  // pointer arrays: (T, G, Y) for Y = T G, then (Y, T, Sigma) for Sigma += Y T^H
+  c->divp_h.resize(6 * nprob);
+  for (int64_t t = 0; t < nt; ++t)
+    for (int64_t k = 0; k < nk; ++k) {
+      const int64_t i = t * nk + k;
+      c->divp_h[i] = c->Tdiv.p + k * per;
+      c->divp_h[nprob + i] = c->G.p + i * per;
+      c->divp_h[2 * nprob + i] = c->divY.p + i * per;
+      c->divp_h[3 * nprob + i] = c->divY.p + i * per;
+      c->divp_h[4 * nprob + i] = c->Tdiv.p + k * per;
+      c->divp_h[5 * nprob + i] = c->Sig.p + i * per;
+    }
+  c->divp.ensure(6 * nprob);
+  upload(c, c->divp.p, c->divp_h.data(), 6 * nprob * sizeof(const double2*));
+  const double2* const* P = c->divp.p;
+  zgemm_rm_ptrs(c, 'N', 'N', nb, nb, nb, make_double2(1, 0), P, nb, P + nprob, nb,
+                make_double2(0, 0), const_cast<double2* const*>(P + 2 * nprob), nb, nprob);
+  cq::scale_slices(c->divY.p, c->divf.p, nt, nk * per, c->st);
+  zgemm_rm_ptrs(c, 'N', 'C', nb, nb, nb, make_double2(1, 0), P + 3 * nprob, nb, P + 4 * nprob,
+                nb, make_double2(1, 0), const_cast<double2* const*>(P + 5 * nprob), nb, nprob);
 }
 
 void download_w_qt(Ctx* c, double* dW_qtPQ) {
@@ -1110,6 +1274,8 @@ void download_w_qt(Ctx* c, double* dW_qtPQ) {
 // Sigma(tau) for all tau into c->Sig (device, complex128), thc_gw.icc:70-213 twice.
 // host_out (may be null) receives Sigma_tskij; from page-locked memory it is filled chunk by
 // chunk on the copy stream while the following chunks are computed.
+void w_to_q_space(Ctx* c);
+
 void sigma_device(Ctx* c, double* host_out) {
   CQ_REQUIRE(c->w_valid, COQUI_B200_EINVAL, "no screened interaction: call update_w or set_w");
   const int64_t nk = c->nk, nb = c->nb, Np = c->Np, ncol = Np * Np, nt = c->nt;
@@ -1118,6 +1284,15 @@ void sigma_device(Ctx* c, double* host_out) {
   c->Gp.ensure(slab);
   c->Gn.ensure(slab);
   c->Sig.ensure((size_t)nt * gsz);
+  // the gygi treatments need the eps^-1 head of this W (thc_gw.icc:30-33): taken while W is
+  // in q-space (a W left in R by an earlier call is transformed back once)
+  const bool corr = div_active(c);
+  if (corr) {
+    CQ_REQUIRE(c->chi0c.n >= (size_t)Np, COQUI_B200_EINVAL,
+               "the gygi treatments of Sigma need chi_head (coqui_b200_set_div_treatment)");
+    if (!c->eps_raw_valid && c->w_in_R) w_to_q_space(c);
+    eps_head(c, nullptr);
+  }
   // W q -> R once (thc_gw.icc:148-153); stays in R until the next update
   if (!c->w_in_R) {
     cq::Prof::Scope sc(&c->prof, "dft_w");
@@ -1135,7 +1310,8 @@ void sigma_device(Ctx* c, double* host_out) {
   // then formed in place there and projected back in batches
   unsigned char* cache = c->gcache_valid ? c->Gcache.p : nullptr;
   c->gcache_valid = false;
-  const bool pipe_out = host_out && is_pinned(host_out);
+  // with the q -> 0 correction, Sigma leaves once it is complete
+  const bool pipe_out = host_out && is_pinned(host_out) && !corr;
   for (int64_t i = 0; i < n_tau_chunks(c); ++i) {
     int64_t a, b;
     tau_chunk_range(c, i, &a, &b);
@@ -1181,6 +1357,7 @@ void sigma_device(Ctx* c, double* host_out) {
                                     cudaMemcpyDeviceToHost, c->cs));
     }
   }
+  if (corr) sigma_div_correction(c);
   c->mark("EVALUATE_SIGMA_R");
   if (host_out) {
     if (pipe_out) {  // the compute stream's timeline ends when the last copy landed
@@ -1193,7 +1370,7 @@ void sigma_device(Ctx* c, double* host_out) {
   }
 }
 
-[[maybe_unused]] void w_to_q_space(Ctx* c) {
+void w_to_q_space(Ctx* c) {
   if (!c->w_in_R) return;
   const int64_t ncol = c->Np * c->Np;
   if (c->mode == COQUI_B200_FP64)
@@ -1359,6 +1536,7 @@ int coqui_b200_set_w(coqui_b200_ctx* c, const double* dW_qtPQ) {
     c->stage.release();
     c->w_valid = true;
     c->w_in_R = false;
+    c->eps_raw_valid = false;
   });
 }
 
@@ -1382,7 +1560,7 @@ int coqui_b200_gw_iteration(coqui_b200_ctx* c, const double* G_tskij, double* Si
     // runs as one CUDA graph, captured on the first of a run of such calls with the same
     // buffers and replayed by the following ones
     // page-locked host buffers: the copies join the graph
-    if (!eps_inv_head && c->mode == COQUI_B200_MIXED && !c->prof.on &&
+    if (!eps_inv_head && c->mode == COQUI_B200_MIXED && !c->prof.on && !div_active(c) &&
         (G_tskij ? is_pinned(G_tskij) : c->g_resident) && (!Sigma_tskij || is_pinned(Sigma_tskij))) {
       gw_iteration_graph(c, G_tskij, Sigma_tskij);
       return;
@@ -1588,6 +1766,26 @@ int coqui_b200_set_iter_alg(coqui_b200_ctx* c, int alg, double mixing, int64_t m
     c->mixing = mixing;
     c->max_subsp = max_subsp;
     c->diis_start = diis_start;
+  });
+}
+
+int coqui_b200_set_div_treatment(coqui_b200_ctx* c, int div_treatment, double madelung,
+                                 const double* chi_head_P) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(div_treatment >= 0 && div_treatment <= 3, COQUI_B200_EINVAL,
+               "div_treatment must be 0 (ignore_g0), 1 (gygi), 2 (gygi_extrplt) or "
+               "3 (gygi_extrplt_2d)");
+    c->div = div_treatment;
+    c->madelung = madelung;
+    if (chi_head_P) {
+      std::vector<double2> h(c->Np);
+      std::memcpy(h.data(), chi_head_P, c->Np * sizeof(double2));
+      for (auto& v : h) v.y = -v.y;  // conj(chi_head), thc_gw.icc:485
+      c->chi0c.ensure(c->Np);
+      upload(c, c->chi0c.p, h.data(), c->Np * sizeof(double2));
+      CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+      c->tdiv_valid = false;
+    }
   });
 }
 

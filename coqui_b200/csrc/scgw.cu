@@ -285,7 +285,24 @@ __global__ void k_scale_rows(const double2* __restrict__ X, const double2* __res
     Y[i] = cmul2(d[(i / nb) % Np], X[i]);
 }
 
+// A[s * per + e] *= f[s]
+__global__ void k_scale_slices(double2* __restrict__ A, const double* __restrict__ f,
+                               int64_t nslice, int64_t per) {
+  const int64_t n = nslice * per;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = f[i / per];
+    A[i] = make_double2(v * A[i].x, v * A[i].y);
+  }
+}
+
 }  // namespace
+
+void scale_slices(double2* A, const double* f, int64_t nslice, int64_t per, cudaStream_t s) {
+  k_scale_slices<<<grid_for(nslice * per, 256), 256, 0, s>>>(A, f, nslice, per);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
 
 void aux_diag(const double2* T, const double2* X, double2* rho, int64_t nk, int64_t Np,
               int64_t nb, double scale, cudaStream_t s) {

@@ -53,6 +53,9 @@ void aux_diag(const double2* T, const double2* X, double2* rho, int64_t nk, int6
 void scale_rows(const double2* X, const double2* d, double2* Y, int64_t nk, int64_t Np,
                 int64_t nb, cudaStream_t s);
 
+// A[s * per + e] *= f[s] (real f) for nslice consecutive slices of per complex values
+void scale_slices(double2* A, const double* f, int64_t nslice, int64_t per, cudaStream_t s);
+
 // Eigen-decomposition of a small real symmetric matrix by cyclic Jacobi rotations (host):
 // A (n x n, row-major) -> ev (n), U (n x n, row-major, column k = eigenvector k).
 void sym_eigen(const std::vector<double>& A, int64_t n, std::vector<double>& ev,

@@ -36,7 +36,8 @@ class THCData:
     lattv: np.ndarray  # (3, 3) rows = lattice vectors
     kp_grid: tuple
     chi_bar: Optional[np.ndarray] = None  # (nq, Np) basis_bar_head
-    madelung: float = 0.0  # MF::madelung(), used by the gygi exchange correction
+    madelung: float = 0.0  # MF::madelung(), used by the gygi corrections
+    chi_head: Optional[np.ndarray] = None  # (Np) basis_head at q = 0 (gygi Sigma correction)
 
     @property
     def Np(self):
@@ -118,6 +119,7 @@ class scr_coulomb_t:
         if mb_state.sG_tskij is None:
             raise capi.CoquiB200Error(-1, "update_w: sG_tskij is not initialized in MBState")
         ctx = context_for(thc, self.ft, self.mode)
+        ctx.set_div_treatment(self.div_treatment, thc.madelung, thc.chi_head)
         W, head = ctx.update_w(mb_state.sG_tskij)
         mb_state.dW_qtPQ = W
         mb_state.eps_inv_head = head
@@ -143,9 +145,6 @@ class gw_t:
     def __init__(self, ft: IAFT, div_treatment: str = "ignore_g0", mode: int = capi.MIXED):
         if div_treatment not in DIV_TREATMENTS:
             raise ValueError(f"unknown div_treatment {div_treatment}")
-        if div_treatment != "ignore_g0":
-            # the q->0 correction (thc_gw.icc:446-526) is outside this path
-            raise NotImplementedError("only div_treatment='ignore_g0' is on this path")
         self.ft, self.div_treatment, self.mode = ft, div_treatment, mode
 
     def evaluate(self, mb_state: MBState, thc: THCData, verbose: bool = False):
@@ -156,6 +155,7 @@ class gw_t:
         if not self.ft.check_ph_symmetric():
             raise capi.CoquiB200Error(-6, "thc-gw: IAFT grid is not compatible with PH symmetry")
         ctx = context_for(thc, self.ft, self.mode)
+        ctx.set_div_treatment(self.div_treatment, thc.madelung, thc.chi_head)
         if mb_state.meta.get("w_on_device") is not ctx:
             ctx.set_w(mb_state.dW_qtPQ)
         mb_state.sSigma_tskij = ctx.eval_sigma(mb_state.sG_tskij)

@@ -123,6 +123,20 @@ COQUI_B200_API int coqui_b200_rpa_energy(coqui_b200_ctx* ctx, const double* G_ts
 COQUI_B200_API int coqui_b200_gw_iteration(coqui_b200_ctx* ctx, const double* G_tskij,
                                            double* Sigma_tskij, double* eps_inv_head);
 
+/* ---- long-wavelength (q -> 0) treatment of scr_coulomb_t and gw_t (div_treatment_e) ---- */
+
+/* div_treatment 0 = ignore_g0 (default), 1 = gygi, 2 = gygi_extrplt, 3 = gygi_extrplt_2d.
+   The eps^-1 head (update_w, gw_iteration) follows eps_inv_head_t
+   (src/methods/GW/g0_div_utils.hpp:55-111): the smallest nonzero |q| for 0 and 1; for 2 and 3
+   a quadratic in |q| fitted per bosonic frequency through the q with 0 < |q| <= 0.8 (q_z = 0
+   for 3) and extrapolated to q = 0.  For 1-3 the self-energy also gets Sigma_div_correction
+   (src/methods/GW/thc_gw.icc:446-526): -madelung Re head(tau) T G(tau) T^H with
+   T = X^H diag(conj chi_head) X; chi_head_P is basis_head at q = 0 (Np complex128; needed
+   before the first such Sigma, NULL keeps the last one).  With one q-point every treatment
+   acts as ignore_g0, as in the reference. */
+COQUI_B200_API int coqui_b200_set_div_treatment(coqui_b200_ctx* ctx, int div_treatment,
+                                                double madelung, const double* chi_head_P);
+
 /* ---- THC Hartree-Fock (hf_t::evaluate, src/methods/HF/thc_hf.cpp:21-60 ->
    thc_hf.icc:17-272 for q-independent THC without symmetry; hf_t.cpp:45-84) ---- */
 

@@ -261,13 +261,105 @@ def eval_eps_inv_q(W_tqPQ, chi_bar_qP, Qpts, lattv) -> np.ndarray:
     return (q2 / fpi * vol)[None, :] * np.einsum("qP,tqP->tq", chi_bar_qP, buf)
 
 
+def find_smallest_qabs(Qpts, two_dim=False) -> int:
+    """g0_div_utils.hpp:263-282: index of the smallest nonzero |q| (the first one on ties);
+    0 for a single q-point."""
+    Qpts = np.asarray(Qpts, np.float64)
+    if Qpts.shape[0] == 1:
+        return 0
+    mn, idx = -1.0, -1
+    for i, q in enumerate(Qpts):
+        norm = float(np.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]))
+        if norm > 0.0 and mn == -1 and (not two_dim or q[2] != 0.0):
+            mn, idx = norm, i
+        elif norm > 0.0 and norm < mn and (not two_dim or q[2] == 0.0):
+            mn, idx = norm, i
+    return idx
+
+
 def eps_inv_head_ignore_g0(eps_inv_tq, Qpts) -> np.ndarray:
-    """g0_div_utils.hpp:102-107: head taken at the q with the smallest |q|."""
-    q2 = (np.asarray(Qpts) ** 2).sum(axis=1)
-    return eps_inv_tq[:, int(np.argmin(q2))]
+    """eps_inv_head_t without extrapolation (g0_div_utils.hpp:104-108, the ignore_g0 and gygi
+    treatments): the head at the smallest nonzero |q|."""
+    return eps_inv_tq[:, find_smallest_qabs(Qpts)]
 
 
-def update_w(G_tskij, X_skPa, V_qPQ, ft: IAFT, kpts, lattv, kp_grid, chi_bar_qP=None):
+def filter_qpts(Qpts, threshold, order, two_dim=False):
+    """g0_div_utils.hpp:26-42: indices of the q with 0 < |q|^order <= threshold (and q_z = 0
+    for two_dim), the first q of each distinct |q|^order only, in q order."""
+    idx, seen = [], set()
+    for i, q in enumerate(np.asarray(Qpts, np.float64)):
+        norm = float(np.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2])) ** order
+        if norm > 0.0 and norm <= threshold and (not two_dim or q[2] == 0.0):
+            if norm not in seen:
+                seen.add(norm)
+                idx.append(i)
+    return idx
+
+
+def extrapolate_to_q0(Q, eps_n, fit_order=2):
+    """g0_div_utils.hpp:284-311: least-squares polynomial eps(Q) = sum_j x_j Q^j through the
+    samples (normal equations); returns x_0."""
+    Q = np.asarray(Q, np.complex128)
+    A = np.stack([Q ** j for j in range(fit_order + 1)], axis=1)
+    x = np.linalg.inv(A.T @ A) @ (A.T @ np.asarray(eps_n, np.complex128))
+    return x[0]
+
+
+DIVS = ("ignore_g0", "gygi", "gygi_extrplt", "gygi_extrplt_2d")
+
+
+def eps_inv_head_t(eps_inv_tq, Qpts, ft, div="ignore_g0", q_max=0.8, fit_order=2,
+                   poly_in_q2=False):
+    """g0_div_utils.hpp:55-111: the head eps^{-1}(q -> 0, tau) on the half tau grid.
+    One q-point: ignore_g0.  gygi_extrplt(_2d): per bosonic frequency (tau_to_w_PHsym) a
+    fit_order polynomial in |q| (|q|^2 with poly_in_q2) through the q with 0 < |q| <= q_max,
+    extrapolated to q = 0 and brought back with w_to_tau_PHsym (the first such q alone when
+    fewer than 3).  ignore_g0 and gygi: the smallest nonzero |q|."""
+    Qpts = np.asarray(Qpts, np.float64)
+    if Qpts.shape[0] == 1:
+        div = "ignore_g0"
+    if div in ("gygi_extrplt", "gygi_extrplt_2d"):
+        two_dim = div == "gygi_extrplt_2d"
+        eps_w = ft.tau_to_w_PHsym(eps_inv_tq)
+        idx = filter_qpts(Qpts, q_max, 2 if poly_in_q2 else 1, two_dim)
+        if not idx:
+            raise ValueError("gygi_extrplt: no q-point with 0 < |q| <= q_max")
+        if len(idx) < 3:
+            return eps_inv_tq[:, idx[0]]
+        q2 = (Qpts[idx] ** 2).sum(axis=1)
+        Qf = q2 if poly_in_q2 else np.sqrt(q2)
+        e0_w = np.array([extrapolate_to_q0(Qf, eps_w[n, idx], fit_order)
+                         for n in range(eps_w.shape[0])])
+        return ft.w_to_tau_PHsym(e0_w[:, None])[:, 0]
+    if div not in ("ignore_g0", "gygi"):
+        raise ValueError(f"unknown div_treatment {div}")
+    return eps_inv_tq[:, find_smallest_qabs(Qpts)]
+
+
+def sigma_div_correction(Sigma_tskij, G_tskij, X_skPa, chi_head_P, eps_inv_head, madelung,
+                         div="ignore_g0", nq=None):
+    """gw_t::Sigma_div_correction (thc_gw.icc:446-526): nothing for ignore_g0 or one q-point;
+    for the gygi treatments Sigma(t) += -madelung Re eps_head(t_pos) T G(t) T^H with
+    T^k_ia = sum_P conj(X^k_Pi) X^k_Pa conj(chi_head_P) and t_pos = t for t < nt_half, else
+    nt - t - 1."""
+    nq = X_skPa.shape[1] if nq is None else nq
+    if div == "ignore_g0" or nq == 1:
+        return Sigma_tskij
+    if div not in DIVS:
+        raise ValueError(f"unknown div_treatment {div}")
+    nt = G_tskij.shape[0]
+    nt_half = (nt + 1) // 2
+    T = np.einsum("skPi,skPa,P->skia", np.conj(X_skPa), X_skPa, np.conj(chi_head_P))
+    out = Sigma_tskij.copy()
+    for t in range(nt):
+        t_pos = t if t < nt_half else nt - t - 1
+        f = -madelung * np.real(eps_inv_head[t_pos])
+        out[t] += f * (T @ G_tskij[t] @ np.conj(np.swapaxes(T, -1, -2)))
+    return out
+
+
+def update_w(G_tskij, X_skPa, V_qPQ, ft: IAFT, kpts, lattv, kp_grid, chi_bar_qP=None,
+             div="ignore_g0"):
     """scr_coulomb_t.cpp:37-95: Pi -> tau_to_w -> Dyson -> w_to_tau -> head -> dW_qtPQ."""
     Pi_t = eval_Pi_rpa_Rspace(G_tskij, X_skPa, kpts, lattv, kp_grid)
     Pi_w = ft.tau_to_w_PHsym(Pi_t)
@@ -277,7 +369,7 @@ def update_w(G_tskij, X_skPa, V_qPQ, ft: IAFT, kpts, lattv, kp_grid, chi_bar_qP=
     if chi_bar_qP is None:
         chi_bar_qP = np.zeros((nq, Np), np.complex128)
     eps_tq = eval_eps_inv_q(W_t, chi_bar_qP, kpts, lattv)
-    head = eps_inv_head_ignore_g0(eps_tq, kpts)
+    head = eps_inv_head_t(eps_tq, kpts, ft, div)
     dW_qtPQ = np.ascontiguousarray(np.swapaxes(W_t, 0, 1))  # scr_coulomb_t.cpp:73-86
     return dW_qtPQ, head, eps_tq
 

@@ -94,6 +94,8 @@ def test_update_w_and_sigma(base, mode, tol):
     W, head = c.update_w(base.G)
     assert maxabs(W, base.dW) < tol
     assert maxabs(head, base.head) < tol
+    # the head is taken at the smallest nonzero |q| (find_smallest_qabs), not at q = 0
+    assert np.abs(base.head).max() > 1e-3
     S = c.eval_sigma(base.G)
     assert maxabs(S, base.Sigma) < tol
     # Sigma from an uploaded W equals Sigma from the resident W

@@ -43,8 +43,10 @@ def test_solver_argument_checks():
     ft = IAFT(1000.0, 10.0, "low")
     with pytest.raises(ValueError):
         solvers.scr_coulomb_t(ft, screen_type="edmft")
-    with pytest.raises(NotImplementedError):
-        solvers.gw_t(ft, div_treatment="gygi")
+    for div in ("ignore_g0", "gygi", "gygi_extrplt", "gygi_extrplt_2d"):
+        assert solvers.gw_t(ft, div_treatment=div).div_treatment == div
+    with pytest.raises(ValueError):
+        solvers.gw_t(ft, div_treatment="ewald")
     with pytest.raises(capi.CoquiB200Error):
         solvers.gw_t(ft).evaluate(solvers.MBState(), None)
 

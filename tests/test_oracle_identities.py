@@ -143,3 +143,76 @@ def test_hf_gygi_correction(small):
     np.testing.assert_allclose(F1 - F0, -0.37 * S @ Dm @ S, atol=1e-13)
     J1 = O.thc_hf(Dm, *args, exchange=False, div="gygi", madelung=0.37)
     np.testing.assert_allclose(J1, O.thc_hf(Dm, *args, exchange=False), atol=0)
+
+
+def test_smallest_nonzero_q_selects_the_head(small, ft_low):
+    """find_smallest_qabs (g0_div_utils.hpp:263-282) skips q = 0, whose head prefactor
+    |q|^2 Omega / 4 pi vanishes: on a grid of more than one q-point the head is taken at the
+    first smallest nonzero |q| and is not zero."""
+    from coqui_b200.synthetic import kgrid
+    assert O.find_smallest_qabs(kgrid(2)) == 1  # (0, 0, pi) comes before (0, pi, 0)
+    assert O.find_smallest_qabs(kgrid((1, 2, 3))) == 1
+    assert O.find_smallest_qabs(kgrid((3, 1, 1))) == 1
+    assert O.find_smallest_qabs(kgrid(1)) == 0
+    q = np.array([[0, 0, 0], [0.5, 0, 0], [0, 0.3, 0], [0, 0, 0.3]])
+    assert O.find_smallest_qabs(q) == 2
+    s, G = small
+    _, head, eps_tq = O.update_w(G, s.X, s.V, ft_low, s.kpts, s.lattv, s.kp_grid, s.chi_bar)
+    np.testing.assert_array_equal(head, eps_tq[:, 1])
+    assert np.abs(eps_tq[:, 0]).max() == 0.0 and np.abs(head).max() > 0.0
+
+
+def _scaled_grid(n, L):
+    """Gamma-centred grid of an L x L x L cubic cell (lattv = L I)."""
+    from coqui_b200.synthetic import kgrid
+    return kgrid(n) / L, np.eye(3) * L
+
+
+def test_filter_and_extrapolation(ft_low):
+    """filter_qpts / extrapolate_to_q0 / eps_inv_head_t (g0_div_utils.hpp:26-111): distinct
+    |q| within q_max in q order; a quadratic in |q| is extrapolated exactly; the extrapolated
+    head of a q-independent eps is its tau -> w -> tau round trip."""
+    Q, _ = _scaled_grid(4, 10.0)
+    idx = O.filter_qpts(Q, 0.8, 1)
+    norms = np.sqrt((Q[idx] ** 2).sum(axis=1))
+    # distinct as doubles (the reference's std::set<double>): |q| of permuted components can
+    # differ in the last bit and then both are kept
+    assert idx[0] == 1 and len(set(norms.tolist())) == len(idx)
+    assert (norms > 0).all() and (norms <= 0.8).all()
+    assert all(np.isclose(np.sqrt((Q[i] ** 2).sum()), norms).any() for i in range(1, len(Q))
+               if 0 < np.sqrt((Q[i] ** 2).sum()) <= 0.8)
+    idx2d = O.filter_qpts(Q, 0.8, 1, two_dim=True)
+    assert all(Q[i][2] == 0.0 for i in idx2d)
+    q = np.array([0.1, 0.2, 0.35, 0.5])
+    assert abs(O.extrapolate_to_q0(q, 0.3 - 2j + (1 + 1j) * q - 0.7 * q ** 2) - (0.3 - 2j)) < 1e-12
+    nth = ft_low.nt_half
+    a = np.linspace(-0.5, -0.1, nth) + 0j
+    eps = np.repeat(a[:, None], len(Q), axis=1)
+    eps[:, 0] = 0.0  # q = 0: vanishing prefactor
+    head = O.eps_inv_head_t(eps, Q, ft_low, "gygi_extrplt")
+    np.testing.assert_allclose(head, ft_low.w_to_tau_PHsym(ft_low.tau_to_w_PHsym(a)), atol=1e-12)
+    np.testing.assert_array_equal(O.eps_inv_head_t(eps, Q, ft_low, "gygi"), eps[:, 1])
+    # one q-point: ignore_g0 whatever the treatment
+    np.testing.assert_array_equal(O.eps_inv_head_t(eps[:, :1], Q[:1], ft_low, "gygi_extrplt"),
+                                  eps[:, 0])
+    with pytest.raises(ValueError):
+        O.eps_inv_head_t(eps, Q * 100, ft_low, "gygi_extrplt")  # no q within q_max
+
+
+def test_sigma_div_correction_form(small):
+    """Sigma_div_correction: T = X^H diag(conj chi_head) X per k, Delta(t) = f(t_pos) T G T^H,
+    nothing for ignore_g0 or one q-point."""
+    s, G = small
+    rng = np.random.default_rng(9)
+    chi = (rng.standard_normal(s.Np) + 1j * rng.standard_normal(s.Np)) / np.sqrt(s.Np)
+    nth = (G.shape[0] + 1) // 2
+    head = rng.standard_normal(nth) + 0.1j
+    S0 = np.zeros_like(G)
+    D = O.sigma_div_correction(S0, G, s.X, chi, head, 0.6, "gygi")
+    X = s.X[0, 1]
+    T = np.conj(X).T @ np.diag(np.conj(chi)) @ X
+    t = G.shape[0] - 2  # mirrored half: t_pos = 1
+    np.testing.assert_allclose(D[t, 0, 1], -0.6 * head[1].real * T @ G[t, 0, 1] @ np.conj(T).T,
+                               atol=1e-14)
+    assert O.sigma_div_correction(S0, G, s.X, chi, head, 0.6, "ignore_g0") is S0
+    assert O.sigma_div_correction(S0, G, s.X, chi, head, 0.6, "gygi", nq=1) is S0
