@@ -342,6 +342,25 @@ def run_ours(args, rank, world, local):
           "h2d_bytes": int(Dm.nbytes + S_ov.nbytes),
           "d2h_bytes": int(F_hf.nbytes)}
 
+    # the gygi treatment (head at the smallest nonzero |q| and Sigma_div_correction): the
+    # iteration with the correction (it takes the plain path: the head goes through the host)
+    # and the correction's own device time
+    ctx.set_div_treatment("gygi", 0.5, s.chi_bar[0])
+    gy = []
+    for i in range(args.warmup + args.steps):
+        ctx.gw_iteration(None, want_sigma=False)
+        if i >= args.warmup:
+            gy.append(total_ms(ctx))
+    ctx.set_profiling(True)
+    ctx.gw_iteration(None, want_sigma=False)
+    gst = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    ctx.set_div_treatment("ignore_g0")
+    gygi = {"what": "GW iteration with div_treatment gygi (Sigma_div_correction, FP64)",
+            "gw_iteration_ms": float(np.mean(gy)),
+            "correction_ms": float(gst.get("sigma_div", (0.0, 0))[0]),
+            "eps_head_ms": float(gst.get("eps_head", (0.0, 0))[0])}
+
     fp64 = None
     if not args.no_fp64:
         c64 = make_ctx(s, ft, capi.FP64)
@@ -458,6 +477,7 @@ def run_ours(args, rank, world, local):
         "gpu_launches": int(launches),
         "rpa_energy_ms": t_rpa, "E_c": e_c,
         "hartree_fock": hf,
+        "div_gygi": gygi,
         "fp64_form": fp64,
         "phases_ms": phases,
         "steps_ms": [round(t, 3) for t in times],
