@@ -63,7 +63,9 @@ def max_over_ranks(vals, world, device="cuda"):
 
 
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock and the throttle reasons during the timed region (NVML in-process
+    every 10 ms, one sample as the region starts and one as it ends; nvidia-smi when NVML is
+    unavailable)."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -84,19 +86,37 @@ class Clocks:
 
     def _nvml_row(self):
         nv, h = self.nvml
-        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+
+        def q(f, *a):
+            try:
+                return f(h, *a)
+            except Exception:
+                return None
+        bits = q(nv.nvmlDeviceGetCurrentClocksEventReasons)
+        sm = q(nv.nvmlDeviceGetClockInfo, nv.NVML_CLOCK_SM)
+        if bits is None or sm is None:
+            raise RuntimeError("NVML clock query failed")
+        mx = q(nv.nvmlDeviceGetMaxClockInfo, nv.NVML_CLOCK_SM)
+        pw = q(nv.nvmlDeviceGetPowerUsage)
         flags = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
                  nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
-        return ([str(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
-                 str(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
-                 str(nv.nvmlDeviceGetPowerUsage(h) / 1000.0)]
+        return ([str(sm), str(mx) if mx is not None else "", str(pw / 1000.0) if pw else ""]
                 + ["Active" if bits & f else "Not Active" for f in flags])
 
+    def _sample_nvml(self):
+        try:
+            self.rows.append(self._nvml_row())
+            self.src.add("nvml")
+            return True
+        except Exception:
+            self.fails += 1
+            return False
+
     def _run(self):
+        bad = 0
         while self.nvml is not None and not self.stop.is_set():
-            try:
-                self.rows.append(self._nvml_row())
-            except Exception:
+            bad = 0 if self._sample_nvml() else bad + 1
+            if bad >= 5:  # NVML keeps failing: fall back to nvidia-smi
                 self.nvml = None
                 break
             self.stop.wait(0.01)
@@ -107,11 +127,15 @@ class Clocks:
                                      text=True, timeout=5).stdout.strip()
                 if out:
                     self.rows.append([v.strip() for v in out.split(",")])
+                    self.src.add("nvidia-smi")
             except Exception:
                 pass
             self.stop.wait(0.2)
 
     def __enter__(self):
+        self.src, self.fails = set(), 0
+        if self.nvml is not None:
+            self._sample_nvml()  # the state as the timed region starts
         self.t = threading.Thread(target=self._run, daemon=True)
         self.t.start()
         return self
@@ -119,6 +143,8 @@ class Clocks:
     def __exit__(self, *a):
         self.stop.set()
         self.t.join(timeout=10)
+        if self.nvml is not None:
+            self._sample_nvml()  # and as it ends
 
     def summary(self):
         if not self.rows:
@@ -129,7 +155,8 @@ class Clocks:
         reasons = sorted({names[i] for r in self.rows for i in range(4)
                           if len(r) > 3 + i and r[3 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows),
+                "source": sorted(self.src), "failed_queries": self.fails}
 
 
 def make_case(name):

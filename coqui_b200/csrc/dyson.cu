@@ -40,38 +40,50 @@ __global__ void k_zero_upper_adjoint(double2* __restrict__ L, double2* __restric
   }
 }
 
-// E = DH + DH^H + F with only the lower triangle (i >= j) of the Hermitian F computed
-// (32 x 32 tiles through shared memory for the transposed reads)
-__global__ void k_herm_sum(const float2* __restrict__ DH, const float2* __restrict__ F,
-                           float2* __restrict__ E, int64_t Np) {
-  __shared__ float2 tile[32][33];
-  __shared__ float2 ftile[32][33];
-  const int64_t p = blockIdx.z;
+// E = DH + DH^H + F with only the lower triangle (i >= j) of the Hermitian F computed.  One
+// CTA per pair of 32 x 32 tiles (I, J), I >= J: the tiles DH(I, J), DH(J, I) and F(I, J) are
+// loaded in one round, E(I, J) and its adjoint E(J, I) are written (E is Hermitian).
+__global__ void __launch_bounds__(256) k_herm_sum(const float2* __restrict__ DH,
+                                                  const float2* __restrict__ F,
+                                                  float2* __restrict__ E, int64_t Np) {
+  __shared__ float2 a[32][33];  // DH(I, J)
+  __shared__ float2 b[32][33];  // DH(J, I)
+  __shared__ float2 f[32][33];  // F(I, J) on and below the diagonal
+  const int64_t p = blockIdx.y;
+  const int pair = (int)blockIdx.x;  // pair = I (I + 1) / 2 + J
+  int I = (int)((sqrtf(8.f * (float)pair + 1.f) - 1.f) * 0.5f);
+  while ((I + 1) * (I + 2) / 2 <= pair) ++I;
+  while (I > 0 && I * (I + 1) / 2 > pair) --I;
+  const int J = pair - I * (I + 1) / 2;
+  const int64_t i0 = (int64_t)I * 32, j0 = (int64_t)J * 32;
   const float2* d = DH + p * Np * Np;
-  const float2* f = F + p * Np * Np;
-  const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
-  // transposed block: DH[j0 + ty][i0 + tx], F[j0 + ty][i0 + tx] (read only where lower)
-  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
-    const int64_t r = j0 + ty, c = i0 + threadIdx.x;
-    const bool in = r < Np && c < Np;
-    tile[ty][threadIdx.x] = in ? d[r * Np + c] : make_float2(0.f, 0.f);
-    ftile[ty][threadIdx.x] = (in && r >= c) ? f[r * Np + c] : make_float2(0.f, 0.f);
+  const float2* fp = F + p * Np * Np;
+  float2* e = E + p * Np * Np;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const float2 z = make_float2(0.f, 0.f);
+  for (int r = ty; r < 32; r += 8) {
+    const int64_t gi = i0 + r, gj = j0 + tx;  // tile (I, J)
+    const int64_t hi = j0 + r, hj = i0 + tx;  // tile (J, I)
+    const bool in = gi < Np && gj < Np;
+    a[r][tx] = in ? d[gi * Np + gj] : z;
+    b[r][tx] = (hi < Np && hj < Np) ? d[hi * Np + hj] : z;
+    f[r][tx] = (in && gi >= gj) ? fp[gi * Np + gj] : z;
   }
   __syncthreads();
-  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
-    const int64_t i = i0 + ty, j = j0 + threadIdx.x;
-    if (i < Np && j < Np) {
-      const float2 a = d[i * Np + j];
-      const float2 b = tile[threadIdx.x][ty];  // DH[j][i]
-      float2 fv;
-      if (i >= j) {
-        fv = f[i * Np + j];
-      } else {
-        const float2 t = ftile[threadIdx.x][ty];  // F[j][i], lower
-        fv = make_float2(t.x, -t.y);
-      }
-      E[p * Np * Np + i * Np + j] =
-          make_float2(a.x + b.x + fv.x, a.y - b.y + fv.y);
+  for (int r = ty; r < 32; r += 8) {
+    // E[i][j] = DH[i][j] + conj(DH[j][i]) + F[i][j], F[i][j] = conj(F[j][i]) above the diagonal
+    const int64_t gi = i0 + r, gj = j0 + tx;
+    float2 fv = f[r][tx];
+    if (gi < gj) fv = make_float2(f[tx][r].x, -f[tx][r].y);  // diagonal tile only
+    const float2 x = a[r][tx], y = b[tx][r];
+    if (gi < Np && gj < Np) e[gi * Np + gj] = make_float2(x.x + y.x + fv.x, x.y - y.y + fv.y);
+  }
+  if (I != J) {
+    for (int r = ty; r < 32; r += 8) {
+      // E[j0 + r][i0 + tx] = conj(E[i0 + tx][j0 + r])
+      const int64_t gi = j0 + r, gj = i0 + tx;
+      const float2 x = a[tx][r], y = b[r][tx], t = f[tx][r];
+      if (gi < Np && gj < Np) e[gi * Np + gj] = make_float2(x.x + y.x + t.x, -x.y + y.y - t.y);
     }
   }
 }
@@ -332,8 +344,8 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         s3.b_lower = true;     // D lower
         s3.lower_only = true;  // F Hermitian
         tc_cgemm_nt(Z, false, false, Np, NN, Z, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s3);
-        dim3 hb(32, 8), hg((unsigned)((Np + 31) / 32), (unsigned)((Np + 31) / 32), (unsigned)nb);
-        k_herm_sum<<<hg, hb, 0, s>>>(Z, F, E, Np);
+        const int64_t nt32 = (Np + 31) / 32;
+        k_herm_sum<<<dim3((unsigned)(nt32 * (nt32 + 1) / 2), (unsigned)nb), 256, 0, s>>>(Z, F, E, Np);
         count_launch();
         // W is Hermitian: its lower triangle W_ij (j <= i) = sum_{k <= j} T_ik conj(L_jk) needs
         // T = L E only on and below the diagonal tiles, and the upper triangle is its mirror.
