@@ -50,37 +50,15 @@ struct HermProblem {
   int64_t n;
 };
 
-// E = DH + DH^H + F (F lower triangle only) for problems of different sizes; 32 x 32 tiles over
-// the largest edge, tiles outside a problem exit at once
-__global__ void k_herm_sum_grouped(const HermProblem* __restrict__ probs) {
-  __shared__ float2 tile[32][33];
-  __shared__ float2 ftile[32][33];
-  const HermProblem pr = probs[blockIdx.z];
-  const int64_t n = pr.n;
-  const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
-  if (i0 >= n || j0 >= n) return;
-  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
-    const int64_t r = j0 + ty, c = i0 + threadIdx.x;
-    const bool in = r < n && c < n;
-    tile[ty][threadIdx.x] = in ? pr.DH[r * n + c] : make_float2(0.f, 0.f);
-    ftile[ty][threadIdx.x] = (in && r >= c) ? pr.F[r * n + c] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
-    const int64_t i = i0 + ty, j = j0 + threadIdx.x;
-    if (i < n && j < n) {
-      const float2 a = pr.DH[i * n + j];
-      const float2 b = tile[threadIdx.x][ty];  // DH[j][i]
-      float2 fv;
-      if (i >= j) {
-        fv = pr.F[i * n + j];
-      } else {
-        const float2 t = ftile[threadIdx.x][ty];
-        fv = make_float2(t.x, -t.y);
-      }
-      pr.E[i * n + j] = make_float2(a.x + b.x + fv.x, a.y - b.y + fv.y);
-    }
-  }
+// E = DH + DH^H + F (F lower triangle only) for problems of different sizes: one CTA per lower
+// pair of 32 x 32 tiles over the largest edge (problem blockIdx.y); pairs outside a problem
+// exit at once
+__global__ void __launch_bounds__(256) k_herm_sum_grouped(const HermProblem* __restrict__ probs) {
+  const HermProblem pr = probs[blockIdx.y];
+  int I, J;
+  tile_pair((int)blockIdx.x, I, J);
+  if ((int64_t)I * 32 >= pr.n) return;
+  herm_sum_pair(pr.DH, pr.F, pr.E, pr.n, I, J);
 }
 
 #define CQ_SOLVER_CHECK(expr)                                                                   \
@@ -304,7 +282,7 @@ void batch_gw(Batch* b) {
   CQ_CHECK_CUDA(cudaMemcpyAsync(b->htab.p, hp.data(), hp.size() * sizeof(cq::HermProblem),
                                 cudaMemcpyHostToDevice, s));
   const unsigned tiles = (unsigned)((b->nmax + 31) / 32);
-  cq::k_herm_sum_grouped<<<dim3(tiles, tiles, (unsigned)hp.size()), dim3(32, 8), 0, s>>>(
+  cq::k_herm_sum_grouped<<<dim3(tiles * (tiles + 1) / 2, (unsigned)hp.size()), 256, 0, s>>>(
       (const cq::HermProblem*)b->htab.p);
   cq::count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());

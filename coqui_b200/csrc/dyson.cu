@@ -40,52 +40,15 @@ __global__ void k_zero_upper_adjoint(double2* __restrict__ L, double2* __restric
   }
 }
 
-// E = DH + DH^H + F with only the lower triangle (i >= j) of the Hermitian F computed.  One
-// CTA per pair of 32 x 32 tiles (I, J), I >= J: the tiles DH(I, J), DH(J, I) and F(I, J) are
-// loaded in one round, E(I, J) and its adjoint E(J, I) are written (E is Hermitian).
+// E = DH + DH^H + F with only the lower triangle (i >= j) of the Hermitian F computed: one CTA
+// per lower pair of 32 x 32 tiles (E is Hermitian), problem blockIdx.y.
 __global__ void __launch_bounds__(256) k_herm_sum(const float2* __restrict__ DH,
                                                   const float2* __restrict__ F,
                                                   float2* __restrict__ E, int64_t Np) {
-  __shared__ float2 a[32][33];  // DH(I, J)
-  __shared__ float2 b[32][33];  // DH(J, I)
-  __shared__ float2 f[32][33];  // F(I, J) on and below the diagonal
-  const int64_t p = blockIdx.y;
-  const int pair = (int)blockIdx.x;  // pair = I (I + 1) / 2 + J
-  int I = (int)((sqrtf(8.f * (float)pair + 1.f) - 1.f) * 0.5f);
-  while ((I + 1) * (I + 2) / 2 <= pair) ++I;
-  while (I > 0 && I * (I + 1) / 2 > pair) --I;
-  const int J = pair - I * (I + 1) / 2;
-  const int64_t i0 = (int64_t)I * 32, j0 = (int64_t)J * 32;
-  const float2* d = DH + p * Np * Np;
-  const float2* fp = F + p * Np * Np;
-  float2* e = E + p * Np * Np;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const float2 z = make_float2(0.f, 0.f);
-  for (int r = ty; r < 32; r += 8) {
-    const int64_t gi = i0 + r, gj = j0 + tx;  // tile (I, J)
-    const int64_t hi = j0 + r, hj = i0 + tx;  // tile (J, I)
-    const bool in = gi < Np && gj < Np;
-    a[r][tx] = in ? d[gi * Np + gj] : z;
-    b[r][tx] = (hi < Np && hj < Np) ? d[hi * Np + hj] : z;
-    f[r][tx] = (in && gi >= gj) ? fp[gi * Np + gj] : z;
-  }
-  __syncthreads();
-  for (int r = ty; r < 32; r += 8) {
-    // E[i][j] = DH[i][j] + conj(DH[j][i]) + F[i][j], F[i][j] = conj(F[j][i]) above the diagonal
-    const int64_t gi = i0 + r, gj = j0 + tx;
-    float2 fv = f[r][tx];
-    if (gi < gj) fv = make_float2(f[tx][r].x, -f[tx][r].y);  // diagonal tile only
-    const float2 x = a[r][tx], y = b[tx][r];
-    if (gi < Np && gj < Np) e[gi * Np + gj] = make_float2(x.x + y.x + fv.x, x.y - y.y + fv.y);
-  }
-  if (I != J) {
-    for (int r = ty; r < 32; r += 8) {
-      // E[j0 + r][i0 + tx] = conj(E[i0 + tx][j0 + r])
-      const int64_t gi = j0 + r, gj = i0 + tx;
-      const float2 x = a[tx][r], y = b[r][tx], t = f[tx][r];
-      if (gi < Np && gj < Np) e[gi * Np + gj] = make_float2(x.x + y.x + t.x, -x.y + y.y - t.y);
-    }
-  }
+  int I, J;
+  tile_pair((int)blockIdx.x, I, J);
+  const int64_t off = (int64_t)blockIdx.y * Np * Np;
+  herm_sum_pair(DH + off, F + off, E + off, Np, I, J);
 }
 
 // Hermitian completion: A[i][j] = conj(A[j][i]) for j > i (32 x 32 tiles on or above the
