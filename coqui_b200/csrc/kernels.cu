@@ -56,6 +56,41 @@ void upload_twiddles() {
   if (dev < 32) done_mask |= 1 << dev;
 }
 
+// sign i a (sign = +1 or -1)
+template <typename C>
+__device__ __forceinline__ C mul_si(C a, int sign) {
+  C r;
+  if (sign > 0) {
+    r.x = -a.y;
+    r.y = a.x;
+  } else {
+    r.x = a.y;
+    r.y = -a.x;
+  }
+  return r;
+}
+
+// 3-point DFT in place (Winograd's form: 12 real additions, 4 real multiplications):
+// y0 = x0 + (x1 + x2), y1,2 = x0 - (x1 + x2)/2 +- sign i (sqrt(3)/2) (x1 - x2)
+template <typename C>
+__device__ __forceinline__ void dft3pt(C& x0, C& x1, C& x2, int sign) {
+  using R = decltype(x0.x);
+  const R h = R(0.5), s3 = R(0.86602540378443864676);
+  const C t1 = cadd(x1, x2), d = csub(x1, x2);
+  C t2, t3;
+  t2.x = x0.x - h * t1.x;
+  t2.y = x0.y - h * t1.y;
+  t3.x = s3 * d.x;
+  t3.y = s3 * d.y;
+  const C u = mul_si(t3, sign);
+  x0 = cadd(x0, t1);
+  x1 = cadd(t2, u);
+  x2 = csub(t2, u);
+}
+
+// y_j = sum_m x_m exp(sign 2 pi i j m / N), in place.  N = 2, 3, 4, 6, 8 in closed form
+// (N = 6 as Good-Thomas 2 x 3: input n = (3 n1 + 2 n2) mod 6, output k = (3 k1 + 4 k2) mod 6,
+// no twiddles; N = 8 as radix 2 over two 4-point transforms); N = 5, 7 as the plain sum.
 template <typename C, int N>
 __device__ __forceinline__ void dft_line(C (&x)[N], int sign) {
   if constexpr (N == 1) {
@@ -64,16 +99,47 @@ __device__ __forceinline__ void dft_line(C (&x)[N], int sign) {
     C a = x[0], b = x[1];
     x[0] = cadd(a, b);
     x[1] = csub(a, b);
+  } else if constexpr (N == 3) {
+    dft3pt(x[0], x[1], x[2], sign);
   } else if constexpr (N == 4) {
     C a0 = cadd(x[0], x[2]), a1 = csub(x[0], x[2]);
     C b0 = cadd(x[1], x[3]), b1 = csub(x[1], x[3]);
-    C b1w;  // b1 * exp(sign i pi / 2)
-    if (sign > 0) { b1w.x = -b1.y; b1w.y = b1.x; }
-    else { b1w.x = b1.y; b1w.y = -b1.x; }
+    const C b1w = mul_si(b1, sign);  // b1 * exp(sign i pi / 2)
     x[0] = cadd(a0, b0);
     x[2] = csub(a0, b0);
     x[1] = cadd(a1, b1w);
     x[3] = csub(a1, b1w);
+  } else if constexpr (N == 6) {
+    C a0 = x[0], a1 = x[2], a2 = x[4];  // n1 = 0: n = 0, 2, 4
+    C b0 = x[3], b1 = x[5], b2 = x[1];  // n1 = 1: n = 3, 5, 1
+    dft3pt(a0, a1, a2, sign);
+    dft3pt(b0, b1, b2, sign);
+    x[0] = cadd(a0, b0);  // (k1, k2) = (0, 0)
+    x[3] = csub(a0, b0);  // (1, 0)
+    x[4] = cadd(a1, b1);  // (0, 1)
+    x[1] = csub(a1, b1);  // (1, 1)
+    x[2] = cadd(a2, b2);  // (0, 2)
+    x[5] = csub(a2, b2);  // (1, 2)
+  } else if constexpr (N == 8) {
+    using R = decltype(x[0].x);
+    const R h = R(0.70710678118654752440);
+    C e[4] = {x[0], x[2], x[4], x[6]}, o[4] = {x[1], x[3], x[5], x[7]};
+    dft_line<C, 4>(e, sign);
+    dft_line<C, 4>(o, sign);
+    // o[k] exp(sign 2 pi i k / 8): k = 1: (1 + sign i)/sqrt2, 2: sign i, 3: (-1 + sign i)/sqrt2
+    const R sg = sign > 0 ? R(1) : R(-1);
+    C w[4];
+    w[0] = o[0];
+    w[1].x = h * (o[1].x - sg * o[1].y);
+    w[1].y = h * (o[1].y + sg * o[1].x);
+    w[2] = mul_si(o[2], sign);
+    w[3].x = h * (-o[3].x - sg * o[3].y);
+    w[3].y = h * (-o[3].y + sg * o[3].x);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      x[k] = cadd(e[k], w[k]);
+      x[k + 4] = csub(e[k], w[k]);
+    }
   } else {
     C y[N];
 #pragma unroll

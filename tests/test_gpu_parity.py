@@ -127,7 +127,11 @@ def test_rpa_energy(base, mode, tol):
 @pytest.mark.parametrize("grid,nb,nocc,Np,lam", [
     (1, 12, 6, 40, 1e4),          # Gamma only: no DFT
     ((1, 2, 3), 10, 5, 50, 1e5),  # non-cubic grid, odd nt (61), Np not a multiple of 32
-    (3, 8, 4, 36, 1e4),           # 27 k-points (generic radix-3 DFT)
+    (3, 8, 4, 36, 1e4),           # 27 k-points (3-point DFT lines)
+    ((2, 1, 6), 8, 4, 24, 1e4),   # 6-point lines (Good-Thomas 2 x 3) on the inner edge
+    (6, 4, 2, 16, 1e4),           # 216 k-points: the compile-time cubic edge 6
+    ((2, 8, 2), 6, 3, 20, 1e4),   # 8-point lines (radix 2) on the middle edge
+    ((1, 5, 7), 6, 3, 20, 1e4),   # 5- and 7-point lines (plain sums)
 ])
 def test_edge_cases(mode, tol, grid, nb, nocc, Np, lam):
     cs = Case(grid, nb, nocc, Np, lam=lam, seed=11)
