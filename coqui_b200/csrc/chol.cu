@@ -4,9 +4,12 @@
 //   A = C C^H (C lower, FP64), logdet = 2 sum_i ln C_ii, trace = sum_i M_ii,
 //   optional DH = C^{-H} - I (upper triangular, FP64) for W = L (D + D^H + D^H D) L^H.
 //
-// Right-looking blocked algorithm (chol_blk.cuh): the diagonal block is factored and
-// inverted in shared memory, the panel below is L_ib = A_ib C_jj^{-H}, the trailing lower
-// triangle gets A_ik -= L_ij L_kj^H.  The inverse is formed block column by block column:
+// Blocked algorithm (chol_blk.cuh), by default in left-looking order: block column j is
+// A_ij - sum_{k<j} L_ik L_jk^H formed from I - M and the finished columns, the diagonal block
+// is factored and inverted in shared memory and the panel below is L_ib = (...) C_jj^{-H}.
+// COQUI_B200_CHOL_ORDER=right selects the right-looking order (the trailing lower triangle
+// gets A_ik -= L_ij L_kj^H after every column), which subtracts the same products in the same
+// order and gives identical results with more memory traffic.  The inverse is formed block column by block column:
 // X_ij = -C_ii^{-1} sum_{k=j}^{i-1} C_ik X_kj.  The 32 x 32 block products run on the FP64
 // tensor cores (mma.sync m8n8k4, four real products per complex one; each of the two warps
 // holds a 16 x 32 accumulator as 8 x 8 fragments), operands staged in shared memory; the
@@ -52,14 +55,19 @@ static_assert(!DMMA || (CB == 32 && CT == 64), "DMMA tiles: 32-blocks, two warps
 }  // namespace b32
 
 // Problems of different sizes in one launch (one CTA each, 32-blocks).
+template <bool LEFT>
 __global__ void __launch_bounds__(b32::CT, b32::MINB) k_chol_inv_grouped(const CholProblem* __restrict__ probs,
                                                                  double* __restrict__ logdet,
                                                                  double2* __restrict__ trace,
                                                                  int* __restrict__ info,
                                                                  int inv_group) {
   const CholProblem pr = probs[blockIdx.x];
-  b32::chol_inv_problem<true>(pr.M, pr.A, logdet + blockIdx.x, trace + blockIdx.x,
-                              info + blockIdx.x, pr.n, inv_group);
+  if constexpr (LEFT)
+    b32::chol_inv_problem_left<true>(pr.M, pr.A, logdet + blockIdx.x, trace + blockIdx.x,
+                                     info + blockIdx.x, pr.n, inv_group);
+  else
+    b32::chol_inv_problem<true>(pr.M, pr.A, logdet + blockIdx.x, trace + blockIdx.x,
+                                info + blockIdx.x, pr.n, inv_group);
 }
 
 // ---- tiled factorisation (several CTAs per problem) ----
@@ -189,6 +197,12 @@ void run_tiled(const CholProblem* t, const TiledRuns& R, int64_t np, double* log
   go(3, 0);
 }
 
+// Block order of the one-CTA factorisation: left-looking unless COQUI_B200_CHOL_ORDER=right.
+bool chol_left_looking() {
+  const char* v = std::getenv("COQUI_B200_CHOL_ORDER");
+  return !(v && v[0] == 'r');
+}
+
 // k_chol_inv<INV> of the block size chosen for n; the inverse is formed within diagonal groups
 // of inv_cols columns (a multiple of 64).
 template <bool INV>
@@ -202,7 +216,10 @@ void launch_factor(const float2* M, double2* A, double* logdet, double2* trace, 
     count_launch();
     CQ_CHECK_CUDA(cudaGetLastError());
   };
-  go(b32::k_chol_inv<INV>, b32::CB, b32::CT, b32::PITCH);
+  if (chol_left_looking())
+    go(b32::k_chol_inv_left<INV>, b32::CB, b32::CT, b32::PITCH);
+  else
+    go(b32::k_chol_inv<INV>, b32::CB, b32::CT, b32::PITCH);
 }
 
 // grouped Z = X^H - I, blockIdx.y = problem
@@ -438,14 +455,15 @@ void launch_chol_inv_grouped(const std::vector<CholProblem>& probs, DevBuf<unsig
   for (const auto& p : probs) nmax = std::max(nmax, p.n);
   const unsigned gx = (unsigned)std::min<int64_t>((nmax * nmax + 255) / 256, 1024);
   const size_t smem = (size_t)2 * b32::CB * b32::PITCH * sizeof(double2);
-  static bool set = false;
-  if (!set) {
-    CQ_CHECK_CUDA(cudaFuncSetAttribute(k_chol_inv_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-    set = true;
-  }
   const int inv_group = group_inverse ? (int)(kInvGroup / b32::CB) : (1 << 30);
-  k_chol_inv_grouped<<<(unsigned)np, b32::CT, smem, s>>>(t, logdet, trace, info, inv_group);
+  auto go = [&](auto kern) {
+    CQ_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)np, b32::CT, smem, s>>>(t, logdet, trace, info, inv_group);
+  };
+  if (chol_left_looking())
+    go(k_chol_inv_grouped<true>);
+  else
+    go(k_chol_inv_grouped<false>);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
   if (group_inverse) return;

@@ -552,6 +552,128 @@ __device__ __forceinline__ void chol_inv_problem(const float2* __restrict__ M,
   }
 }
 
+// The same factorisation in left-looking (Crout) order: block column j is formed from I - M
+// and the finished columns kb < j, A_ij - sum_kb L_ib,kb L_j,kb^H, so each block of M is read
+// once and each block of C written once (the right-looking order above reads and rewrites the
+// trailing lower triangle after every column).  Both staging blocks hold the two panel blocks
+// of a product; C_jj^{-1} is reloaded from the upper triangle of the diagonal block, where
+// C_jj^{-H} is kept.  Every block starts from I - M and has the same block products
+// subtracted in the same order (kb = 0, 1, ...) in FP64 as in the right-looking order, which
+// keeps the running sums in global memory: the results are identical.
+template <bool INV>
+__device__ __forceinline__ void chol_inv_problem_left(const float2* __restrict__ M,
+                                                      double2* __restrict__ A,
+                                                      double* __restrict__ logdet,
+                                                      double2* __restrict__ trace,
+                                                      int* __restrict__ info, int64_t n,
+                                                      int inv_group) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* S0 = reinterpret_cast<double2*>(smem_raw);
+  double2* S1 = S0 + CB * PITCH;
+  __shared__ double s_ld;
+  __shared__ int s_bad;
+  __shared__ double s_red[2][CT];
+  const int nblk = (int)((n + CB - 1) / CB);
+
+  if (threadIdx.x == 0) {
+    s_ld = 0.0;
+    s_bad = 0;
+  }
+  double tr = 0, ti = 0;
+  for (int64_t i = threadIdx.x; i < n; i += CT) {
+    const float2 m = M[i * n + i];
+    tr += m.x;
+    ti += m.y;
+  }
+  s_red[0][threadIdx.x] = tr;
+  s_red[1][threadIdx.x] = ti;
+  __syncthreads();
+
+  for (int j = 0; j < nblk; ++j) {
+    const int64_t j0 = (int64_t)j * CB;
+    const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+    // 1. diagonal block: (I - M)_jj - sum_kb L_j,kb L_j,kb^H, factor, invert
+    double2 acc[AR][AC];
+    acc_init(acc, A, M, true, n, j0, j0, jb, jb, false);
+    for (int kb = 0; kb < j; ++kb) {  // blocks kb < j are full
+      load_blk(S0, A, n, j0, (int64_t)kb * CB, jb, CB);
+      __syncthreads();
+      mma_tile_sub(S0, S0, CB, acc);
+      __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < AR; ++i)
+#pragma unroll
+      for (int jj = 0; jj < AC; ++jj) S0[acc_row(i, jj) * PITCH + acc_col(i, jj)] = acc[i][jj];
+    __syncthreads();
+    factor_diag(S0, jb, &s_ld, &s_bad);
+    invert_lower(S0, S1, jb);
+    store_blk_adjU(S1, A, n, j0, jb);  // C_jj^{-H} in the upper triangle
+    __syncthreads();
+    // 2. panel: L_ib,j = [(I - M)_ib,j - sum_kb L_ib,kb L_j,kb^H] C_jj^{-H}
+    for (int ib = j + 1; ib < nblk; ++ib) {
+      const int64_t i0 = (int64_t)ib * CB;
+      const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+      acc_init(acc, A, M, true, n, i0, j0, rb, jb, true);
+      for (int kb = 0; kb < j; ++kb) {
+        const int64_t k0 = (int64_t)kb * CB;
+        load_blk(S0, A, n, i0, k0, rb, CB);
+        load_blk(S1, A, n, j0, k0, jb, CB);
+        __syncthreads();
+        mma_tile_sub(S0, S1, CB, acc);
+        __syncthreads();
+      }
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int jj = 0; jj < AC; ++jj) S0[acc_row(i, jj) * PITCH + acc_col(i, jj)] = acc[i][jj];
+      load_blk_adjU(S1, A, n, j0, jb);  // C_jj^{-1}
+      __syncthreads();
+      double2 l[AR][AC];
+      zero_acc(l);
+      mma_tile<true>(S0, S1, jb, l);
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int jj = 0; jj < AC; ++jj) {
+          const int r = acc_row(i, jj), c = acc_col(i, jj);
+          if (r < rb && c < jb) A[(i0 + r) * n + j0 + c] = l[i][jj];
+        }
+      __syncthreads();
+    }
+  }
+
+  if (INV) {
+    for (int j = 0; j < nblk; ++j)
+      inverse_column(A, n, j, min(nblk, (j / inv_group + 1) * inv_group), S0, S1);
+  }
+
+  for (int w = CT / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s_red[0][threadIdx.x] += s_red[0][threadIdx.x + w];
+      s_red[1][threadIdx.x] += s_red[1][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *logdet = 2.0 * s_ld;
+    *trace = make_double2(s_red[0][0], s_red[1][0]);
+    *info = s_bad;
+  }
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(CT, MINB) k_chol_inv_left(const float2* __restrict__ Mall,
+                                                         double2* __restrict__ Aall,
+                                                         double* __restrict__ logdet,
+                                                         double2* __restrict__ trace,
+                                                         int* __restrict__ info, int64_t n,
+                                                         int inv_group) {
+  const int64_t p = blockIdx.x;
+  chol_inv_problem_left<INV>(Mall + p * n * n, Aall + p * n * n, logdet + p, trace + p, info + p,
+                             n, inv_group);
+}
+
 template <bool INV>
 __global__ void __launch_bounds__(CT, MINB) k_chol_inv(const float2* __restrict__ Mall,
                                                     double2* __restrict__ Aall,
