@@ -978,36 +978,53 @@ void launch_logdet_trace(const double2* C, const cplx_t<R>* M, double* logdet, d
   CQ_LAUNCHED();
 }
 
+// eps[t q] = fac[q] sum_PQ chi_P W_PQ conj(chi_Q) for one (t, q) matrix per CTA: each warp
+// takes rows P, its lanes sweep Q (coalesced rows of W), t_P = sum_Q W_PQ conj(chi_Q) is
+// formed per lane and multiplied by chi_P once per row; FP64 accumulation.
 template <typename R>
-__global__ void k_eps_head(const cplx_t<R>* __restrict__ W, const double2* __restrict__ chi,
-                           const double* __restrict__ fac, double2* __restrict__ eps, int64_t nq,
-                           int64_t Np) {
+__global__ void __launch_bounds__(256) k_eps_head(const cplx_t<R>* __restrict__ W,
+                                                  const double2* __restrict__ chi,
+                                                  const double* __restrict__ fac,
+                                                  double2* __restrict__ eps, int64_t nq,
+                                                  int64_t Np) {
   const int64_t tq = blockIdx.x;  // t * nq + q
   const int64_t q = tq % nq;
   const cplx_t<R>* w = W + tq * Np * Np;
   const double2* x = chi + q * Np;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   double ar = 0, ai = 0;
-  for (int64_t i = threadIdx.x; i < Np * Np; i += blockDim.x) {
-    const int64_t P = i / Np, Q = i % Np;
-    const cplx_t<R> v = w[i];
-    // chi_P * W_PQ * conj(chi_Q)
-    const double2 a = x[P], b = x[Q];
-    const double pr = a.x * v.x - a.y * v.y, pi = a.x * v.y + a.y * v.x;
-    ar += pr * b.x + pi * b.y;
-    ai += pi * b.x - pr * b.y;
-  }
-  __shared__ double s0[256], s1[256];
-  s0[threadIdx.x] = ar;
-  s1[threadIdx.x] = ai;
-  __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-    if (threadIdx.x < k) {
-      s0[threadIdx.x] += s0[threadIdx.x + k];
-      s1[threadIdx.x] += s1[threadIdx.x + k];
+  for (int64_t P = warp; P < Np; P += nwarp) {
+    const cplx_t<R>* row = w + P * Np;
+    double tr = 0, ti = 0;
+#pragma unroll 4
+    for (int64_t Q = lane; Q < Np; Q += 32) {
+      const cplx_t<R> v = row[Q];
+      const double2 b = __ldg(x + Q);
+      tr += (double)v.x * b.x + (double)v.y * b.y;  // v conj(b)
+      ti += (double)v.y * b.x - (double)v.x * b.y;
     }
-    __syncthreads();
+    const double2 a = __ldg(x + P);
+    ar += a.x * tr - a.y * ti;
+    ai += a.x * ti + a.y * tr;
   }
-  if (threadIdx.x == 0) eps[tq] = make_double2(fac[q] * s0[0], fac[q] * s1[0]);
+  for (int o = 16; o > 0; o >>= 1) {
+    ar += __shfl_down_sync(0xffffffffu, ar, o);
+    ai += __shfl_down_sync(0xffffffffu, ai, o);
+  }
+  __shared__ double s0[8], s1[8];
+  if (lane == 0) {
+    s0[warp] = ar;
+    s1[warp] = ai;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0, i = 0;
+    for (int k = 0; k < nwarp; ++k) {
+      r += s0[k];
+      i += s1[k];
+    }
+    eps[tq] = make_double2(fac[q] * r, fac[q] * i);
+  }
 }
 template <typename R>
 void launch_eps_head(const cplx_t<R>* W, const double2* chi, const double* fac, double2* eps,
