@@ -108,7 +108,11 @@ COQUI_B200_API int coqui_b200_eval_pi(coqui_b200_ctx* ctx, const double* G_tskij
 COQUI_B200_API int coqui_b200_update_w(coqui_b200_ctx* ctx, const double* G_tskij, double* dW_qtPQ,
                         double* eps_inv_head);
 
-/* Self-energy from G and the device-resident W of the last update_w (or set_w). */
+/* Self-energy from G and the device-resident W of the last update_w (or set_w).
+   G_tskij == NULL (here and in eval_pi, update_w, rpa_energy, gw_iteration) reuses the G that
+   the previous call of this context left on the device; after update_w of that G the
+   self-energy then also reuses the auxiliary-basis G(tau) that the polarizability formed,
+   instead of copying G in and projecting it again. */
 COQUI_B200_API int coqui_b200_eval_sigma(coqui_b200_ctx* ctx, const double* G_tskij, double* Sigma_tskij);
 
 /* Upload a screened interaction dW_qtPQ (nq, nt_half, Np, Np) for eval_sigma. */
