@@ -1,8 +1,9 @@
 """FP64 CPU oracle for the THC-RPA/GW imaginary-time path -- TEST INFRASTRUCTURE ONLY.
 
 This module restates, in numpy complex128, the CoQui reference algorithm for the
-polarizability, the screened interaction, the GW self-energy, the RPA correlation energy
-and the scGW loop pieces.  It is the checker for the CUDA path: only tests, the smoke
+polarizability, the screened interaction, the GW self-energy, the RPA correlation energy,
+the long-wavelength treatments of the dielectric head and of the self-energy, THC
+Hartree-Fock, and the scGW loop pieces.  It is the checker for the CUDA path: only tests, the smoke
 check and the benchmark's CPU-baseline leg may import it.  Nothing in the product path
 calls it.
 
@@ -15,9 +16,10 @@ Conventions kept from the reference:
 * complex values are complex128.
 
 Parity pin: the IR transforms and G0 are checked against the reference's own fixtures
-(tests/golden); Pi, W, Sigma and E_c have no reference golden vectors on synthetic THC
-inputs (the reference cannot be built here), so they are pinned by this restatement and
-by internal identities (LU vs Cholesky Dyson forms, dense DFT vs FFT).
+(tests/golden); Pi, W, Sigma, E_c and Hartree-Fock have no reference golden vectors on
+synthetic THC inputs (the reference cannot be built here), so they are pinned by this
+restatement and by internal identities (LU vs Cholesky Dyson forms, dense DFT vs FFT, the
+exchange as a k-convolution and, at one k-point, as the explicit four-index contraction).
 """
 from __future__ import annotations
 
