@@ -149,3 +149,25 @@ def test_pinned_host_buffer_iteration_runs_as_a_graph(case):
     for S in outs:
         assert np.array_equal(S, S_direct)
     c.close()
+
+
+def test_rpa_energy_graph_matches_direct_launches(case):
+    """In mixed mode the RPA energy of a resident or page-locked G runs as a CUDA graph
+    (captured on the first of consecutive calls with the same G argument, replayed by the
+    next): the same energy as the directly launched call on a pageable G."""
+    import torch
+
+    c = make_ctx(case, capi.MIXED)
+    e0 = c.rpa_energy(np.ascontiguousarray(case["G"]))  # pageable: launched directly
+    assert abs(e0 - case["e_rpa"]) < 1e-6
+    G_pinned = torch.from_numpy(np.ascontiguousarray(case["G"])).pin_memory().numpy()
+    energies = [c.rpa_energy(G_pinned), c.rpa_energy(G_pinned),  # capture (copy inside), replay
+                c.rpa_energy(None), c.rpa_energy(None)]          # resident G: capture, replay
+    for e in energies:
+        assert abs(e - e0) < 1e-12, (e, e0)
+    names = [n for n, _ in c.timings()]
+    assert names == ["RPA_GRAPH"], names
+    # a GW iteration between two RPA calls: the RPA graph is captured again, same energy
+    c.gw_iteration(None, want_sigma=False)
+    assert abs(c.rpa_energy(None) - e0) < 1e-12
+    c.close()
