@@ -113,3 +113,26 @@ def test_learned_features_of_a_geometric_sequence():
     np.testing.assert_allclose(tgt, rho / (1 - rho), rtol=1e-12)
     Xd, Td = learned.dataset([np.concatenate([hist, s_inf[None]])], max_samples=10)
     assert Xd.shape == (2, 4) and Td.shape == (2, 2)
+
+
+def test_bench_clock_record_reports_reasons_and_median():
+    """The bench's clock record (used to accept or reject a timed region): median SM clock,
+    the highest maximum clock, and every throttle reason seen active in any sample; rows
+    without a power reading or maximum clock still count."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+
+    clk = bench.Clocks(0)
+    clk.src, clk.fails = {"nvml"}, 0
+    na, act = "Not Active", "Active"
+    clk.rows = [["1905", "1965", "812.5", na, na, na, act],
+                ["1890", "1965", "", na, na, na, na],
+                ["1920", "", "799.0", na, act, na, na]]
+    s = clk.summary()
+    assert s["sm_mhz"] == 1905.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]
+    assert s["samples"] == 3 and s["source"] == ["nvml"] and s["failed_queries"] == 0
+    empty = bench.Clocks(0)
+    assert empty.summary()["reasons"] == ["unsampled"]
