@@ -78,6 +78,19 @@ void set_msg(char* buf, int len, const char* msg) {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// a * b * c * elem bytes, or false when that exceeds `limit`.  Each factor is compared with
+// the limit divided by the product so far, so no multiplication can wrap around.
+bool bytes_within(size_t a, size_t b, size_t c, size_t elem, size_t limit, size_t* out) {
+  size_t room = limit / elem;
+  if (a > room) return false;
+  room /= a;
+  if (b > room) return false;
+  room /= b;
+  if (c > room) return false;
+  *out = a * b * c * elem;
+  return true;
+}
+
 }  // namespace
 }  // namespace cq
 
@@ -90,15 +103,26 @@ extern "C" COQUI_B200_API int coqui_b200_primary_to_aux_noalloc(
     set_msg(errbuf, errlen, "nk, Np and nb must be positive");
     return COQUI_B200_EINVAL;
   }
-  const size_t bytes_xs = align256((size_t)nk * Np * nb * sizeof(float4));
-  const size_t bytes_t = align256((size_t)nk * Np * nb * sizeof(float2));
-  const size_t bytes_gt = align256((size_t)nk * nb * nb * sizeof(float2));
-  const size_t need = bytes_xs + bytes_t + bytes_gt;
-  if (need > kNoAllocScratchBytes) {
-    char m[192];
-    std::snprintf(m, sizeof(m),
-                  "problem needs %zu bytes of scratch; the static limit is %zu bytes (32 MiB)",
-                  need, kNoAllocScratchBytes);
+  // Every size is checked against the limit before it is formed (no wrap-around for huge
+  // dimensions); each part is at most the limit, so their aligned sum cannot wrap either.
+  size_t raw_xs = 0, raw_t = 0, raw_gt = 0;
+  const size_t lim = kNoAllocScratchBytes;
+  const bool fits = bytes_within(nk, Np, nb, sizeof(float4), lim, &raw_xs) &&
+                    bytes_within(nk, Np, nb, sizeof(float2), lim, &raw_t) &&
+                    bytes_within(nk, nb, nb, sizeof(float2), lim, &raw_gt);
+  const size_t bytes_xs = align256(raw_xs), bytes_t = align256(raw_t),
+               bytes_gt = align256(raw_gt);
+  if (!fits || bytes_xs + bytes_t + bytes_gt > lim) {
+    char m[224];
+    if (fits)
+      std::snprintf(m, sizeof(m),
+                    "problem needs %zu bytes of scratch; the static limit is %zu bytes (32 MiB)",
+                    bytes_xs + bytes_t + bytes_gt, lim);
+    else
+      std::snprintf(m, sizeof(m),
+                    "problem (nk %lld, Np %lld, nb %lld) exceeds the static limit of %zu bytes "
+                    "(32 MiB) of scratch",
+                    (long long)nk, (long long)Np, (long long)nb, lim);
     set_msg(errbuf, errlen, m);
     return COQUI_B200_EINVAL;
   }

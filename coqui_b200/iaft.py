@@ -31,7 +31,7 @@ class IAFT:
         self.wmax = lam / beta
         path = os.path.join(IR_DIR, f"{tag}.{PREC_FILE[prec]}.npz")
         if not os.path.exists(path):
-            raise FileNotFoundError(f"IR table {path} not shipped; convert it with convert_ir_tables.py")
+            raise FileNotFoundError(f"IR table {path} not shipped; convert it with tests/golden/convert_ir_tables.py")
         d = np.load(path)
         self.nt_f, self.nw_f, self.nw_b = int(d["nt_f"]), int(d["nw_f"]), int(d["nw_b"])
         self.tau_mesh_x = d["tau_mesh_f"]

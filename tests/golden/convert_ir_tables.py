@@ -2,13 +2,13 @@
 
 The reference reads ``src/numerics/imag_axes_ft/ir/data/{lambda}.{eps}.h5`` at run time
 (``src/numerics/imag_axes_ft/ir/ir_driver.hpp:41-66``).  This package ships the same
-numbers as ``{lambda}.{eps}.npz`` beside this script so that no HDF5 library is needed
+numbers as ``coqui_b200/ir_data/{lambda}.{eps}.npz`` (written by this script) so that no HDF5 library is needed
 where the GPU path runs.  The tables are copied value for value (dimensionless, before
 the beta rescaling that ``IAFT`` applies, ``ir_driver.hpp:68-73``).
 
 Usage::
 
-    python coqui_b200/ir_data/convert_ir_tables.py <reference-ir-data-dir> [names...]
+    python tests/golden/convert_ir_tables.py <reference-ir-data-dir> [names...]
 
 ``names`` default to the grids the benchmark and test workloads use.
 """
@@ -19,8 +19,9 @@ import sys
 
 import numpy as np
 
-sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-from h5lite import as_complex, read_h5  # noqa: E402
+ROOT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..")
+sys.path.insert(0, ROOT)
+from coqui_b200.h5lite import as_complex, read_h5  # noqa: E402
 
 DEFAULT_NAMES = ["1e4.1e-06", "1e4.1e-10", "1e4.1e-15", "1e5.1e-06", "1e5.1e-15", "1e3.1e-06"]
 
@@ -53,7 +54,7 @@ def main(argv):
         return 2
     src = argv[1]
     names = argv[2:] or DEFAULT_NAMES
-    out_dir = os.path.dirname(os.path.abspath(__file__))
+    out_dir = os.path.join(ROOT, "coqui_b200", "ir_data")
     for n in names:
         print(convert(src, n, out_dir))
     return 0

@@ -24,8 +24,8 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.join(HERE, "..", "..", "coqui_b200", "ir_data"))
-from h5lite import as_complex, read_h5  # noqa: E402
+sys.path.insert(0, os.path.join(HERE, "..", ".."))
+from coqui_b200.h5lite import as_complex, read_h5  # noqa: E402
 
 KEEP_K = [0, 3]
 

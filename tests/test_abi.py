@@ -62,3 +62,12 @@ def test_tile_configuration_pinning_validates_its_argument(lib):
         capi.set_tile_config(-2)
     capi.set_tile_config(n - 1)
     capi.set_tile_config(-1)
+
+
+def test_noalloc_rejects_wrapping_shapes_before_any_device_work(lib):
+    """Dimensions whose byte counts would wrap around a 64-bit size are rejected by the
+    argument check (EINVAL), which runs before the library touches the device."""
+    for nk, Np, nb in ((1, 1 << 61, 1), (1 << 40, 1 << 40, 1), (1, 1, 1 << 62), (3, 1 << 62, 5)):
+        with pytest.raises(capi.CoquiB200Error) as e:
+            capi.primary_to_aux_noalloc(1, 1, 1, nk, Np, nb)
+        assert e.value.code == -1 and "static limit" in str(e.value)

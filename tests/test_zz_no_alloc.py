@@ -35,13 +35,20 @@ def test_noalloc_projection_matches_context_projection_twice():
     dev = torch.device("cuda", 0)
     X_d = torch.from_numpy(np.ascontiguousarray(s.X[0])).to(dev)
     out = torch.empty((s.nk, s.Np, s.Np), dtype=torch.complex64, device=dev)
+    free_after = []
     for i, t in enumerate(taus):  # two calls in a row share the static scratch array
         G_d = torch.from_numpy(np.ascontiguousarray(G[t, 0])).to(dev)
         torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         capi.primary_to_aux_noalloc(X_d.data_ptr(), G_d.data_ptr(), out.data_ptr(), s.nk, s.Np,
                                     s.nb)
+        torch.cuda.synchronize()
+        free_after.append((free_before, torch.cuda.mem_get_info(dev)[0]))
         got = out.cpu().numpy().astype(np.complex128)
         assert float(np.abs(got - ref[i, 0]).max()) < TOL
+    # the first call may load the library's device code (and with it the static array);
+    # from then on a call leaves the device's free memory exactly as it found it
+    assert free_after[1][0] == free_after[1][1]
     c.close()
 
 
