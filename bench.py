@@ -1,15 +1,20 @@
 """Benchmark: THC-GW iteration time (and RPA E_c time) on one B200, mixed vs FP64.
 
-One step = one THC-GW iteration of the G0W0 workload
-``g0w0_k4_nb64_np512`` (4x4x4 k-grid = 64 k, 64 orbitals / 24 occupied, N_mu = 512,
-beta = 1000, IR Lambda = 1e4 "low" -> 48 tau points): Pi(tau) -> Pi(iW) -> Dyson W(iW) ->
-W(tau) -> Sigma(tau), i.e. scr_coulomb_t::update_w + gw_t::evaluate.
+One step = one THC-GW iteration of the RPA + GW workload ``rpa_gw_k6_nb96_np1024``
+(6x6x6 k-grid = 216 k, 96 orbitals / 48 occupied, N_mu = 1024, beta = 1000, IR
+Lambda = 1e5 "low" -> 61 tau points, 6,696 (q, iW) Dyson problems): Pi(tau) -> Pi(iW) ->
+Dyson W(iW) -> W(tau) -> Sigma(tau), i.e. scr_coulomb_t::update_w + gw_t::evaluate.  It is
+the largest of the reference-shaped configurations and fits one B200 (Pi/W as complex64,
+56 GB).  ``--workload`` selects another (``g0w0_k4_nb64_np512``, ``batch32_gamma``,
+``scgw_k3_nb48_np384``).
 
 * ``value``: device time per iteration with G resident in HBM (CUDA events on the
   library's stream), mixed precision; ``e2e``: the same through the public C ABI with the
   host G copied in and Sigma copied out every step (pinned host buffers).
+* ``rpa_energy_ms``: the RPA E_c time (Pi -> Pi(iW) -> FP64 log-det), resident G.
+* ``fp64_form``: the same path in FP64, its times, and the mixed path's errors against it.
 * ``--impl reference``: the FP64 oracle (numpy/OpenBLAS restatement of the reference
-  algorithm) on the host cores, bounded samples extrapolated to one iteration.
+  algorithm) on the host cores, per-unit samples extrapolated to one iteration.
 * Multi-GPU (torchrun): the path does not shard; ranks run independent replicas.
 """
 from __future__ import annotations
@@ -27,7 +32,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "g0w0_k4_nb64_np512"
+WORKLOAD = "rpa_gw_k6_nb96_np1024"
 METRIC = "THC-GW iteration time (mixed precision, 1 B200)"
 
 
@@ -214,70 +219,171 @@ def algorithmic_work(w, s, ft):
     }
 
 
-def cpu_sample(s, ft, threads):
-    """Time the FP64 oracle on bounded samples and extrapolate one GW iteration (ms)."""
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count()
+
+
+def _best(fn, reps=2):
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        best = min(best, time.perf_counter() - t0)
+    return best
+
+
+def reference_unit_counts(s, ft):
+    """How often the reference algorithm performs each unit in one GW iteration without
+    symmetry (nq = nk): the polarizability (rpa_pi.icc:102-176), the IR transforms
+    (IAFT.icc:49-128), the LU Dyson solve (scr_coulomb_t.cpp:171-199) and the R-space
+    self-energy with its aux -> primary step (thc_gw.icc:70-213, 37-65)."""
+    nk, nth, nwh = s.nk, ft.nt_half, ft.nw_half
+    return {
+        # G(tau) and G(beta - tau) for every tau < beta/2, once for Pi and again for Sigma
+        "proj_p2a": 4 * nth * nk,
+        "proj_a2p": 2 * nth * nk,
+        # (nk x nk) x (nk x Np^2) DFT GEMMs: Pi 3 per tau; Sigma: W q->R and back (nth
+        # each) plus 2 per tau and half
+        "dft": 3 * nth + 6 * nth,
+        "hadamard": nth + 2 * nth,
+        "ir_columns": 2,  # tau -> iW and iW -> tau over all nq Np^2 columns
+        "dyson": nk * nwh,
+    }
+
+
+def cpu_sample(s, ft, reps=2):
+    """One GW iteration of the FP64 oracle (numpy complex128 on OpenBLAS, every host core),
+    extrapolated from timed samples of its units: each unit is timed on a bounded sample
+    (best of `reps`) and scaled by the number of times the reference algorithm performs it
+    (`reference_unit_counts`).  Returns (total ms, {unit: ms per iteration})."""
     from oracle import thc_oracle as O
     nk, Np, nt, nth, nwh = s.nk, s.Np, ft.nt_f, ft.nt_half, ft.nw_half
+    ncol = Np * Np
     G = s.G0(ft)
     f_Rk = O.k_to_R_coefficients(s.kpts, s.lattv, s.kp_grid)
-    f_qR = O.R_to_k_coefficients(s.kpts, s.lattv, s.kp_grid)
-    parts = {}
-    # Pi: one tau slice (rpa_pi.icc:102-176)
-    t0 = time.perf_counter()
-    Gp = O.primary_to_aux(G[0], s.X)[0]
-    Gn = O.primary_to_aux(G[nt - 1], s.X)[0]
-    GpR = f_Rk @ Gp.reshape(nk, -1)
-    GnR = f_Rk @ Gn.reshape(nk, -1)
-    Pi1 = (f_qR @ (-2.0 * GpR * np.conj(GnR))).reshape(nk, Np, Np)
-    parts["Pi"] = (time.perf_counter() - t0) * nth
-    # tau <-> w: 1/8 of the columns of one full transform
-    cols = nk * Np * Np // 8
-    X = np.repeat(Pi1.reshape(1, -1)[:, :cols], nth, axis=0)
-    t0 = time.perf_counter()
-    Xw = ft.Twt_pos() @ X
-    parts["IR"] = (time.perf_counter() - t0) * 8 * 2
-    # Dyson: two (q, w) problems in the reference's LU form (scr_coulomb_t.cpp:171-199)
-    t0 = time.perf_counter()
-    O.dyson_W_in_place(Pi1[None, :2] * 0.1, s.V[:2])
-    parts["Dyson"] = (time.perf_counter() - t0) / 2 * nk * nwh
-    # Sigma: one tau, both halves (thc_gw.icc:70-213)
-    t0 = time.perf_counter()
-    for Gx in (Gp, Gn):
-        GR = f_Rk @ Gx.reshape(nk, -1)
-        Sk = (f_qR @ (-GR * GpR)).reshape(1, nk, Np, Np)
-        O.aux_to_primary(Sk, s.X)
-    GR = O.primary_to_aux(G[1], s.X)  # the G projections of the sigma step
-    GR = O.primary_to_aux(G[nt - 2], s.X)
-    parts["Sigma"] = (time.perf_counter() - t0) * nth
-    del Xw, GR
-    total = sum(parts.values()) * 1e3
-    return total, parts
+    kk = min(nk, 4)
+    cols = min(ncol, 1 << 15)
+    rng = np.random.default_rng(1)
+    slab = (rng.standard_normal((nk, cols)) + 1j * rng.standard_normal((nk, cols)))
+    S_k = (rng.standard_normal((1, kk, Np, Np)) + 1j * rng.standard_normal((1, kk, Np, Np)))
+    tslab = np.resize(slab, (nth, cols))
+    per = {
+        "proj_p2a": _best(lambda: O.primary_to_aux(G[0][:, :kk], s.X[:, :kk]), reps) / kk,
+        "proj_a2p": _best(lambda: O.aux_to_primary(S_k, s.X[:, :kk]), reps) / kk,
+        "dft": _best(lambda: f_Rk @ slab, reps) * ncol / cols,
+        "hadamard": _best(lambda: -2.0 * slab * np.conj(slab), reps) * ncol / cols,
+        "ir_columns": _best(lambda: ft.Twt_pos() @ tslab, reps)
+        * nk * ncol / cols,
+        "dyson": _best(lambda: O.dyson_W_in_place(S_k[:, :1] * 1e-3, s.V[:1]), reps),
+    }
+    counts = reference_unit_counts(s, ft)
+    parts = {k: per[k] * counts[k] * 1e3 for k in per}
+    return float(sum(parts.values())), parts
+
+
+CPU_SAMPLE_NOTE = ("FP64 numpy/OpenBLAS oracle, extrapolated: per-unit times (projections of 4 "
+                   "k-points, one DFT and one Hadamard product over 32768 columns, one IR "
+                   "transform over the same columns, one (q, iW) LU Dyson solve) scaled by the "
+                   "reference algorithm's unit counts for one GW iteration")
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
     w, s, ft = make_case(args.workload)
-    threads = os.cpu_count()
+    cores = host_cores()
     vals = []
     for i in range(args.warmup + args.steps):
-        t, parts = cpu_sample(s, ft, threads)
+        t, parts = cpu_sample(s, ft, reps=1)
         if i >= args.warmup:
             vals.append(t)
-    v = float(np.mean(vals))
+    v = float(np.median(vals))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "ms",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-        "data": "synthetic", "config": {"workload": args.workload, "nk": s.nk, "nb": s.nb,
-                                        "Np": s.Np, "nt": ft.nt_f, "prec": w["prec"]},
-        "cpu_baseline": {"value": v, "unit": "ms", "cores": threads, "kind": "port",
-                         "sample": "FP64 numpy/OpenBLAS oracle: 1 tau of Pi and Sigma, 1/8 of one "
-                                   "IR transform, 2 (q,W) LU Dyson solves; extrapolated to one "
-                                   "iteration"},
+        "data": "synthetic", "config": config_of(args.workload, w, s, ft),
+        "cpu_baseline": {"value": v, "unit": "ms", "cores": cores, "kind": "port",
+                         "extrapolated": True, "sample": CPU_SAMPLE_NOTE,
+                         "parts_ms": {k: round(x, 1) for k, x in parts.items()}},
         "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def config_of(name, w, s, ft):
+    return {"workload": name, "nk": s.nk, "nb": s.nb, "Np": s.Np, "nt": ft.nt_f,
+            "nw_b": ft.nw_b, "prec": w["prec"], "beta": w["beta"], "lambda": w["lam"],
+            "parallelism": "replicas",
+            "l2": "working set (Pi/W %.1f GB) far above L2 (126 MB); no flush" % (
+                max(ft.nt_half, ft.nw_half) * s.nk * s.Np ** 2 * 8 / 1e9)}
+
+
+def measure_fp64_peak(device):
+    """Dense FP64 rate of cuBLAS on this GPU (TFLOP/s): DGEMM 8192^3 (2 N^3 flop) and ZGEMM
+    4096^3 (8 N^3 flop), best of 8 each, CUDA events; the larger of the two."""
+    import torch
+    out = {}
+    for name, n, dt, fl in (("dgemm", 8192, torch.float64, 2.0), ("zgemm", 4096, torch.complex128,
+                                                                    8.0)):
+        a = torch.randn(n, n, dtype=dt, device=device)
+        b = torch.randn(n, n, dtype=dt, device=device)
+        c = a @ b
+        best = float("inf")
+        for _ in range(8):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b, out=c)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        out[name + "_tflops"] = fl * n ** 3 / (best * 1e-3) / 1e12
+        del a, b, c
+    torch.cuda.empty_cache()
+    out["tflops"] = max(out["dgemm_tflops"], out["zgemm_tflops"])
+    out["how"] = "cuBLAS through torch.matmul: DGEMM 8192^3 and ZGEMM 4096^3, best of 8"
+    return out
+
+
+def group_rates(stats, steps, work, hbm, bf16, fp64):
+    """Per-kernel-group time and achieved rate against its own roof (HBM copy, bf16 tensor,
+    or the measured FP64 rate)."""
+    groups = {}
+    for name, (ms_tot, n) in stats.items():
+        ms_it = ms_tot / steps
+        kind, per_launch, per_iter = work.get(name, (None, None, None))
+        amount = per_iter if per_iter is not None else (
+            per_launch * n / steps if per_launch is not None else None)
+        g = {"ms_per_step": ms_it, "launch_groups_per_step": n / steps, "bound": kind}
+        if amount and ms_it > 0:
+            if kind == "hbm":
+                g["achieved_GBps"] = amount / (ms_it * 1e-3) / 1e9
+                g["frac_of_hbm"] = g["achieved_GBps"] / hbm
+            else:
+                g["achieved_TFLOPs"] = amount / (ms_it * 1e-3) / 1e12
+                if kind == "tensor":
+                    g["frac_of_bf16"] = g["achieved_TFLOPs"] / bf16
+                    g["frac_of_split_tf32_ceiling"] = g["achieved_TFLOPs"] / (bf16 / 6.0)
+                elif kind == "fp64":
+                    g["frac_of_fp64_measured"] = g["achieved_TFLOPs"] / fp64
+        groups[name] = g
+    return groups
+
+
+def profile_traffic(kernel, Np):
+    """DRAM bytes per (q, iW) problem of a kernel group from a committed ncu summary
+    (`profiles/dram_traffic_<group>_np<Np>.md`, line `bytes_per_problem: B`), or None."""
+    path = os.path.join(ROOT, "profiles", f"dram_traffic_{kernel}_np{Np}.md")
+    try:
+        for ln in open(path):
+            if ln.startswith("bytes_per_problem:"):
+                return float(ln.split(":")[1]), os.path.relpath(path, ROOT)
+    except OSError:
+        pass
+    return None, None
 
 
 def run_ours(args, rank, world, local):
@@ -291,13 +397,16 @@ def run_ours(args, rank, world, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     w, s, ft = make_case(args.workload)
     G = s.G0(ft)
-    ctx = make_ctx(s, ft, capi.MIXED)
+    side = max(1, min(args.steps, 3))  # repetitions of the legs beside the headline
 
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
+
+    fp64_peak = measure_fp64_peak(local)
+    ctx = make_ctx(s, ft, capi.MIXED)
 
     # warm-up (resident G)
     ctx.gw_iteration(G, want_sigma=False)
@@ -317,7 +426,7 @@ def run_ours(args, rank, world, local):
     # per-kernel-group CUDA-event timing in separate steps (the events add host work between
     # launches, so they stay out of the timed steps above)
     ctx.set_profiling(True)
-    for _ in range(args.steps):
+    for _ in range(side):
         ctx.gw_iteration(None, want_sigma=False)
     barrier()
     stats = ctx.kernel_stats()
@@ -341,9 +450,10 @@ def run_ours(args, rank, world, local):
     # RPA energy time (resident G) and E_c
     ctx.rpa_energy(Gh)
     rpa = []
-    for _ in range(max(1, args.steps)):
-        e_c = ctx.rpa_energy(None)
-        rpa.append(total_ms(ctx))
+    with Clocks(local) as clk_rpa:
+        for _ in range(max(1, args.steps)):
+            e_c = ctx.rpa_energy(None)
+            rpa.append(total_ms(ctx))
     t_rpa = float(np.mean(rpa))
     rpa_phases = dict(ctx.timings())
 
@@ -354,18 +464,18 @@ def run_ours(args, rank, world, local):
     S_ov = np.ascontiguousarray(np.broadcast_to(np.eye(s.nb, dtype=np.complex128), Dm.shape))
     hf_dev, hf_e2e, hf_wall = [], [], []
     l0 = ctx.kernel_launches()
-    for i in range(args.warmup + args.steps):
+    for i in range(1 + side):
         t0 = time.perf_counter()
         F_hf = ctx.hf_evaluate(Dm, S_ov, True, True, "gygi", 0.5)
         wall = (time.perf_counter() - t0) * 1e3
-        if i >= args.warmup:
+        if i >= 1:
             hf_dev.append(dict(ctx.timings())["HF"])
             hf_e2e.append(total_ms(ctx))
             hf_wall.append(wall)
     hf = {"what": "THC Hartree-Fock J + K with the gygi term (hf_t::evaluate), FP64",
           "ms": float(np.mean(hf_dev)), "e2e_ms": float(np.mean(hf_e2e)),
           "e2e_wall_ms": float(np.mean(hf_wall)),
-          "gpu_launches": int((ctx.kernel_launches() - l0) // (args.warmup + args.steps)),
+          "gpu_launches": int((ctx.kernel_launches() - l0) // (1 + side)),
           "h2d_bytes": int(Dm.nbytes + S_ov.nbytes),
           "d2h_bytes": int(F_hf.nbytes)}
 
@@ -374,9 +484,9 @@ def run_ours(args, rank, world, local):
     # and the correction's own device time
     ctx.set_div_treatment("gygi", 0.5, s.chi_bar[0])
     gy = []
-    for i in range(args.warmup + args.steps):
+    for i in range(1 + side):
         ctx.gw_iteration(None, want_sigma=False)
-        if i >= args.warmup:
+        if i >= 1:
             gy.append(total_ms(ctx))
     ctx.set_profiling(True)
     ctx.gw_iteration(None, want_sigma=False)
@@ -388,27 +498,51 @@ def run_ours(args, rank, world, local):
             "correction_ms": float(gst.get("sigma_div", (0.0, 0))[0]),
             "eps_head_ms": float(gst.get("eps_head", (0.0, 0))[0])}
 
+    # the dielectric head of the mixed iteration (it reads all of W) for the accuracy figures
+    _, head_mixed = ctx.gw_iteration(None, want_sigma=False, want_head=True)
+
+    # the oracle on a bounded sample at this size: the projection of G(tau = 0) for every k
+    oracle_sample = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import thc_oracle as O
+        got = ctx.primary_to_aux(G[:1])
+        ref = O.primary_to_aux(G[:1], s.X[None])
+        oracle_sample = {"what": "primary -> aux projection X G(tau_0) X^H, all k, mixed path "
+                                 "against the FP64 oracle", "max_abs_diff":
+                         float(np.abs(got - ref).max()), "max_abs": float(np.abs(ref).max())}
+        del got, ref
+    ctx.close()  # the FP64 form needs the memory
+
     fp64 = None
+    fp64_stats = {}
     if not args.no_fp64:
         c64 = make_ctx(s, ft, capi.FP64)
-        S64, _ = c64.gw_iteration(Gh)
-        t64 = []
-        for _ in range(2):
-            c64.gw_iteration(None, want_sigma=False)
-            t64.append(total_ms(c64))
+        S64, head64 = c64.gw_iteration(Gh, want_head=True)
+        c64.set_profiling(True)
+        c64.gw_iteration(None, want_sigma=False)
+        fp64_stats = c64.kernel_stats()
+        c64.set_profiling(False)
+        c64.gw_iteration(None, want_sigma=False)
+        t64 = total_ms(c64)
         e64 = c64.rpa_energy(None)
         r64 = total_ms(c64)
-        dS = float(np.abs(Sh - S64).max())
-        fp64 = {"gw_iteration_ms": float(np.mean(t64)), "rpa_energy_ms": r64, "E_c": e64,
-                "max_abs_dSigma_mixed_vs_fp64": dS, "abs_dE_c_mixed_vs_fp64": abs(e_c - e64),
-                "speedup_gw_iteration": float(np.mean(t64)) / t_step,
-                "speedup_rpa": r64 / t_rpa}
+        fp64 = {"what": "the same path with complex128 storage, FP64 products (cuBLAS ZGEMM) and "
+                        "FP64 factorisations (cuSOLVER), one frequency at a time",
+                "gw_iteration_ms": t64, "rpa_energy_ms": r64, "E_c": e64,
+                "max_abs_dSigma_mixed_vs_fp64": float(np.abs(Sh - S64).max()),
+                "max_abs_Sigma": float(np.abs(S64).max()),
+                "max_abs_d_eps_inv_head_mixed_vs_fp64": float(np.abs(head_mixed - head64).max()),
+                "abs_dE_c_mixed_vs_fp64": abs(e_c - e64),
+                "speedup_gw_iteration": t64 / t_step, "speedup_rpa": r64 / t_rpa,
+                "note": "the FP64 form is checked against the FP64 oracle at the 2x2x2 / 128 and "
+                        "4x4x4 / 512 configurations by tests/test_gpu_configs.py"}
         c64.close()
+        del S64
 
     # max over ranks
     t_step, t_e2e = max_over_ranks([t_step, t_e2e], world)
 
-    # per-group achieved rates and the roofline of the dominant HBM- or tensor-bound group
+    # per-group achieved rates and the roofline of the dominant group
     work = algorithmic_work(w, s, ft)
     peaks = {}
     try:
@@ -417,70 +551,48 @@ def run_ours(args, rank, world, local):
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     bf16 = peaks.get("bf16_tflops", 1590.0)
-    # FP64 (CUDA-core FMA and DMMA alike): 64 multiply-adds per clock per SM, nominal clock
-    fp64_nom = 148 * 64 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    fp64_tf = fp64_peak["tflops"]
     peak_src = "measured" if peaks else "fallback"
-    groups = {}
-    for name, (ms_tot, n) in stats.items():
-        ms_it = ms_tot / args.steps
-        kind, per_launch, per_iter = work.get(name, (None, None, None))
-        amount = per_iter if per_iter is not None else (
-            per_launch * n / args.steps if per_launch is not None else None)
-        g = {"ms_per_step": ms_it, "launch_groups_per_step": n / args.steps, "bound": kind}
-        if amount and ms_it > 0:
-            if kind == "hbm":
-                g["achieved_GBps"] = amount / (ms_it * 1e-3) / 1e9
-                g["frac_of_hbm"] = g["achieved_GBps"] / hbm
-            else:
-                g["achieved_TFLOPs"] = amount / (ms_it * 1e-3) / 1e12
-                if kind == "tensor":
-                    g["frac_of_bf16"] = g["achieved_TFLOPs"] / bf16
-                elif kind == "fp64":
-                    g["frac_of_fp64_nominal"] = g["achieved_TFLOPs"] / fp64_nom
-        groups[name] = g
-    # DRAM bytes of the screened-interaction products per (q, iW) problem from the committed
-    # ncu summary (measured on a smaller case; the traffic grows with the problem count)
-    w_bytes_per_problem = None
-    try:
-        for ln in open(os.path.join(ROOT, "profiles", "dram_traffic_g0w0_k2_nb64_np512.md")):
-            if ln.startswith("bytes_per_problem:"):
-                w_bytes_per_problem = float(ln.split(":")[1])
-    except OSError:
-        pass
+    groups = group_rates(stats, side, work, hbm, bf16, fp64_tf)
+    if fp64_stats:
+        fp64["kernel_groups_ms"] = {k: v[0] for k, v in fp64_stats.items()}
     roof = None
-    cand = [(g["ms_per_step"], k) for k, g in groups.items() if g["bound"] in ("hbm", "tensor")
-            and ("achieved_GBps" in g or "achieved_TFLOPs" in g)]
+    cand = [(g["ms_per_step"], k) for k, g in groups.items()
+            if "achieved_GBps" in g or "achieved_TFLOPs" in g]
     if cand:
         _, name = max(cand)
         g = groups[name]
         n_l = max(g["launch_groups_per_step"], 1e-9)
         per_ms = g["ms_per_step"] / n_l
+        nprob = s.nk * ft.nw_half
+        traffic, tsrc = profile_traffic(name, s.Np)
         if g["bound"] == "hbm":
             roof = {"kernel": name, "bound": "hbm", "achieved": g["achieved_GBps"], "peak": hbm,
                     "unit": "GB/s", "frac": g["achieved_GBps"] / hbm, "traffic": None,
                     "avg_launch_ms": per_ms, "peak_source": peak_src + " HBM copy"}
+        elif g["bound"] == "fp64":
+            roof = {"kernel": name, "bound": "tensor", "pipe": "FP64 tensor cores (DMMA)",
+                    "achieved": g["achieved_TFLOPs"], "peak": fp64_tf, "unit": "TFLOP/s",
+                    "frac": g["achieved_TFLOPs"] / fp64_tf,
+                    "traffic": traffic * nprob / n_l if traffic else None,
+                    "traffic_source": tsrc, "avg_launch_ms": per_ms,
+                    "peak_source": "measured in this run: " + fp64_peak["how"]}
         else:
-            traffic = None
-            if name == "dyson_W_gemm" and w_bytes_per_problem and s.Np == 512:
-                traffic = w_bytes_per_problem * s.nk * ft.nw_half
             roof = {"kernel": name, "bound": "tensor", "achieved": g["achieved_TFLOPs"],
                     "peak": bf16, "unit": "TFLOP/s", "frac": g["achieved_TFLOPs"] / bf16,
-                    "traffic": traffic, "traffic_note": "DRAM bytes per step (ncu, scaled from the "
-                    "200-problem case by the problem count)" if traffic else None,
-                    "avg_launch_ms": per_ms,
+                    "traffic": traffic * nprob / n_l if traffic else None,
+                    "traffic_source": tsrc, "avg_launch_ms": per_ms,
                     "peak_source": peak_src + " dense bf16 cuBLAS; split-TF32 complex products "
                                    "issue 3 TF32 MMAs at half the bf16 rate per counted flop",
-                    # the rate the split form can reach at that peak: peak / 6 per counted flop
                     "split_tf32_ceiling": bf16 / 6.0,
                     "frac_of_split_tf32_ceiling": g["achieved_TFLOPs"] / (bf16 / 6.0)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, parts = cpu_sample(s, ft, os.cpu_count())
-        cpu = {"value": v, "unit": "ms", "cores": os.cpu_count(), "kind": "port",
-               "sample": "FP64 numpy/OpenBLAS oracle: 1 tau of Pi and Sigma, 1/8 of one IR "
-                         "transform, 2 (q,W) LU Dyson solves; extrapolated to one iteration",
-               "parts_ms": {k: v * 1e3 for k, v in parts.items()}}
+        v, parts = cpu_sample(s, ft, reps=2)
+        cpu = {"value": v, "unit": "ms", "cores": host_cores(), "kind": "port",
+               "extrapolated": True, "sample": CPU_SAMPLE_NOTE,
+               "parts_ms": {k: round(x, 1) for k, x in parts.items()}}
         # the oracle's Hartree-Fock on the same density matrix: time and full-size parity
         from oracle import thc_oracle as O
         t0 = time.perf_counter()
@@ -494,18 +606,16 @@ def run_ours(args, rank, world, local):
         "metric": METRIC, "value": t_step / world, "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c64/f64",
-        "data": "synthetic",
-        "config": {"workload": args.workload, "nk": s.nk, "nb": s.nb, "Np": s.Np,
-                   "nt": ft.nt_f, "nw_b": ft.nw_b, "prec": w["prec"], "parallelism": "replicas",
-                   "l2": "working set (Pi/W %.1f GB) far above L2 (126 MB); no flush" % (
-                       max(ft.nt_half, ft.nw_half) * s.nk * s.Np ** 2 * 8 / 1e9)},
+        "data": "synthetic", "config": config_of(args.workload, w, s, ft),
         "e2e": {"value": t_e2e / world, "unit": "ms", "h2d_bytes_per_step": gbytes,
                 "d2h_bytes_per_step": gbytes},
         "gpu_launches": int(launches),
-        "rpa_energy_ms": t_rpa, "E_c": e_c,
+        "rpa_energy_ms": t_rpa, "E_c": e_c, "rpa_clocks": clk_rpa.summary(),
+        "fp64_form": fp64,
+        "oracle_sample": oracle_sample,
+        "fp64_peak_measured": fp64_peak,
         "hartree_fock": hf,
         "div_gygi": gygi,
-        "fp64_form": fp64,
         "phases_ms": phases,
         "steps_ms": [round(t, 3) for t in times],
         "e2e_steps_ms": [round(t, 3) for t in e2e],
@@ -521,7 +631,6 @@ def run_ours(args, rank, world, local):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ctx.close()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

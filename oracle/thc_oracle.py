@@ -216,8 +216,8 @@ def eval_Pi_rpa_Rspace(G_tskij, X_skPa, kpts, lattv, kp_grid, Qpts=None) -> np.n
         Gp = primary_to_aux(G_tskij[it], X_skPa)  # (ns, nk, Np, Np)
         Gn = primary_to_aux(G_tskij[nt - it - 1], X_skPa)
         if nk != 1:
-            Gp = np.einsum("Rk,skx->sRx", f_Rk, Gp.reshape(ns, nk, -1)).reshape(Gp.shape)
-            Gn = np.einsum("Rk,skx->sRx", f_Rk, Gn.reshape(ns, nk, -1)).reshape(Gn.shape)
+            Gp = np.matmul(f_Rk, Gp.reshape(ns, nk, -1)).reshape(Gp.shape)  # sum_k f_Rk G^k
+            Gn = np.matmul(f_Rk, Gn.reshape(ns, nk, -1)).reshape(Gn.shape)
         GG = (Gp * np.conj(Gn)).sum(axis=0) * sp  # rpa_pi.icc:156-162
         if nk != 1:
             Pi[it] = (f_qR @ GG.reshape(nk, -1)).reshape(nq, Np, Np)
@@ -259,7 +259,7 @@ def eval_eps_inv_q(W_tqPQ, chi_bar_qP, Qpts, lattv) -> np.ndarray:
     vol = abs(np.linalg.det(np.asarray(lattv, np.float64)))
     q2 = (np.asarray(Qpts) ** 2).sum(axis=1)
     fpi = 4.0 * 3.14159265358979323846
-    buf = np.einsum("tqPQ,qQ->tqP", W_tqPQ, np.conj(chi_bar_qP))
+    buf = np.matmul(W_tqPQ, np.conj(chi_bar_qP)[None, :, :, None])[..., 0]  # W conj(chi)
     return (q2 / fpi * vol)[None, :] * np.einsum("qP,tqP->tq", chi_bar_qP, buf)
 
 
@@ -402,10 +402,10 @@ def eval_Sigma_all_Rspace(G_tskij, dW_qtPQ, X_skPa, kpts, lattv, kp_grid) -> np.
         G_tsk = primary_to_aux(G_tskij[idx], X_skPa[None])  # (nt_half, ns, nk, Np, Np)
         G_skt = np.transpose(G_tsk, (1, 2, 0, 3, 4))
         if nk != 1:
-            G_skt = np.einsum("Rk,skx->sRx", f_Rk, G_skt.reshape(ns, nk, -1)).reshape(G_skt.shape)
+            G_skt = np.matmul(f_Rk, G_skt.reshape(ns, nk, -1)).reshape(G_skt.shape)
         S_skt = -(G_skt * W_R[None])  # thc_gw.icc:161-167
         if nk != 1:
-            S_skt = np.einsum("kR,sRx->skx", f_kR, S_skt.reshape(ns, nk, -1)).reshape(S_skt.shape)
+            S_skt = np.matmul(f_kR, S_skt.reshape(ns, nk, -1)).reshape(S_skt.shape)
         S_tsk = np.transpose(S_skt, (2, 0, 1, 3, 4))
         S_ab = aux_to_primary(S_tsk, X_skPa[None])  # (nt_half, ns, nk, nb, nb)
         if not minus_t:
@@ -442,7 +442,7 @@ def thc_hf(Dm_skij, X_skPa, V_qPQ, kpts, lattv, kp_grid, S_skij=None, hartree=Tr
     f_Rk = k_to_R_coefficients(kpts, lattv, kp_grid)
     f_kR = R_to_k_coefficients(kpts, lattv, kp_grid)
     if nk != 1:
-        Dp = np.einsum("Rk,skx->sRx", f_Rk, Dp.reshape(ns, nk, -1)).reshape(Dp.shape)
+        Dp = np.matmul(f_Rk, Dp.reshape(ns, nk, -1)).reshape(Dp.shape)
     F_PQ = np.zeros((ns, nk, Np, Np), np.complex128)
     if hartree:
         factor = 2.0 if ns == 1 else 1.0
@@ -455,7 +455,7 @@ def thc_hf(Dm_skij, X_skPa, V_qPQ, kpts, lattv, kp_grid, S_skij=None, hartree=Tr
         U_R = (f_Rk @ U) if nk != 1 else U
         K_R = -(Dp * U_R.reshape(nk, Np, Np)[None])
         if nk != 1:
-            K_R = np.einsum("kR,sRx->skx", f_kR, K_R.reshape(ns, nk, -1)).reshape(K_R.shape)
+            K_R = np.matmul(f_kR, K_R.reshape(ns, nk, -1)).reshape(K_R.shape)
         F_PQ += K_R
     F = aux_to_primary(F_PQ, X_skPa)
     if exchange and div == "gygi":

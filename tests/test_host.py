@@ -136,3 +136,23 @@ def test_bench_clock_record_reports_reasons_and_median():
     assert s["samples"] == 3 and s["source"] == ["nvml"] and s["failed_queries"] == 0
     empty = bench.Clocks(0)
     assert empty.summary()["reasons"] == ["unsampled"]
+
+
+def test_bench_cpu_sample_counts_and_scaling():
+    """The CPU baseline's extrapolation: unit counts of one GW iteration of the reference
+    algorithm, and per-unit samples that scale to positive per-iteration times."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    from coqui_b200.iaft import IAFT
+    from coqui_b200.synthetic import make_system
+
+    s = make_system(2, 8, 4, 32, seed=3)
+    ft = IAFT(1000.0, 10.0, "low")
+    c = bench.reference_unit_counts(s, ft)
+    assert c["proj_p2a"] == 4 * ft.nt_half * s.nk and c["proj_a2p"] == 2 * ft.nt_half * s.nk
+    assert c["dft"] == 9 * ft.nt_half and c["dyson"] == s.nk * ft.nw_half
+    total, parts = bench.cpu_sample(s, ft, reps=1)
+    assert set(parts) == set(c) and all(v > 0 for v in parts.values())
+    assert abs(total - sum(parts.values())) < 1e-9 * total
