@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "chol.cuh"
@@ -53,6 +54,10 @@ constexpr int AR = DMMA ? 2 : RT, AC = DMMA ? 8 : CTT;
 static_assert(!DMMA || (CB == 32 && CT == 64), "DMMA tiles: 32-blocks, two warps");
 #include "chol_blk.cuh"
 }  // namespace b32
+
+// Four-warp left-looking kernel (two panel row blocks per step, cp.async staging): the same
+// arithmetic as b32::k_chol_inv_left with less block traffic per product.
+#include "chol_pair.cuh"
 
 // Problems of different sizes in one launch (one CTA each, 32-blocks).
 template <bool LEFT>
@@ -197,11 +202,22 @@ void run_tiled(const CholProblem* t, const TiledRuns& R, int64_t np, double* log
   go(3, 0);
 }
 
-// Block order of the one-CTA factorisation: left-looking unless COQUI_B200_CHOL_ORDER=right.
-bool chol_left_looking() {
+// Form of the one-CTA factorisation, COQUI_B200_CHOL_ORDER: "pair" (default: four warps,
+// two panel row blocks per step, double-buffered half-width K slices), "pair1" (the same with
+// whole blocks copied and then used), "pair2" (double-buffered whole blocks), "left" (two
+// warps, left-looking), "right" (two warps, right-looking).  All give identical results.
+enum class CholForm { kPair, kPair1, kPair2, kLeft, kRight };
+CholForm chol_form() {
   const char* v = std::getenv("COQUI_B200_CHOL_ORDER");
-  return !(v && v[0] == 'r');
+  if (!v || !v[0]) return CholForm::kPair;
+  const std::string f(v);
+  if (f == "right") return CholForm::kRight;
+  if (f == "left") return CholForm::kLeft;
+  if (f == "pair2") return CholForm::kPair2;
+  if (f == "pair1") return CholForm::kPair1;
+  return CholForm::kPair;
 }
+bool chol_left_looking() { return chol_form() != CholForm::kRight; }
 
 // k_chol_inv<INV> of the block size chosen for n; the inverse is formed within diagonal groups
 // of inv_cols columns (a multiple of 64).
@@ -216,10 +232,20 @@ void launch_factor(const float2* M, double2* A, double* logdet, double2* trace, 
     count_launch();
     CQ_CHECK_CUDA(cudaGetLastError());
   };
-  if (chol_left_looking())
-    go(b32::k_chol_inv_left<INV>, b32::CB, b32::CT, b32::PITCH);
-  else
-    go(b32::k_chol_inv<INV>, b32::CB, b32::CT, b32::PITCH);
+  auto go_pair = [&](auto kern, size_t smem) {
+    CQ_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int groups = (int)std::min<int64_t>(inv_cols / p32::CB, 1 << 30);
+    kern<<<(unsigned)nprob, p32::NT, smem, s>>>(M, A, logdet, trace, info, n, groups);
+    count_launch();
+    CQ_CHECK_CUDA(cudaGetLastError());
+  };
+  switch (chol_form()) {
+    case CholForm::kPair: go_pair(p32::k_chol_pair<INV, 2, 2>, p32::smem_bytes<2, 2>()); break;
+    case CholForm::kPair1: go_pair(p32::k_chol_pair<INV, 1, 1>, p32::smem_bytes<1, 1>()); break;
+    case CholForm::kPair2: go_pair(p32::k_chol_pair<INV, 2, 1>, p32::smem_bytes<2, 1>()); break;
+    case CholForm::kLeft: go(b32::k_chol_inv_left<INV>, b32::CB, b32::CT, b32::PITCH); break;
+    default: go(b32::k_chol_inv<INV>, b32::CB, b32::CT, b32::PITCH); break;
+  }
 }
 
 // grouped Z = X^H - I, blockIdx.y = problem
@@ -393,6 +419,34 @@ bool chol_prefer_tiled(const std::vector<int64_t>& sizes) {
   }
   const int64_t nmax = sizes.empty() ? 0 : *std::max_element(sizes.begin(), sizes.end());
   return nmax >= 4 * b32::CB && total / ((double)sms * b32::MINB) < mx;
+}
+
+int64_t chol_wave_size() {
+  int dev = 0, sms = 148, per_sm = 0;
+  CQ_CHECK_CUDA(cudaGetDevice(&dev));
+  CQ_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  size_t smem = (size_t)2 * b32::CB * b32::PITCH * sizeof(double2);
+  int threads = b32::CT;
+  const void* kern = nullptr;
+  switch (chol_form()) {
+    case CholForm::kPair:
+      kern = (const void*)p32::k_chol_pair<true, 2, 2>, smem = p32::smem_bytes<2, 2>();
+      threads = p32::NT;
+      break;
+    case CholForm::kPair1:
+      kern = (const void*)p32::k_chol_pair<true, 1, 1>, smem = p32::smem_bytes<1, 1>();
+      threads = p32::NT;
+      break;
+    case CholForm::kPair2:
+      kern = (const void*)p32::k_chol_pair<true, 2, 1>, smem = p32::smem_bytes<2, 1>();
+      threads = p32::NT;
+      break;
+    case CholForm::kLeft: kern = (const void*)b32::k_chol_inv_left<true>; break;
+    default: kern = (const void*)b32::k_chol_inv<true>; break;
+  }
+  CQ_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CQ_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+  return (int64_t)sms * std::max(per_sm, 1);
 }
 
 void launch_chol_tiled_strided(const float2* M, double2* A, double* logdet, double2* trace,

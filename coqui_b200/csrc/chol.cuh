@@ -48,6 +48,11 @@ void launch_chol_tiled_strided(const float2* M, double2* A, double* logdet, doub
 // COQUI_B200_CHOL_TILED=1 or 0 forces the choice.
 bool chol_prefer_tiled(const std::vector<int64_t>& sizes);
 
+// Problems one launch of the one-CTA factorisation (launch_chol_group_inv) runs at once on
+// the current device: SMs x resident CTAs per SM.  A batch of a multiple of this size leaves
+// no partly filled last wave.
+int64_t chol_wave_size();
+
 // As launch_chol_inv without Z, but the inverse U = C^{-H} is formed only inside the
 // kInvGroup x kInvGroup diagonal groups (upper triangle of A there).
 void launch_chol_group_inv(const float2* M, double2* A, double* logdet, double2* trace, int* info,

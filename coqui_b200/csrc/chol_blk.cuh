@@ -113,11 +113,13 @@ __device__ __forceinline__ int acc_col(int i, int j) {
   else return (int)(threadIdx.x % TWC) + TWC * j;
 }
 
-// D (8 x 8, two values per lane) += A (8 x 4, one per lane) * B (4 x 8, one per lane), FP64
+// D (8 x 8, two values per lane) += A (8 x 4, one per lane) * B (4 x 8, one per lane), FP64.
+// Not volatile: the compiler may interleave independent products (their operands and
+// accumulators are the only dependencies).
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
 }
 
 // acc += sign * sum_k X[r][k] * Y'(k, c) over k < K, with Y'(k, c) = conj(Y[c][k]) if ADJ_Y
@@ -136,26 +138,34 @@ __device__ __forceinline__ void block_mma(const double2* X, const double2* Y, in
       for (int i = 0; i < AR; ++i) x[i] = X[(8 * (2 * w + i) + g) * PITCH + k];
 #pragma unroll
       for (int t = 0; t < 4; ++t) y[t] = ADJ_Y ? Y[(8 * t + g) * PITCH + k] : Y[k * PITCH + 8 * t + g];
+      // four passes over the AR x 4 fragment pairs: consecutive products feed different
+      // accumulators, and every accumulator still receives its terms in the same order
+      // (real part: xr yr then the xi yi term; imaginary part: the xi yr term then xr yi)
+      double xr[AR], xi[AR];
 #pragma unroll
       for (int i = 0; i < AR; ++i) {
-        const double xr = sg * x[i].x, xi = sg * x[i].y;
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          double2& c0 = acc[i][2 * t];
-          double2& c1 = acc[i][2 * t + 1];
-          if (ADJ_Y) {  // x conj(y) = (xr yr + xi yi) + i (xi yr - xr yi)
-            dmma(c0.x, c1.x, xr, y[t].x);
-            dmma(c0.x, c1.x, xi, y[t].y);
-            dmma(c0.y, c1.y, xi, y[t].x);
-            dmma(c0.y, c1.y, -xr, y[t].y);
-          } else {      // x y = (xr yr - xi yi) + i (xr yi + xi yr)
-            dmma(c0.x, c1.x, xr, y[t].x);
-            dmma(c0.x, c1.x, -xi, y[t].y);
-            dmma(c0.y, c1.y, xr, y[t].y);
-            dmma(c0.y, c1.y, xi, y[t].x);
-          }
-        }
+        xr[i] = sg * x[i].x;
+        xi[i] = sg * x[i].y;
       }
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) dmma(acc[i][2 * t].x, acc[i][2 * t + 1].x, xr[i], y[t].x);
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int t = 0; t < 4; ++t)  // x conj(y): + xi yi; x y: - xi yi
+          dmma(acc[i][2 * t].x, acc[i][2 * t + 1].x, ADJ_Y ? xi[i] : -xi[i], y[t].y);
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int t = 0; t < 4; ++t)  // x conj(y): + xi yr (then - xr yi); x y: + xr yi (then + xi yr)
+          dmma(acc[i][2 * t].y, acc[i][2 * t + 1].y, ADJ_Y ? xi[i] : xr[i], ADJ_Y ? y[t].x : y[t].y);
+#pragma unroll
+      for (int i = 0; i < AR; ++i)
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          dmma(acc[i][2 * t].y, acc[i][2 * t + 1].y, ADJ_Y ? -xr[i] : xi[i], ADJ_Y ? y[t].y : y[t].x);
     }
   } else {
     const int tx = threadIdx.x % TWC, ty = threadIdx.x / TWC;

@@ -139,8 +139,14 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
     if (a.keep_scratch && scratch.n >= per + 1024) budget = scratch.n - 1024;
   }
   const int64_t nprob = nw * nq;
-  const int64_t nbq = a.mixed ? std::max<int64_t>(1, std::min<int64_t>(nprob, (int64_t)(budget / per)))
-                              : std::max<int64_t>(1, std::min<int64_t>(nq, (int64_t)(budget / per)));
+  int64_t nbq = a.mixed ? std::max<int64_t>(1, std::min<int64_t>(nprob, (int64_t)(budget / per)))
+                        : std::max<int64_t>(1, std::min<int64_t>(nq, (int64_t)(budget / per)));
+  if (a.mixed && nbq < nprob) {
+    // several chunks: whole waves of the one-CTA factorisation per chunk (a chunk of 1.5 waves
+    // leaves half the GPU idle during its second wave)
+    const int64_t wave = chol_wave_size();
+    if (nbq >= wave) nbq = nbq / wave * wave;
+  }
   scratch.ensure(per * nbq + 1024);
   unsigned char* base = scratch.p;
   auto carve = [&](size_t bytes) {

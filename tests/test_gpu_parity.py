@@ -174,19 +174,22 @@ def test_tiled_and_one_cta_factorisations_agree(monkeypatch):
 
 @pytest.mark.parametrize("grid,Np", [(2, 64), ((1, 1, 2), 300)])
 def test_left_and_right_looking_factorisations_agree(monkeypatch, grid, Np):
-    """The left-looking one-CTA factorisation starts every block from I - M and subtracts the
-    same block products in the same order as the right-looking one (which keeps the running
-    sums in global memory between block columns): W and E_c agree bit for bit."""
+    """The left-looking one-CTA factorisations (two warps; four warps with two panel row
+    blocks per step, single- or double-buffered copies) start every block from I - M and
+    subtract the same block products in the same order as the right-looking one (which keeps
+    the running sums in global memory between block columns): W and E_c agree bit for bit."""
     cs = Case(grid, 16, 8, Np, seed=17)
     monkeypatch.setenv("COQUI_B200_CHOL_TILED", "0")
     out = {}
-    for order in ("left", "right"):
+    forms = ("left", "right", "pair", "pair1", "pair2")
+    for order in forms:
         monkeypatch.setenv("COQUI_B200_CHOL_ORDER", order)
         c = cs.ctx(capi.MIXED)
         out[order] = (c.dyson_w(cs.Pi_w), c.rpa_energy(cs.G))
         c.close()
-    assert np.array_equal(out["left"][0], out["right"][0])
-    assert out["left"][1] == out["right"][1]
+    for order in forms[1:]:
+        assert np.array_equal(out["left"][0], out[order][0]), order
+        assert out["left"][1] == out[order][1], order
     assert maxabs(out["left"][0], cs.W_w) < 1e-6
 
 
