@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <string>
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -49,6 +50,7 @@ constexpr int kBKR = 32;  // real K per stage (128 bytes of fp32)
 // smaller footprint lets several CTAs share an SM so one tile's epilogue overlaps another's
 // main loop.
 template <int BNC, int NP, int ST> struct TileCfg {
+  static constexpr int BNC_ = BNC;                     // complex columns per tile
   static constexpr int NR = 2 * BNC;                   // UMMA N (real columns)
   static constexpr int NPROD = NP;
   static constexpr int NPW = NP / 32;
@@ -570,6 +572,342 @@ __global__ void __launch_bounds__(NP + 32, (NP == 128 ? 2 : 1))
   tc_tile<BNC, NP, ST, A64, B64>(sp, s_bz, s_m0, s_n0, smem_raw);
 }
 
+// ---------------------------------------------------------------------------------------
+// Persistent form: one CTA per SM slot walks the tiles blockIdx.x, + gridDim.x, ... of the
+// whole batch.  The producer warps stage K blocks across tile boundaries (the next tile's
+// first blocks are loaded while this tile's last ones are stored), one lane issues the MMAs
+// into one of two TMEM accumulators, and four epilogue warps drain the other accumulator
+// (TMEM -> registers -> a 32 x 32 shared transpose per warp -> coalesced rows) while the next
+// tile accumulates.  Each element is formed from the same products in the same K order as in
+// k_tc_cgemm, so the results are identical.
+// ---------------------------------------------------------------------------------------
+template <int BNC, int NP, int ST> struct PCfg {
+  using Base = TileCfg<BNC, NP, ST>;
+  static constexpr int NPW = NP / 32;
+  static constexpr int MMA_WARP = NPW;
+  static constexpr int EPI_WARP0 = NPW + 1;  // four warps; TMEM lane quadrant = warp % 4
+  static constexpr int THREADS = NP + 32 + 128;
+  static constexpr int EPI_PITCH = 36;       // floats per row of a warp's 32 x 32 buffer
+  static constexpr int EPI_BYTES = 4 * 32 * EPI_PITCH * 4;
+  static constexpr int TMEM_COLS = 2 * Base::NR;  // two accumulators
+  static constexpr int SMEM_USED = ST * Base::STAGE + EPI_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+  // at least 120 KB, so that one CTA occupies an SM (two CTAs' TMEM accumulators could exceed
+  // the SM's 512 columns, and a CTA waiting in tcgen05.alloc for a persistent neighbour would
+  // wait for good)
+  static constexpr int SMEM = SMEM_USED > 120 * 1024 ? SMEM_USED : 120 * 1024;
+  // registers per thread: the whole register file for one CTA per SM.  Each of the four SM
+  // sub-partitions holds 16384 registers for its share of the warps (allocated 256 per warp).
+  static constexpr int WARPS_PER_SUB = (THREADS / 32 + 3) / 4;
+  static constexpr int MAXREG_RAW = (16384 / (WARPS_PER_SUB * 256)) * 8;
+  static constexpr int MAXREG = MAXREG_RAW > 255 ? 255 : MAXREG_RAW;
+};
+
+// K blocks (16 complex each) of one tile that can be nonzero, and whether the tile is
+// written at all (lower_only tiles strictly above the diagonal are not)
+struct TileK {
+  int kb_lo, nkb;
+  bool live;
+};
+__device__ __forceinline__ TileK tile_k(const TcParams& p, int64_t m0, int64_t n0, int bnc) {
+  TileK t;
+  t.live = !(p.lower_only && n0 > m0 + kBM - 1);
+  int kb_lo = 0, kb_hi = (int)((p.K + 15) / 16);
+  if (p.a_upper) kb_lo = max(kb_lo, (int)(m0 / 16));
+  if (p.b_lower) kb_lo = max(kb_lo, (int)(n0 / 16));
+  if (p.a_lower) kb_hi = min(kb_hi, (int)((m0 + kBM - 1) / 16) + 1);
+  if (p.b_upper) kb_hi = min(kb_hi, (int)((n0 + bnc - 1) / 16) + 1);
+  t.kb_lo = kb_lo;
+  t.nkb = max(kb_hi - kb_lo, 0);
+  return t;
+}
+
+struct TileId {
+  int64_t bz, m0, n0;
+};
+__device__ __forceinline__ TileId tile_id(int64_t t, int64_t tm, int64_t tn, int bnc) {
+  const int64_t per = tm * tn, r = t % per;
+  return TileId{t / per, (r / tn) * kBM, (r % tn) * bnc};
+}
+
+// Producer cursor over the (tile, K block) pairs of this CTA that have work.
+template <class Cfg>
+struct PCursor {
+  int64_t t;      // tile index
+  int k;          // K block within the tile (0 .. nkb - 1)
+  bool valid;
+  int kb_lo, nkb;
+  OpRows ra, rb;
+};
+
+template <class Cfg, bool A64, bool B64>
+__device__ __forceinline__ void pcursor_tile(const TcParams& p, PCursor<Cfg>& c, int64_t total,
+                                             int64_t tm, int64_t tn) {
+  // first tile >= c.t (in steps of gridDim.x) with live K blocks
+  for (; c.t < total; c.t += gridDim.x) {
+    const TileId id = tile_id(c.t, tm, tn, Cfg::BNC_);
+    const TileK tk = tile_k(p, id.m0, id.n0, Cfg::BNC_);
+    if (!tk.live || tk.nkb == 0) continue;
+    const int64_t ba = p.a_mod ? (p.a_q0 + id.bz) % p.a_mod : id.bz;
+    const int64_t bb = p.b_mod ? (p.b_q0 + id.bz) % p.b_mod : id.bz;
+    c.kb_lo = tk.kb_lo;
+    c.nkb = tk.nkb;
+    c.k = 0;
+    c.ra = op_rows<Cfg::A_CHUNKS, Cfg::NPROD>(p.A, p.lda, p.sA, ba, p.M, id.m0, Pair<A64>::kBytes);
+    c.rb = op_rows<Cfg::B_CHUNKS, Cfg::NPROD>(p.Bt, p.ldb, p.sB, bb, p.N, id.n0, Pair<B64>::kBytes);
+    c.valid = true;
+    return;
+  }
+  c.valid = false;
+}
+
+template <class Cfg, bool A64, bool B64>
+__device__ __forceinline__ void pcursor_next(const TcParams& p, PCursor<Cfg>& c, int64_t total,
+                                             int64_t tm, int64_t tn) {
+  if (++c.k < c.nkb) return;
+  c.t += gridDim.x;
+  pcursor_tile<Cfg, A64, B64>(p, c, total, tm, tn);
+}
+
+template <int BNC, int NP, int ST, bool A64, bool B64>
+__global__ void __maxnreg__((PCfg<BNC, NP, ST>::MAXREG))
+    k_tc_persistent(const __grid_constant__ TcParams p, int64_t batch) {
+  using PC = PCfg<BNC, NP, ST>;
+  using Cfg = TileCfg<BNC, NP, ST>;
+  constexpr int kStages = ST;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  float* epi = reinterpret_cast<float*>(smem + kStages * Cfg::STAGE);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * Cfg::STAGE + PC::EPI_BYTES);
+  // bars[0..ST) full, [ST..2ST) empty, acc_full[2], acc_empty[2], done, then the TMEM base
+  uint64_t* acc_full = bars + 2 * kStages;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* done_bar = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done_bar + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t tm = (p.M + kBM - 1) / kBM, tn = (p.N + BNC - 1) / BNC;
+  const int64_t total = tm * tn * batch;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(smem_u32(&bars[s]), Cfg::NPW);
+      mbar_init(smem_u32(&bars[kStages + s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&acc_full[b]), 1);
+      mbar_init(smem_u32(&acc_empty[b]), 4);  // one arrival per epilogue warp
+    }
+    mbar_init(smem_u32(done_bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == PC::MMA_WARP) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"((uint32_t)PC::TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < Cfg::NPW) {
+    // ---------------- producers ----------------
+    constexpr int kAhead = (NP == 256) ? 2 : 1;
+    PCursor<Cfg> L, S;
+    L.t = blockIdx.x;
+    pcursor_tile<Cfg, A64, B64>(p, L, total, tm, tn);
+    S = L;
+    int64_t g = 0;  // stage sequence number
+    auto step = [&](Staging<Cfg, A64, B64>& st) -> bool {
+      const int s = (int)(g % kStages);
+      const uint32_t ph = (uint32_t)(g / kStages) & 1u;
+      if (!mbar_wait(smem_u32(&bars[kStages + s]), ph ^ 1u)) return false;
+      unsigned char* sp = smem + s * Cfg::STAGE;
+      const uint32_t a_hi = smem_u32(sp), a_lo = a_hi + Cfg::A_PLANE;
+      const uint32_t b_hi = a_lo + Cfg::A_PLANE, b_lo = b_hi + Cfg::B_PLANE;
+      st.store(p, a_hi, a_lo, b_hi, b_lo);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&bars[s]));
+      if (L.valid) {
+        st.load(p, L.ra, L.rb, (int64_t)(L.kb_lo + L.k) * 16);
+        pcursor_next<Cfg, A64, B64>(p, L, total, tm, tn);
+      }
+      pcursor_next<Cfg, A64, B64>(p, S, total, tm, tn);
+      ++g;
+      return true;
+    };
+    if constexpr (kAhead == 2) {
+      Staging<Cfg, A64, B64> st0, st1;
+      if (L.valid) {
+        st0.load(p, L.ra, L.rb, (int64_t)(L.kb_lo + L.k) * 16);
+        pcursor_next<Cfg, A64, B64>(p, L, total, tm, tn);
+      }
+      if (L.valid) {
+        st1.load(p, L.ra, L.rb, (int64_t)(L.kb_lo + L.k) * 16);
+        pcursor_next<Cfg, A64, B64>(p, L, total, tm, tn);
+      }
+      while (S.valid) {
+        if (!step(st0)) break;
+        if (!S.valid || !step(st1)) break;
+      }
+    } else {
+      Staging<Cfg, A64, B64> st0;
+      if (L.valid) {
+        st0.load(p, L.ra, L.rb, (int64_t)(L.kb_lo + L.k) * 16);
+        pcursor_next<Cfg, A64, B64>(p, L, total, tm, tn);
+      }
+      while (S.valid)
+        if (!step(st0)) break;
+    }
+  } else if (warp == PC::MMA_WARP) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int64_t g = 0, u = 0;  // stage sequence, accumulator uses
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < total && ok; t += gridDim.x) {
+        const TileId id = tile_id(t, tm, tn, BNC);
+        const TileK tk = tile_k(p, id.m0, id.n0, BNC);
+        if (!tk.live || tk.nkb == 0) continue;
+        const int b = (int)(u & 1);
+        if (!mbar_wait(smem_u32(&acc_empty[b]), (uint32_t)((u >> 1) & 1) ^ 1u)) { ok = false; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc_t = tmem + (uint32_t)(b * Cfg::NR);
+        for (int it = 0; it < tk.nkb; ++it, ++g) {
+          const int s = (int)(g % kStages);
+          const uint32_t ph = (uint32_t)(g / kStages) & 1u;
+          if (!mbar_wait(smem_u32(&bars[s]), ph)) { ok = false; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a_hi = smem_u32(smem + s * Cfg::STAGE), a_lo = a_hi + Cfg::A_PLANE;
+          const uint32_t b_hi = a_lo + Cfg::A_PLANE, b_lo = b_hi + Cfg::B_PLANE;
+#pragma unroll
+          for (int kk = 0; kk < kBKR / 8; ++kk) {
+            const uint32_t o = (uint32_t)kk * 32;
+            const uint64_t ah = make_desc(a_hi + o), al = make_desc(a_lo + o);
+            const uint64_t bh = make_desc(b_hi + o), bl = make_desc(b_lo + o);
+            const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+            mma_tf32(acc_t, al, bh, Cfg::IDESC, acc);
+            mma_tf32(acc_t, ah, bl, Cfg::IDESC, 1u);
+            mma_tf32(acc_t, ah, bh, Cfg::IDESC, 1u);
+          }
+          mma_commit(smem_u32(&bars[kStages + s]));
+        }
+        if (!ok) break;
+        mma_commit(smem_u32(&acc_full[b]));
+        ++u;
+      }
+      // every MMA this lane issued has retired before TMEM is released
+      mma_commit(smem_u32(done_bar));
+      mbar_wait(smem_u32(done_bar), 0u);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue: TMEM -> registers -> smem -> coalesced rows ----------------
+    const int q = warp & 3;  // TMEM lane quadrant
+    float* buf = epi + (warp - PC::EPI_WARP0) * 32 * PC::EPI_PITCH;
+    int64_t u = 0;
+    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+      const TileId id = tile_id(t, tm, tn, BNC);
+      const TileK tk = tile_k(p, id.m0, id.n0, BNC);
+      if (!tk.live) continue;
+      const bool have = tk.nkb > 0;
+      const int b = (int)(u & 1);
+      if (have) {
+        if (!mbar_wait(smem_u32(&acc_full[b]), (uint32_t)((u >> 1) & 1))) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      }
+      const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * Cfg::NR);
+#pragma unroll 1
+      for (int j = 0; j < Cfg::NR / 32; ++j) {
+        uint32_t v[32];
+        if (have) {
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+              "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+              "%28, %29, %30, %31}, [%32];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+                "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+                "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+                "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+                "=r"(v[31])
+              : "r"(trow + (uint32_t)(j * 32)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (j == Cfg::NR / 32 - 1) {
+            // the accumulator is read out: the MMA lane may reuse it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+          }
+        } else {
+#pragma unroll
+          for (int x = 0; x < 32; ++x) v[x] = 0u;
+        }
+        float4* dst = reinterpret_cast<float4*>(buf + lane * PC::EPI_PITCH);
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+          dst[x] = make_float4(__uint_as_float(v[4 * x]), __uint_as_float(v[4 * x + 1]),
+                               __uint_as_float(v[4 * x + 2]), __uint_as_float(v[4 * x + 3]));
+        __syncwarp();
+        // 32 rows x 16 complex columns: lanes 8 r' .. 8 r' + 7 write one row (128 bytes)
+        const int64_t nc = id.n0 + j * 16 + (lane & 7) * 2;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int rr = 4 * i + (lane >> 3);
+          const int64_t m = id.m0 + q * 32 + rr;
+          if (m >= p.M) continue;
+          const float4 val = *reinterpret_cast<const float4*>(buf + rr * PC::EPI_PITCH + (lane & 7) * 4);
+          float2* cp = p.C + id.bz * p.sC + m * p.ldc + nc;
+          if (nc + 1 < p.N && ((reinterpret_cast<uintptr_t>(cp) & 15) == 0)) {
+            *reinterpret_cast<float4*>(cp) = val;
+          } else {
+            if (nc < p.N) cp[0] = make_float2(val.x, val.y);
+            if (nc + 1 < p.N) cp[1] = make_float2(val.z, val.w);
+          }
+        }
+        __syncwarp();
+      }
+      if (have) ++u;
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == PC::MMA_WARP) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"((uint32_t)PC::TMEM_COLS)
+                 : "memory");
+  }
+}
+
+template <int BNC, int NP, int ST, bool A64, bool B64>
+void launch_tc_persistent(const TcParams& p, int64_t batch, cudaStream_t s) {
+  using PC = PCfg<BNC, NP, ST>;
+  auto fn = k_tc_persistent<BNC, NP, ST, A64, B64>;
+  static int slots[64] = {};
+  int dev = 0;
+  CQ_CHECK_CUDA(cudaGetDevice(&dev));
+  if (dev < 64 && slots[dev] == 0) {
+    CQ_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, PC::SMEM));
+    int per_sm = 0, sms = 0;
+    CQ_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PC::THREADS, PC::SMEM));
+    CQ_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // co-resident CTAs must fit their TMEM accumulators (512 columns per SM): tcgen05.alloc of
+    // a CTA would otherwise wait for another CTA that never exits
+    CQ_REQUIRE(per_sm >= 1 && per_sm * PC::TMEM_COLS <= 512, COQUI_B200_ECUDA,
+               "tc_cgemm: persistent tile configuration does not fit an SM (" +
+                   std::to_string(per_sm) + " CTAs of " + std::to_string(PC::TMEM_COLS) +
+                   " TMEM columns)");
+    slots[dev] = sms * per_sm;
+  }
+  const int64_t tiles = ((p.M + kBM - 1) / kBM) * ((p.N + BNC - 1) / BNC) * batch;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(tiles, dev < 64 ? slots[dev] : 148));
+  fn<<<(unsigned)grid, PC::THREADS, PC::SMEM, s>>>(p, batch);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
 template <int BNC, int NP, int ST, bool A64, bool B64>
 void launch_tc(const TcParams& p, int64_t batch, cudaStream_t s) {
   using Cfg = TileCfg<BNC, NP, ST>;
@@ -600,12 +938,23 @@ void launch_tc(const TcParams& p, int64_t batch, cudaStream_t s) {
   }
 }
 
-// Tile configurations: (BNC, producer threads, stages).  Every configuration forms the same
-// products in the same K order, so the results are identical and only the speed differs.
-constexpr int kNumCfg = 6;
+// Tile configurations: (BNC, producer threads, stages), 0-5 with one tile per CTA
+// (k_tc_cgemm) and 6-11 the same tiles in the persistent kernel.  Every configuration forms
+// the same products in the same K order, so the results are identical and only the speed
+// differs.
+constexpr int kNumCfg = 12;
 
 template <bool A64, bool B64>
 void launch_cfg(int cfg, const TcParams& p, int64_t batch, cudaStream_t s) {
+  switch (cfg) {
+    case 6: return launch_tc_persistent<32, 128, 1, A64, B64>(p, batch, s);
+    case 7: return launch_tc_persistent<64, 128, 1, A64, B64>(p, batch, s);
+    case 8: return launch_tc_persistent<128, 128, 1, A64, B64>(p, batch, s);
+    case 9: return launch_tc_persistent<32, 256, 2, A64, B64>(p, batch, s);
+    case 10: return launch_tc_persistent<64, 256, 2, A64, B64>(p, batch, s);
+    case 11: return launch_tc_persistent<128, 256, 2, A64, B64>(p, batch, s);
+    default: break;
+  }
   switch (cfg) {
     case 0: launch_tc<32, 128, 1, A64, B64>(p, batch, s); break;
     case 1: launch_tc<64, 128, 1, A64, B64>(p, batch, s); break;
