@@ -24,6 +24,7 @@
 #include "mlp.cuh"
 #include "scgw.cuh"
 #include "tc_gemm.cuh"
+#include "zgemm.cuh"
 
 using cq::Error;
 using cq::KGrid;
@@ -46,10 +47,6 @@ const char* kVersion = "coqui_b200 0.1.0 (sm_100a)";
   } while (0)
 
 using cq::DevBuf;
-
-cublasOperation_t blas_op(char c) {
-  return c == 'N' ? CUBLAS_OP_N : (c == 'T' ? CUBLAS_OP_T : CUBLAS_OP_C);
-}
 
 }  // namespace
 
@@ -238,30 +235,52 @@ template <typename F> int guarded(Ctx* c, F&& f) {
   }
 }
 
-// Row-major complex128 GEMM through cuBLAS (column-major): C = alpha op(A) op(B) + beta C,
-// batched with constant strides.
+// Row-major complex128 GEMM on the FP64 tensor cores (zgemm.cu): C = alpha op(A) op(B) +
+// beta C, batched with constant strides (0 broadcasts an operand).
 void zgemm_rm(Ctx* c, char opA, char opB, int64_t M, int64_t N, int64_t K, double2 alpha,
               const double2* A, int64_t lda, int64_t sA, const double2* B, int64_t ldb,
               int64_t sB, double2 beta, double2* C, int64_t ldc, int64_t sC, int64_t batch) {
-  CQ_CHECK_BLAS(cublasZgemmStridedBatched(
-      c->blas, blas_op(opB), blas_op(opA), (int)N, (int)M, (int)K,
-      reinterpret_cast<const cuDoubleComplex*>(&alpha), reinterpret_cast<const cuDoubleComplex*>(B),
-      (int)ldb, sB, reinterpret_cast<const cuDoubleComplex*>(A), (int)lda, sA,
-      reinterpret_cast<const cuDoubleComplex*>(&beta), reinterpret_cast<cuDoubleComplex*>(C),
-      (int)ldc, sC, (int)batch));
+  cq::ZgemmArgs z;
+  z.opA = opA;
+  z.opB = opB;
+  z.M = M;
+  z.N = N;
+  z.K = K;
+  z.alpha = alpha;
+  z.beta = beta;
+  z.A = A;
+  z.lda = lda;
+  z.sA = sA;
+  z.B = B;
+  z.ldb = ldb;
+  z.sB = sB;
+  z.C = C;
+  z.ldc = ldc;
+  z.sC = sC;
+  z.batch = batch;
+  cq::zgemm(z, c->st);
 }
 
 // The same with per-problem operand pointers (device arrays of batch pointers each).
 void zgemm_rm_ptrs(Ctx* c, char opA, char opB, int64_t M, int64_t N, int64_t K, double2 alpha,
                    const double2* const* A, int64_t lda, const double2* const* B, int64_t ldb,
                    double2 beta, double2* const* C, int64_t ldc, int64_t batch) {
-  CQ_CHECK_BLAS(cublasZgemmBatched(
-      c->blas, blas_op(opB), blas_op(opA), (int)N, (int)M, (int)K,
-      reinterpret_cast<const cuDoubleComplex*>(&alpha),
-      reinterpret_cast<const cuDoubleComplex* const*>(B), (int)ldb,
-      reinterpret_cast<const cuDoubleComplex* const*>(A), (int)lda,
-      reinterpret_cast<const cuDoubleComplex*>(&beta), reinterpret_cast<cuDoubleComplex* const*>(C),
-      (int)ldc, (int)batch));
+  cq::ZgemmArgs z;
+  z.opA = opA;
+  z.opB = opB;
+  z.M = M;
+  z.N = N;
+  z.K = K;
+  z.alpha = alpha;
+  z.beta = beta;
+  z.Ap = A;
+  z.lda = lda;
+  z.Bp = B;
+  z.ldb = ldb;
+  z.Cp = C;
+  z.ldc = ldc;
+  z.batch = batch;
+  cq::zgemm(z, c->st);
 }
 
 void upload(Ctx* c, void* dst, const void* src, size_t bytes) {
