@@ -39,6 +39,7 @@ SYMBOLS = [
     "coqui_b200_batch_last_error", "coqui_b200_batch_set_ir", "coqui_b200_batch_set_thc",
     "coqui_b200_batch_gw_iteration", "coqui_b200_batch_last_ms", "coqui_b200_set_autotune",
     "coqui_b200_tuned_shapes", "coqui_b200_set_tile_config", "coqui_b200_num_tile_configs",
+    "coqui_b200_set_wait_limit_ns",
 ]
 
 
@@ -137,6 +138,8 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_set_tile_config.restype = ctypes.c_int
     lib.coqui_b200_num_tile_configs.argtypes = []
     lib.coqui_b200_num_tile_configs.restype = ctypes.c_int
+    lib.coqui_b200_set_wait_limit_ns.argtypes = [ctypes.c_int, I64]
+    lib.coqui_b200_set_wait_limit_ns.restype = ctypes.c_int
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -580,3 +583,10 @@ def set_tile_config(cfg: int):
 
 def num_tile_configs() -> int:
     return int(load().coqui_b200_num_tile_configs())
+
+
+def set_wait_limit_ns(ns: int, device: int = 0):
+    """Time limit of the tensor-core kernels' bounded device waits (ns; <= 0: the default 2 s)."""
+    rc = load().coqui_b200_set_wait_limit_ns(int(device), int(ns))
+    if rc != OK:
+        raise CoquiB200Error(rc, "set_wait_limit_ns failed")

@@ -2122,4 +2122,14 @@ int coqui_b200_set_tile_config(int cfg) {
 
 int coqui_b200_num_tile_configs(void) { return cq::tc_num_cfgs(); }
 
+int coqui_b200_set_wait_limit_ns(int device, int64_t ns) {
+  try {
+    CQ_CHECK_CUDA(cudaSetDevice(device));
+    cq::tc_set_wait_ns(ns);
+    return COQUI_B200_OK;
+  } catch (const cq::Error& e) {
+    return e.code;
+  }
+}
+
 }  // extern "C"

@@ -34,6 +34,9 @@ namespace cq {
 namespace {
 
 __device__ int g_tc_error = 0;
+// time limit of every bounded wait (ns); 2 s unless a test shortens it
+constexpr unsigned long long kDefaultWaitNs = 2000000000ull;
+__device__ unsigned long long g_tc_wait_ns = kDefaultWaitNs;
 
 // Whether every row of an operand starts 16-byte aligned at even K: a complex64 operand needs
 // an aligned base and even row and batch strides; pre-split values are 16 bytes each.
@@ -118,18 +121,52 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return done != 0;
 }
 
+// try_wait that suspends the thread for at most hint_ns before reporting an incomplete phase
+__device__ __forceinline__ bool mbar_try_hint(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(bar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return done != 0;
+}
+
 // Bounded wait for the phase with the given parity; returns false (and flags) on timeout.
-// The clock is read only after a first failed attempt and then every 16 attempts.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  if (mbar_try(bar, parity)) return true;
-  const uint64_t t0 = global_ns();
-  for (uint32_t i = 1;; ++i) {
+// With the default limit the clock is read only after a first failed attempt and then every
+// 16 attempts; a shorter limit also bounds each attempt's suspension and is checked after
+// every attempt.
+__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, uint64_t limit) {
+  if (limit >= kDefaultWaitNs) {
     if (mbar_try(bar, parity)) return true;
-    if ((i & 15u) == 0 && global_ns() - t0 > 2000000000ull) {
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 1;; ++i) {
+      if (mbar_try(bar, parity)) return true;
+      if ((i & 15u) == 0 && global_ns() - t0 > limit) {
+        atomicExch(&g_tc_error, 1);
+        return false;
+      }
+    }
+  }
+  const uint32_t hint = (uint32_t)(limit < 1000000ull ? (limit > 0 ? limit : 1) : 1000000ull);
+  if (mbar_try_hint(bar, parity, hint)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    if (mbar_try_hint(bar, parity, hint)) return true;
+    if (global_ns() - t0 > limit) {
       atomicExch(&g_tc_error, 1);
       return false;
     }
   }
+}
+// the pipeline's waits: the current limit (g_tc_wait_ns)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, g_tc_wait_ns);
+}
+// the wait for issued tensor-core work to retire before tensor memory is released: always the
+// default limit, also when a test has shortened the pipeline's
+__device__ __forceinline__ bool mbar_drain(uint32_t bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, kDefaultWaitNs);
 }
 
 // Rounds to TF32 (10 explicit mantissa bits), to nearest with ties away from zero, as integer
@@ -362,9 +399,11 @@ __device__ __forceinline__ void tc_tile(const TcParams& p, int64_t bz, int64_t m
   constexpr int kStages = ST;
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * Cfg::STAGE);
-  // bars[0..ST) full, bars[ST..2ST) empty, bars[2ST] accumulator ready, then the TMEM base
+  // bars[0..ST) full, bars[ST..2ST) empty, bars[2ST] accumulator ready, bars[2ST + 1] all
+  // issued MMAs retired, then the TMEM base
   uint64_t* acc_bar = bars + 2 * kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 1);
+  uint64_t* done_bar = acc_bar + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (p.lower_only && n0 > m0 + kBM - 1) return;  // tile strictly above the diagonal
 
@@ -382,6 +421,7 @@ __device__ __forceinline__ void tc_tile(const TcParams& p, int64_t bz, int64_t m
       mbar_init(smem_u32(&bars[kStages + s]), 1);
     }
     mbar_init(smem_u32(acc_bar), 1);
+    mbar_init(smem_u32(done_bar), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == Cfg::NPW) {
@@ -520,6 +560,9 @@ __device__ __forceinline__ void tc_tile(const TcParams& p, int64_t bz, int64_t m
       mma_commit(smem_u32(&bars[kStages + s]));  // frees the stage once these MMAs retire
     }
     if (ok && nkb > 0) mma_commit(smem_u32(acc_bar));
+    // every issued MMA has retired before TMEM is released, also when a wait gave up
+    mma_commit(smem_u32(done_bar));
+    mbar_drain(smem_u32(done_bar), 0u);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -799,7 +842,7 @@ __global__ void __maxnreg__((PCfg<BNC, NP, ST>::MAXREG))
       }
       // every MMA this lane issued has retired before TMEM is released
       mma_commit(smem_u32(done_bar));
-      mbar_wait(smem_u32(done_bar), 0u);
+      mbar_drain(smem_u32(done_bar), 0u);
     }
     __syncwarp();
   } else {
@@ -1074,6 +1117,11 @@ void tc_cgemm_nt(const void* A, bool a_split, bool conj_a, int64_t lda, int64_t 
   else if (a_c128) dispatch_n<true, false>(p, batch, s);
   else if (b_c128) dispatch_n<false, true>(p, batch, s);
   else dispatch_n<false, false>(p, batch, s);
+}
+
+void tc_set_wait_ns(int64_t ns) {
+  const unsigned long long v = ns > 0 ? (unsigned long long)ns : kDefaultWaitNs;
+  CQ_CHECK_CUDA(cudaMemcpyToSymbol(g_tc_wait_ns, &v, sizeof(v)));
 }
 
 int tc_take_error() {

@@ -96,5 +96,8 @@ int tc_num_cfgs();
 // Returns (and clears) the device flag set when a bounded wait inside a tensor-core kernel
 // gave up (nonzero = a kernel timed out).
 int tc_take_error();
+// Time limit of the tensor-core kernels' bounded waits on the current device (ns; <= 0: the
+// default 2 s).
+void tc_set_wait_ns(int64_t ns);
 
 }  // namespace cq

@@ -304,6 +304,13 @@ COQUI_B200_API int64_t coqui_b200_tuned_shapes(void);
 COQUI_B200_API int coqui_b200_set_tile_config(int cfg);
 COQUI_B200_API int coqui_b200_num_tile_configs(void);
 
+/* Time limit (ns) of the bounded device-side waits of the tensor-core kernels on `device`
+   (ns <= 0 restores the default of 2 s).  A kernel whose wait runs out sets an error flag,
+   lets its issued tensor-core work retire, frees its tensor memory and returns; the call
+   that launched it returns COQUI_B200_ETIMEDOUT and the context stays usable.  A test hook
+   for that path (a limit of a few ns makes the waits run out); no reference counterpart. */
+COQUI_B200_API int coqui_b200_set_wait_limit_ns(int device, int64_t ns);
+
 /* Number of kernels this library launched since the context was created. */
 COQUI_B200_API int64_t coqui_b200_kernel_launches(const coqui_b200_ctx* ctx);
 
