@@ -526,8 +526,10 @@ def run_ours(args, rank, world, local):
         t64 = total_ms(c64)
         e64 = c64.rpa_energy(None)
         r64 = total_ms(c64)
-        fp64 = {"what": "the same path with complex128 storage, FP64 products (cuBLAS ZGEMM) and "
-                        "FP64 factorisations (cuSOLVER), one frequency at a time",
+        fp64 = {"what": "the same algorithm in FP64 on the library's own kernels: complex128 "
+                        "storage, FP64 tensor-core (DMMA) products with the same triangular "
+                        "structure, the same batched FP64 factorisation (whole inverse in FP64) "
+                        "and W = L E L^H, chunks of all (q, iW) problems",
                 "gw_iteration_ms": t64, "rpa_energy_ms": r64, "E_c": e64,
                 "max_abs_dSigma_mixed_vs_fp64": float(np.abs(Sh - S64).max()),
                 "max_abs_Sigma": float(np.abs(S64).max()),

@@ -421,6 +421,40 @@ bool chol_prefer_tiled(const std::vector<int64_t>& sizes) {
   return nmax >= 4 * b32::CB && total / ((double)sms * b32::MINB) < mx;
 }
 
+void launch_chol_inv_c128(const double2* M, double2* A, double* logdet, double2* trace, int* info,
+                          int64_t Np, int64_t nprob, cudaStream_t s) {
+  auto kern = p32::k_chol_pair<true, 2, 2, double2>;
+  const size_t smem = p32::smem_bytes<2, 2>();
+  CQ_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CQ_REQUIRE(nprob <= 2147483647, COQUI_B200_EINVAL, "chol: too many problems");
+  kern<<<(unsigned)nprob, p32::NT, smem, s>>>(M, A, logdet, trace, info, Np, 1 << 30);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
+// Z = U - I from the upper triangle U of A (complex128), zero below the diagonal
+__global__ void k_upper_minus_eye(const double2* __restrict__ A, double2* __restrict__ Z, int64_t n,
+                                  int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = i % (n * n), r = e / n, c = e % n;
+    double2 z = make_double2(0.0, 0.0);
+    if (c >= r) {
+      z = A[i];
+      if (c == r) z.x -= 1.0;
+    }
+    Z[i] = z;
+  }
+}
+
+void launch_upper_minus_eye(const double2* A, double2* Z, int64_t Np, int64_t nprob,
+                            cudaStream_t s) {
+  const int64_t total = Np * Np * nprob;
+  k_upper_minus_eye<<<grid_for(total, 256), 256, 0, s>>>(A, Z, Np, total);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
 int64_t chol_wave_size() {
   int dev = 0, sms = 148, per_sm = 0;
   CQ_CHECK_CUDA(cudaGetDevice(&dev));

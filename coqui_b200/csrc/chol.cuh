@@ -48,6 +48,15 @@ void launch_chol_tiled_strided(const float2* M, double2* A, double* logdet, doub
 // COQUI_B200_CHOL_TILED=1 or 0 forces the choice.
 bool chol_prefer_tiled(const std::vector<int64_t>& sizes);
 
+// FP64 form: A = I - M with M complex128 (lower triangle read), A <- C (lower, FP64), the
+// whole inverse C^{-H} in the upper triangle, logdet, trace, info per problem (four-warp
+// kernel, same arithmetic as the complex64 form).
+void launch_chol_inv_c128(const double2* M, double2* A, double* logdet, double2* trace, int* info,
+                          int64_t Np, int64_t nprob, cudaStream_t s);
+// Z = U - I from the upper triangle U of A, zero below the diagonal (complex128, batched).
+void launch_upper_minus_eye(const double2* A, double2* Z, int64_t Np, int64_t nprob,
+                            cudaStream_t s);
+
 // Problems one launch of the one-CTA factorisation (launch_chol_group_inv) runs at once on
 // the current device: SMs x resident CTAs per SM.  A batch of a multiple of this size leaves
 // no partly filled last wave.

@@ -162,8 +162,8 @@ __device__ __forceinline__ void zero(double2 (&acc)[AR][8]) {
 
 // acc <- block (i0.., k0..) of I - M, restricted to rb x kb and, unless off_diag, to the
 // lower triangle
-template <int AR>
-__device__ __forceinline__ void init_im(double2 (&acc)[AR][8], const float2* M, int64_t n,
+template <int AR, typename MT>
+__device__ __forceinline__ void init_im(double2 (&acc)[AR][8], const MT* M, int64_t n,
                                         int64_t i0, int64_t k0, int rb, int kb, bool off_diag,
                                         int tr0) {
 #pragma unroll
@@ -172,7 +172,7 @@ __device__ __forceinline__ void init_im(double2 (&acc)[AR][8], const float2* M, 
     for (int j = 0; j < 8; ++j) {
       const int r = fr_row(tr0, i), c = fr_col(j);
       if (r < rb && c < kb && (off_diag || c <= r)) {
-        const float2 m = M[(i0 + r) * n + k0 + c];
+        const MT m = M[(i0 + r) * n + k0 + c];
         acc[i][j] = make_double2(((i0 + r) == (k0 + c) ? 1.0 : 0.0) - (double)m.x, -(double)m.y);
       } else {
         acc[i][j] = make_double2(0, 0);
@@ -323,8 +323,8 @@ __device__ __forceinline__ void pipeline(int nit, Issue&& issue, Compute&& compu
 // on ib + 1, two tile rows each); AR = 1: row block ib alone, one tile row per warp.
 // L_i,j = [(I - M)_i,j - sum_kb L_i,kb L_j,kb^H] C_jj^{-H} with C_jj^{-H} read from the upper
 // triangle of the diagonal block.  SB / SA(stage, t): K-slice tiles; F(i): whole blocks.
-template <int AR, int STAGES, int NS, typename FB, typename FA, typename FF>
-__device__ __forceinline__ void panel_step(const float2* __restrict__ M, double2* __restrict__ A,
+template <int AR, int STAGES, int NS, typename MT, typename FB, typename FA, typename FF>
+__device__ __forceinline__ void panel_step(const MT* __restrict__ M, double2* __restrict__ A,
                                            int64_t n, int j, int ib, FB&& SB, FA&& SA, FF&& F) {
   constexpr int W = CB / NS;
   const int w = threadIdx.x >> 5;
@@ -367,8 +367,8 @@ __device__ __forceinline__ void panel_step(const float2* __restrict__ M, double2
 // One problem.  The block products stream K slices of width W = 32 / NS through STAGES
 // buffer sets (SB, SA0, SA1) of 32 x W values each; the diagonal factorisation, the panel
 // finalisation and the inverse columns reuse the same memory as whole 32 x 32 blocks F(0..2).
-template <bool INV, int STAGES, int NS>
-__device__ __forceinline__ void chol_problem(const float2* __restrict__ M, double2* __restrict__ A,
+template <bool INV, int STAGES, int NS, typename MT>
+__device__ __forceinline__ void chol_problem(const MT* __restrict__ M, double2* __restrict__ A,
                                              double* __restrict__ logdet,
                                              double2* __restrict__ trace, int* __restrict__ info,
                                              int64_t n, int inv_group) {
@@ -393,7 +393,7 @@ __device__ __forceinline__ void chol_problem(const float2* __restrict__ M, doubl
   double tr = 0, ti = 0;
   if (threadIdx.x < 64)
     for (int64_t i = threadIdx.x; i < n; i += 64) {
-      const float2 m = M[i * n + i];
+      const MT m = M[i * n + i];
       tr += m.x;
       ti += m.y;
     }
@@ -426,8 +426,8 @@ __device__ __forceinline__ void chol_problem(const float2* __restrict__ M, doubl
     // 2. panel, two row blocks per step, the last one alone when their number is odd:
     // L_i,j = [(I - M)_i,j - sum_kb L_i,kb L_j,kb^H] C_jj^{-H}
     int ib = j + 1;
-    for (; ib + 1 < nblk; ib += 2) panel_step<2, STAGES, NS>(M, A, n, j, ib, SB, SA, F);
-    if (ib < nblk) panel_step<1, STAGES, NS>(M, A, n, j, ib, SB, SA, F);
+    for (; ib + 1 < nblk; ib += 2) panel_step<2, STAGES, NS, MT>(M, A, n, j, ib, SB, SA, F);
+    if (ib < nblk) panel_step<1, STAGES, NS, MT>(M, A, n, j, ib, SB, SA, F);
   }
 
   if (INV) {
@@ -459,14 +459,15 @@ constexpr int min_blocks() {
   return smem_bytes<STAGES, NS>() > 64 * 1024 ? 2 : 4;
 }
 
-template <bool INV, int STAGES, int NS>
+// M: complex64 (the mixed form) or complex128 (the FP64 form)
+template <bool INV, int STAGES, int NS, typename MT = float2>
 __global__ void __launch_bounds__(NT, (min_blocks<STAGES, NS>()))
-    k_chol_pair(const float2* __restrict__ Mall, double2* __restrict__ Aall,
+    k_chol_pair(const MT* __restrict__ Mall, double2* __restrict__ Aall,
                 double* __restrict__ logdet, double2* __restrict__ trace, int* __restrict__ info,
                 int64_t n, int inv_group) {
   const int64_t p = blockIdx.x;
-  chol_problem<INV, STAGES, NS>(Mall + p * n * n, Aall + p * n * n, logdet + p, trace + p,
-                                info + p, n, inv_group);
+  chol_problem<INV, STAGES, NS, MT>(Mall + p * n * n, Aall + p * n * n, logdet + p, trace + p,
+                                    info + p, n, inv_group);
 }
 
 }  // namespace p32

@@ -6,6 +6,7 @@
 #include "dyson.cuh"
 #include "kernels.cuh"
 #include "tc_gemm.cuh"
+#include "zgemm.cuh"
 
 namespace cq {
 
@@ -52,33 +53,54 @@ __global__ void __launch_bounds__(256) k_herm_sum(const float2* __restrict__ DH,
 }
 
 // Hermitian completion: A[i][j] = conj(A[j][i]) for j > i (32 x 32 tiles on or above the
-// diagonal, the lower tile read through shared memory)
-__global__ void k_mirror_upper(float2* __restrict__ A, int64_t n, int64_t stride) {
-  __shared__ float2 tile[32][33];
+// diagonal, the lower tile read through shared memory); complex64 or complex128
+template <typename C>
+__global__ void k_mirror_upper(C* __restrict__ A, int64_t n, int64_t stride) {
+  __shared__ C tile[32][33];
   const int64_t i0 = (int64_t)blockIdx.y * 32, j0 = (int64_t)blockIdx.x * 32;
   if (j0 < i0) return;
-  float2* a = A + (int64_t)blockIdx.z * stride;
+  C* a = A + (int64_t)blockIdx.z * stride;
   for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {  // lower tile (j0.., i0..)
     const int64_t r = j0 + ty, c = i0 + threadIdx.x;
-    tile[ty][threadIdx.x] = (r < n && c < n) ? a[r * n + c] : make_float2(0.f, 0.f);
+    tile[ty][threadIdx.x] = (r < n && c < n) ? a[r * n + c] : mk<C>(0.0, 0.0);
   }
   __syncthreads();
   for (int ty = threadIdx.y; ty < 32; ty += blockDim.y) {
     const int64_t i = i0 + ty, j = j0 + threadIdx.x;
     if (i < n && j < n && j > i) {
-      const float2 v = tile[threadIdx.x][ty];  // A[j][i]
-      a[i * n + j] = make_float2(v.x, -v.y);
+      const C v = tile[threadIdx.x][ty];  // A[j][i]
+      a[i * n + j] = mk<C>(v.x, -v.y);
     }
   }
 }
 
-void launch_mirror_upper(float2* A, int64_t n, int64_t nbatch, cudaStream_t s, int64_t stride) {
+template <typename C>
+void mirror_upper(C* A, int64_t n, int64_t nbatch, cudaStream_t s, int64_t stride) {
   CQ_REQUIRE(nbatch <= 65535, COQUI_B200_EINVAL, "mirror: too many problems per launch");
   const unsigned t = (unsigned)((n + 31) / 32);
-  k_mirror_upper<<<dim3(t, t, (unsigned)nbatch), dim3(32, 8), 0, s>>>(A, n, stride > 0 ? stride : n * n);
+  k_mirror_upper<C><<<dim3(t, t, (unsigned)nbatch), dim3(32, 8), 0, s>>>(A, n, stride > 0 ? stride : n * n);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
 }
+
+void launch_mirror_upper(float2* A, int64_t n, int64_t nbatch, cudaStream_t s, int64_t stride) {
+  mirror_upper<float2>(A, n, nbatch, s, stride);
+}
+
+// FP64 form: E = Z + Z^H + F (Hermitian, written whole) with Z = D^H upper triangular and F
+// Hermitian with only its lower triangle formed
+__global__ void k_herm_sum_c128(const double2* __restrict__ Z, const double2* __restrict__ F,
+                                double2* __restrict__ E, int64_t n, int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / (n * n), e = i % (n * n), r = e / n, c = e % n;
+    const int64_t t = b * n * n + c * n + r;  // the transposed element
+    const double2 z = Z[i], zt = Z[t];
+    const double2 f = r >= c ? F[i] : make_double2(F[t].x, -F[t].y);
+    E[i] = make_double2(z.x + zt.x + f.x, z.y - zt.y + f.y);
+  }
+}
+
 
 void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t nbatch,
                                    cudaStream_t s) {
@@ -119,29 +141,25 @@ int cholesky_lower_batched(cusolverDnHandle_t sol, double2* A, int64_t Np, int64
 void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
                DevBuf<unsigned char>& scratch, cudaStream_t s, std::vector<double>* logdet,
                std::vector<double2>* trace) {
+  (void)blas;
+  (void)sol;
   const int64_t Np = a.Np, NN = Np * Np, nq = a.nq, nw = a.nw;
   const size_t es = a.mixed ? sizeof(float2) : sizeof(double2);
-  // per problem: T1 (es), M (es), A (c128, own region in mixed mode), Y (c128 if want_w)
-  const size_t per = NN * (es + es + (a.mixed ? sizeof(double2) : 0) +
-                           (a.want_w ? sizeof(double2) : 0)) +
-                     4 * sizeof(void*) + sizeof(int) + sizeof(double) + sizeof(double2) + 64;
-  // FP64 form: one frequency at a time (cuBLAS strided batches over q); mixed form: chunks of
-  // the flattened (w, q) problem list, per-q operands addressed periodically.
-  // mixed form: as many problems per chunk as ~60% of the free device memory allows, so the
-  // FP64 factorisation kernel sees whole waves of problems (one CTA per problem)
-  size_t budget = (size_t)4 << 30;
-  if (a.mixed) {
-    size_t fr = 0, tot = 0;
-    CQ_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
-    budget = std::max(scratch.n, (size_t)(0.6 * (double)(fr + scratch.n)));
-    // while a graph is captured the scratch keeps its size (no device allocation or free
-    // inside the capture) when it holds at least one problem
-    if (a.keep_scratch && scratch.n >= per + 1024) budget = scratch.n - 1024;
-  }
+  // per problem: T1 (es), M (es), A (c128), Y (c128; the mixed form's W operands)
+  const size_t per = NN * (es + es + sizeof(double2) + (a.mixed && a.want_w ? sizeof(double2) : 0)) +
+                     64;
+  // Chunks of the flattened (w, q) problem list (per-q operands addressed periodically), as
+  // many problems per chunk as ~60% of the free device memory allows, so the factorisation
+  // kernel sees whole waves of problems (one CTA per problem)
+  size_t fr = 0, tot = 0;
+  CQ_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+  size_t budget = std::max(scratch.n, (size_t)(0.6 * (double)(fr + scratch.n)));
+  // while a graph is captured the scratch keeps its size (no device allocation or free inside
+  // the capture) when it holds at least one problem
+  if (a.keep_scratch && scratch.n >= per + 1024) budget = scratch.n - 1024;
   const int64_t nprob = nw * nq;
-  int64_t nbq = a.mixed ? std::max<int64_t>(1, std::min<int64_t>(nprob, (int64_t)(budget / per)))
-                        : std::max<int64_t>(1, std::min<int64_t>(nq, (int64_t)(budget / per)));
-  if (a.mixed && nbq < nprob) {
+  int64_t nbq = std::max<int64_t>(1, std::min<int64_t>(nprob, (int64_t)(budget / per)));
+  if (nbq < nprob) {
     // several chunks: whole waves of the one-CTA factorisation per chunk (a chunk of 1.5 waves
     // leaves half the GPU idle during its second wave)
     const int64_t wave = chol_wave_size();
@@ -156,57 +174,22 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
   };
   unsigned char* T1 = carve(nbq * NN * es);
   unsigned char* Mb = carve(nbq * NN * es);
-  double2* A = a.mixed ? (double2*)carve(nbq * NN * sizeof(double2)) : (double2*)T1;
-  double2* Y = a.want_w ? (double2*)carve(nbq * NN * sizeof(double2)) : nullptr;
-  double2** dptrA = (double2**)carve(nbq * sizeof(void*));
-  double2** dptrY = (double2**)carve(nbq * sizeof(void*));
-  int* dinfo = (int*)carve(nbq * sizeof(int));
-  double* dld = (double*)carve(nbq * sizeof(double));
-  double2* dtr = (double2*)carve(nbq * sizeof(double2));
-
-  std::vector<double2*> hA(nbq), hY(nbq);
-  for (int64_t i = 0; i < nbq; ++i) {
-    hA[i] = A + i * NN;
-    hY[i] = Y ? Y + i * NN : nullptr;
-  }
-  if (!a.mixed) {  // pointer arrays of the cuSOLVER / cuBLAS batched calls (FP64 form)
-    CQ_CHECK_CUDA(cudaMemcpyAsync(dptrA, hA.data(), nbq * sizeof(void*), cudaMemcpyHostToDevice, s));
-    CQ_CHECK_CUDA(cudaMemcpyAsync(dptrY, hY.data(), nbq * sizeof(void*), cudaMemcpyHostToDevice, s));
-  }
-  CQ_REQUIRE(!a.mixed || (a.info && a.logdet && a.trace), COQUI_B200_EINVAL,
-             "dyson_run: result arrays missing");
+  double2* A = (double2*)carve(nbq * NN * sizeof(double2));
+  double2* Y = a.mixed && a.want_w ? (double2*)carve(nbq * NN * sizeof(double2)) : nullptr;
+  CQ_REQUIRE(a.info && a.logdet && a.trace, COQUI_B200_EINVAL, "dyson_run: result arrays missing");
 
   if (a.want_e) {
     logdet->assign(nw * nq, 0.0);
     trace->assign(nw * nq, make_double2(0, 0));
   }
-  std::vector<int> info_all;
-  std::vector<double> ld_h(nbq);
-  std::vector<double2> tr_h(nbq);
-  std::vector<int> info_h(nbq);
-
-  const double2 one = make_double2(1, 0), zero = make_double2(0, 0), mone = make_double2(-1, 0);
-  // chunk list: (first flattened problem, count)
-  std::vector<std::pair<int64_t, int64_t>> chunks;
-  if (a.mixed) {
-    for (int64_t p0 = 0; p0 < nprob; p0 += nbq) chunks.emplace_back(p0, std::min(nbq, nprob - p0));
-  } else {
-    for (int64_t n = 0; n < nw; ++n)
-      for (int64_t q0 = 0; q0 < nq; q0 += nbq) chunks.emplace_back(n * nq + q0, std::min(nbq, nq - q0));
-  }
-  for (const auto& ch : chunks) {
+  for (int64_t p0 = 0; p0 < nprob; p0 += nbq) {
+    const int64_t nb = std::min(nbq, nprob - p0);
+    const int64_t q0 = p0 % nq;
+    unsigned char* Pi = a.PW + (size_t)p0 * NN * es;
+    const float2* Lc = a.Lc;  // mixed form: complex64 factors, addressed periodically in q
+    const float2* LHc = a.LHc;
+    // M = L^H (Pi L)
     {
-      const int64_t p0 = ch.first, nb = ch.second;
-      const int64_t q0 = p0 % nq;
-      unsigned char* Pi = a.PW + (size_t)p0 * NN * es;
-      // the mixed form addresses the per-q factors periodically from their bases
-      const double2* L = a.L + q0 * NN;
-      const double2* LH = a.LH + q0 * NN;
-      const float2* Lc = a.Lc;    // mixed form: complex64 factors, addressed periodically in q
-      const float2* LHc = a.LHc;
-      const double2* V = a.V + q0 * NN;
-      // M = L^H (Pi L)
-      {
       Prof::Scope sc(a.prof, "dyson_M_gemm");
       if (a.mixed) {
         // P1 = L^H Pi  (Pi Hermitian: B(k, n) = Pi[k][n] = conj(Pi[n][k]))
@@ -226,151 +209,166 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
         tc_cgemm_nt(LHc, false, false, Np, NN, T1, false, true, Np, NN, (float2*)Mb, Np, NN, Np, Np,
                     Np, nb, s, s2);
       } else {
-        // row-major C = A B  ->  column-major C^T = B^T A^T
-        CQ_BLAS(cublasZgemmStridedBatched(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)Np, (int)Np, (int)Np,
-                                          (const cuDoubleComplex*)&one, (const cuDoubleComplex*)L,
-                                          (int)Np, NN, (const cuDoubleComplex*)Pi, (int)Np, NN,
-                                          (const cuDoubleComplex*)&zero, (cuDoubleComplex*)T1,
-                                          (int)Np, NN, (int)nb));
-        CQ_BLAS(cublasZgemmStridedBatched(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)Np, (int)Np, (int)Np,
-                                          (const cuDoubleComplex*)&one, (const cuDoubleComplex*)T1,
-                                          (int)Np, NN, (const cuDoubleComplex*)LH, (int)Np, NN,
-                                          (const cuDoubleComplex*)&zero, (cuDoubleComplex*)Mb,
-                                          (int)Np, NN, (int)nb));
-        launch_eye_minus<double>((const double2*)Mb, A, Np, nb, s);
-      }
-      }
-      // I - M = C C^H (FP64)
-      // above one kInvGroup the off-group blocks of the inverse come from the tensor cores
-      const bool tc_inverse = a.mixed && a.want_w && Np > kInvGroup;
-      if (a.mixed) {
-        Prof::Scope sc(a.prof, "dyson_chol_inv");
-        if (tc_inverse && chol_prefer_tiled(std::vector<int64_t>((size_t)nb, Np)))
-          launch_chol_tiled_strided((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0,
-                                    Np, nb, s);  // few large problems: many CTAs per problem
-        else if (tc_inverse)
-          launch_chol_group_inv((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0, Np,
-                                nb, s);
-        else
-          launch_chol_inv((const float2*)Mb, A, a.want_w ? (float2*)Y : nullptr, a.logdet + p0,
-                          a.trace + p0, a.info + p0, Np, nb, s);
-      } else {
-        Prof::Scope sc(a.prof, "dyson_potrf");
-        potrf_ptrs(sol, dptrA, Np, dinfo, nb);
-      }
-      if (!a.mixed)
-        CQ_CHECK_CUDA(cudaMemcpyAsync(info_h.data(), dinfo, nb * sizeof(int), cudaMemcpyDeviceToHost, s));
-      if (a.want_e && !a.mixed) {
-        Prof::Scope sc(a.prof, "rpa_logdet");
-        if (a.mixed)
-          launch_logdet_trace<float>(A, (const float2*)Mb, dld, dtr, Np, nb, s);
-        else
-          launch_logdet_trace<double>(A, (const double2*)Mb, dld, dtr, Np, nb, s);
-        CQ_CHECK_CUDA(cudaMemcpyAsync(ld_h.data(), dld, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CQ_CHECK_CUDA(cudaMemcpyAsync(tr_h.data(), dtr, nb * sizeof(double2), cudaMemcpyDeviceToHost, s));
-      }
-      if (a.want_w && a.mixed) {
-        // W = L E L^H with E = (I - M)^{-1} - I = D + D^H + D^H D, D = C^{-1} - I: no
-        // cancellation against V, so the split-TF32 products keep W to ~1e-8.
-        if (tc_inverse) {
-          // U = C^{-H} by doubling: FP64 inverses of the kInvGroup diagonal groups, then for
-          // each level b the pairs of diagonal blocks (r0: b, r1: b1) get
-          //   U01 = -U00 C10^H U11
-          // as two split-TF32 products.  Z holds U - I (the D^H of the W products), Zl holds
-          // U^H - I where a later level needs it, Zc = -C off the groups.
-          Prof::Scope sc(a.prof, "dyson_tc_inverse");
-          float2* Z = (float2*)Y;
-          float2* Zl = (float2*)Y + nbq * NN;
-          float2* Zc = (float2*)T1;
-          float2* S = (float2*)Mb;
-          launch_chol_split(A, Z, Zl, Zc, Np, nb, s);
-          for (int64_t b = kInvGroup; b < Np; b *= 2) {
-            for (int64_t r0 = 0; r0 + b < Np; r0 += 2 * b) {
-              const int64_t r1 = r0 + b, b1 = std::min(b, Np - r1);
-              // S = U00 (-C10)^H  (b x b1, K = b): A = Z + I on the 00 block (upper)
-              TcStructure t1;
-              t1.a_upper = true;
-              t1.a_ident = true;
-              tc_cgemm_nt(Z + r0 * Np + r0, false, false, Np, NN, Zc + r1 * Np + r0, false, true,
-                          Np, NN, S + r0 * Np + r1, Np, NN, b, b1, b, nb, s, t1);
-              // U01 = S U11 with U11(k, n) = conj(Zl[n][k]) + delta  (b x b1, K = b1)
-              TcStructure t2;
-              t2.b_upper = true;
-              t2.b_ident = true;
-              tc_cgemm_nt(S + r0 * Np + r1, false, false, Np, NN, Zl + r1 * Np + r1, false, true,
-                          Np, NN, Z + r0 * Np + r1, Np, NN, b, b1, b1, nb, s, t2);
-              if (2 * b < Np) launch_block_adjoint(Z, Zl, Np, r0, r1, b, b1, nb, s);
-            }
-          }
-        }
-        const float2* Z = (const float2*)Y;  // DH = C^{-H} - I
-        Prof::Scope sc(a.prof, "dyson_W_gemm");
-        float2* F = (float2*)T1;
-        float2* E = (float2*)Mb;
-        // F = D^H D  (B(k, n) = D[k][n] = conj(DH[n][k]))
-        TcStructure s3;
-        s3.a_upper = true;     // D^H upper
-        s3.b_lower = true;     // D lower
-        s3.lower_only = true;  // F Hermitian
-        tc_cgemm_nt(Z, false, false, Np, NN, Z, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s3);
-        const int64_t nt32 = (Np + 31) / 32;
-        k_herm_sum<<<dim3((unsigned)(nt32 * (nt32 + 1) / 2), (unsigned)nb), 256, 0, s>>>(Z, F, E, Np);
-        count_launch();
-        // W is Hermitian: its lower triangle W_ij (j <= i) = sum_{k <= j} T_ik conj(L_jk) needs
-        // T = L E only on and below the diagonal tiles, and the upper triangle is its mirror.
-        // T = L E  (E Hermitian: B(k, n) = conj(E[n][k]))
-        TcStructure s4;
-        s4.a_lower = true;  // L lower
-        s4.lower_only = true;
-        s4.a_mod = nq;
-        s4.a_q0 = q0;
-        tc_cgemm_nt(Lc, false, false, Np, NN, E, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s4);
-        // W = T L^H  (B(k, n) = conj(L[n][k])), written over Pi
-        TcStructure s5;
-        s5.b_upper = true;  // B(k, n) = conj(L[n][k]) vanishes for k > n
-        s5.lower_only = true;
-        s5.b_mod = nq;
-        s5.b_q0 = q0;
-        tc_cgemm_nt(F, false, false, Np, NN, Lc, false, true, Np, NN, (float2*)Pi, Np, NN, Np, Np,
-                    Np, nb, s, s5);
-        launch_mirror_upper((float2*)Pi, Np, nb, s);
-      } else if (a.want_w) {
-        // Y = C^{-1} L^H: column-major Y^T C^T = (L^H)^T  (right, upper)
-        CQ_CHECK_CUDA(cudaMemcpyAsync(Y, LH, nb * NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-        {
-        Prof::Scope sc(a.prof, "dyson_trsm");
-        CQ_BLAS(cublasZtrsmBatched(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                                   CUBLAS_DIAG_NON_UNIT, (int)Np, (int)Np,
-                                   (const cuDoubleComplex*)&one,
-                                   (const cuDoubleComplex* const*)dptrA, (int)Np,
-                                   (cuDoubleComplex* const*)dptrY, (int)Np, (int)nb));
-        }
-        Prof::Scope sc(a.prof, "dyson_W_gemm");
-        // W = Y^H Y - V, written over Pi (FP64 form)
-        {
-          CQ_CHECK_CUDA(cudaMemcpyAsync(Pi, V, nb * NN * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-          CQ_BLAS(cublasZgemmStridedBatched(blas, CUBLAS_OP_N, CUBLAS_OP_C, (int)Np, (int)Np, (int)Np,
-                                            (const cuDoubleComplex*)&one, (const cuDoubleComplex*)Y,
-                                            (int)Np, NN, (const cuDoubleComplex*)Y, (int)Np, NN,
-                                            (const cuDoubleComplex*)&mone, (cuDoubleComplex*)Pi,
-                                            (int)Np, NN, (int)nb));
-        }
-      }
-      if (a.mixed) continue;  // results stay on the device until all chunks ran
-      CQ_CHECK_CUDA(cudaStreamSynchronize(s));
-      for (int64_t i = 0; i < nb; ++i) {
-        if (info_h[i] != 0)
-          throw Error(COQUI_B200_ENOTHPD, "I - L^H Pi L is not positive definite at (w=" +
-                                              std::to_string((p0 + i) / nq) + ", q=" +
-                                              std::to_string((p0 + i) % nq) + ")");
-        if (a.want_e) {
-          (*logdet)[p0 + i] = ld_h[i];
-          (*trace)[p0 + i] = tr_h[i];
-        }
+        // the same two triangular products in FP64 (zgemm.cu): P1 = L^H Pi, M = L^H P1^H
+        ZgemmArgs z1;
+        z1.M = z1.N = z1.K = Np;
+        z1.A = a.LH;
+        z1.lda = Np;
+        z1.sA = NN;
+        z1.a_upper = true;
+        z1.a_mod = nq;
+        z1.a_q0 = q0;
+        z1.B = (const double2*)Pi;
+        z1.ldb = Np;
+        z1.sB = NN;
+        z1.C = (double2*)T1;
+        z1.ldc = Np;
+        z1.sC = NN;
+        z1.batch = nb;
+        zgemm(z1, s);
+        ZgemmArgs z2 = z1;
+        z2.opB = 'C';
+        z2.B = (const double2*)T1;
+        z2.C = (double2*)Mb;
+        z2.lower_only = true;
+        zgemm(z2, s);
       }
     }
+    // I - M = C C^H (FP64): log-determinant, trace of M, and the inverse
+    // above one kInvGroup the mixed form's off-group blocks of the inverse come from the
+    // tensor cores; the FP64 form forms the whole inverse in the factorisation kernel
+    const bool tc_inverse = a.mixed && a.want_w && Np > kInvGroup;
+    {
+      Prof::Scope sc(a.prof, "dyson_chol_inv");
+      if (!a.mixed)
+        launch_chol_inv_c128((const double2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0, Np,
+                             nb, s);
+      else if (tc_inverse && chol_prefer_tiled(std::vector<int64_t>((size_t)nb, Np)))
+        launch_chol_tiled_strided((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0,
+                                  Np, nb, s);  // few large problems: many CTAs per problem
+      else if (tc_inverse)
+        launch_chol_group_inv((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0, Np,
+                              nb, s);
+      else
+        launch_chol_inv((const float2*)Mb, A, a.want_w ? (float2*)Y : nullptr, a.logdet + p0,
+                        a.trace + p0, a.info + p0, Np, nb, s);
+    }
+    if (!a.want_w) continue;
+    // W = L E L^H with E = (I - M)^{-1} - I = D + D^H + D^H D, D = C^{-1} - I: no
+    // cancellation against V, so the split-TF32 products keep W to ~1e-8.
+    if (a.mixed) {
+      if (tc_inverse) {
+        // U = C^{-H} by doubling: FP64 inverses of the kInvGroup diagonal groups, then for
+        // each level b the pairs of diagonal blocks (r0: b, r1: b1) get
+        //   U01 = -U00 C10^H U11
+        // as two split-TF32 products.  Z holds U - I (the D^H of the W products), Zl holds
+        // U^H - I where a later level needs it, Zc = -C off the groups.
+        Prof::Scope sc(a.prof, "dyson_tc_inverse");
+        float2* Z = (float2*)Y;
+        float2* Zl = (float2*)Y + nbq * NN;
+        float2* Zc = (float2*)T1;
+        float2* S = (float2*)Mb;
+        launch_chol_split(A, Z, Zl, Zc, Np, nb, s);
+        for (int64_t b = kInvGroup; b < Np; b *= 2) {
+          for (int64_t r0 = 0; r0 + b < Np; r0 += 2 * b) {
+            const int64_t r1 = r0 + b, b1 = std::min(b, Np - r1);
+            // S = U00 (-C10)^H  (b x b1, K = b): A = Z + I on the 00 block (upper)
+            TcStructure t1;
+            t1.a_upper = true;
+            t1.a_ident = true;
+            tc_cgemm_nt(Z + r0 * Np + r0, false, false, Np, NN, Zc + r1 * Np + r0, false, true,
+                        Np, NN, S + r0 * Np + r1, Np, NN, b, b1, b, nb, s, t1);
+            // U01 = S U11 with U11(k, n) = conj(Zl[n][k]) + delta  (b x b1, K = b1)
+            TcStructure t2;
+            t2.b_upper = true;
+            t2.b_ident = true;
+            tc_cgemm_nt(S + r0 * Np + r1, false, false, Np, NN, Zl + r1 * Np + r1, false, true,
+                        Np, NN, Z + r0 * Np + r1, Np, NN, b, b1, b1, nb, s, t2);
+            if (2 * b < Np) launch_block_adjoint(Z, Zl, Np, r0, r1, b, b1, nb, s);
+          }
+        }
+      }
+      const float2* Z = (const float2*)Y;  // DH = C^{-H} - I
+      Prof::Scope sc(a.prof, "dyson_W_gemm");
+      float2* F = (float2*)T1;
+      float2* E = (float2*)Mb;
+      // F = D^H D  (B(k, n) = D[k][n] = conj(DH[n][k]))
+      TcStructure s3;
+      s3.a_upper = true;     // D^H upper
+      s3.b_lower = true;     // D lower
+      s3.lower_only = true;  // F Hermitian
+      tc_cgemm_nt(Z, false, false, Np, NN, Z, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s3);
+      const int64_t nt32 = (Np + 31) / 32;
+      k_herm_sum<<<dim3((unsigned)(nt32 * (nt32 + 1) / 2), (unsigned)nb), 256, 0, s>>>(Z, F, E, Np);
+      count_launch();
+      // W is Hermitian: its lower triangle W_ij (j <= i) = sum_{k <= j} T_ik conj(L_jk) needs
+      // T = L E only on and below the diagonal tiles, and the upper triangle is its mirror.
+      // T = L E  (E Hermitian: B(k, n) = conj(E[n][k]))
+      TcStructure s4;
+      s4.a_lower = true;  // L lower
+      s4.lower_only = true;
+      s4.a_mod = nq;
+      s4.a_q0 = q0;
+      tc_cgemm_nt(Lc, false, false, Np, NN, E, false, true, Np, NN, F, Np, NN, Np, Np, Np, nb, s, s4);
+      // W = T L^H  (B(k, n) = conj(L[n][k])), written over Pi
+      TcStructure s5;
+      s5.b_upper = true;  // B(k, n) = conj(L[n][k]) vanishes for k > n
+      s5.lower_only = true;
+      s5.b_mod = nq;
+      s5.b_q0 = q0;
+      tc_cgemm_nt(F, false, false, Np, NN, Lc, false, true, Np, NN, (float2*)Pi, Np, NN, Np, Np,
+                  Np, nb, s, s5);
+      launch_mirror_upper((float2*)Pi, Np, nb, s);
+    } else {
+      // the same W = L E L^H in FP64: Z = D^H, F = D^H D, E = Z + Z^H + F, T = L E, W = T L^H
+      Prof::Scope sc(a.prof, "dyson_W_gemm");
+      double2* Z = (double2*)T1;
+      double2* F = (double2*)Mb;
+      double2* E = A;  // the factorisation is not needed once Z holds C^{-H} - I
+      launch_upper_minus_eye(A, Z, Np, nb, s);
+      ZgemmArgs f;  // F = Z Z^H: Z upper, B(k, n) = conj(Z[n][k]) lower
+      f.M = f.N = f.K = Np;
+      f.opB = 'C';
+      f.A = f.B = Z;
+      f.lda = f.ldb = f.ldc = Np;
+      f.sA = f.sB = f.sC = NN;
+      f.C = F;
+      f.batch = nb;
+      f.a_upper = f.b_lower = f.lower_only = true;
+      zgemm(f, s);
+      const int64_t total = NN * nb;
+      k_herm_sum_c128<<<grid_for(total, 256), 256, 0, s>>>(Z, F, E, Np, total);
+      count_launch();
+      CQ_CHECK_CUDA(cudaGetLastError());
+      ZgemmArgs t;  // T = L E (lower tiles), L lower, E Hermitian (stored whole)
+      t.M = t.N = t.K = Np;
+      t.A = a.L;
+      t.lda = t.ldb = t.ldc = Np;
+      t.sA = t.sB = t.sC = NN;
+      t.a_mod = nq;
+      t.a_q0 = q0;
+      t.a_lower = t.lower_only = true;
+      t.B = E;
+      t.C = F;
+      t.batch = nb;
+      zgemm(t, s);
+      ZgemmArgs w;  // W = T L^H (lower tiles), B(k, n) = conj(L[n][k]) upper
+      w.M = w.N = w.K = Np;
+      w.opB = 'C';
+      w.A = F;
+      w.B = a.L;
+      w.lda = w.ldb = w.ldc = Np;
+      w.sA = w.sB = w.sC = NN;
+      w.b_mod = nq;
+      w.b_q0 = q0;
+      w.b_upper = w.lower_only = true;
+      w.C = (double2*)Pi;
+      w.batch = nb;
+      zgemm(w, s);
+      mirror_upper<double2>((double2*)Pi, Np, nb, s, 0);
+    }
   }
-  if (a.mixed && !a.defer_check) {
+  if (!a.defer_check) {
     std::vector<int> info(nprob);
     CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), a.info, nprob * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (a.want_e) {

@@ -35,6 +35,7 @@ struct ZP {
   double2* const* Cp;
   int64_t b0;
   int a_upper, a_lower, b_lower, b_upper, lower_only;
+  int64_t a_mod, a_q0, b_mod, b_q0;
 };
 
 __device__ __forceinline__ int swz(int r) { return ((r & 1) << 2) | ((r >> 1) & 3); }
@@ -81,8 +82,8 @@ __global__ void __launch_bounds__(NT, 2) k_zgemm(const __grid_constant__ ZP p) {
   const int64_t b = p.b0 + blockIdx.z;
   const int64_t m0 = (int64_t)blockIdx.y * TM, n0 = (int64_t)blockIdx.x * TN;
   if (p.lower_only && n0 > m0 + TM - 1) return;  // uniform over the CTA
-  const double2* A = p.Ap ? p.Ap[b] : p.A + b * p.sA;
-  const double2* B = p.Bp ? p.Bp[b] : p.B + b * p.sB;
+  const double2* A = p.Ap ? p.Ap[b] : p.A + (p.a_mod ? (p.a_q0 + b) % p.a_mod : b) * p.sA;
+  const double2* B = p.Bp ? p.Bp[b] : p.B + (p.b_mod ? (p.b_q0 + b) % p.b_mod : b) * p.sB;
   double2* C = p.Cp ? p.Cp[b] : p.C + b * p.sC;
 
   int64_t klo = 0, khi = p.K;
@@ -221,6 +222,10 @@ void zgemm(const ZgemmArgs& a, cudaStream_t s) {
   p.b_lower = a.b_lower;
   p.b_upper = a.b_upper;
   p.lower_only = a.lower_only;
+  p.a_mod = a.a_mod;
+  p.a_q0 = a.a_q0;
+  p.b_mod = a.b_mod;
+  p.b_q0 = a.b_q0;
   // CTA tile 64 x 64, 128 x 32 or 32 x 128: the least padding of M x N (64 x 64 on ties)
   auto padded = [&](int64_t tm, int64_t tn) {
     return ((a.M + tm - 1) / tm * tm) * ((a.N + tn - 1) / tn * tn);
