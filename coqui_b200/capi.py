@@ -39,7 +39,7 @@ SYMBOLS = [
     "coqui_b200_batch_last_error", "coqui_b200_batch_set_ir", "coqui_b200_batch_set_thc",
     "coqui_b200_batch_gw_iteration", "coqui_b200_batch_last_ms", "coqui_b200_set_autotune",
     "coqui_b200_tuned_shapes", "coqui_b200_set_tile_config", "coqui_b200_num_tile_configs",
-    "coqui_b200_set_wait_limit_ns",
+    "coqui_b200_set_wait_limit_ns", "coqui_b200_factor_dielectric",
 ]
 
 
@@ -140,6 +140,8 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_num_tile_configs.restype = ctypes.c_int
     lib.coqui_b200_set_wait_limit_ns.argtypes = [ctypes.c_int, I64]
     lib.coqui_b200_set_wait_limit_ns.restype = ctypes.c_int
+    lib.coqui_b200_factor_dielectric.argtypes = [P, P, P, P, P, I64, I64, P]
+    lib.coqui_b200_factor_dielectric.restype = ctypes.c_int
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -583,6 +585,16 @@ def set_tile_config(cfg: int):
 
 def num_tile_configs() -> int:
     return int(load().coqui_b200_num_tile_configs())
+
+
+def factor_dielectric(M_ptr, A_ptr, logdet_ptr, trace_ptr, info_ptr, Np, nprob, stream=None):
+    """Batched FP64 factorisation I - M = C C^H of the Dyson step on device buffers (pointers as
+    integers): M complex64 (nprob, Np, Np), A complex128 workspace, logdet float64 (nprob),
+    trace complex128 (nprob), info int32 (nprob)."""
+    rc = load().coqui_b200_factor_dielectric(M_ptr, A_ptr, logdet_ptr, trace_ptr, info_ptr,
+                                             int(Np), int(nprob), stream)
+    if rc != OK:
+        raise CoquiB200Error(rc, "factor_dielectric failed")
 
 
 def set_wait_limit_ns(ns: int, device: int = 0):

@@ -418,7 +418,7 @@ bool chol_prefer_tiled(const std::vector<int64_t>& sizes) {
     mx = std::max(mx, c);
   }
   const int64_t nmax = sizes.empty() ? 0 : *std::max_element(sizes.begin(), sizes.end());
-  return nmax >= 4 * b32::CB && total / ((double)sms * b32::MINB) < mx;
+  return nmax >= 4 * b32::CB && total / (double)chol_wave_size() < mx;
 }
 
 void launch_chol_inv_c128(const double2* M, double2* A, double* logdet, double2* trace, int* info,

@@ -19,6 +19,7 @@
 #include <string>
 #include <vector>
 
+#include "chol.cuh"
 #include "dyson.cuh"
 #include "kernels.cuh"
 #include "mlp.cuh"
@@ -2121,6 +2122,37 @@ int coqui_b200_set_tile_config(int cfg) {
 }
 
 int coqui_b200_num_tile_configs(void) { return cq::tc_num_cfgs(); }
+
+int coqui_b200_factor_dielectric(const float* M_dev, double* A_dev, double* logdet_dev,
+                                 double* trace_dev, int* info_dev, int64_t Np, int64_t nprob,
+                                 void* stream) {
+  try {
+    CQ_REQUIRE(M_dev && A_dev && logdet_dev && trace_dev && info_dev, COQUI_B200_EINVAL,
+               "factor_dielectric: null argument");
+    CQ_REQUIRE(Np > 0 && nprob > 0 && nprob <= 2147483647, COQUI_B200_EINVAL,
+               "factor_dielectric: bad sizes");
+    const void* ptrs[] = {M_dev, A_dev, logdet_dev, trace_dev, info_dev};
+    int dev = -1;
+    for (const void* q : ptrs) {
+      cudaPointerAttributes at{};
+      CQ_CHECK_CUDA(cudaPointerGetAttributes(&at, q));
+      CQ_REQUIRE(at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged,
+                 COQUI_B200_EINVAL, "factor_dielectric: arguments must be device memory");
+      CQ_REQUIRE(dev < 0 || at.device == dev, COQUI_B200_EINVAL,
+                 "factor_dielectric: arguments on different devices");
+      dev = at.device;
+    }
+    CQ_CHECK_CUDA(cudaSetDevice(dev));
+    cudaStream_t st = (cudaStream_t)stream;
+    cq::launch_chol_group_inv(reinterpret_cast<const float2*>(M_dev),
+                              reinterpret_cast<double2*>(A_dev), logdet_dev,
+                              reinterpret_cast<double2*>(trace_dev), info_dev, Np, nprob, st);
+    CQ_CHECK_CUDA(cudaStreamSynchronize(st));
+    return COQUI_B200_OK;
+  } catch (const cq::Error& e) {
+    return e.code;
+  }
+}
 
 int coqui_b200_set_wait_limit_ns(int device, int64_t ns) {
   try {

@@ -243,12 +243,21 @@ void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
       if (!a.mixed)
         launch_chol_inv_c128((const double2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0, Np,
                              nb, s);
-      else if (tc_inverse && chol_prefer_tiled(std::vector<int64_t>((size_t)nb, Np)))
-        launch_chol_tiled_strided((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0,
-                                  Np, nb, s);  // few large problems: many CTAs per problem
-      else if (tc_inverse)
-        launch_chol_group_inv((const float2*)Mb, A, a.logdet + p0, a.trace + p0, a.info + p0, Np,
-                              nb, s);
+      else if (tc_inverse) {
+        // whole waves of the one-CTA kernel, and a remainder of less than a wave spread over
+        // many CTAs per problem when that finishes sooner (identical results either way)
+        const int64_t wave = chol_wave_size();
+        const int64_t full = nb >= wave ? nb / wave * wave : 0, rest = nb - full;
+        const float2* M0 = (const float2*)Mb;
+        if (full > 0)
+          launch_chol_group_inv(M0, A, a.logdet + p0, a.trace + p0, a.info + p0, Np, full, s);
+        if (rest > 0 && chol_prefer_tiled(std::vector<int64_t>((size_t)rest, Np)))
+          launch_chol_tiled_strided(M0 + full * NN, A + full * NN, a.logdet + p0 + full,
+                                    a.trace + p0 + full, a.info + p0 + full, Np, rest, s);
+        else if (rest > 0)
+          launch_chol_group_inv(M0 + full * NN, A + full * NN, a.logdet + p0 + full,
+                                a.trace + p0 + full, a.info + p0 + full, Np, rest, s);
+      }
       else
         launch_chol_inv((const float2*)Mb, A, a.want_w ? (float2*)Y : nullptr, a.logdet + p0,
                         a.trace + p0, a.info + p0, Np, nb, s);

@@ -304,6 +304,19 @@ COQUI_B200_API int64_t coqui_b200_tuned_shapes(void);
 COQUI_B200_API int coqui_b200_set_tile_config(int cfg);
 COQUI_B200_API int coqui_b200_num_tile_configs(void);
 
+/* The FP64 factorisation step of coqui_b200_dyson_w on caller-owned device buffers (from
+   scr_coulomb_t::dyson_W_in_place, scr_coulomb_t.cpp:171-199, and the log-determinant of
+   thc_rpa.icc:130-165, in the Hermitian form M = L^H Pi L, I - M = C C^H): for each of nprob
+   Np x Np problems, M_dev complex64 (lower triangle read), A_dev complex128 workspace with
+   C (lower, off the diagonal blocks) and C^{-H} inside the 128-column diagonal groups (upper)
+   on return, logdet_dev[p] = 2 sum ln C_ii, trace_dev[p] (re, im) = sum M_ii, info_dev[p] = 1
+   for a non-positive pivot.  Runs on `stream` (a cudaStream_t, NULL = default stream) and
+   returns after it finished; allocates nothing. */
+COQUI_B200_API int coqui_b200_factor_dielectric(const float* M_dev, double* A_dev,
+                                                double* logdet_dev, double* trace_dev,
+                                                int* info_dev, int64_t Np, int64_t nprob,
+                                                void* stream);
+
 /* Time limit (ns) of the bounded device-side waits of the tensor-core kernels on `device`
    (ns <= 0 restores the default of 2 s).  A kernel whose wait runs out sets an error flag,
    lets its issued tensor-core work retire, frees its tensor memory and returns; the call
