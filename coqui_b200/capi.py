@@ -39,7 +39,7 @@ SYMBOLS = [
     "coqui_b200_batch_last_error", "coqui_b200_batch_set_ir", "coqui_b200_batch_set_thc",
     "coqui_b200_batch_gw_iteration", "coqui_b200_batch_last_ms", "coqui_b200_set_autotune",
     "coqui_b200_tuned_shapes", "coqui_b200_set_tile_config", "coqui_b200_num_tile_configs",
-    "coqui_b200_set_wait_limit_ns", "coqui_b200_factor_dielectric",
+    "coqui_b200_set_wait_limit_ns", "coqui_b200_factor_dielectric", "coqui_b200_qp_solve",
 ]
 
 
@@ -142,6 +142,9 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_set_wait_limit_ns.restype = ctypes.c_int
     lib.coqui_b200_factor_dielectric.argtypes = [P, P, P, P, P, I64, I64, P]
     lib.coqui_b200_factor_dielectric.restype = ctypes.c_int
+    lib.coqui_b200_qp_solve.argtypes = [P, P, P, P, I64, ctypes.c_int, D, D, D, ctypes.c_int,
+                                        ctypes.c_int, P, P, P, ctypes.c_char_p, ctypes.c_int]
+    lib.coqui_b200_qp_solve.restype = ctypes.c_int
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
     _lib = lib
@@ -595,6 +598,33 @@ def factor_dielectric(M_ptr, A_ptr, logdet_ptr, trace_ptr, info_ptr, Np, nprob, 
                                              int(Np), int(nprob), stream)
     if rc != OK:
         raise CoquiB200Error(rc, "factor_dielectric failed")
+
+
+QP_METHODS = {"sc": 0, "sc_bisection": 0, "sc_newton": 1, "linearized": 2, "spectral": 3}
+
+
+def qp_solve(w_fit, sigma_fit, vhf, e0, mu, eta=1e-4, tol=1e-8, qp_type="sc", device=0):
+    """Quasiparticle energies E (nel,) from Sigma(i w_n) at the Pade fit points: w_fit (nfit,)
+    real, sigma_fit (nfit, nel) complex, vhf and e0 (nel,) real.  Returns (E, residual,
+    converged)."""
+    w = np.ascontiguousarray(w_fit, np.float64)
+    sig = np.ascontiguousarray(sigma_fit, np.complex128)
+    v = np.ascontiguousarray(vhf, np.float64)
+    e = np.ascontiguousarray(e0, np.float64)
+    nfit, nel = sig.shape
+    if w.shape != (nfit,) or v.shape != (nel,) or e.shape != (nel,):
+        raise ValueError("qp_solve: inconsistent shapes")
+    E = np.empty(nel, np.float64)
+    R = np.empty(nel, np.float64)
+    C = np.empty(nel, np.int32)
+    err = ctypes.create_string_buffer(512)
+    rc = load().coqui_b200_qp_solve(_ptr(w, "w"), _ptr(sig, "sigma"), _ptr(v, "vhf"),
+                                    _ptr(e, "e0"), nel, nfit, float(mu), float(eta), float(tol),
+                                    QP_METHODS[qp_type], int(device), _ptr(E, "E"), _ptr(R, "R"),
+                                    _ptr(C, "conv"), err, 512)
+    if rc != OK:
+        raise CoquiB200Error(rc, err.value.decode())
+    return E, R, C.astype(bool)
 
 
 def set_wait_limit_ns(ns: int, device: int = 0):

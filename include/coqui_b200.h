@@ -317,6 +317,22 @@ COQUI_B200_API int coqui_b200_factor_dielectric(const float* M_dev, double* A_de
                                                 int* info_dev, int64_t Np, int64_t nprob,
                                                 void* stream);
 
+/* Quasiparticle equation per element I < nel (solve_qp_eqn, src/methods/SCF/
+   qp_scf_common.cpp:150-311): the diagonal self-energy Sigma_I(i w_n) given at nfit fermionic
+   Matsubara frequencies w_fit[n] (real w_n of i w_n; sigma_fit complex128 (nfit, nel)) is
+   continued to the real axis by Thiele's nfit-point Pade approximant (analyt_cont::pade_t,
+   src/numerics/ac/pade/pade_t.hpp; double-double arithmetic here) and
+   E_I = vhf[I] + Re Sigma_I(E_I - mu + i eta) is solved from e0[I] with method 0 "sc"
+   (bisection, qp_eqn_bisection), 1 "sc_newton" (secant, qp_eqn_secant), 2 "linearized"
+   (qp_eqn_linearized) or 3 "spectral" (qp_eqn_spectral), tolerance tol.  Host arrays;
+   e_out, res_out (the residual at E) and conv_out (1 = converged) are written.  2 <= nfit
+   <= 64.  A message goes to errbuf (may be NULL) on an error. */
+COQUI_B200_API int coqui_b200_qp_solve(const double* w_fit, const double* sigma_fit,
+                                       const double* vhf, const double* e0, int64_t nel, int nfit,
+                                       double mu, double eta, double tol, int method, int device,
+                                       double* e_out, double* res_out, int* conv_out, char* errbuf,
+                                       int errlen);
+
 /* Time limit (ns) of the bounded device-side waits of the tensor-core kernels on `device`
    (ns <= 0 restores the default of 2 s).  A kernel whose wait runs out sets an error flag,
    lets its issued tensor-core work retire, frees its tensor memory and returns; the call
