@@ -91,6 +91,7 @@ struct coqui_b200_ctx {
 
   // Dyson results per (iW, q) problem on the device
   DevBuf<int> dinfo;
+  DevBuf<int> flag;  // input checks
   DevBuf<double> dlogdet;
   DevBuf<double2> dtrace;
   // CUDA graph of the resident-G GW iteration (captured on the first of consecutive calls)
@@ -217,6 +218,8 @@ template <typename F> int guarded(Ctx* c, F&& f) {
     f();
     if (c->st) CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     if (c->cs) CQ_CHECK_CUDA(cudaStreamSynchronize(c->cs));
+    if (cq::tc_take_nonfinite())
+      throw Error(COQUI_B200_EINVAL, "G holds NaN or Inf values");
     if (cq::tc_take_error())
       throw Error(COQUI_B200_ETIMEDOUT, "a tensor-core kernel gave up a bounded wait");
     c->err.clear();
@@ -224,6 +227,17 @@ template <typename F> int guarded(Ctx* c, F&& f) {
   } catch (const Error& e) {
     c->err = e.what();
     settle(c);
+    // a non-finite G is the cause of whatever failed downstream of it (a factorisation without
+    // positive pivots, say): report it as such
+    bool nonfinite = false;
+    try {
+      nonfinite = cq::tc_take_nonfinite() != 0;
+    } catch (const Error&) {
+    }
+    if (nonfinite) {
+      c->err = "G holds NaN or Inf values";
+      return COQUI_B200_EINVAL;
+    }
     return e.code;
   } catch (const std::bad_alloc&) {
     c->err = "host allocation failed";
@@ -988,6 +1002,15 @@ int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_
     c->V.ensure((size_t)nk * Np * Np);
     upload(c, c->X.p, X_skPa, (size_t)nk * Np * nb * sizeof(double2));
     upload(c, c->V.p, V_qPQ, (size_t)nk * Np * Np * sizeof(double2));
+    // NaN or Inf would pass the factorisation's pivot test (it compares with zero): refuse them
+    c->flag.ensure(1);
+    CQ_CHECK_CUDA(cudaMemsetAsync(c->flag.p, 0, sizeof(int), c->st));
+    cq::launch_check_finite(c->X.p, nk * Np * nb, c->flag.p, c->st);
+    cq::launch_check_finite(c->V.p, nk * Np * Np, c->flag.p, c->st);
+    int bad = 0;
+    CQ_CHECK_CUDA(cudaMemcpyAsync(&bad, c->flag.p, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    CQ_REQUIRE(!bad, COQUI_B200_EINVAL, "X or V holds NaN or Inf values");
     // V^q = L L^H once per q (FP64)
     c->L.ensure((size_t)nk * Np * Np);
     c->LH.ensure((size_t)nk * Np * Np);

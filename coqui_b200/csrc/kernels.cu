@@ -1200,4 +1200,23 @@ void ph_symmetric_matrices(const double* Twt_bb, const double* Ttw_bb, int64_t n
     }
 }
 
+namespace {
+__global__ void k_check_finite(const double2* __restrict__ p, int64_t n, int* __restrict__ flag) {
+  bool bad = false;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = p[i];
+    bad |= !isfinite(v.x) || !isfinite(v.y);
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(flag, 1);
+}
+}  // namespace
+
+void launch_check_finite(const double2* p, int64_t n, int* flag, cudaStream_t s) {
+  if (n <= 0) return;
+  k_check_finite<<<grid_for(n, 256), 256, 0, s>>>(p, n, flag);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
+}
+
 }  // namespace cq

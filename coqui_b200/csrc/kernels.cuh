@@ -93,4 +93,7 @@ void launch_gemm_simt(const GemmDesc& d, const TA* A, const TB* B, TC* C, cudaSt
 void ph_symmetric_matrices(const double* Twt_bb, const double* Ttw_bb, int64_t nt, int64_t nwb,
                            std::vector<double2>& Twt_pos, std::vector<double2>& Ttw_pos);
 
+// *flag = 1 if any of the n complex values holds NaN or Inf (flag left as it is otherwise).
+void launch_check_finite(const double2* p, int64_t n, int* flag, cudaStream_t s);
+
 }  // namespace cq

@@ -34,6 +34,9 @@ namespace cq {
 namespace {
 
 __device__ int g_tc_error = 0;
+// set when an input of the primary -> auxiliary projection holds NaN or Inf (the split-TF32
+// products do not carry non-finite values through reliably, so they are caught on the way in)
+__device__ int g_nonfinite = 0;
 // time limit of every bounded wait (ns); 2 s unless a test shortens it
 constexpr unsigned long long kDefaultWaitNs = 2000000000ull;
 __device__ unsigned long long g_tc_wait_ns = kDefaultWaitNs;
@@ -1119,6 +1122,13 @@ void tc_cgemm_nt(const void* A, bool a_split, bool conj_a, int64_t lda, int64_t 
   else dispatch_n<false, false>(p, batch, s);
 }
 
+int tc_take_nonfinite() {
+  int h = 0, z = 0;
+  CQ_CHECK_CUDA(cudaMemcpyFromSymbol(&h, g_nonfinite, sizeof(int)));
+  if (h) CQ_CHECK_CUDA(cudaMemcpyToSymbol(g_nonfinite, &z, sizeof(int)));
+  return h;
+}
+
 void tc_set_wait_ns(int64_t ns) {
   const unsigned long long v = ns > 0 ? (unsigned long long)ns : kDefaultWaitNs;
   CQ_CHECK_CUDA(cudaMemcpyToSymbol(g_tc_wait_ns, &v, sizeof(v)));
@@ -1176,6 +1186,7 @@ __global__ void k_transpose_c64(const double2* __restrict__ in, float2* __restri
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t b = i / (rows * cols), e = i % (rows * cols);
     const double2 x = in[i];
+    if (!isfinite(x.x) || !isfinite(x.y)) atomicExch(&g_nonfinite, 1);
     out[b * rows * cols + (e % cols) * rows + e / cols] = make_float2((float)x.x, (float)x.y);
   }
 }

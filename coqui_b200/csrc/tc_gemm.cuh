@@ -96,6 +96,9 @@ int tc_num_cfgs();
 // Returns (and clears) the device flag set when a bounded wait inside a tensor-core kernel
 // gave up (nonzero = a kernel timed out).
 int tc_take_error();
+// Whether a primary -> auxiliary projection since the last call saw NaN or Inf in G (read and
+// cleared).
+int tc_take_nonfinite();
 // Time limit of the tensor-core kernels' bounded waits on the current device (ns; <= 0: the
 // default 2 s).
 void tc_set_wait_ns(int64_t ns);

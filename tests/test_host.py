@@ -1,4 +1,6 @@
 """Host-side logic that needs no GPU: synthetic inputs, argument validation."""
+import os
+
 import numpy as np
 import pytest
 
@@ -156,3 +158,18 @@ def test_bench_cpu_sample_counts_and_scaling():
     total, parts = bench.cpu_sample(s, ft, reps=1)
     assert set(parts) == set(c) and all(v > 0 for v in parts.values())
     assert abs(total - sum(parts.values())) < 1e-9 * total
+
+
+def test_truncated_ir_table_is_an_error(tmp_path, monkeypatch):
+    """A damaged IR table is refused when it is loaded, before any device work."""
+    import shutil
+    from coqui_b200 import iaft
+    src = os.path.join(iaft.IR_DIR, "1e4.1e-06.npz")
+    data = open(src, "rb").read()
+    d = tmp_path / "ir"
+    d.mkdir()
+    (d / "1e4.1e-06.npz").write_bytes(data[: len(data) // 2])
+    monkeypatch.setattr(iaft, "IR_DIR", str(d))
+    with pytest.raises(Exception):
+        iaft.IAFT(1000.0, 10.0, "low")
+    shutil.rmtree(d)
