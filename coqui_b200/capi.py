@@ -40,6 +40,7 @@ SYMBOLS = [
     "coqui_b200_batch_gw_iteration", "coqui_b200_batch_last_ms", "coqui_b200_set_autotune",
     "coqui_b200_tuned_shapes", "coqui_b200_set_tile_config", "coqui_b200_num_tile_configs",
     "coqui_b200_set_wait_limit_ns", "coqui_b200_factor_dielectric", "coqui_b200_qp_solve",
+    "coqui_b200_set_symmetry",
 ]
 
 
@@ -48,6 +49,17 @@ class Dims(ctypes.Structure):
                 ("Np", ctypes.c_int64), ("nt_f", ctypes.c_int64), ("nw_b", ctypes.c_int64),
                 ("kp_grid", ctypes.c_int64 * 3), ("precision_mode", ctypes.c_int32),
                 ("device", ctypes.c_int32)]
+
+
+class Symmetry(ctypes.Structure):
+    """coqui_b200_symmetry: the mean field's bz_symm maps in the reference's k order."""
+    _fields_ = [("nk_ibz", ctypes.c_int64), ("nq_ibz", ctypes.c_int64), ("nsym", ctypes.c_int64),
+                ("ld_Qs", ctypes.c_int64), ("k_lex", ctypes.c_void_p),
+                ("kp_to_ibz", ctypes.c_void_p), ("kp_trev", ctypes.c_void_p),
+                ("kp_trev_pair", ctypes.c_void_p), ("qp_to_ibz", ctypes.c_void_p),
+                ("qp_trev", ctypes.c_void_p), ("qminus", ctypes.c_void_p),
+                ("nq_per_s", ctypes.c_void_p), ("Qs", ctypes.c_void_p),
+                ("ks_to_k", ctypes.c_void_p), ("D", ctypes.c_void_p)]
 
 
 class CoquiB200Error(RuntimeError):
@@ -147,6 +159,8 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_qp_solve.restype = ctypes.c_int
     lib.coqui_b200_kernel_launches.argtypes = [P]
     lib.coqui_b200_kernel_launches.restype = ctypes.c_int64
+    lib.coqui_b200_set_symmetry.argtypes = [P, ctypes.POINTER(Symmetry)]
+    lib.coqui_b200_set_symmetry.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -184,6 +198,8 @@ class Context:
         self.nk, self.nb, self.Np, self.nt, self.nw_b = nk, nb, Np, nt_f, nw_b
         self.nt_half, self.nw_half = (nt_f + 1) // 2, (nw_b + 1) // 2
         self.mode = mode
+        # k-points of G / Sigma and q-points of Pi / W: the IBZ ones after set_symmetry
+        self.nkg = self.nqw = nk
 
     def close(self):
         if self.h:
@@ -311,14 +327,44 @@ class Context:
         V = _c128(V, (self.nk, self.Np, self.Np), "V")
         self._check(self.lib.coqui_b200_set_thc(self.h, _ptr(X, "X"), _ptr(V, "V")))
 
+    def set_symmetry(self, sym, D=None):
+        """Switch to the IBZ k-space path (coqui_b200_set_symmetry) with the bz_symm maps of
+        ``sym`` (keys ``k_lex`` or ``lex``, ``nk_ibz``, ``nq_ibz``, ``kp_to_ibz``, ``kp_trev``,
+        ``kp_trev_pair``, ``qp_to_ibz``, ``qp_trev``, ``qminus``, ``nq_per_s``, ``Qs``,
+        ``ks_to_k``) and the rotations D (nsym, nk_ibz, nb, nb) or None; sym = None returns
+        to the full-BZ path.  G / Sigma then cover the IBZ k-points, Pi / W the IBZ q-points."""
+        if sym is None:
+            self._check(self.lib.coqui_b200_set_symmetry(self.h, None))
+            self.nkg = self.nqw = self.nk
+            self._sym_keep = None
+            return
+        i64 = lambda a: np.ascontiguousarray(a, np.int64)  # noqa: E731
+        i32 = lambda a: np.ascontiguousarray(np.asarray(a).astype(np.int32))  # noqa: E731
+        keep = dict(k_lex=i64(sym["k_lex"] if "k_lex" in sym else sym["lex"]),
+                    kp_to_ibz=i64(sym["kp_to_ibz"]), kp_trev=i32(sym["kp_trev"]),
+                    kp_trev_pair=i64(sym["kp_trev_pair"]), qp_to_ibz=i64(sym["qp_to_ibz"]),
+                    qp_trev=i32(sym["qp_trev"]), qminus=i64(sym["qminus"]),
+                    nq_per_s=i64(sym["nq_per_s"]), Qs=i64(np.atleast_2d(sym["Qs"])),
+                    ks_to_k=i64(np.atleast_2d(sym["ks_to_k"])))
+        nsym = int(keep["nq_per_s"].shape[0])
+        nk_ibz, nq_ibz = int(sym["nk_ibz"]), int(sym["nq_ibz"])
+        if D is not None:
+            keep["D"] = _c128(D, (nsym, nk_ibz, self.nb, self.nb), "D")
+        s = Symmetry(nk_ibz=nk_ibz, nq_ibz=nq_ibz, nsym=nsym, ld_Qs=keep["Qs"].shape[1],
+                     D=None if D is None else keep["D"].ctypes.data,
+                     **{k: keep[k].ctypes.data for k in keep if k != "D"})
+        self._check(self.lib.coqui_b200_set_symmetry(self.h, ctypes.byref(s)))
+        self._sym_keep = keep
+        self.nkg, self.nqw = nk_ibz, nq_ibz
+
     # -- solvers -----------------------------------------------------------------------
     def _G(self, G):
-        return _c128(G, (self.nt, 1, self.nk, self.nb, self.nb), "G_tskij")
+        return _c128(G, (self.nt, 1, self.nkg, self.nb, self.nb), "G_tskij")
 
     def eval_pi(self, G, out=None):
         G = self._G(G)
         if out is None:
-            out = np.empty((self.nt_half, self.nk, self.Np, self.Np), np.complex128)
+            out = np.empty((self.nt_half, self.nqw, self.Np, self.Np), np.complex128)
         self._check(self.lib.coqui_b200_eval_pi(self.h, _ptr(G, "G"), _ptr(out, "Pi")))
         return out
 
@@ -326,7 +372,7 @@ class Context:
         G = self._G(G)
         W = None
         if want_w:
-            W = out if out is not None else np.empty((self.nk, self.nt_half, self.Np, self.Np),
+            W = out if out is not None else np.empty((self.nqw, self.nt_half, self.Np, self.Np),
                                                      np.complex128)
         head = np.empty(self.nt_half, np.complex128) if want_head else None
         self._check(self.lib.coqui_b200_update_w(self.h, _ptr(G, "G"), _ptr(W, "W"),
@@ -334,14 +380,14 @@ class Context:
         return W, head
 
     def set_w(self, dW_qtPQ):
-        W = _c128(dW_qtPQ, (self.nk, self.nt_half, self.Np, self.Np), "dW_qtPQ")
+        W = _c128(dW_qtPQ, (self.nqw, self.nt_half, self.Np, self.Np), "dW_qtPQ")
         self._check(self.lib.coqui_b200_set_w(self.h, _ptr(W, "W")))
 
     def eval_sigma(self, G, out=None):
         """G = None reuses the device-resident G of the previous call."""
         G = None if G is None else self._G(G)
         if out is None:
-            out = np.empty((self.nt, 1, self.nk, self.nb, self.nb), np.complex128)
+            out = np.empty((self.nt, 1, self.nkg, self.nb, self.nb), np.complex128)
         self._check(self.lib.coqui_b200_eval_sigma(self.h, _ptr(G, "G"), _ptr(out, "Sigma")))
         return out
 
@@ -359,7 +405,7 @@ class Context:
         S = None
         if want_sigma:
             S = sigma_out if sigma_out is not None else np.empty(
-                (self.nt, 1, self.nk, self.nb, self.nb), np.complex128)
+                (self.nt, 1, self.nkg, self.nb, self.nb), np.complex128)
         head = np.empty(self.nt_half, np.complex128) if want_head else None
         self._check(self.lib.coqui_b200_gw_iteration(self.h, _ptr(G, "G"), _ptr(S, "Sigma"),
                                                      _ptr(head, "head")))

@@ -24,6 +24,7 @@
 #include "kernels.cuh"
 #include "mlp.cuh"
 #include "scgw.cuh"
+#include "sym.cuh"
 #include "tc_gemm.cuh"
 #include "zgemm.cuh"
 
@@ -51,6 +52,35 @@ using cq::DevBuf;
 
 }  // namespace
 
+// Symmetry-reduced k-space path (coqui_b200_set_symmetry): the mean field's maps translated to
+// lexicographic k positions, the per-symmetry self-energy term lists, and the IBZ buffers.
+struct SymState {
+  int64_t nk_ibz = 0, nq_ibz = 0, nsym = 0;
+  std::vector<int64_t> lex;       // the reference's k index -> lexicographic position
+  std::vector<int64_t> ks_lex;    // (nsym, nk_ibz) lexicographic position of ks_to_k
+  std::vector<int64_t> q_lex;     // (nq_ibz) lexicographic position of the IBZ q-points
+  std::vector<double> qw;         // (nq_ibz) number of 1st-BZ q-points mapped to each
+  std::vector<int64_t> nterm;     // (nsym) self-energy terms per IBZ k-point (nq_per_s)
+  std::vector<size_t> term_off;   // (nsym) offset of the isym block in terms
+  std::vector<double2> D_h;       // (nsym, nk_ibz, nb, nb), block 0 the identity
+  DevBuf<int> unfold;             // (nk) lexicographic k -> IBZ index | time reversal << 30
+  DevBuf<int> qsrc;               // (nq_ibz) lexicographic position of -q
+  DevBuf<int4> terms;             // (w slab, G slab, conj flags) per (isym, ik, term)
+  DevBuf<int2> rows;              // (nsym * nk_ibz): (first term, term count)
+  DevBuf<double2> D;
+  // built from the THC data on first use (set_thc clears thc_ready)
+  bool thc_ready = false;
+  DevBuf<double2> Xs;             // (nsym, nk_ibz, Np, nb): X at ks_to_k(isym, ik)
+  cq::TcOperand Xtc;              // mixed form: Xs packed for the tensor-core projection
+  DevBuf<double2> Li, LHi, Vi;    // (nq_ibz, Np, Np) at the IBZ q-points
+  DevBuf<float2> Lci, LHci;
+  DevBuf<double2> Gi;             // (nt, nk_ibz, nb, nb) G on the IBZ k-points
+  DevBuf<unsigned char> PWi;      // (nmax, nq_ibz, Np, Np) Pi / W on the IBZ q-points
+  DevBuf<unsigned char> Sq;       // (nsym, nk_ibz, Np, Np) Sigma_PQ rows of one tau
+  DevBuf<double2> Sab, Tab, Rab;  // (nsym, nk_ibz, nb, nb)
+  bool w_valid = false;
+};
+
 struct coqui_b200_ctx {
   coqui_b200_dims d{};
   int64_t ns = 1, nk = 0, nq = 0, nb = 0, Np = 0, nt = 0, nth = 0, nwb = 0, nwh = 0, nmax = 0;
@@ -65,6 +95,7 @@ struct coqui_b200_ctx {
   bool have_ir = false, have_k = false, have_thc = false, w_valid = false, w_in_R = false;
   bool g_resident = false;
   cq::Prof prof;
+  std::unique_ptr<SymState> sym;  // set: the IBZ k-space path
 
   // host-side IR data
   std::vector<double2> Twt_pos, Ttw_pos, Ttw_bb, T_beta;
@@ -449,21 +480,24 @@ void eval_pi_device(Ctx* c) {
   c->gcache_valid = (cache != nullptr);
   c->w_valid = false;
 }
-void ir_inplace(Ctx* c, int n_in, int n_out, const double2* M) {
+// in-place tau <-> iW transform of buf (rows of ncol elements in storage precision)
+void ir_apply(Ctx* c, unsigned char* buf, int64_t ncol, int n_in, int n_out, const double2* M) {
   cq::Prof::Scope sc(&c->prof, "ir_transform");
-  const int64_t ncol = c->nq * c->Np * c->Np;
   if (c->ir_real) {
     const double* Mr = (M == c->dTwt.p) ? c->dTwtR.p : c->dTtwR.p;
     if (c->mode == COQUI_B200_FP64)
-      cq::launch_ir_transform_real<double>((double2*)c->PW.p, ncol, n_in, n_out, Mr, c->st);
+      cq::launch_ir_transform_real<double>((double2*)buf, ncol, n_in, n_out, Mr, c->st);
     else
-      cq::launch_ir_transform_real<float>((float2*)c->PW.p, ncol, n_in, n_out, Mr, c->st);
+      cq::launch_ir_transform_real<float>((float2*)buf, ncol, n_in, n_out, Mr, c->st);
     return;
   }
   if (c->mode == COQUI_B200_FP64)
-    cq::launch_ir_transform<double>((double2*)c->PW.p, ncol, n_in, n_out, M, c->st);
+    cq::launch_ir_transform<double>((double2*)buf, ncol, n_in, n_out, M, c->st);
   else
-    cq::launch_ir_transform<float>((float2*)c->PW.p, ncol, n_in, n_out, M, c->st);
+    cq::launch_ir_transform<float>((float2*)buf, ncol, n_in, n_out, M, c->st);
+}
+void ir_inplace(Ctx* c, int n_in, int n_out, const double2* M) {
+  ir_apply(c, c->PW.p, c->nq * c->Np * c->Np, n_in, n_out, M);
 }
 
 void upload_G(Ctx* c, const double* G_tskij) {
@@ -504,14 +538,17 @@ void upload_G(Ctx* c, const double* G_tskij) {
   c->g_pipelined = true;
 }
 
-// E_c accumulation (thc_rpa.icc:130-173) from per-(w, q) log det and traces.
-double rpa_energy_from(Ctx* c, const std::vector<double>& logdet, const std::vector<double2>& tr) {
-  const int64_t nwb = c->nwb, nwh = c->nwh, nq = c->nq;
+// E_c accumulation (thc_rpa.icc:130-173) from per-(w, q) log det and traces; qw holds the
+// q weights of the IBZ path (thc_rpa.icc:133), empty: every q-point once.
+double rpa_energy_from(Ctx* c, const std::vector<double>& logdet, const std::vector<double2>& tr,
+                       const std::vector<double>& qw = {}) {
+  const int64_t nwb = c->nwb, nwh = c->nwh, nq = qw.empty() ? c->nq : (int64_t)qw.size();
   std::vector<std::complex<double>> e_w(nwb, 0.0);
   for (int64_t n = 0; n < nwh; ++n)
     for (int64_t q = 0; q < nq; ++q) {
       const int64_t p = n * nq + q;
-      const std::complex<double> v(tr[p].x + logdet[p], tr[p].y);  // q_weight = 1
+      const double w = qw.empty() ? 1.0 : qw[q];
+      const std::complex<double> v(w * (tr[p].x + logdet[p]), w * tr[p].y);
       const int64_t wn = nwb / 2 + n, mwn = nwb / 2 - n;
       e_w[wn] += v;
       if (mwn != wn) e_w[mwn] += v;
@@ -778,6 +815,8 @@ std::pair<double, double> diis_device(Ctx* c, double2* FS, int64_t it) {
   return {cF, cS};
 }
 
+// the symmetry-reduced (IBZ) k-space path and coqui_b200_set_symmetry
+#include "ctx_sym.cuh"
 
 // =======================================================================================
 // ABI
@@ -1028,6 +1067,10 @@ int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_
     }
     CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
     c->have_thc = true;
+    if (c->sym) {
+      c->sym->thc_ready = false;
+      c->sym->w_valid = false;
+    }
     c->gcache_valid = false;
     c->w_valid = false;
     c->vr_valid = false;
@@ -1087,6 +1130,10 @@ int coqui_b200_aux_to_primary(coqui_b200_ctx* c, int64_t n_tau, const double* O_
 int coqui_b200_eval_pi(coqui_b200_ctx* c, const double* G_tskij, double* Pi_tqPQ) {
   return guarded(c, [&] {
     require_ready(c, true, true, true);
+    if (c->sym) {
+      sym_eval_pi(c, G_tskij, Pi_tqPQ);
+      return;
+    }
     c->begin_timing();
     upload_G(c, G_tskij);
     c->mark("h2d_G");
@@ -1608,6 +1655,19 @@ int coqui_b200_update_w(coqui_b200_ctx* c, const double* G_tskij, double* dW_qtP
                         double* eps_inv_head) {
   return guarded(c, [&] {
     require_ready(c, true, true, true);
+    if (c->sym) {
+      sym_require_plain(c, eps_inv_head);
+      c->begin_timing();
+      sym_upload_g(c, G_tskij);
+      c->mark("h2d_G");
+      sym_update_w(c);
+      if (dW_qtPQ) {
+        sym_download_w(c, dW_qtPQ);
+        c->mark("d2h_W");
+      }
+      c->end_timing();
+      return;
+    }
     c->begin_timing();
     upload_G(c, G_tskij);
     c->mark("h2d_G");
@@ -1628,6 +1688,10 @@ int coqui_b200_set_w(coqui_b200_ctx* c, const double* dW_qtPQ) {
   return guarded(c, [&] {
     require_ready(c, true, true, true);
     CQ_REQUIRE(dW_qtPQ, COQUI_B200_EINVAL, "null W");
+    if (c->sym) {
+      sym_set_w(c, dW_qtPQ);
+      return;
+    }
     const int64_t ncol = c->Np * c->Np, n = c->nq * c->nth * ncol;
     c->PW.ensure((size_t)c->nmax * c->nq * ncol * c->elem());
     c->stage.ensure(n);
@@ -1647,6 +1711,17 @@ int coqui_b200_set_w(coqui_b200_ctx* c, const double* dW_qtPQ) {
 int coqui_b200_eval_sigma(coqui_b200_ctx* c, const double* G_tskij, double* Sigma_tskij) {
   return guarded(c, [&] {
     require_ready(c, true, true, true);
+    if (c->sym) {
+      sym_require_plain(c, nullptr);
+      CQ_REQUIRE(c->sym->w_valid, COQUI_B200_EINVAL,
+                 "no screened interaction: call update_w or set_w");
+      c->begin_timing();
+      sym_upload_g(c, G_tskij);
+      c->mark("h2d_G");
+      sym_sigma(c, Sigma_tskij);
+      c->end_timing();
+      return;
+    }
     CQ_REQUIRE(c->w_valid, COQUI_B200_EINVAL, "no screened interaction: call update_w or set_w");
     c->begin_timing();
     upload_G(c, G_tskij);
@@ -1660,6 +1735,16 @@ int coqui_b200_gw_iteration(coqui_b200_ctx* c, const double* G_tskij, double* Si
                             double* eps_inv_head) {
   return guarded(c, [&] {
     require_ready(c, true, true, true);
+    if (c->sym) {
+      sym_require_plain(c, eps_inv_head);
+      c->begin_timing();
+      sym_upload_g(c, G_tskij);
+      c->mark("h2d_G");
+      sym_update_w(c);
+      sym_sigma(c, Sigma_tskij);
+      c->end_timing();
+      return;
+    }
     // resident G or page-locked host buffers, no eps head: the iteration (the copies included)
     // runs as one CUDA graph, captured on the first of a run of such calls with the same
     // buffers and replayed by the following ones
@@ -1724,6 +1809,10 @@ int coqui_b200_rpa_energy(coqui_b200_ctx* c, const double* G_tskij, double* e_rp
     require_ready(c, true, true, true);
     CQ_REQUIRE(e_rpa, COQUI_B200_EINVAL, "null e_rpa");
     CQ_REQUIRE(c->Ttw_bb.size() == (size_t)(c->nt * c->nwb), COQUI_B200_EINVAL, "IR tables");
+    if (c->sym) {
+      *e_rpa = sym_rpa_energy(c, G_tskij);
+      return;
+    }
     // resident G or a page-locked host G: one CUDA graph, captured on the first of a run of
     // such calls and replayed by the following ones
     if (c->mode == COQUI_B200_MIXED && !c->prof.on &&

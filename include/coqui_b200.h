@@ -141,6 +141,46 @@ COQUI_B200_API int coqui_b200_gw_iteration(coqui_b200_ctx* ctx, const double* G_
 COQUI_B200_API int coqui_b200_set_div_treatment(coqui_b200_ctx* ctx, int div_treatment,
                                                 double madelung, const double* chi_head_P);
 
+/* ---- symmetry-reduced (IBZ) k-space path: scr_coulomb_t::eval_Pi_rpa_kspace
+   (src/methods/scr_coulomb/rpa_pi.icc:182-336), gw_t::eval_Sigma_all_kspace
+   (src/methods/GW/thc_gw.icc:216-443, selected by thc_gw.icc:31-32 when nqpts_ibz < nqpts)
+   and the IBZ-weighted RPA energy (src/methods/GW/thc_rpa.icc:130-173) ---- */
+
+/* The mean field's bz_symm maps (src/mean_field/symmetry/bz_symmetry.hpp), indexed as the
+   reference indexes them: its k list (IBZ points first, their time-reversal images last) and
+   Qpts = kpts (Gamma-centred grid).  k_lex[i] is the position of the reference's k-point i in
+   the lexicographic grid that set_kmesh and set_thc use (X and V stay in that order).
+   Qs is (nsym, ld_Qs) with row s holding nq_per_s[s] q indices; ks_to_k is (nsym, nk);
+   D is symmetry_rotation(isym, k) as dense (nsym, nk_ibz, nb, nb) complex128 (row 0, the
+   identity operation, is not read; NULL: every rotation is the identity). */
+typedef struct {
+  int64_t nk_ibz;               /* IBZ k-points: the reference's k indices [0, nk_ibz) */
+  int64_t nq_ibz;               /* IBZ q-points: the reference's q indices [0, nq_ibz) */
+  int64_t nsym;                 /* qsymms.size() */
+  int64_t ld_Qs;                /* row length of Qs */
+  const int64_t* k_lex;         /* (nk) */
+  const int64_t* kp_to_ibz;     /* (nk) */
+  const int32_t* kp_trev;       /* (nk) 0 / 1 */
+  const int64_t* kp_trev_pair;  /* (nk), -1 where there is none */
+  const int64_t* qp_to_ibz;     /* (nq) */
+  const int32_t* qp_trev;       /* (nq) 0 / 1 */
+  const int64_t* qminus;        /* (nq) */
+  const int64_t* nq_per_s;      /* (nsym) */
+  const int64_t* Qs;            /* (nsym, ld_Qs) */
+  const int64_t* ks_to_k;       /* (nsym, nk) */
+  const double* D;              /* (nsym, nk_ibz, nb, nb) complex128 or NULL */
+} coqui_b200_symmetry;
+
+/* Checks the maps against the grid of set_kmesh (ranges, IBZ first, time-reversal pairs at -k,
+   qminus, every q in exactly one Qs row) and switches the context to the k-space path:
+   eval_pi, update_w, set_w, eval_sigma, gw_iteration and rpa_energy then take G_tskij and
+   return Sigma_tskij on the IBZ k-points (nt_f, ns, nk_ibz, nb, nb) and Pi / W on the IBZ
+   q-points (nt_half, nq_ibz, Np, Np) / dW_qtPQ (nq_ibz, nt_half, Np, Np); G must be given
+   (no resident G).  The q -> 0 treatments other than ignore_g0 and the eps^-1 head are not
+   available on this path (EUNSUPPORTED).  sym == NULL returns to the full-BZ path.
+   Needs set_kmesh. */
+COQUI_B200_API int coqui_b200_set_symmetry(coqui_b200_ctx* ctx, const coqui_b200_symmetry* sym);
+
 /* ---- THC Hartree-Fock (hf_t::evaluate, src/methods/HF/thc_hf.cpp:21-60 ->
    thc_hf.icc:17-272 for q-independent THC without symmetry; hf_t.cpp:45-84) ---- */
 

@@ -1,0 +1,119 @@
+"""GPU parity of the symmetry-reduced (IBZ) k-space path (coqui_b200_set_symmetry) against the
+k-space oracle (oracle/sym_oracle.py), on symmetric synthetic systems: time reversal alone, and
+the x <-> y mirror with a sign representation on the mirror line.
+
+Tolerances as the full-BZ parity tests: 1e-10 max-abs (FP64 form), 1e-6 (mixed form) for Pi,
+W, Sigma and 1e-6 Ha for E_c."""
+import numpy as np
+import pytest
+
+from coqui_b200 import capi
+from coqui_b200.iaft import IAFT as ProductIAFT
+from oracle import sym_oracle as SO
+from oracle import thc_oracle as O
+from coqui_b200.symmetry import symmetric_system as make_sym_system
+
+pytestmark = pytest.mark.gpu
+
+EINVAL, EUNSUPPORTED = -1, -2
+
+MODES = [(capi.FP64, 1e-10), (capi.MIXED, 1e-6)]
+MODE_IDS = ["fp64", "mixed"]
+CASES = [("trev", (3, 3, 1)), ("swap", (4, 4, 1))]
+CASE_IDS = ["trev-331", "swap-441"]
+
+
+def maxabs(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max())
+
+
+class SymCase:
+    def __init__(self, kind, grid, nb=8, Np=24):
+        self.ft = O.IAFT(1000.0, 10.0, "low")
+        self.pft = ProductIAFT(1000.0, 10.0, "low")
+        self.d = d = make_sym_system(kind, grid, nb, Np, self.ft)
+        self.sym = sym = d["sym"]
+        self.Pi = SO.eval_Pi_rpa_kspace(d["G_ibz"], d["X"], sym)
+        self.dW = SO.update_w_kspace(d["G_ibz"], d["X"], d["V"], self.ft, sym)
+        self.Sigma = SO.eval_Sigma_all_kspace(d["G_ibz"], self.dW, d["X"], sym, d["D"])
+        self.e_rpa = SO.rpa_energy_kspace(d["G_ibz"], d["X"], d["V"], self.ft, sym)
+
+    def ctx(self, mode, with_sym=True):
+        d = self.d
+        nk = d["sym"]["nk"]
+        c = capi.Context(nk, d["X"].shape[3], d["X"].shape[2], self.ft.nt_f, self.ft.nw_b,
+                         d["grid"], mode=mode)
+        c.set_ir(self.pft)
+        c.set_kmesh(d["kpts_lex"], d["lattv"])
+        c.set_thc(d["X_lex"], d["V_lex"])
+        if with_sym:
+            c.set_symmetry(self.sym, d["D"])
+        return c
+
+
+_cases = {}
+
+
+def case(kind, grid):
+    key = (kind, grid)
+    if key not in _cases:
+        _cases[key] = SymCase(kind, grid)
+    return _cases[key]
+
+
+@pytest.mark.parametrize("kind,grid", CASES, ids=CASE_IDS)
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_ibz_pi_w_sigma_rpa(kind, grid, mode, tol):
+    b = case(kind, grid)
+    c = b.ctx(mode)
+    G = b.d["G_ibz"]
+    assert maxabs(c.eval_pi(G), b.Pi) < tol
+    W, _ = c.update_w(G, want_head=False)
+    assert maxabs(W, b.dW) < tol
+    assert maxabs(c.eval_sigma(G), b.Sigma) < tol
+    S, _ = c.gw_iteration(G)
+    assert maxabs(S, b.Sigma) < tol
+    # Sigma of an uploaded W
+    c.set_w(b.dW)
+    assert maxabs(c.eval_sigma(G), b.Sigma) < tol
+    assert abs(c.rpa_energy(G) - b.e_rpa) < tol
+    assert np.abs(b.Sigma).max() > 1e-3
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_time_reversal_ibz_sigma_is_the_full_bz_sigma(mode, tol):
+    # with time reversal the IBZ path reproduces the full-BZ path of the same context at the
+    # IBZ k-points (and the RPA energy); back on the full-BZ path after set_symmetry(None)
+    b = case("trev", (3, 3, 1))
+    c = b.ctx(mode)
+    S_ibz, _ = c.gw_iteration(b.d["G_ibz"])
+    e_ibz = c.rpa_energy(b.d["G_ibz"])
+    c.set_symmetry(None)
+    S_full, _ = c.gw_iteration(b.d["G_lex"])
+    kl = b.d["lex"][:b.sym["nk_ibz"]]
+    assert maxabs(S_ibz, S_full[:, :, kl]) < 2 * tol
+    assert abs(e_ibz - c.rpa_energy(b.d["G_lex"])) < 2 * tol
+
+
+def test_symmetry_map_errors_are_codes():
+    b = case("swap", (4, 4, 1))
+    c = b.ctx(capi.FP64, with_sym=False)
+    bad = dict(b.sym)
+    bad["qminus"] = np.roll(b.sym["qminus"], 1)
+    with pytest.raises(capi.CoquiB200Error) as e:
+        c.set_symmetry(bad)
+    assert e.value.code == EINVAL
+    bad = dict(b.sym)
+    Qs = b.sym["Qs"].copy()
+    Qs[1, 0] = Qs[0, 0]  # a q-point listed twice
+    bad["Qs"] = Qs
+    with pytest.raises(capi.CoquiB200Error) as e:
+        c.set_symmetry(bad)
+    assert e.value.code == EINVAL
+    c.set_symmetry(b.sym, b.d["D"])
+    with pytest.raises(capi.CoquiB200Error) as e:
+        c.update_w(b.d["G_ibz"], want_head=True)
+    assert e.value.code == EUNSUPPORTED
+    with pytest.raises(capi.CoquiB200Error) as e:
+        c.eval_sigma(None)
+    assert e.value.code == EINVAL
