@@ -78,6 +78,11 @@ struct SymState {
   DevBuf<unsigned char> PWi;      // (nmax, nq_ibz, Np, Np) Pi / W on the IBZ q-points
   DevBuf<unsigned char> Sq;       // (nsym, nk_ibz, Np, Np) Sigma_PQ rows of one tau
   DevBuf<double2> Sab, Tab, Rab;  // (nsym, nk_ibz, nb, nb)
+  // long-wavelength treatments on the IBZ: X of the IBZ k-points, chi-bar heads and prefactors
+  // of the IBZ q-points, T^k of Sigma_div_correction, eps^-1 per (tau, q_ibz)
+  DevBuf<double2> Xibz, chi_i, Tdiv;
+  DevBuf<double> fac_i;
+  std::vector<double2> eps_i;
   bool w_valid = false;
 };
 
@@ -1229,24 +1234,25 @@ void eps_raw_heads(Ctx* c) {
   c->eps_raw_valid = true;
 }
 
-// eps_inv_head_t (g0_div_utils.hpp:55-111): c->head_h (nth) from c->eps_raw.  ignore_g0 and
-// gygi: the first smallest nonzero |q|.  gygi_extrplt(_2d): through the q with
-// 0 < |q| <= 0.8 (q_z = 0 for _2d; distinct |q| only, filter_qpts :26-42), per bosonic
-// frequency (tau_to_w_PHsym), the least-squares quadratic in |q| extrapolated to q = 0
-// (extrapolate_to_q0 :284-311), back with w_to_tau_PHsym; the first such q alone when fewer
-// than 3.
-void select_head(Ctx* c) {
-  const int64_t nth = c->nth, nq = c->nq, nwh = c->nwh;
-  const std::vector<double2>& eps = c->eps_raw;
+// eps_inv_head_t (g0_div_utils.hpp:55-111): c->head_h (nth) from eps (nth, nq) over the
+// q-points with norms qnorm and z components qz.  ignore_g0 and gygi: the first smallest
+// nonzero |q| (q_smallest).  gygi_extrplt(_2d): through the q with 0 < |q| <= 0.8 (q_z = 0 for
+// _2d; distinct |q| only, filter_qpts :26-42), per bosonic frequency (tau_to_w_PHsym), the
+// least-squares quadratic in |q| extrapolated to q = 0 (extrapolate_to_q0 :284-311), back with
+// w_to_tau_PHsym; the first such q alone when fewer than 3.
+void select_head_from(Ctx* c, const std::vector<double2>& eps, int64_t nq,
+                      const std::vector<double>& qnorm, const std::vector<double>& qz,
+                      int64_t q_smallest) {
+  const int64_t nth = c->nth, nwh = c->nwh;
   c->head_h.assign(nth, make_double2(0, 0));
   const int div = nq == 1 ? 0 : c->div;
-  int64_t col = c->q_smallest;
+  int64_t col = q_smallest;
   if (div >= 2) {
     std::vector<int64_t> idx;
     std::set<double> seen;
     for (int64_t q = 0; q < nq; ++q) {
-      const double n = c->qnorm[q];
-      if (n > 0.0 && n <= 0.8 && (div != 3 || c->qz[q] == 0.0) && seen.insert(n).second)
+      const double n = qnorm[q];
+      if (n > 0.0 && n <= 0.8 && (div != 3 || qz[q] == 0.0) && seen.insert(n).second)
         idx.push_back(q);
     }
     CQ_REQUIRE(!idx.empty(), COQUI_B200_EINVAL,
@@ -1257,7 +1263,7 @@ void select_head(Ctx* c) {
       // normal equations of A(i, j) = |q_i|^j, j = 0..2
       double a[3][3] = {};
       for (size_t i = 0; i < m; ++i) {
-        const double Q = c->qnorm[idx[i]], p[3] = {1.0, Q, Q * Q};
+        const double Q = qnorm[idx[i]], p[3] = {1.0, Q, Q * Q};
         for (int j = 0; j < 3; ++j)
           for (int l = 0; l < 3; ++l) a[j][l] += p[j] * p[l];
       }
@@ -1277,7 +1283,7 @@ void select_head(Ctx* c) {
             const double2 T = c->Twt_pos[n * nth + t], e = eps[t * nq + idx[i]];
             ew += cd(T.x, T.y) * cd(e.x, e.y);
           }
-          const double Q = c->qnorm[idx[i]], p[3] = {1.0, Q, Q * Q};
+          const double Q = qnorm[idx[i]], p[3] = {1.0, Q, Q * Q};
           for (int j = 0; j < 3; ++j) atb[j] += p[j] * ew;
         }
         e0[n] = r0[0] * atb[0] + r0[1] * atb[1] + r0[2] * atb[2];
@@ -1296,6 +1302,9 @@ void select_head(Ctx* c) {
   }
   for (int64_t t = 0; t < nth; ++t) c->head_h[t] = eps[t * nq + col];
 }
+void select_head(Ctx* c) {
+  select_head_from(c, c->eps_raw, c->nq, c->qnorm, c->qz, c->q_smallest);
+}
 
 // the eps^-1 head of the current W (nth complex values as (re, im) into out, if not null)
 void eps_head(Ctx* c, double* out) {
@@ -1308,20 +1317,23 @@ void eps_head(Ctx* c, double* out) {
     }
 }
 
-// gw_t::Sigma_div_correction (thc_gw.icc:446-526) on the device Sigma (FP64), for the gygi
+// gw_t::Sigma_div_correction (thc_gw.icc:446-526) on a device Sigma (FP64), for the gygi
 // treatments: Sigma(t, k) += -madelung Re head(t_pos) T^k G(t, k) T^kH with
-// T^k = X^kH diag(conj chi_head) X^k, t_pos = t below nt_half, else nt - 1 - t.
-void sigma_div_correction(Ctx* c) {
+// T^k = X^kH diag(conj chi_head) X^k, t_pos = t below nt_half, else nt - 1 - t; nk k-points
+// with collocation X (nk, Np, nb), G and Sigma (nt, nk, nb, nb); T^k kept in Tdiv while
+// tdiv_valid.
+void sigma_div_correction_on(Ctx* c, int64_t nk, const double2* X, const double2* G,
+                             double2* Sig, DevBuf<double2>& Tdiv, bool& tdiv_valid) {
   cq::Prof::Scope sc(&c->prof, "sigma_div");
-  const int64_t nk = c->nk, nb = c->nb, Np = c->Np, nt = c->nt, nth = c->nth, per = nb * nb;
+  const int64_t nb = c->nb, Np = c->Np, nt = c->nt, nth = c->nth, per = nb * nb;
   const int64_t nprob = nt * nk;
-  if (!c->tdiv_valid) {
-    c->Tdiv.ensure(nk * per);
+  if (!tdiv_valid) {
+    Tdiv.ensure(nk * per);
     c->Tproj.ensure((size_t)nk * Np * nb);
-    cq::scale_rows(c->X.p, c->chi0c.p, c->Tproj.p, nk, Np, nb, c->st);
-    zgemm_rm(c, 'C', 'N', nb, nb, Np, make_double2(1, 0), c->X.p, nb, Np * nb, c->Tproj.p, nb,
-             Np * nb, make_double2(0, 0), c->Tdiv.p, nb, per, nk);
-    c->tdiv_valid = true;
+    cq::scale_rows(X, c->chi0c.p, c->Tproj.p, nk, Np, nb, c->st);
+    zgemm_rm(c, 'C', 'N', nb, nb, Np, make_double2(1, 0), X, nb, Np * nb, c->Tproj.p, nb,
+             Np * nb, make_double2(0, 0), Tdiv.p, nb, per, nk);
+    tdiv_valid = true;
   }
   std::vector<double> f(nt);
   for (int64_t t = 0; t < nt; ++t) f[t] = -c->madelung * c->head_h[t < nth ? t : nt - t - 1].x;
@@ -1333,12 +1345,12 @@ void sigma_div_correction(Ctx* c) {
   for (int64_t t = 0; t < nt; ++t)
     for (int64_t k = 0; k < nk; ++k) {
       const int64_t i = t * nk + k;
-      c->divp_h[i] = c->Tdiv.p + k * per;
-      c->divp_h[nprob + i] = c->G.p + i * per;
+      c->divp_h[i] = Tdiv.p + k * per;
+      c->divp_h[nprob + i] = G + i * per;
       c->divp_h[2 * nprob + i] = c->divY.p + i * per;
       c->divp_h[3 * nprob + i] = c->divY.p + i * per;
-      c->divp_h[4 * nprob + i] = c->Tdiv.p + k * per;
-      c->divp_h[5 * nprob + i] = c->Sig.p + i * per;
+      c->divp_h[4 * nprob + i] = Tdiv.p + k * per;
+      c->divp_h[5 * nprob + i] = Sig + i * per;
     }
   c->divp.ensure(6 * nprob);
   upload(c, c->divp.p, c->divp_h.data(), 6 * nprob * sizeof(const double2*));
@@ -1348,6 +1360,9 @@ void sigma_div_correction(Ctx* c) {
   cq::scale_slices(c->divY.p, c->divf.p, nt, nk * per, c->st);
   zgemm_rm_ptrs(c, 'N', 'C', nb, nb, nb, make_double2(1, 0), P + 3 * nprob, nb, P + 4 * nprob,
                 nb, make_double2(1, 0), const_cast<double2* const*>(P + 5 * nprob), nb, nprob);
+}
+void sigma_div_correction(Ctx* c) {
+  sigma_div_correction_on(c, c->nk, c->X.p, c->G.p, c->Sig.p, c->Tdiv, c->tdiv_valid);
 }
 
 void download_w_qt(Ctx* c, double* dW_qtPQ) {
@@ -1656,11 +1671,14 @@ int coqui_b200_update_w(coqui_b200_ctx* c, const double* G_tskij, double* dW_qtP
   return guarded(c, [&] {
     require_ready(c, true, true, true);
     if (c->sym) {
-      sym_require_plain(c, eps_inv_head);
       c->begin_timing();
       sym_upload_g(c, G_tskij);
       c->mark("h2d_G");
       sym_update_w(c);
+      if (eps_inv_head) {
+        sym_eps_head(c, eps_inv_head);
+        c->mark("EPS_INV_HEAD");
+      }
       if (dW_qtPQ) {
         sym_download_w(c, dW_qtPQ);
         c->mark("d2h_W");
@@ -1712,7 +1730,6 @@ int coqui_b200_eval_sigma(coqui_b200_ctx* c, const double* G_tskij, double* Sigm
   return guarded(c, [&] {
     require_ready(c, true, true, true);
     if (c->sym) {
-      sym_require_plain(c, nullptr);
       CQ_REQUIRE(c->sym->w_valid, COQUI_B200_EINVAL,
                  "no screened interaction: call update_w or set_w");
       c->begin_timing();
@@ -1736,11 +1753,14 @@ int coqui_b200_gw_iteration(coqui_b200_ctx* c, const double* G_tskij, double* Si
   return guarded(c, [&] {
     require_ready(c, true, true, true);
     if (c->sym) {
-      sym_require_plain(c, eps_inv_head);
       c->begin_timing();
       sym_upload_g(c, G_tskij);
       c->mark("h2d_G");
       sym_update_w(c);
+      if (eps_inv_head) {
+        sym_eps_head(c, eps_inv_head);
+        c->mark("EPS_INV_HEAD");
+      }
       sym_sigma(c, Sigma_tskij);
       c->end_timing();
       return;

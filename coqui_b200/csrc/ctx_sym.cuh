@@ -18,6 +18,17 @@
 // both give the same sums.  The self-energy keeps the reference's term lists: per tau slice one
 // pass stages each column tile of every G(k) and W(q_ibz) in shared memory and forms the rows
 // of all (isym, k_ibz) from there, so G and W cross HBM once however many terms read them.
+// defined further down in ctx.cu, inside its extern "C" block (shared with the full-BZ route)
+extern "C" {
+namespace {
+void select_head_from(Ctx* c, const std::vector<double2>& eps, int64_t nq,
+                      const std::vector<double>& qnorm, const std::vector<double>& qz,
+                      int64_t q_smallest);
+void sigma_div_correction_on(Ctx* c, int64_t nk, const double2* X, const double2* G,
+                             double2* Sig, DevBuf<double2>& Tdiv, bool& tdiv_valid);
+}  // namespace
+}
+
 namespace {
 
 void lex_coords(const Ctx* c, int64_t p, int64_t x[3]) {
@@ -50,6 +61,10 @@ void sym_prepare_thc(Ctx* c) {
   S.Xs.ensure((size_t)S.nsym * nki * per);
   for (int64_t i = 0; i < S.nsym * nki; ++i)
     CQ_CHECK_CUDA(cudaMemcpyAsync(S.Xs.p + i * per, c->X.p + S.ks_lex[i] * per,
+                                  per * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  S.Xibz.ensure((size_t)nki * per);
+  for (int64_t i = 0; i < nki; ++i)
+    CQ_CHECK_CUDA(cudaMemcpyAsync(S.Xibz.p + i * per, c->X.p + S.lex[i] * per,
                                   per * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
   S.Li.ensure((size_t)nqi * pp);
   S.LHi.ensure((size_t)nqi * pp);
@@ -161,6 +176,51 @@ void a2p_with(Ctx* c, const double2* X, int64_t nkx, const double2* Sk, double2*
            Np * nb, make_double2(0, 0), out, nb, nb * nb, nkx);
 }
 
+bool sym_div_active(const Ctx* c) { return c->div != 0 && c->sym->nq_ibz > 1; }
+
+// eps_inv_head_t over Qpts_ibz (g0_div_utils.hpp:55-111, 180-214): eps^-1 per (tau, q_ibz) of
+// the IBZ W, then the head of the treatment in effect into c->head_h (and out, if not null)
+void sym_eps_head(Ctx* c, double* out) {
+  SymState& S = *c->sym;
+  cq::Prof::Scope sc(&c->prof, "eps_head");
+  CQ_REQUIRE(S.w_valid, COQUI_B200_EINVAL, "no screened interaction: call update_w or set_w");
+  const int64_t nqi = S.nq_ibz, Np = c->Np, nth = c->nth;
+  S.chi_i.ensure((size_t)nqi * Np);
+  S.fac_i.ensure((size_t)nqi);
+  std::vector<double> qn(nqi), qz(nqi);
+  int64_t qsm = 0;
+  double best = -1;
+  for (int64_t i = 0; i < nqi; ++i) {
+    const int64_t q = S.q_lex[i];
+    CQ_CHECK_CUDA(cudaMemcpyAsync(S.chi_i.p + i * Np, c->chi.p + q * Np, Np * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, c->st));
+    CQ_CHECK_CUDA(cudaMemcpyAsync(S.fac_i.p + i, c->fac.p + q, sizeof(double),
+                                  cudaMemcpyDeviceToDevice, c->st));
+    qn[i] = c->qnorm[q];
+    qz[i] = c->qz[q];
+    if (nqi > 1 && qn[i] > 0.0 && (best < 0 || qn[i] < best)) {  // find_smallest_qabs
+      best = qn[i];
+      qsm = i;
+    }
+  }
+  c->eps.ensure((size_t)nth * nqi);
+  if (c->mode == COQUI_B200_FP64)
+    cq::launch_eps_head<double>((const double2*)S.PWi.p, S.chi_i.p, S.fac_i.p, c->eps.p, nth, nqi,
+                                Np, c->st);
+  else
+    cq::launch_eps_head<float>((const float2*)S.PWi.p, S.chi_i.p, S.fac_i.p, c->eps.p, nth, nqi,
+                               Np, c->st);
+  S.eps_i.resize((size_t)nth * nqi);
+  download(c, S.eps_i.data(), c->eps.p, S.eps_i.size() * sizeof(double2));
+  CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+  select_head_from(c, S.eps_i, nqi, qn, qz, qsm);
+  if (out)
+    for (int64_t t = 0; t < nth; ++t) {
+      out[2 * t] = c->head_h[t].x;
+      out[2 * t + 1] = c->head_h[t].y;
+    }
+}
+
 // eval_Sigma_all_kspace for t and beta - t into c->Sig (nt, nk_ibz, nb, nb).  Per tau slice:
 // one gather pass forms the Sigma_PQ rows of every (isym, ik), one batched projection takes
 // them to the orbitals at ks_to_k, D^H Sigma_ab D per row, and the rows of each ik are summed.
@@ -219,18 +279,19 @@ void sym_sigma(Ctx* c, double* host_out) {
       cq::launch_add_blocks(S.Rab.p, c->Sig.p + itg * nki * bb, S.nsym, nki * bb, c->st);
     }
   }
+  // Sigma_div_correction on the IBZ k-points (thc_gw.icc:31-33, 446-526)
+  if (sym_div_active(c)) {
+    CQ_REQUIRE(c->chi0c.n >= (size_t)Np, COQUI_B200_EINVAL,
+               "the gygi treatments of Sigma need chi_head (coqui_b200_set_div_treatment)");
+    sym_eps_head(c, nullptr);
+    bool fresh = false;  // T^k from the current X and chi_head
+    sigma_div_correction_on(c, nki, S.Xibz.p, S.Gi.p, c->Sig.p, S.Tdiv, fresh);
+  }
   c->mark("EVALUATE_SIGMA_K");
   if (host_out) {
     download(c, host_out, c->Sig.p, (size_t)nt * nki * bb * sizeof(double2));
     c->mark("d2h_Sigma");
   }
-}
-
-void sym_require_plain(Ctx* c, const double* eps_inv_head) {
-  CQ_REQUIRE(!eps_inv_head, COQUI_B200_EUNSUPPORTED,
-             "the eps^-1 head is not available on the IBZ k-space path");
-  CQ_REQUIRE(c->div == 0 || c->nq == 1, COQUI_B200_EUNSUPPORTED,
-             "only ignore_g0 is available on the IBZ k-space path");
 }
 
 void sym_eval_pi(Ctx* c, const double* G_tskij, double* Pi_tqPQ) {

@@ -175,8 +175,8 @@ def green_tau(H0_kij, ft, mu=0.0):
     return np.einsum("kia,tka,kja->tkij", C, g, np.conj(C))
 
 
-def symmetric_system(kind, kp_grid, nb, Np, ft, seed=7, mu=0.0):
-    """Seeded THC inputs with a symmetry on a cubic lattice (lattv = I):
+def symmetric_system(kind, kp_grid, nb, Np, ft, seed=7, mu=0.0, alat=1.0):
+    """Seeded THC inputs with a symmetry on a cubic lattice (lattv = alat I):
 
     * ``"trev"``: time reversal alone: X^{-k} = conj(X^k), H0^{-k} = conj(H0^k); at k = -k
       X and H0 are real;
@@ -188,9 +188,10 @@ def symmetric_system(kind, kp_grid, nb, Np, ft, seed=7, mu=0.0):
 
     V is a physical Coulomb matrix in both, V^{-q} = conj(V^q), with the model's symmetry:
     one random Hermitian positive definite matrix per orbit of {E, S} x {1, T}, averaged over
-    the stabilizer of the orbit's first point.  Returns the maps (``sym``), D, X / V / G_ibz
-    in the reference's order, and X_lex / V_lex / G_lex (G unfolded to every k-point with the
-    reference's rule) / kpts_lex in lexicographic order."""
+    the stabilizer of the orbit's first point.  The chi-bar heads are CN(0, 1/Np) per q-point.
+    Returns the maps (``sym``), D, X / V / G_ibz / chi_bar / kpts in the reference's order, and
+    X_lex / V_lex / G_lex (G unfolded to every k-point with the reference's rule) / chi_lex /
+    kpts_lex in lexicographic order."""
     rng = np.random.default_rng(seed)
     grid = tuple(int(g) for g in kp_grid)
     if kind == "trev":
@@ -255,6 +256,7 @@ def symmetric_system(kind, kp_grid, nb, Np, ft, seed=7, mu=0.0):
         for n, p, t in imgs:
             V[n] = act(Vi, p, t)
             done[n] = True
+    chi = _cn(rng, (nk, Np), 1.0 / np.sqrt(Np))
     G_ibz = green_tau(H0[:nk_ibz], ft, mu)[:, None]  # (nt, 1, nk_ibz, nb, nb)
     lex = sym["lex"]
     G_full = G_ibz[:, :, sym["kp_to_ibz"]]
@@ -262,7 +264,8 @@ def symmetric_system(kind, kp_grid, nb, Np, ft, seed=7, mu=0.0):
     G_full = np.where(tr[None, None, :, None, None], np.swapaxes(G_full, -1, -2), G_full)
     inv = np.empty(nk, np.int64)
     inv[lex] = np.arange(nk)
-    kpts_lex = 2.0 * np.pi * kc[inv] / np.array(grid, np.float64)
-    return dict(sym=sym, D=D, X=X[None], V=V, G_ibz=G_ibz, lattv=np.eye(3), grid=grid,
-                X_lex=X[inv][None], V_lex=V[inv], G_lex=np.ascontiguousarray(G_full[:, :, inv]),
-                kpts_lex=kpts_lex, lex=lex, inv=inv, pi=pi)
+    kpts = 2.0 * np.pi * kc / (np.array(grid, np.float64) * alat)
+    return dict(sym=sym, D=D, X=X[None], V=V, G_ibz=G_ibz, lattv=alat * np.eye(3), grid=grid,
+                chi_bar=chi, kpts=kpts, X_lex=X[inv][None], V_lex=V[inv],
+                G_lex=np.ascontiguousarray(G_full[:, :, inv]), chi_lex=chi[inv],
+                kpts_lex=kpts[inv], lex=lex, inv=inv, pi=pi)

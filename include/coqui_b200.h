@@ -31,8 +31,9 @@
  *   - G_tskij and Sigma_tskij are (nt_f, ns, nk, nb, nb); X is (ns, nk, Np, nb);
  *     V is (nq, Np, Np); W is returned as dW_qtPQ (nq, nt_half, Np, Np);
  *   - Sigma is overwritten (thc_gw.cpp:136);
- *   - no symmetry: nq == nk, k-points form a Gamma-centred kp_grid in lexicographic order
- *     (kpts = 2 pi (i,j,l)/n in units where lattv rows are the lattice vectors).
+ *   - X and V cover the whole k-mesh, nq == nk, k-points form a Gamma-centred kp_grid in
+ *     lexicographic order (kpts = 2 pi (i,j,l)/n in units where lattv rows are the lattice
+ *     vectors); after coqui_b200_set_symmetry, G, Sigma, Pi and W cover the IBZ points.
  * Errors: every entry point returns 0 or a negative COQUI_B200_E* code and never aborts;
  * coqui_b200_last_error() gives the message.  One host thread per context; calls are
  * synchronous (they return after the device work finished).
@@ -176,9 +177,9 @@ typedef struct {
    eval_pi, update_w, set_w, eval_sigma, gw_iteration and rpa_energy then take G_tskij and
    return Sigma_tskij on the IBZ k-points (nt_f, ns, nk_ibz, nb, nb) and Pi / W on the IBZ
    q-points (nt_half, nq_ibz, Np, Np) / dW_qtPQ (nq_ibz, nt_half, Np, Np); G must be given
-   (no resident G).  The q -> 0 treatments other than ignore_g0 and the eps^-1 head are not
-   available on this path (EUNSUPPORTED).  sym == NULL returns to the full-BZ path.
-   Needs set_kmesh. */
+   (no resident G).  The eps^-1 head runs over the IBZ q-points (eps_inv_head_t with
+   Qpts_ibz) and Sigma_div_correction over the IBZ k-points, as in the reference.
+   sym == NULL returns to the full-BZ path.  Needs set_kmesh. */
 COQUI_B200_API int coqui_b200_set_symmetry(coqui_b200_ctx* ctx, const coqui_b200_symmetry* sym);
 
 /* ---- THC Hartree-Fock (hf_t::evaluate, src/methods/HF/thc_hf.cpp:21-60 ->

@@ -15,7 +15,10 @@ maps those paths read.  Only tests, the smoke check and the benchmark's CPU legs
 * ``eval_Sigma_all_kspace``: src/methods/GW/thc_gw.icc:216-443 (both tau halves,
   thc_gw.cpp:170-172);
 * ``update_w_kspace`` / ``rpa_energy_kspace``: scr_coulomb_t.cpp:37-95 and
-  thc_rpa.icc:130-173 over the IBZ q-points with q weights.
+  thc_rpa.icc:130-173 over the IBZ q-points with q weights;
+* ``eps_inv_head_kspace`` / ``sigma_div_correction_kspace``: eps_inv_head_t over Qpts_ibz
+  (g0_div_utils.hpp:55-111, 180-214) and Sigma_div_correction on the IBZ k-points
+  (thc_gw.icc:446-526).
 
 Operations act on integer crystal coordinates of the k grid: ``ops[is]`` is the integer
 matrix that generates the images of the IBZ (the reference's R^-1 transposed); index 0 is the
@@ -276,3 +279,20 @@ def rpa_energy_kspace(G_tskij, X_skPa, V_qPQ, ft, sym) -> float:
     Pi_w = ft.tau_to_w_PHsym(Pi_t)
     return O.rpa_energy_from_Pi_w(Pi_w, V_qPQ[:sym["nq_ibz"]], ft, X_skPa.shape[1],
                                   q_weight=q_weights(sym))
+
+
+def eps_inv_head_kspace(dW_qtPQ, chi_bar_qP, Qpts_ibz, lattv, ft, div="ignore_g0"):
+    """eps_inv_head_t on the IBZ q-points: eps^-1(t, q) of W(q_ibz) with the chi-bar heads of
+    those q-points, then the head of the treatment (g0_div_utils.hpp:55-111, 180-214)."""
+    W_tq = np.swapaxes(dW_qtPQ, 0, 1)
+    eps = O.eval_eps_inv_q(W_tq, chi_bar_qP, Qpts_ibz, lattv)
+    return O.eps_inv_head_t(eps, Qpts_ibz, ft, div)
+
+
+def sigma_div_correction_kspace(Sigma_tskij, G_tskij, X_skPa, chi_head_P, eps_inv_head,
+                                madelung, div, nq_ibz):
+    """Sigma_div_correction (thc_gw.icc:446-526) on the IBZ k-points: X of the first nk_ibz
+    k-points (the IBZ), nothing when nqpts_ibz == 1."""
+    nk_ibz = G_tskij.shape[2]
+    return O.sigma_div_correction(Sigma_tskij, G_tskij, X_skPa[:, :nk_ibz], chi_head_P,
+                                  eps_inv_head, madelung, div, nq=nq_ibz)

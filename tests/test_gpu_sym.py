@@ -15,7 +15,7 @@ from coqui_b200.symmetry import symmetric_system as make_sym_system
 
 pytestmark = pytest.mark.gpu
 
-EINVAL, EUNSUPPORTED = -1, -2
+EINVAL = -1
 
 MODES = [(capi.FP64, 1e-10), (capi.MIXED, 1e-6)]
 MODE_IDS = ["fp64", "mixed"]
@@ -28,10 +28,10 @@ def maxabs(a, b):
 
 
 class SymCase:
-    def __init__(self, kind, grid, nb=8, Np=24):
+    def __init__(self, kind, grid, nb=8, Np=24, alat=1.0):
         self.ft = O.IAFT(1000.0, 10.0, "low")
         self.pft = ProductIAFT(1000.0, 10.0, "low")
-        self.d = d = make_sym_system(kind, grid, nb, Np, self.ft)
+        self.d = d = make_sym_system(kind, grid, nb, Np, self.ft, alat=alat)
         self.sym = sym = d["sym"]
         self.Pi = SO.eval_Pi_rpa_kspace(d["G_ibz"], d["X"], sym)
         self.dW = SO.update_w_kspace(d["G_ibz"], d["X"], d["V"], self.ft, sym)
@@ -44,7 +44,7 @@ class SymCase:
         c = capi.Context(nk, d["X"].shape[3], d["X"].shape[2], self.ft.nt_f, self.ft.nw_b,
                          d["grid"], mode=mode)
         c.set_ir(self.pft)
-        c.set_kmesh(d["kpts_lex"], d["lattv"])
+        c.set_kmesh(d["kpts_lex"], d["lattv"], d["chi_lex"])
         c.set_thc(d["X_lex"], d["V_lex"])
         if with_sym:
             c.set_symmetry(self.sym, d["D"])
@@ -54,10 +54,10 @@ class SymCase:
 _cases = {}
 
 
-def case(kind, grid):
-    key = (kind, grid)
+def case(kind, grid, alat=1.0):
+    key = (kind, grid, alat)
     if key not in _cases:
-        _cases[key] = SymCase(kind, grid)
+        _cases[key] = SymCase(kind, grid, alat=alat)
     return _cases[key]
 
 
@@ -110,10 +110,46 @@ def test_symmetry_map_errors_are_codes():
     with pytest.raises(capi.CoquiB200Error) as e:
         c.set_symmetry(bad)
     assert e.value.code == EINVAL
+    bad = dict(b.sym)
+    bad["kp_to_ibz"] = np.roll(b.sym["kp_to_ibz"], 1)  # the IBZ no longer first
+    with pytest.raises(capi.CoquiB200Error) as e:
+        c.set_symmetry(bad)
+    assert e.value.code == EINVAL
     c.set_symmetry(b.sym, b.d["D"])
     with pytest.raises(capi.CoquiB200Error) as e:
-        c.update_w(b.d["G_ibz"], want_head=True)
-    assert e.value.code == EUNSUPPORTED
-    with pytest.raises(capi.CoquiB200Error) as e:
-        c.eval_sigma(None)
+        c.eval_sigma(None)  # no resident G on the IBZ route
     assert e.value.code == EINVAL
+    # the context stays usable
+    S, _ = c.gw_iteration(b.d["G_ibz"])
+    assert maxabs(S, b.Sigma) < 1e-10
+
+
+DIVS = ["gygi", "gygi_extrplt"]
+
+
+@pytest.mark.parametrize("div", DIVS)
+@pytest.mark.parametrize("kind,grid", CASES, ids=CASE_IDS)
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_ibz_long_wavelength_treatments(kind, grid, mode, tol, div):
+    # eps_inv_head_t over the IBZ q-points and Sigma_div_correction on the IBZ k-points;
+    # a lattice constant of 8 bohr puts several |q| below the 0.8 cut of the extrapolation
+    b = case(kind, grid, alat=8.0)
+    d, sym = b.d, b.sym
+    nqi = sym["nq_ibz"]
+    rng = np.random.default_rng(3)
+    chi_head = (rng.standard_normal(d["X"].shape[2]) + 1j * rng.standard_normal(d["X"].shape[2]))
+    chi_head /= np.sqrt(2.0 * d["X"].shape[2])
+    madelung = 0.25
+    head = SO.eps_inv_head_kspace(b.dW, d["chi_bar"][:nqi], d["kpts"][:nqi], d["lattv"], b.ft,
+                                  div)
+    Sigma = SO.sigma_div_correction_kspace(b.Sigma, d["G_ibz"], d["X"], chi_head, head,
+                                           madelung, div, nqi)
+    c = b.ctx(mode)
+    c.set_div_treatment(div, madelung, chi_head)
+    W, h = c.update_w(d["G_ibz"], want_head=True)
+    assert maxabs(W, b.dW) < tol and maxabs(h, head) < tol
+    assert np.abs(head).max() > 1e-3
+    assert maxabs(c.eval_sigma(d["G_ibz"]), Sigma) < tol
+    S, h2 = c.gw_iteration(d["G_ibz"], want_head=True)
+    assert maxabs(S, Sigma) < tol and maxabs(h2, head) < tol
+    assert maxabs(Sigma, b.Sigma) > 1e-4  # the correction is not negligible
