@@ -1,6 +1,7 @@
 """Build the in-tree CUDA library ``coqui_b200/_lib/libcoqui_b200.so`` for sm_100a.
 
-Each ``csrc/*.cu`` is compiled with nvcc (in parallel) and linked with cuBLAS/cuSOLVER.
+Each ``csrc/*.cu`` is compiled with nvcc (in parallel) and linked against the CUDA runtime
+alone (every product and factorisation is the library's own kernel).
 Objects are cached by content hash under ``coqui_b200/_build`` so rebuilds are incremental.
 
     python -m coqui_b200.build [--force]
@@ -22,7 +23,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr"]
-LIBS = ["-lcublas", "-lcusolver"]
+LIBS: list = []
 
 
 def _sources():

@@ -15,8 +15,6 @@
 #include <string>
 #include <vector>
 
-#include <cusolverDn.h>
-
 #include "chol.cuh"
 #include "dyson.cuh"
 #include "kernels.cuh"
@@ -61,12 +59,6 @@ __global__ void __launch_bounds__(256) k_herm_sum_grouped(const HermProblem* __r
   herm_sum_pair(pr.DH, pr.F, pr.E, pr.n, I, J);
 }
 
-#define CQ_SOLVER_CHECK(expr)                                                                   \
-  do {                                                                                          \
-    cusolverStatus_t _s = (expr);                                                               \
-    if (_s != CUSOLVER_STATUS_SUCCESS)                                                          \
-      throw cq::Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
-  } while (0)
 
 }  // namespace
 }  // namespace cq
@@ -76,7 +68,6 @@ using cq::DevBuf;
 struct coqui_b200_batch {
   int dev = 0;
   cudaStream_t st = nullptr;
-  cusolverDnHandle_t sol = nullptr;
   std::string err;
   int64_t nmol = 0, nt = 0, nth = 0, nwb = 0, nwh = 0, nmax = 0;
   std::vector<int64_t> nb, Np;
@@ -336,9 +327,6 @@ int coqui_b200_batch_create(coqui_b200_batch** out, int64_t nmol, const int64_t*
     CQ_CHECK_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
     CQ_CHECK_CUDA(cudaEventCreate(&b->ev0));
     CQ_CHECK_CUDA(cudaEventCreate(&b->ev1));
-    if (cusolverDnCreate(&b->sol) != CUSOLVER_STATUS_SUCCESS)
-      throw cq::Error(COQUI_B200_ECUDA, "cusolverDnCreate failed");
-    CQ_SOLVER_CHECK(cusolverDnSetStream(b->sol, b->st));
     b->nmol = nmol;
     b->nt = nt_f;
     b->nth = (nt_f + 1) / 2;
@@ -399,11 +387,9 @@ void coqui_b200_batch_destroy(coqui_b200_batch* b) {
   cudaSetDevice(b->dev);
   if (b->st) cudaStreamSynchronize(b->st);
   cudaStream_t st = b->st;
-  cusolverDnHandle_t sol = b->sol;
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   delete b;
-  if (sol) cusolverDnDestroy(sol);
   if (st) cudaStreamDestroy(st);
 }
 
@@ -454,7 +440,7 @@ int coqui_b200_batch_set_thc(coqui_b200_batch* b, int64_t m, const double* X_Pa,
     LH.ensure(Np * Np);
     CQ_CHECK_CUDA(cudaMemcpyAsync(X.p, X_Pa, Np * nb * sizeof(double2), cudaMemcpyHostToDevice, b->st));
     CQ_CHECK_CUDA(cudaMemcpyAsync(L.p, V_PQ, Np * Np * sizeof(double2), cudaMemcpyHostToDevice, b->st));
-    const int info = cq::cholesky_lower_batched(b->sol, L.p, Np, 1, b->st);
+    const int info = cq::cholesky_lower_batched(L.p, Np, 1, b->st);
     CQ_REQUIRE(info == 0, COQUI_B200_ENOTHPD, "Coulomb matrix V is not positive definite");
     cq::launch_zero_upper_and_adjoint(L.p, LH.p, Np, 1, b->st);
     cq::to_c64(X.p, b->Xs.p + b->offX[m], Np, nb, 1, false, b->st);

@@ -8,9 +8,6 @@
 //   per (q, iW): V = L L^H, M = L^H Pi L, I - M = C C^H (FP64), W = Y^H Y - V, Y = C^{-1} L^H
 //   W(iW) -> W(tau)    (in-place IR transform), eps^-1 head.
 // The self-energy and the RPA energy reuse the same stages.
-#include <cublas_v2.h>
-#include <cusolverDn.h>
-
 #include <algorithm>
 #include <complex>
 #include <cstring>
@@ -34,19 +31,6 @@ using cq::KGrid;
 namespace {
 
 const char* kVersion = "coqui_b200 0.1.0 (sm_100a)";
-
-#define CQ_CHECK_BLAS(expr)                                                              \
-  do {                                                                                   \
-    cublasStatus_t _s = (expr);                                                          \
-    if (_s != CUBLAS_STATUS_SUCCESS)                                                     \
-      throw Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
-  } while (0)
-#define CQ_CHECK_SOLVER(expr)                                                            \
-  do {                                                                                   \
-    cusolverStatus_t _s = (expr);                                                        \
-    if (_s != CUSOLVER_STATUS_SUCCESS)                                                   \
-      throw Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
-  } while (0)
 
 using cq::DevBuf;
 
@@ -94,8 +78,6 @@ struct coqui_b200_ctx {
   int dev = 0;
   std::string err;
   cudaStream_t st = nullptr;
-  cublasHandle_t blas = nullptr;
-  cusolverDnHandle_t sol = nullptr;
   int64_t launch_base = 0;
   bool have_ir = false, have_k = false, have_thc = false, w_valid = false, w_in_R = false;
   bool g_resident = false;
@@ -618,7 +600,7 @@ void dyson_g_device(Ctx* c, const double2* Sig) {
   tau_to_w_ff(c, Sig, c->Sw.p, ncol);
   cq::build_dyson_matrix(c->Sov.p, c->H0.p, c->F.p, c->Sw.p, c->Xw.p, c->dwnf.p, c->beta, c->mu,
                          nw, nk, nb, c->st);
-  cq::invert_batched(c->Xw.p, nb, nw * nk, c->ginfo.p, c->blas, c->st);
+  cq::invert_batched(c->Xw.p, nb, nw * nk, c->ginfo.p, c->st);
   w_to_tau_ff(c, c->Xw.p, c->G.p, ncol);
   dm_from_g(c);
   cq::hermitize_c128(c->G.p, nb, c->nt * nk, c->st);
@@ -859,11 +841,6 @@ int coqui_b200_create(coqui_b200_ctx** out, const coqui_b200_dims* dims) {
     CQ_CHECK_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     CQ_CHECK_CUDA(cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking));
     CQ_CHECK_CUDA(cudaEventCreateWithFlags(&c->ev_st, cudaEventDisableTiming));
-    CQ_CHECK_BLAS(cublasCreate(&c->blas));
-    CQ_CHECK_BLAS(cublasSetStream(c->blas, c->st));
-    CQ_CHECK_BLAS(cublasSetMathMode(c->blas, CUBLAS_DEFAULT_MATH));
-    CQ_CHECK_SOLVER(cusolverDnCreate(&c->sol));
-    CQ_CHECK_SOLVER(cusolverDnSetStream(c->sol, c->st));
     c->prof.st = c->st;
     cq::upload_twiddles();
     c->launch_base = cq::launches_total();
@@ -901,8 +878,6 @@ void coqui_b200_destroy(coqui_b200_ctx* c) {
   c->LHc.release();
   c->Xtc.release();
   for (auto& m : c->marks) cudaEventDestroy(m.second);
-  if (c->sol) cusolverDnDestroy(c->sol);
-  if (c->blas) cublasDestroy(c->blas);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -1060,7 +1035,7 @@ int coqui_b200_set_thc(coqui_b200_ctx* c, const double* X_skPa, const double* V_
     c->LH.ensure((size_t)nk * Np * Np);
     CQ_CHECK_CUDA(cudaMemcpyAsync(c->L.p, c->V.p, (size_t)nk * Np * Np * sizeof(double2),
                                   cudaMemcpyDeviceToDevice, c->st));
-    int info = cq::cholesky_lower_batched(c->sol, c->L.p, Np, nk, c->st);
+    int info = cq::cholesky_lower_batched(c->L.p, Np, nk, c->st);
     CQ_REQUIRE(info == 0, COQUI_B200_ENOTHPD, "Coulomb matrix V^q is not positive definite");
     cq::launch_zero_upper_and_adjoint(c->L.p, c->LH.p, Np, nk, c->st);
     if (c->mode == COQUI_B200_MIXED) {
@@ -1193,7 +1168,7 @@ void dyson_all(Ctx* c, bool want_w, bool want_e, std::vector<double>* logdet,
   a.keep_scratch = c->capturing;
   std::vector<double> ld;
   std::vector<double2> t;
-  cq::dyson_run(a, c->blas, c->sol, c->dyn, c->st, want_e ? &ld : nullptr, want_e ? &t : nullptr);
+  cq::dyson_run(a, c->dyn, c->st, want_e ? &ld : nullptr, want_e ? &t : nullptr);
   if (logdet) *logdet = std::move(ld);
   if (tr) *tr = std::move(t);
 }

@@ -148,7 +148,7 @@ void sym_dyson(Ctx* c, bool want_w, bool want_e, std::vector<double>* ld,
   a.info = c->dinfo.p;
   a.logdet = c->dlogdet.p;
   a.trace = c->dtrace.p;
-  cq::dyson_run(a, c->blas, c->sol, c->dyn, c->st, ld, tr);
+  cq::dyson_run(a, c->dyn, c->st, ld, tr);
 }
 
 void sym_update_w(Ctx* c) {

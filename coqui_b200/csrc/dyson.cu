@@ -10,19 +10,6 @@
 
 namespace cq {
 
-#define CQ_BLAS(expr)                                                                     \
-  do {                                                                                    \
-    cublasStatus_t _s = (expr);                                                           \
-    if (_s != CUBLAS_STATUS_SUCCESS)                                                      \
-      throw Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
-  } while (0)
-#define CQ_SOLVER(expr)                                                                   \
-  do {                                                                                    \
-    cusolverStatus_t _s = (expr);                                                         \
-    if (_s != CUSOLVER_STATUS_SUCCESS)                                                    \
-      throw Error(COQUI_B200_ECUDA, std::string(#expr) + " failed: " + std::to_string(_s)); \
-  } while (0)
-
 __global__ void k_zero_upper_adjoint(double2* __restrict__ L, double2* __restrict__ LH, int64_t Np,
                                      int64_t total) {
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
@@ -110,39 +97,29 @@ void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t 
   CQ_CHECK_CUDA(cudaGetLastError());
 }
 
-// cuSOLVER is column-major: the row-major buffer of a Hermitian A reads as conj(A); its
-// upper factor U (conj(A) = U^H U) reads back row-major as the lower C with A = C C^H.
-static void potrf_ptrs(cusolverDnHandle_t sol, double2** dptrs, int64_t Np, int* dinfo,
-                       int64_t nb) {
-  CQ_SOLVER(cusolverDnZpotrfBatched(sol, CUBLAS_FILL_MODE_UPPER, (int)Np,
-                                    reinterpret_cast<cuDoubleComplex**>(dptrs), (int)Np, dinfo,
-                                    (int)nb));
-}
-
-int cholesky_lower_batched(cusolverDnHandle_t sol, double2* A, int64_t Np, int64_t nbatch,
-                           cudaStream_t s) {
-  std::vector<double2*> h(nbatch);
-  for (int64_t b = 0; b < nbatch; ++b) h[b] = A + b * Np * Np;
-  DevBuf<unsigned char> buf;
-  buf.ensure(nbatch * (sizeof(double2*) + sizeof(int)));
-  double2** dp = (double2**)buf.p;
-  int* dinfo = (int*)(buf.p + nbatch * sizeof(double2*));
-  CQ_CHECK_CUDA(cudaMemcpyAsync(dp, h.data(), nbatch * sizeof(double2*), cudaMemcpyHostToDevice, s));
-  potrf_ptrs(sol, dp, Np, dinfo, nbatch);
+// A = L L^H for nbatch Hermitian matrices on the library's FP64 factorisation: it factors
+// I - M, so M = I - A goes in; L lands in A's lower triangle (its upper triangle then holds
+// L^{-H}).  The first nonzero per-problem status (a pivot that was not positive) is returned.
+int cholesky_lower_batched(double2* A, int64_t Np, int64_t nbatch, cudaStream_t s) {
+  DevBuf<double2> M, tr;
+  DevBuf<double> ld;
+  DevBuf<int> dinfo;
+  M.ensure((size_t)nbatch * Np * Np);
+  tr.ensure(nbatch);
+  ld.ensure(nbatch);
+  dinfo.ensure(nbatch);
+  launch_eye_minus<double>(A, M.p, Np, nbatch, s);
+  launch_chol_inv_c128(M.p, A, ld.p, tr.p, dinfo.p, Np, nbatch, s);
   std::vector<int> info(nbatch);
-  CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), dinfo, nbatch * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), dinfo.p, nbatch * sizeof(int), cudaMemcpyDeviceToHost, s));
   CQ_CHECK_CUDA(cudaStreamSynchronize(s));
-  buf.release();
   for (int v : info)
     if (v != 0) return v;
   return 0;
 }
 
-void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
-               DevBuf<unsigned char>& scratch, cudaStream_t s, std::vector<double>* logdet,
-               std::vector<double2>* trace) {
-  (void)blas;
-  (void)sol;
+void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t s,
+               std::vector<double>* logdet, std::vector<double2>* trace) {
   const int64_t Np = a.Np, NN = Np * Np, nq = a.nq, nw = a.nw;
   const size_t es = a.mixed ? sizeof(float2) : sizeof(double2);
   // per problem: T1 (es), M (es), A (c128), Y (c128; the mixed form's W operands)

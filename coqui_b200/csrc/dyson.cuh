@@ -9,20 +9,16 @@
 //   W = Y^H Y - V,  Y = C^{-1} L^H  (FP64 form).
 #pragma once
 
-#include <cublas_v2.h>
-#include <cusolverDn.h>
-
 #include <vector>
 
 #include "common.cuh"
 
 namespace cq {
 
-// In-place lower Cholesky factor (row-major, A = L L^H) of nbatch Np x Np matrices.
-// Returns the first nonzero LAPACK info (0 = success).  The strict upper triangle is left
-// undefined.
-int cholesky_lower_batched(cusolverDnHandle_t sol, double2* A, int64_t Np, int64_t nbatch,
-                           cudaStream_t s);
+// In-place lower Cholesky factor (row-major, A = L L^H) of nbatch Np x Np matrices on the
+// library's FP64 factorisation.  Returns the first nonzero per-problem status (0 = success).
+// The strict upper triangle is left as workspace.
+int cholesky_lower_batched(double2* A, int64_t Np, int64_t nbatch, cudaStream_t s);
 
 // Lower tile pair (I, J), I >= J, of the 32 x 32 tiling: pair = I (I + 1) / 2 + J.
 __device__ __forceinline__ void tile_pair(int pair, int& I, int& J) {
@@ -100,8 +96,7 @@ struct DysonArgs {
 };
 
 // Runs every (iW, q) problem; fills logdet / trace (indexed n * nq + q) if want_e.
-void dyson_run(const DysonArgs& a, cublasHandle_t blas, cusolverDnHandle_t sol,
-               DevBuf<unsigned char>& scratch, cudaStream_t s, std::vector<double>* logdet,
-               std::vector<double2>* trace);
+void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t s,
+               std::vector<double>* logdet, std::vector<double2>* trace);
 
 }  // namespace cq

@@ -784,26 +784,26 @@ __global__ void __launch_bounds__(256) k_ir_transform_f32(float2* __restrict__ b
     for (int t = 0; t < MAXT; ++t)
       x[t] = (t < n_in) ? buf[(int64_t)t * ncol + e] : make_float2(0.f, 0.f);
     for (int o4 = 0; o4 < n_out4; ++o4) {
-      float ar[4] = {0.f, 0.f, 0.f, 0.f}, ai[4] = {0.f, 0.f, 0.f, 0.f};
+      // (re, im) accumulated together by the packed FP32 FMA of sm_100 (one instruction per
+      // complex multiply-add by a real coefficient; each half rounds as fmaf does)
+      float2 acc[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = make_float2(0.f, 0.f);
       const float4* rows = sM4 + (size_t)o4 * 4 * (MAXT / 4);
 #pragma unroll
       for (int t4 = 0; t4 < MAXT / 4; ++t4) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const float4 m = rows[q * (MAXT / 4) + t4];
-          ar[q] = fmaf(m.x, x[4 * t4 + 0].x, ar[q]);
-          ai[q] = fmaf(m.x, x[4 * t4 + 0].y, ai[q]);
-          ar[q] = fmaf(m.y, x[4 * t4 + 1].x, ar[q]);
-          ai[q] = fmaf(m.y, x[4 * t4 + 1].y, ai[q]);
-          ar[q] = fmaf(m.z, x[4 * t4 + 2].x, ar[q]);
-          ai[q] = fmaf(m.z, x[4 * t4 + 2].y, ai[q]);
-          ar[q] = fmaf(m.w, x[4 * t4 + 3].x, ar[q]);
-          ai[q] = fmaf(m.w, x[4 * t4 + 3].y, ai[q]);
+          acc[q] = __ffma2_rn(make_float2(m.x, m.x), x[4 * t4 + 0], acc[q]);
+          acc[q] = __ffma2_rn(make_float2(m.y, m.y), x[4 * t4 + 1], acc[q]);
+          acc[q] = __ffma2_rn(make_float2(m.z, m.z), x[4 * t4 + 2], acc[q]);
+          acc[q] = __ffma2_rn(make_float2(m.w, m.w), x[4 * t4 + 3], acc[q]);
         }
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        if (o4 * 4 + q < n_out) __stcs(buf + (int64_t)(o4 * 4 + q) * ncol + e, make_float2(ar[q], ai[q]));
+        if (o4 * 4 + q < n_out) __stcs(buf + (int64_t)(o4 * 4 + q) * ncol + e, acc[q]);
     }
   }
 }

@@ -342,9 +342,7 @@ void build_dyson_matrix(const double2* S, const double2* H0, const double2* F,
   CQ_CHECK_CUDA(cudaGetLastError());
 }
 
-void invert_batched(double2* A, int64_t nb, int64_t nmat, int* info, cublasHandle_t blas,
-                    cudaStream_t s) {
-  (void)blas;
+void invert_batched(double2* A, int64_t nb, int64_t nmat, int* info, cudaStream_t s) {
   CQ_REQUIRE(nb >= 1 && nb <= kGjMaxN, COQUI_B200_EUNSUPPORTED,
              "Dyson equation for G supports at most 96 orbitals");
   CQ_REQUIRE(nmat <= 2147483647, COQUI_B200_EINVAL, "invert_batched: too many matrices");

@@ -6,8 +6,6 @@
 #include <complex>
 #include <vector>
 
-#include <cublas_v2.h>
-
 #include "common.cuh"
 
 namespace cq {
@@ -25,10 +23,9 @@ void build_dyson_matrix(const double2* S, const double2* H0, const double2* F,
                         double mu, int64_t nw, int64_t nk, int64_t nb, cudaStream_t s);
 
 // In-place FP64 inverse of nmat nb x nb complex matrices (Gauss-Jordan with partial pivoting,
-// one CTA per matrix, the matrix in shared memory; cuBLAS batched LU above 96).  info[m] = 1
-// marks a singular matrix.
-void invert_batched(double2* A, int64_t nb, int64_t nmat, int* info, cublasHandle_t blas,
-                    cudaStream_t s);
+// one CTA per matrix, the matrix in shared memory; nb <= 96).  info[m] = 1 marks a singular
+// matrix.
+void invert_batched(double2* A, int64_t nb, int64_t nmat, int* info, cudaStream_t s);
 
 // y = a x + b y (real a, b), n complex values
 void axpby_c128(const double2* x, double2* y, double a, double b, int64_t n, cudaStream_t s);

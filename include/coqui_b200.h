@@ -63,7 +63,7 @@ extern "C" {
 #define COQUI_B200_ETIMEDOUT -7    /* a bounded device-side wait gave up */
 
 /* precision_mode */
-#define COQUI_B200_FP64 0  /* complex128 everywhere: cuBLAS ZGEMM + FP64 factorizations */
+#define COQUI_B200_FP64 0  /* complex128 everywhere: FP64 tensor-core GEMMs + factorizations */
 #define COQUI_B200_MIXED 1 /* split-TF32 tensor-core products, complex64 intermediates,
                               FP64 Cholesky / log-det */
 
