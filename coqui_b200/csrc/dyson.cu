@@ -97,9 +97,20 @@ void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t 
   CQ_CHECK_CUDA(cudaGetLastError());
 }
 
+// The factorisation leaves the diagonal of its inverse U = L^{-H}, 1 / L_ii, on A's diagonal:
+// put L_ii = 1 / U_ii back (real, positive).
+__global__ void k_restore_diag(double2* __restrict__ A, int64_t Np, int64_t total) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double2* d = A + (i / Np) * Np * Np + (i % Np) * (Np + 1);
+    *d = make_double2(1.0 / d->x, 0.0);
+  }
+}
+
 // A = L L^H for nbatch Hermitian matrices on the library's FP64 factorisation: it factors
-// I - M, so M = I - A goes in; L lands in A's lower triangle (its upper triangle then holds
-// L^{-H}).  The first nonzero per-problem status (a pivot that was not positive) is returned.
+// I - M, so M = I - A goes in; L lands in A's lower triangle (its strict upper triangle then
+// holds part of L^{-H}).  The first nonzero per-problem status (a pivot that was not
+// positive) is returned.
 int cholesky_lower_batched(double2* A, int64_t Np, int64_t nbatch, cudaStream_t s) {
   DevBuf<double2> M, tr;
   DevBuf<double> ld;
@@ -110,6 +121,9 @@ int cholesky_lower_batched(double2* A, int64_t Np, int64_t nbatch, cudaStream_t 
   dinfo.ensure(nbatch);
   launch_eye_minus<double>(A, M.p, Np, nbatch, s);
   launch_chol_inv_c128(M.p, A, ld.p, tr.p, dinfo.p, Np, nbatch, s);
+  k_restore_diag<<<grid_for(nbatch * Np, 256), 256, 0, s>>>(A, Np, nbatch * Np);
+  count_launch();
+  CQ_CHECK_CUDA(cudaGetLastError());
   std::vector<int> info(nbatch);
   CQ_CHECK_CUDA(cudaMemcpyAsync(info.data(), dinfo.p, nbatch * sizeof(int), cudaMemcpyDeviceToHost, s));
   CQ_CHECK_CUDA(cudaStreamSynchronize(s));

@@ -38,6 +38,13 @@ class THCData:
     chi_bar: Optional[np.ndarray] = None  # (nq, Np) basis_bar_head
     madelung: float = 0.0  # MF::madelung(), used by the gygi corrections
     chi_head: Optional[np.ndarray] = None  # (Np) basis_head at q = 0 (gygi Sigma correction)
+    # MF::bz() maps of a symmetric mean field (keys as coqui_b200.symmetry.bz_symmetry, with
+    # "lex" the lexicographic position of each of the mean field's k-points) and the rotations
+    # symmetry_rotation(isym, k) as (nsym, nk_ibz, nb, nb); with them update_w / evaluate /
+    # rpa_energy take the reference's k-space routes (G, Sigma on the IBZ k-points, W on the
+    # IBZ q-points).  X, V, kpts and chi_bar stay on the whole lexicographic grid.
+    bz: Optional[dict] = None
+    bz_rotations: Optional[np.ndarray] = None
 
     @property
     def Np(self):
@@ -79,6 +86,8 @@ def context_for(thc: THCData, ft: IAFT, mode: int = capi.MIXED, device: int = 0)
         ctx.set_ir(ft)
         ctx.set_kmesh(thc.kpts, thc.lattv, thc.chi_bar)
         ctx.set_thc(thc.X, thc.V)
+        if thc.bz is not None:  # nqpts_ibz < nqpts: the k-space routes (thc_gw.icc:31-32)
+            ctx.set_symmetry(thc.bz, thc.bz_rotations)
         _ctx_cache[key] = ctx
     return ctx
 
@@ -86,6 +95,9 @@ def context_for(thc: THCData, ft: IAFT, mode: int = capi.MIXED, device: int = 0)
 def hf_context_for(thc: THCData, mode: int = capi.MIXED, device: int = 0) -> capi.Context:
     """A context holding thc: any context of the same (thc, mode, device), else one without
     imaginary-time grids (Hartree-Fock needs none)."""
+    if thc.bz is not None:
+        raise capi.CoquiB200Error(-2, "THC Hartree-Fock takes the whole k-mesh; the "
+                                      "symmetry-reduced form is not on this path")
     for (t, _, m, d), ctx in _ctx_cache.items():
         if t == id(thc) and m == mode and d == device:
             return ctx

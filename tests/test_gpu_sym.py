@@ -153,3 +153,25 @@ def test_ibz_long_wavelength_treatments(kind, grid, mode, tol, div):
     S, h2 = c.gw_iteration(d["G_ibz"], want_head=True)
     assert maxabs(S, Sigma) < tol and maxabs(h2, head) < tol
     assert maxabs(Sigma, b.Sigma) > 1e-4  # the correction is not negligible
+
+
+def test_solver_mirror_takes_the_kspace_route():
+    # THCData carrying the mean field's bz maps: update_w / evaluate / rpa_energy of the
+    # reference-shaped interface run the IBZ route, as the reference does when
+    # nqpts_ibz < nqpts (thc_gw.icc:31-32)
+    from coqui_b200 import solvers
+    b = case("swap", (4, 4, 1))
+    d = b.d
+    thc = solvers.THCData(X=d["X_lex"], V=d["V_lex"], kpts=d["kpts_lex"], lattv=d["lattv"],
+                          kp_grid=d["grid"], chi_bar=d["chi_lex"], bz=b.sym,
+                          bz_rotations=d["D"])
+    mb = solvers.MBState(sG_tskij=d["G_ibz"])
+    try:
+        solvers.scr_coulomb_t(b.pft, mode=capi.FP64).update_w(mb, thc)
+        assert maxabs(mb.dW_qtPQ, b.dW) < 1e-10
+        gw = solvers.gw_t(b.pft, mode=capi.FP64)
+        gw.evaluate(mb, thc)
+        assert maxabs(mb.sSigma_tskij, b.Sigma) < 1e-10
+        assert abs(gw.rpa_energy(d["G_ibz"], thc) - b.e_rpa) < 1e-10
+    finally:
+        solvers.clear_contexts()
