@@ -15,9 +15,16 @@ trailing (re, im) dimension).  Datasets of the root group:
   nkpts before it was written), which is V here.
 
 The lattice vectors and the k-grid come from the mean field, as in the reference.  Checks and
-their messages follow ``thc_reader_t::read``; this library's path takes the whole k-mesh
-without symmetry (nkpts_ibz = nqpts_ibz = nkpts) and X and Y over the same band range, and
-refuses other files with a ValueError.
+their messages follow ``thc_reader_t::read``; X and Y must cover the same band range.
+
+A file of a symmetric mean field (nkpts_ibz or nqpts_ibz below nkpts) stores X on every
+k-point in the mean field's order (IBZ first) and V only on the IBZ q-points.  It is read with
+the mean field's bz maps (``bz``, as :func:`coqui_b200.symmetry.bz_symmetry` lays them out,
+and the rotations ``bz_rotations``): X, kpts and the heads are put in lexicographic grid
+order, and every 1st-BZ q-point's V slot holds the matrix of its IBZ point (the k-space routes
+read only the IBZ slots; the full-BZ routes must not be used on such data, and the solver
+mirror's Hartree-Fock refuses it).  The returned THCData carries the maps, so the solver
+mirror takes the reference's k-space routes.
 """
 from __future__ import annotations
 
@@ -31,8 +38,10 @@ def _scalar(a):
     return int(np.asarray(a).reshape(-1)[0])
 
 
-def read_thc_file(path: str, lattv, kp_grid, madelung: float = 0.0) -> THCData:
-    """THCData from a THC ERI file; lattv (3, 3) and kp_grid (3,) are the mean field's."""
+def read_thc_file(path: str, lattv, kp_grid, madelung: float = 0.0, bz=None,
+                  bz_rotations=None) -> THCData:
+    """THCData from a THC ERI file; lattv (3, 3) and kp_grid (3,) are the mean field's, and bz
+    / bz_rotations its symmetry maps (needed for a symmetry-reduced file)."""
     d = h5lite.read_h5(path)
     need = ("Np", "X_orbital_range", "Y_orbital_range", "interpolating_points",
             "collocation_matrix", "coulomb_matrix")
@@ -64,9 +73,10 @@ def read_thc_file(path: str, lattv, kp_grid, madelung: float = 0.0) -> THCData:
         raise ValueError("thc_reader_t::read(): coulomb_matrix is not (nqpts_ibz, Np, Np)")
     nk_ibz = _scalar(d["nkpts_ibz"]) if "nkpts_ibz" in d else nk
     nq_ibz = _scalar(d["nqpts_ibz"]) if "nqpts_ibz" in d else V.shape[0]
-    if nk_ibz != nk or nq_ibz != nk or V.shape[0] != nk:
-        raise ValueError("symmetry-reduced files (nkpts_ibz or nqpts_ibz below nkpts) are not "
-                         "supported: the path runs on the whole k-mesh")
+    reduced = nk_ibz != nk or nq_ibz != nk or V.shape[0] != nk
+    if reduced and bz is None:
+        raise ValueError("symmetry-reduced file (nkpts_ibz or nqpts_ibz below nkpts): pass the "
+                         "mean field's bz maps")
     grid = tuple(int(v) for v in np.asarray(kp_grid).reshape(-1))
     if int(np.prod(grid)) != nk:
         raise ValueError("kp_grid does not match the number of k-points of the file")
@@ -77,6 +87,23 @@ def read_thc_file(path: str, lattv, kp_grid, madelung: float = 0.0) -> THCData:
                if "dual_interpolating_vectors_G0" in d else None)
     chi_head = (h5lite.as_complex(d["interpolating_vectors_G0"]).reshape(-1, Np)[0]
                 if "interpolating_vectors_G0" in d else None)
+    if bz is not None:
+        if int(bz["nk_ibz"]) != nk_ibz or int(bz["nq_ibz"]) != nq_ibz or \
+                V.shape[0] != nq_ibz or len(bz["lex"]) != nk:
+            raise ValueError("the bz maps do not match the file's nkpts, nkpts_ibz, nqpts_ibz")
+        lex = np.asarray(bz["lex"], np.int64)
+        rep = np.asarray(bz["qp_to_ibz"], np.int64)  # 1st-BZ q -> its IBZ point
+
+        def to_lex(a):  # leading axis in the mean field's order -> lexicographic order
+            out = np.empty_like(a)
+            out[lex] = a
+            return out
+        X = np.ascontiguousarray(np.swapaxes(to_lex(np.swapaxes(X, 0, 1)), 0, 1))
+        V = to_lex(V[rep])
+        kpts = to_lex(kpts)
+        if chi_bar is not None:
+            chi_bar = to_lex(chi_bar[rep] if chi_bar.shape[0] == nq_ibz else chi_bar)
     return THCData(X=np.ascontiguousarray(X), V=np.ascontiguousarray(V), kpts=kpts,
                    lattv=np.asarray(lattv, np.float64), kp_grid=grid, chi_bar=chi_bar,
-                   madelung=float(madelung), chi_head=chi_head)
+                   madelung=float(madelung), chi_head=chi_head, bz=bz,
+                   bz_rotations=bz_rotations)

@@ -49,7 +49,7 @@ def test_round_trip(tmp_path, system):
 @pytest.mark.parametrize("bad,msg", [
     (dict(interpolating_points=np.arange(5)), "rp.shape"),
     (dict(X_orbital_range=np.array([0, 99], np.int32)), "X_orbital_range"),
-    (dict(nqpts_ibz=np.int32(3)), "symmetry-reduced"),
+    (dict(nqpts_ibz=np.int32(3)), "bz maps"),
     (dict(Y_orbital_range=np.array([0, 4], np.int32)), "Y collocation"),
 ])
 def test_inconsistent_files_are_refused(tmp_path, system, bad, msg):
@@ -88,3 +88,64 @@ def test_solvers_from_a_thc_file_match_the_oracle(tmp_path):
     dW, _, _ = O.update_w(G, s.X, s.V, oft, s.kpts, s.lattv, s.kp_grid, s.chi_bar)
     S_ref = O.eval_Sigma_all_Rspace(G, dW, s.X, s.kpts, s.lattv, s.kp_grid)
     assert np.abs(mb.sSigma_tskij - S_ref).max() < 1e-6
+
+
+def sym_datasets(d):
+    """A symmetric mean field's file: X on every k-point and kpts in the mean field's order
+    (IBZ first), V and the dual heads on the IBZ q-points only."""
+    sym = d["sym"]
+    nk, nqi = sym["nk"], sym["nq_ibz"]
+    X = d["X"]
+    Np, nb = X.shape[2], X.shape[3]
+    return {
+        "Np": np.int32(Np), "number_of_bands": np.int32(nb),
+        "X_orbital_range": np.array([0, nb], np.int32), "Y_orbital_range": np.array([0, nb], np.int32),
+        "kpts": d["kpts"], "qpts": d["kpts"], "nkpts_ibz": np.int32(sym["nk_ibz"]),
+        "nqpts_ibz": np.int32(nqi), "collocation_matrix": X,
+        "interpolating_points": np.arange(Np, dtype=np.int64),
+        "interpolating_vectors_G0": d["chi_bar"][:1] * 2.0,
+        "dual_interpolating_vectors_G0": d["chi_bar"][:nqi], "coulomb_matrix": d["V"][:nqi],
+    }
+
+
+def test_symmetry_reduced_file_with_the_bz_maps(tmp_path):
+    from coqui_b200.iaft import IAFT
+    from coqui_b200.symmetry import symmetric_system
+    d = symmetric_system("swap", (4, 4, 1), 6, 12, IAFT(1000.0, 10.0, "low"))
+    sym = d["sym"]
+    p = str(tmp_path / "thc_sym.h5")
+    write_h5(p, sym_datasets(d))
+    with pytest.raises(ValueError, match="bz maps"):
+        read_thc_file(p, d["lattv"], d["grid"])
+    t = read_thc_file(p, d["lattv"], d["grid"], bz=sym, bz_rotations=d["D"])
+    assert np.array_equal(t.X, d["X_lex"]) and np.allclose(t.kpts, d["kpts_lex"])
+    ql = d["lex"][:sym["nq_ibz"]]
+    assert np.array_equal(t.V[ql], d["V"][:sym["nq_ibz"]])
+    assert np.array_equal(t.chi_bar[ql], d["chi_bar"][:sym["nq_ibz"]])
+    assert t.bz is sym and t.bz_rotations is d["D"]
+
+
+@pytest.mark.gpu
+def test_solvers_from_a_symmetry_reduced_file_match_the_kspace_oracle(tmp_path):
+    """A symmetric mean field's file read with its bz maps runs the k-space routes."""
+    from coqui_b200 import capi, solvers
+    from coqui_b200.iaft import IAFT
+    from coqui_b200.symmetry import symmetric_system
+    from oracle import sym_oracle as SO
+    from oracle import thc_oracle as O
+    ft, oft = IAFT(1000.0, 10.0, "low"), O.IAFT(1000.0, 10.0, "low")
+    d = symmetric_system("swap", (4, 4, 1), 8, 24, oft)
+    sym = d["sym"]
+    p = str(tmp_path / "thc_sym.h5")
+    write_h5(p, sym_datasets(d))
+    thc = read_thc_file(p, d["lattv"], d["grid"], bz=sym, bz_rotations=d["D"])
+    mb = solvers.MBState(sG_tskij=d["G_ibz"])
+    try:
+        solvers.scr_coulomb_t(ft, mode=capi.FP64).update_w(mb, thc)
+        solvers.gw_t(ft, mode=capi.FP64).evaluate(mb, thc)
+    finally:
+        solvers.clear_contexts()
+    dW = SO.update_w_kspace(d["G_ibz"], d["X"], d["V"], oft, sym)
+    S_ref = SO.eval_Sigma_all_kspace(d["G_ibz"], dW, d["X"], sym, d["D"])
+    assert np.abs(mb.dW_qtPQ - dW).max() < 1e-10
+    assert np.abs(mb.sSigma_tskij - S_ref).max() < 1e-10
