@@ -97,20 +97,83 @@ void launch_zero_upper_and_adjoint(double2* L, double2* LH, int64_t Np, int64_t 
   CQ_CHECK_CUDA(cudaGetLastError());
 }
 
-// The factorisation leaves the diagonal of its inverse U = L^{-H}, 1 / L_ii, on A's diagonal:
-// put L_ii = 1 / U_ii back (real, positive).
-__global__ void k_restore_diag(double2* __restrict__ A, int64_t Np, int64_t total) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double2* d = A + (i / Np) * Np * Np + (i % Np) * (Np + 1);
-    *d = make_double2(1.0 / d->x, 0.0);
+// The factorisation keeps each 32 x 32 diagonal block of its factor in shared memory only
+// (global memory gets the panel blocks below it and, in the upper triangle, the block's
+// inverse adjoint).  This kernel forms the diagonal blocks again the way the factorisation
+// does: C_jj = chol(A_jj - sum_{kb < j} L_j,kb L_j,kb^H) from I - M = A and the stored panel
+// blocks, and writes them into A's lower triangle.  One CTA per (block j, problem).
+constexpr int kDiagB = 32;
+__global__ void __launch_bounds__(256) k_chol_diag_blocks(const double2* __restrict__ Mall,
+                                                          double2* __restrict__ Aall, int64_t n,
+                                                          int* __restrict__ info) {
+  __shared__ double2 S[kDiagB][kDiagB + 1];
+  __shared__ double2 T[kDiagB][kDiagB + 1];
+  const int64_t p = blockIdx.y, j0 = (int64_t)blockIdx.x * kDiagB;
+  const int jb = (int)((n - j0) < kDiagB ? (n - j0) : kDiagB);
+  const double2* M = Mall + p * n * n;
+  double2* A = Aall + p * n * n;
+  for (int i = threadIdx.x; i < kDiagB * kDiagB; i += blockDim.x) {
+    const int r = i / kDiagB, c = i % kDiagB;
+    double2 v = make_double2(0.0, 0.0);
+    if (r < jb && c <= r) {
+      const double2 m = M[(j0 + r) * n + j0 + c];
+      v = make_double2((r == c ? 1.0 : 0.0) - m.x, -m.y);
+    }
+    S[r][c] = v;
+  }
+  for (int64_t k0 = 0; k0 < j0; k0 += kDiagB) {  // panel blocks to the left are whole blocks
+    __syncthreads();
+    for (int i = threadIdx.x; i < kDiagB * kDiagB; i += blockDim.x) {
+      const int r = i / kDiagB, c = i % kDiagB;
+      T[r][c] = r < jb ? A[(j0 + r) * n + k0 + c] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kDiagB * kDiagB; i += blockDim.x) {
+      const int r = i / kDiagB, c = i % kDiagB;
+      if (r >= jb || c > r) continue;
+      double sr = 0.0, si = 0.0;
+      for (int k = 0; k < kDiagB; ++k) {  // T[r][k] conj(T[c][k])
+        const double2 a = T[r][k], b = T[c][k];
+        sr += a.x * b.x + a.y * b.y;
+        si += a.y * b.x - a.x * b.y;
+      }
+      S[r][c].x -= sr;
+      S[r][c].y -= si;
+    }
+  }
+  for (int q = 0; q < jb; ++q) {  // right-looking factorisation of the 32 x 32 block
+    __syncthreads();
+    const double d2 = S[q][q].x;
+    const double d = d2 > 0.0 ? sqrt(d2) : 0.0;
+    if (!(d2 > 0.0) && threadIdx.x == 0) info[p] = 1;
+    const double inv = d > 0.0 ? 1.0 / d : 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) S[q][q] = make_double2(d, 0.0);
+    for (int r = q + 1 + threadIdx.x; r < jb; r += blockDim.x) {
+      S[r][q].x *= inv;
+      S[r][q].y *= inv;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kDiagB * kDiagB; i += blockDim.x) {
+      const int r = i / kDiagB, c = i % kDiagB;
+      if (r >= jb || c <= q || c > r) continue;
+      const double2 a = S[r][q], b = S[c][q];  // S[r][c] -= a conj(b)
+      S[r][c].x -= a.x * b.x + a.y * b.y;
+      S[r][c].y -= a.y * b.x - a.x * b.y;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kDiagB * kDiagB; i += blockDim.x) {
+    const int r = i / kDiagB, c = i % kDiagB;
+    if (r < jb && c <= r) A[(j0 + r) * n + j0 + c] = S[r][c];
   }
 }
 
 // A = L L^H for nbatch Hermitian matrices on the library's FP64 factorisation: it factors
-// I - M, so M = I - A goes in; L lands in A's lower triangle (its strict upper triangle then
-// holds part of L^{-H}).  The first nonzero per-problem status (a pivot that was not
-// positive) is returned.
+// I - M, so M = I - A goes in; the panel blocks of L land in A's lower triangle, the diagonal
+// blocks are formed again from them (k_chol_diag_blocks), and the strict upper triangle is
+// left as workspace.  The first nonzero per-problem status (a pivot that was not positive) is
+// returned.
 int cholesky_lower_batched(double2* A, int64_t Np, int64_t nbatch, cudaStream_t s) {
   DevBuf<double2> M, tr;
   DevBuf<double> ld;
@@ -121,7 +184,10 @@ int cholesky_lower_batched(double2* A, int64_t Np, int64_t nbatch, cudaStream_t 
   dinfo.ensure(nbatch);
   launch_eye_minus<double>(A, M.p, Np, nbatch, s);
   launch_chol_inv_c128(M.p, A, ld.p, tr.p, dinfo.p, Np, nbatch, s);
-  k_restore_diag<<<grid_for(nbatch * Np, 256), 256, 0, s>>>(A, Np, nbatch * Np);
+  const int64_t nblk = (Np + kDiagB - 1) / kDiagB;
+  CQ_REQUIRE(nblk <= 65535 && nbatch <= 65535, COQUI_B200_EUNSUPPORTED,
+             "Cholesky of V: too many blocks or matrices");
+  k_chol_diag_blocks<<<dim3((unsigned)nblk, (unsigned)nbatch), 256, 0, s>>>(M.p, A, Np, dinfo.p);
   count_launch();
   CQ_CHECK_CUDA(cudaGetLastError());
   std::vector<int> info(nbatch);
