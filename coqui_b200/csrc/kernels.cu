@@ -313,6 +313,39 @@ __device__ __forceinline__ void load_dft_inner(C* A, const C* __restrict__ src, 
   }
 }
 
+// load_dft_inner for two tiles at once (A from srcA, B from srcB, or A alone when srcB is
+// null): each thread issues the loads of both lines before either DFT, so twice as many
+// loads are in flight while the tiles cross HBM.  Same arithmetic as two load_dft_inner calls.
+template <typename C, int TILE, int N>
+__device__ __forceinline__ void load_dft_inner2(C* A, const C* __restrict__ srcA, C* B,
+                                                const C* __restrict__ srcB, int nk,
+                                                int64_t ncol, int64_t col0, int sign) {
+  const int lines = nk / N;
+  for (int i = threadIdx.x; i < lines * TILE; i += blockDim.x) {
+    const int c = i % TILE, line = i / TILE;
+    const int64_t col = col0 + c;
+    C x[N], y[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      x[m].x = 0;
+      x[m].y = 0;
+      y[m] = x[m];
+      if (col < ncol) {
+        x[m] = srcA[(int64_t)(line * N + m) * ncol + col];
+        if (srcB) y[m] = srcB[(int64_t)(line * N + m) * ncol + col];
+      }
+    }
+    dft_line<C, N>(x, sign);
+#pragma unroll
+    for (int m = 0; m < N; ++m) A[(line * N + m) * TILE + c] = x[m];
+    if (srcB) {
+      dft_line<C, N>(y, sign);
+#pragma unroll
+      for (int m = 0; m < N; ++m) B[(line * N + m) * TILE + c] = y[m];
+    }
+  }
+}
+
 // Shared tile -> DFT along the innermost dimension in registers -> global rows: the last DFT
 // pass and the store in one sweep.
 template <typename C, int TILE, int N>
@@ -333,15 +366,17 @@ __device__ __forceinline__ void dft_inner_store(const C* A, C* dst, int nk, int6
   }
 }
 
-// The outermost dimension (length N, stride `stride` = n1 n2): forward DFT of the A (and B)
-// lines, op(a, b, k_inner, c) on them in registers, inverse DFT of A (and, if inv_b, B), back to
-// shared memory: the last forward pass, the pointwise product and the first inverse pass in
-// one sweep.
-template <typename C, int TILE, int N, typename Op>
-__device__ __forceinline__ void outer_pointwise(C* A, C* B, bool inv_b, int stride, Op&& op) {
+// The outermost dimension (length N, stride `stride` = n1 n2): pre(w, k_inner, c) issues the
+// global loads of the line's third operand first, then the forward DFT of the A (and B) lines,
+// op(a, b, w) on them in registers, inverse DFT of A (and, if inv_b, B), back to shared memory:
+// the last forward pass, the pointwise product and the first inverse pass in one sweep.
+template <typename C, int TILE, int N, typename Pre, typename Op>
+__device__ __forceinline__ void outer_pointwise(C* A, C* B, bool inv_b, int stride, Pre&& pre,
+                                                Op&& op) {
   for (int i = threadIdx.x; i < stride * TILE; i += blockDim.x) {
     const int c = i % TILE, inner = i / TILE;
-    C a[N], b[N];
+    C a[N], b[N], w[N];
+    pre(w, inner, c);  // global loads of the line's operand, in flight during the DFT below
 #pragma unroll
     for (int m = 0; m < N; ++m) a[m] = A[(inner + m * stride) * TILE + c];
     if (B) {
@@ -350,7 +385,7 @@ __device__ __forceinline__ void outer_pointwise(C* A, C* B, bool inv_b, int stri
       dft_line<C, N>(b, -1);
     }
     dft_line<C, N>(a, -1);
-    op(a, b, inner, c);
+    op(a, b, w);
     dft_line<C, N>(a, +1);
 #pragma unroll
     for (int m = 0; m < N; ++m) A[(inner + m * stride) * TILE + c] = a[m];
@@ -380,8 +415,7 @@ __global__ void __launch_bounds__(256) k_pi_fused(const cplx_t<R>* __restrict__ 
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t col0 = t * TILE;
     with_n(n2, [&](auto N2) {
-      load_dft_inner<C, TILE, decltype(N2)::value>(A, Gp, nk, ncol, col0, -1);
-      load_dft_inner<C, TILE, decltype(N2)::value>(B, Gn, nk, ncol, col0, -1);
+      load_dft_inner2<C, TILE, decltype(N2)::value>(A, Gp, B, Gn, nk, ncol, col0, -1);
     });
     __syncthreads();
     mid_pass<C, TILE, NC>(A, n1, n2, nk, -1);
@@ -389,7 +423,8 @@ __global__ void __launch_bounds__(256) k_pi_fused(const cplx_t<R>* __restrict__ 
     __syncthreads();
     with_n(n0, [&](auto N0) {
       constexpr int N = decltype(N0)::value;
-      outer_pointwise<C, TILE, N>(A, B, false, n1 * n2, [&](C (&a)[N], C (&b)[N], int, int) {
+      outer_pointwise<C, TILE, N>(A, B, false, n1 * n2, [](C (&)[N], int, int) {},
+                                  [&](C (&a)[N], C (&b)[N], C (&)[N]) {
 #pragma unroll
         for (int m = 0; m < N; ++m) a[m] = cscale(cmulc(a[m], b[m]), scale);
       });
@@ -422,8 +457,8 @@ __global__ void __launch_bounds__(256) k_sigma_fused(const cplx_t<R>* Gp, const 
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t col0 = t * TILE;
     with_n(n2, [&](auto N2) {
-      load_dft_inner<C, TILE, decltype(N2)::value>(A, Gp, nk, ncol, col0, -1);
-      if (has_m) load_dft_inner<C, TILE, decltype(N2)::value>(B, Gm, nk, ncol, col0, -1);
+      load_dft_inner2<C, TILE, decltype(N2)::value>(A, Gp, B, has_m ? Gm : nullptr, nk, ncol,
+                                                    col0, -1);
     });
     __syncthreads();
     mid_pass<C, TILE, NC>(A, n1, n2, nk, -1);
@@ -433,17 +468,20 @@ __global__ void __launch_bounds__(256) k_sigma_fused(const cplx_t<R>* Gp, const 
     with_n(n0, [&](auto N0) {
       constexpr int N = decltype(N0)::value;
       outer_pointwise<C, TILE, N>(A, has_m ? B : nullptr, true, stride,
-                                  [&](C (&a)[N], C (&b)[N], int inner, int c) {
+                                  [&](C (&w)[N], int inner, int c) {
         const int64_t col = col0 + c;
 #pragma unroll
         for (int m = 0; m < N; ++m) {
-          C w;
-          w.x = 0;
-          w.y = 0;
-          if (col < ncol) w = WR[(int64_t)(inner + m * stride) * ncol + col];
-          w = cscale(w, scale);
-          a[m] = cmul(a[m], w);
-          if (has_m) b[m] = cmul(b[m], w);
+          w[m].x = 0;
+          w[m].y = 0;
+          if (col < ncol) w[m] = WR[(int64_t)(inner + m * stride) * ncol + col];
+        }
+      }, [&](C (&a)[N], C (&b)[N], C (&w)[N]) {
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+          const C ws = cscale(w[m], scale);
+          a[m] = cmul(a[m], ws);
+          if (has_m) b[m] = cmul(b[m], ws);
         }
       });
     });

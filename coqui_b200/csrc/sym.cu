@@ -3,6 +3,7 @@
 // All three are HBM-bound gathers: one pass over their inputs, coalesced along the
 // contiguous matrix or auxiliary-pair index.
 #include <algorithm>
+#include <type_traits>
 
 #include "sym.cuh"
 
@@ -84,7 +85,9 @@ void launch_gather_transpose(const cplx_t<R>* in, cplx_t<R>* out, const int* qsr
 
 // One CTA per tile of E consecutive auxiliary pairs: the tile of every G(k) and W(q_ibz) is
 // staged in shared memory once, then each (isym, ik) output row of the tile is summed over its
-// terms from there (E threads per row, blockDim / E rows at a time).
+// terms from there (E threads per row, blockDim / E rows at a time).  The sum runs in the
+// storage precision: complex64 terms accumulate in FP32 with packed FMAs (converting every
+// term to FP64 made the FP32 -> FP64 conversions, not memory, the limit), complex128 in FP64.
 template <typename R, int E>
 __global__ void __launch_bounds__(256) k_sigma_ksum(const cplx_t<R>* __restrict__ G,
                                                     const cplx_t<R>* __restrict__ W,
@@ -109,20 +112,28 @@ __global__ void __launch_bounds__(256) k_sigma_ksum(const cplx_t<R>* __restrict_
   const int e = threadIdx.x % E;
   for (int p = threadIdx.x / E; p < nrow; p += blockDim.x / E) {
     const int2 rw = rows[p];  // (first term, term count)
-    double sr = 0.0, si = 0.0;
+    cplx_t<R> acc;
+    acc.x = 0;
+    acc.y = 0;
     for (int j = 0; j < rw.y; ++j) {
       const int4 tj = terms[rw.x + j];
-      const cplx_t<R> g = sv[tj.y * E + e];
-      const cplx_t<R> w = sW[tj.x * E + e];
-      const double gr = g.x, gi = (tj.z & 1) ? -(double)g.y : (double)g.y;
-      const double wr = w.x, wi = (tj.z & 2) ? -(double)w.y : (double)w.y;
-      sr += gr * wr - gi * wi;
-      si += gr * wi + gi * wr;
+      cplx_t<R> g = sv[tj.y * E + e];
+      cplx_t<R> w = sW[tj.x * E + e];
+      if (tj.z & 1) g.y = -g.y;
+      if (tj.z & 2) w.y = -w.y;
+      if constexpr (std::is_same<R, float>::value) {
+        // (re, im) += g * w as two packed FP32 FMAs (sm_100)
+        acc = __ffma2_rn(make_float2(g.x, g.x), w, acc);
+        acc = __ffma2_rn(make_float2(-g.y, g.y), make_float2(w.y, w.x), acc);
+      } else {
+        acc.x = fma(g.x, w.x, fma(-g.y, w.y, acc.x));
+        acc.y = fma(g.x, w.y, fma(g.y, w.x, acc.y));
+      }
     }
     if (e < ne) {
       cplx_t<R> o;
-      o.x = (R)(factor * sr);
-      o.y = (R)(factor * si);
+      o.x = (R)(factor * acc.x);
+      o.y = (R)(factor * acc.y);
       S[(int64_t)p * ncol + e0 + e] = o;
     }
   }

@@ -26,7 +26,8 @@ void launch_gather_transpose(const cplx_t<R>* in, cplx_t<R>* out, const int* qsr
 // Self-energy rows of one tau slice: row p = (isym, ik) is the sum of its terms (w, g, flags),
 // each factor * (flags & 1 ? conj(G[g]) : G[g]) * (flags & 2 ? conj(W[w]) : W[w]) element-wise;
 // rows[p] = (first term, term count).  G (nk, ncol) and W (nqi, ncol) in storage precision R,
-// S (nrow, ncol); FP64 accumulation.  Every G and W column tile is read from HBM once.
+// S (nrow, ncol); accumulation in the storage precision.  Every G and W column tile is read
+// from HBM once.
 template <typename R>
 void launch_sigma_ksum(const cplx_t<R>* G, const cplx_t<R>* W, const int4* terms,
                        const int2* rows, int64_t nrow, int64_t nk, int64_t nqi, int64_t ncol,
