@@ -343,16 +343,29 @@ def measure_fp64_peak(device):
             e1.synchronize()
             best = min(best, e0.elapsed_time(e1))
         out[name + "_tflops"] = fl * n ** 3 / (best * 1e-3) / 1e12
+        if name == "zgemm":
+            # sustained: back to back for ~2.5 s, so that the clocks settle under the power
+            # cap as they do inside a GW iteration (the denominator for kernels timed there)
+            reps = max(8, int(2.5e3 / best))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                torch.matmul(a, b, out=c)
+            e1.record()
+            e1.synchronize()
+            out["zgemm_sustained_tflops"] = fl * n ** 3 * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
         del a, b, c
     torch.cuda.empty_cache()
     out["tflops"] = max(out["dgemm_tflops"], out["zgemm_tflops"])
-    out["how"] = "cuBLAS through torch.matmul: DGEMM 8192^3 and ZGEMM 4096^3, best of 8"
+    out["sustained_tflops"] = out["zgemm_sustained_tflops"]
+    out["how"] = ("cuBLAS through torch.matmul: DGEMM 8192^3 and ZGEMM 4096^3, best of 8 (burst); "
+                  "ZGEMM 4096^3 back to back for ~2.5 s (sustained)")
     return out
 
 
-def group_rates(stats, steps, work, hbm, bf16, fp64):
+def group_rates(stats, steps, work, hbm, bf16, fp64, fp64_sustained=None):
     """Per-kernel-group time and achieved rate against its own roof (HBM copy, bf16 tensor,
-    or the measured FP64 rate)."""
+    or the measured FP64 rate, burst and sustained)."""
     groups = {}
     for name, (ms_tot, n) in stats.items():
         ms_it = ms_tot / steps
@@ -371,6 +384,8 @@ def group_rates(stats, steps, work, hbm, bf16, fp64):
                     g["frac_of_split_tf32_ceiling"] = g["achieved_TFLOPs"] / (bf16 / 6.0)
                 elif kind == "fp64":
                     g["frac_of_fp64_measured"] = g["achieved_TFLOPs"] / fp64
+                    if fp64_sustained:
+                        g["frac_of_fp64_sustained"] = g["achieved_TFLOPs"] / fp64_sustained
         groups[name] = g
     return groups
 
@@ -573,7 +588,8 @@ def run_ours(args, rank, world, local):
     bf16 = peaks.get("bf16_tflops", 1590.0)
     fp64_tf = fp64_peak["tflops"]
     peak_src = "measured" if peaks else "fallback"
-    groups = group_rates(stats, side, work, hbm, bf16, fp64_tf)
+    fp64_sus = fp64_peak.get("sustained_tflops")
+    groups = group_rates(stats, side, work, hbm, bf16, fp64_tf, fp64_sus)
     if fp64_stats:
         fp64["kernel_groups_ms"] = {k: v[0] for k, v in fp64_stats.items()}
     roof = None
@@ -591,12 +607,17 @@ def run_ours(args, rank, world, local):
                     "unit": "GB/s", "frac": g["achieved_GBps"] / hbm, "traffic": None,
                     "avg_launch_ms": per_ms, "peak_source": peak_src + " HBM copy"}
         elif g["bound"] == "fp64":
+            # timed inside a long step: the sustained FP64 rate is the denominator (the
+            # burst fraction is kept beside it)
+            pk = fp64_sus or fp64_tf
             roof = {"kernel": name, "bound": "tensor", "pipe": "FP64 tensor cores (DMMA)",
-                    "achieved": g["achieved_TFLOPs"], "peak": fp64_tf, "unit": "TFLOP/s",
-                    "frac": g["achieved_TFLOPs"] / fp64_tf,
+                    "achieved": g["achieved_TFLOPs"], "peak": pk, "unit": "TFLOP/s",
+                    "frac": g["achieved_TFLOPs"] / pk,
+                    "frac_of_burst": g["achieved_TFLOPs"] / fp64_tf,
                     "traffic": traffic * nprob / n_l if traffic else None,
                     "traffic_source": tsrc, "avg_launch_ms": per_ms,
-                    "peak_source": "measured in this run: " + fp64_peak["how"]}
+                    "peak_source": "measured in this run (" + ("sustained" if fp64_sus else
+                                   "burst") + "): " + fp64_peak["how"]}
         else:
             roof = {"kernel": name, "bound": "tensor", "achieved": g["achieved_TFLOPs"],
                     "peak": bf16, "unit": "TFLOP/s", "frac": g["achieved_TFLOPs"] / bf16,
