@@ -173,3 +173,19 @@ def test_truncated_ir_table_is_an_error(tmp_path, monkeypatch):
     with pytest.raises(Exception):
         iaft.IAFT(1000.0, 10.0, "low")
     shutil.rmtree(d)
+
+
+def test_hartree_fock_refuses_symmetry_reduced_data_before_any_device_work():
+    """THC Hartree-Fock runs on the whole k-mesh: THCData carrying bz maps is refused with
+    EUNSUPPORTED by the solver mirror before a context is created."""
+    import numpy as np
+    import pytest
+    from coqui_b200 import capi, solvers
+    from coqui_b200.symmetry import SWAP, bz_symmetry
+    sym = bz_symmetry((2, 2, 1), [np.eye(3, dtype=int), SWAP], False)
+    thc = solvers.THCData(X=np.zeros((1, 4, 4, 2), complex), V=np.zeros((4, 4, 4), complex),
+                          kpts=np.zeros((4, 3)), lattv=np.eye(3), kp_grid=(2, 2, 1), bz=sym)
+    F = np.zeros((1, 4, 2, 2), complex)
+    with pytest.raises(capi.CoquiB200Error) as e:
+        solvers.hf_t().evaluate(F, F, thc, F)
+    assert e.value.code == -2
