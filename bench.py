@@ -696,13 +696,19 @@ def run_batch(args, rank):
     from coqui_b200 import capi
     if rank != 0:
         return
+    import torch
     ft, mols = batch_molecules()
-    Gs = [m.G0(ft)[:, 0, 0].copy() for m in mols]
+
+    def pinned_like(a):  # page-locked host buffers, as in the single-system e2e
+        h = torch.empty(a.shape, dtype=torch.complex128, pin_memory=True).numpy()
+        h[...] = a
+        return h
+    Gs = [pinned_like(m.G0(ft)[:, 0, 0]) for m in mols]
     b = capi.Batch([m.nb for m in mols], [m.Np for m in mols], ft.nt_f, ft.nw_b)
     b.set_ir(ft)
     for i, m in enumerate(mols):
         b.set_thc(i, m.X[0, 0], m.V[0])
-    out = [np.empty_like(G) for G in Gs]
+    out = [pinned_like(np.zeros_like(G)) for G in Gs]
     for _ in range(args.warmup):
         b.gw_iteration(Gs, out)
     dev, wall = [], []

@@ -478,6 +478,9 @@ int coqui_b200_batch_gw_iteration(coqui_b200_batch* b, const double* const* G_li
           CQ_CHECK_CUDA(cudaMemcpyAsync(Sigma_list[m], b->Sig.p + b->offG[m],
                                         b->nt * b->nb[m] * b->nb[m] * sizeof(double2),
                                         cudaMemcpyDeviceToHost, b->st));
+    // page-locked destinations: the copies above return at once; the call returns after they
+    // landed, as every entry point of the library does
+    CQ_CHECK_CUDA(cudaStreamSynchronize(b->st));
   });
 }
 

@@ -58,3 +58,26 @@ def test_batch_rejects_missing_set_up():
         b.gw_iteration([np.zeros((ft.nt_f, 4, 4)), np.zeros((ft.nt_f, 5, 5))])
     assert e.value.code == -1
     b.close()
+
+
+def test_page_locked_sigma_has_landed_when_the_call_returns(molecules):
+    """With page-locked output buffers the device-to-host copies return at once: the call
+    itself must wait for them, so Sigma read right after it equals Sigma copied to pageable
+    buffers."""
+    import torch
+    ft, mols = molecules
+    b = capi.Batch([m["s"].nb for m in mols], [m["s"].Np for m in mols], ft.nt_f, ft.nw_b)
+    b.set_ir(ft)
+    for i, m in enumerate(mols):
+        b.set_thc(i, m["s"].X[0, 0], m["s"].V[0])
+    Gs = [m["G"][:, 0, 0] for m in mols]
+    ref = b.gw_iteration(Gs)
+    pinned = []
+    for S in ref:
+        h = torch.empty(S.shape, dtype=torch.complex128, pin_memory=True).numpy()
+        h[...] = np.nan
+        pinned.append(h)
+    out = b.gw_iteration(Gs, pinned)
+    for S, P in zip(ref, out):
+        assert np.array_equal(S, P)
+    b.close()
