@@ -118,6 +118,9 @@ WORKLOADS = {
     "g0w0_k2_nb64_np512": dict(n=2, nb=64, nocc=24, Np=512, beta=1000.0, lam=1e4, prec="low"),
     # 64 k-points at a smaller N_mu: the case used for profiles of the k <-> R kernels
     "g0w0_k4_nb48_np384": dict(n=4, nb=48, nocc=24, Np=384, beta=1000.0, lam=1e4, prec="low"),
+    # 6x6x6 k-points (the headline grid's column kernels) at a small N_mu and IR grid: a
+    # 143 MB tau slice (larger than L2) in about 10 GB of device memory, for kernel profiles
+    "g0w0_k6_nb32_np288": dict(n=6, nb=32, nocc=16, Np=288, beta=100.0, lam=1e3, prec="low"),
     "rpa_gw_k6_nb96_np1024": dict(n=6, nb=96, nocc=48, Np=1024, beta=1000.0, lam=1e5, prec="low"),
     "scgw_k3_nb48_np384": dict(n=3, nb=48, nocc=24, Np=384, beta=1000.0, lam=1e4, prec="low"),
 }
