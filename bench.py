@@ -194,16 +194,19 @@ def gemm_flops_c(M, N, K):
 
 def algorithmic_work(w, s, ft):
     """Algorithmic work of each kernel group: (kind, amount per launch group or None,
-    amount per iteration or None).  Flops count a complex multiply-add as 8 (FP64-equivalent
-    count of the product actually formed, triangular structure included); bytes are the
-    compulsory complex64 reads + writes."""
+    amount per iteration or None, amount per work unit or None).  Flops count a complex
+    multiply-add as 8 (FP64-equivalent count of the product actually formed, triangular
+    structure included); bytes are the compulsory complex64 reads + writes.  The projections
+    count per (tau, k) problem, times the problems the library reports (a G(tau) whose
+    projection does not fit the cache is projected again for the self-energy)."""
     nk, nb, Np, nth, nwh, nt = s.nk, s.nb, s.Np, ft.nt_half, ft.nw_half, ft.nt_f
     ncol, P = Np * Np, nk * nwh  # Dyson problems per iteration
     n3 = float(Np) ** 3
     return {
-        # every G(tau) projected once and every Sigma(tau) once (tau-batched launches)
-        "proj_p2a": ("tensor", None, nt * nk * (gemm_flops_c(Np, nb, nb) + gemm_flops_c(Np, Np, nb))),
-        "proj_a2p": ("tensor", None, nt * nk * (gemm_flops_c(nb, Np, Np) + gemm_flops_c(nb, nb, Np))),
+        # per (tau, k) problem: T = X G (Np x nb, K = nb), T X^H (Np x Np, K = nb); and
+        # U = S X (Np x nb, K = Np), X^H U (nb x nb, K = Np)
+        "proj_p2a": ("tensor", None, None, gemm_flops_c(Np, nb, nb) + gemm_flops_c(Np, Np, nb)),
+        "proj_a2p": ("tensor", None, None, gemm_flops_c(Np, nb, Np) + gemm_flops_c(nb, nb, Np)),
         "pi_fused": ("hbm", 3 * nk * ncol * 8, None),
         "sigma_fused": ("hbm", 5 * nk * ncol * 8, None),
         "dft_w": ("hbm", 2 * nth * nk * ncol * 8, None),
@@ -363,16 +366,26 @@ def measure_fp64_peak(device):
     return out
 
 
-def group_rates(stats, steps, work, hbm, bf16, fp64, fp64_sustained=None):
+def group_rates(stats, steps, work, hbm, bf16, fp64, fp64_sustained=None, units=None):
     """Per-kernel-group time and achieved rate against its own roof (HBM copy, bf16 tensor,
     or the measured FP64 rate, burst and sustained)."""
     groups = {}
+    units = units or {}
     for name, (ms_tot, n) in stats.items():
         ms_it = ms_tot / steps
-        kind, per_launch, per_iter = work.get(name, (None, None, None))
-        amount = per_iter if per_iter is not None else (
-            per_launch * n / steps if per_launch is not None else None)
+        kind, per_launch, per_iter, per_unit = (tuple(work.get(name, ())) + (None,) * 4)[:4]
+        u = units.get(name, 0)
+        if per_iter is not None:
+            amount = per_iter
+        elif per_launch is not None:
+            amount = per_launch * n / steps
+        elif per_unit is not None and u > 0:
+            amount = per_unit * u / steps
+        else:
+            amount = None
         g = {"ms_per_step": ms_it, "launch_groups_per_step": n / steps, "bound": kind}
+        if per_unit is not None and u > 0:
+            g["units_per_step"] = u / steps
         if amount and ms_it > 0:
             if kind == "hbm":
                 g["achieved_GBps"] = amount / (ms_it * 1e-3) / 1e9
@@ -463,6 +476,7 @@ def run_ours(args, rank, world, local):
         ctx.gw_iteration(None, want_sigma=False)
     barrier()
     stats = ctx.kernel_stats()
+    stat_units = ctx.kernel_units()
     ctx.set_profiling(False)
 
     # e2e through the public API with pinned host buffers
@@ -589,7 +603,7 @@ def run_ours(args, rank, world, local):
     fp64_tf = fp64_peak["tflops"]
     peak_src = "measured" if peaks else "fallback"
     fp64_sus = fp64_peak.get("sustained_tflops")
-    groups = group_rates(stats, side, work, hbm, bf16, fp64_tf, fp64_sus)
+    groups = group_rates(stats, side, work, hbm, bf16, fp64_tf, fp64_sus, stat_units)
     if fp64_stats:
         fp64["kernel_groups_ms"] = {k: v[0] for k, v in fp64_stats.items()}
     roof = None

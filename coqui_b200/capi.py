@@ -27,7 +27,8 @@ SYMBOLS = [
     "coqui_b200_primary_to_aux", "coqui_b200_aux_to_primary", "coqui_b200_tau_to_w",
     "coqui_b200_w_to_tau", "coqui_b200_dyson_w", "coqui_b200_last_timings",
     "coqui_b200_kernel_launches", "coqui_b200_gw_iteration", "coqui_b200_set_profiling",
-    "coqui_b200_kernel_stats", "coqui_b200_primary_to_aux_noalloc",
+    "coqui_b200_kernel_stats", "coqui_b200_kernel_units", "coqui_b200_set_gcache_limit",
+    "coqui_b200_primary_to_aux_noalloc",
     "coqui_b200_set_ir_fermi", "coqui_b200_set_mean_field", "coqui_b200_set_iter_alg",
     "coqui_b200_hf_evaluate", "coqui_b200_scgw_set_hf", "coqui_b200_set_div_treatment",
     "coqui_b200_scgw_iteration", "coqui_b200_get_scgw_state", "coqui_b200_dyson_g",
@@ -102,6 +103,8 @@ def load() -> ctypes.CDLL:
     lib.coqui_b200_gw_iteration.argtypes = [P, P, P, P]
     lib.coqui_b200_set_profiling.argtypes = [P, ctypes.c_int]
     lib.coqui_b200_kernel_stats.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, P, ctypes.c_int]
+    lib.coqui_b200_kernel_units.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, ctypes.c_int]
+    lib.coqui_b200_set_gcache_limit.argtypes = [P, ctypes.c_int64]
     lib.coqui_b200_primary_to_aux_noalloc.argtypes = [P, P, P, ctypes.c_int64, ctypes.c_int64,
                                                       ctypes.c_int64, P, ctypes.c_char_p,
                                                       ctypes.c_int]
@@ -424,6 +427,20 @@ class Context:
         raw = names.raw
         return {raw[i * L:(i + 1) * L].split(b"\0")[0].decode(): (float(ms[i]), int(cnt[i]))
                 for i in range(k)}
+
+    def set_gcache_limit(self, nbytes: int):
+        """Bytes of device memory for the projected-G cache (-1: half the free memory, 0: none)."""
+        self._check(self.lib.coqui_b200_set_gcache_limit(self.h, int(nbytes)))
+
+    def kernel_units(self):
+        """{name: work units} accumulated while profiling was on: the (tau, k) problems of the
+        projection groups (0 for groups that do not count theirs)."""
+        n, L = 64, 48
+        names = ctypes.create_string_buffer(n * L)
+        units = np.zeros(n, np.int64)
+        k = self.lib.coqui_b200_kernel_units(self.h, names, L, units.ctypes.data, n)
+        raw = names.raw
+        return {raw[i * L:(i + 1) * L].split(b"\0")[0].decode(): int(units[i]) for i in range(k)}
 
     def primary_to_aux(self, O_tskab):
         O = np.ascontiguousarray(O_tskab, np.complex128)

@@ -106,13 +106,15 @@ template <typename T> struct DevBuf {
 struct Prof {
   bool on = false;
   cudaStream_t st = nullptr;
-  std::vector<std::tuple<std::string, cudaEvent_t, cudaEvent_t>> pending;
-  std::map<std::string, std::pair<double, int64_t>> acc;  // name -> (ms, launches)
+  std::vector<std::tuple<std::string, cudaEvent_t, cudaEvent_t, int64_t>> pending;
+  // name -> (ms, launch groups, work units: the problems a group processed, where it counts them)
+  std::map<std::string, std::tuple<double, int64_t, int64_t>> acc;
   struct Scope {
     Prof* p = nullptr;
     std::string name;
     cudaEvent_t a = nullptr;
-    Scope(Prof* pr, const char* n) : p(pr && pr->on ? pr : nullptr), name(n) {
+    int64_t units = 0;
+    Scope(Prof* pr, const char* n, int64_t u = 0) : p(pr && pr->on ? pr : nullptr), name(n), units(u) {
       if (p) {
         nvtxRangePushA(n);  // profilers can select the group's kernels by this range
         cudaEventCreate(&a);
@@ -126,7 +128,7 @@ struct Prof {
       cudaEvent_t b;
       cudaEventCreate(&b);
       cudaEventRecord(b, p->st);
-      p->pending.emplace_back(name, a, b);
+      p->pending.emplace_back(name, a, b, units);
     }
   };
   // call after the stream has been synchronised
@@ -135,8 +137,9 @@ struct Prof {
       float ms = 0;
       cudaEventElapsedTime(&ms, std::get<1>(t), std::get<2>(t));
       auto& e = acc[std::get<0>(t)];
-      e.first += ms;
-      e.second += 1;
+      std::get<0>(e) += ms;
+      std::get<1>(e) += 1;
+      std::get<2>(e) += std::get<3>(t);
       cudaEventDestroy(std::get<1>(t));
       cudaEventDestroy(std::get<2>(t));
     }

@@ -106,6 +106,10 @@ struct coqui_b200_ctx {
   // place) by the self-energy of the same G; allocated when it fits in half the free memory
   DevBuf<unsigned char> Gcache;
   bool gcache_valid = false;
+  // tau pairs the cache holds: slices [0, gcache_pairs) and [nt - gcache_pairs, nt); all nt
+  // slices (indexed by tau) when gcache_pairs == nth
+  int64_t gcache_pairs = 0;
+  int64_t gcache_limit = -1;  // bytes; -1: half the free memory at first use
 
   // Dyson results per (iW, q) problem on the device
   DevBuf<int> dinfo;
@@ -365,7 +369,7 @@ void a2p_fp64(Ctx* c, const double2* Sk, double2* out, int64_t ntau) {
 }
 
 void project_p2a(Ctx* c, const double2* Gk, void* out, int64_t ntau = 1) {
-  cq::Prof::Scope sc(&c->prof, "proj_p2a");
+  cq::Prof::Scope sc(&c->prof, "proj_p2a", ntau * c->nk);
   const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
   if (c->mode == COQUI_B200_FP64) {
     p2a_fp64(c, Gk, (double2*)out, ntau);
@@ -376,7 +380,7 @@ void project_p2a(Ctx* c, const double2* Gk, void* out, int64_t ntau = 1) {
 // ntau consecutive slices (ntau, nk, Np, Np) in storage precision -> out (ntau, nk, nb, nb)
 // complex128.
 void project_a2p(Ctx* c, const void* Sk, double2* out, int64_t ntau = 1) {
-  cq::Prof::Scope sc(&c->prof, "proj_a2p");
+  cq::Prof::Scope sc(&c->prof, "proj_a2p", ntau * c->nk);
   const int64_t nk = c->nk, nb = c->nb, Np = c->Np;
   if (c->mode == COQUI_B200_FP64) {
     a2p_fp64(c, (const double2*)Sk, out, ntau);
@@ -415,15 +419,61 @@ void wait_G_chunk(Ctx* c, int64_t i) {
   if (c->g_pipelined) CQ_CHECK_CUDA(cudaStreamWaitEvent(c->st, c->up_ev[(size_t)i], 0));
 }
 
-// Projected-G cache (nt slabs); nullptr when it does not fit in half the free memory.
+// Projected-G cache: every tau slice when nt slabs fit in half the free memory, else as many
+// whole tau chunks (each a pair of slice ranges [a, b) and [nt - b, nt - a)) as fit, the
+// first chunks; the polarizability fills it and the self-energy reuses it, projecting the
+// slices outside it again.  nullptr when not even one chunk fits.  The size is fixed by the
+// first allocation.
 unsigned char* gcache(Ctx* c) {
-  const size_t bytes = (size_t)c->nt * c->nk * c->Np * c->Np * c->elem();
-  if (c->Gcache.n >= bytes) return c->Gcache.p;
-  size_t fr = 0, tot = 0;
-  CQ_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
-  if (bytes > fr / 2) return nullptr;
-  c->Gcache.ensure(bytes);
-  return c->Gcache.p;
+  const size_t slab = (size_t)c->nk * c->Np * c->Np * c->elem();
+  const size_t full = (size_t)c->nt * slab;
+  const int64_t chunk = tau_chunk(c);
+  const size_t pair = 2 * (size_t)chunk * slab;
+  if (c->Gcache.n == 0) {
+    size_t fr = 0, tot = 0;
+    CQ_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+    // at most half the free memory, and the Dyson step keeps the memory for chunks of two
+    // whole factorisation waves (fewer, smaller chunks cost it more than the cache saves)
+    size_t budget = fr / 2;
+    const size_t reserve =
+        cq::dyson_reserve_bytes(c->Np, c->nwh * c->nq, c->mode != COQUI_B200_FP64);
+    const size_t need = (reserve > c->dyn.n ? reserve - c->dyn.n : 0) + ((size_t)1 << 30);
+    budget = std::min(budget, fr > need ? fr - need : 0);
+    if (c->gcache_limit >= 0) budget = std::min(budget, (size_t)c->gcache_limit);
+    if (full <= budget) {
+      c->Gcache.ensure(full);
+    } else {
+      const int64_t nfit = std::min<int64_t>((int64_t)(budget / pair), n_tau_chunks(c) - 1);
+      if (nfit <= 0) {
+        c->gcache_pairs = 0;
+        return nullptr;
+      }
+      c->Gcache.ensure((size_t)nfit * pair);
+    }
+  }
+  if (c->Gcache.n >= full) {
+    c->gcache_pairs = c->nth;
+  } else {
+    const int64_t nfit = std::min<int64_t>((int64_t)(c->Gcache.n / pair), n_tau_chunks(c) - 1);
+    c->gcache_pairs = std::max<int64_t>(nfit, 0) * chunk;
+  }
+  return c->gcache_pairs > 0 ? c->Gcache.p : nullptr;
+}
+
+// whether the cache holds slice tau, and where
+bool gcached(const Ctx* c, int64_t tau) {
+  const int64_t A = c->gcache_pairs;
+  return A >= c->nth || tau < A || tau >= c->nt - A;
+}
+unsigned char* gslab(Ctx* c, int64_t tau) {
+  const size_t slab = (size_t)c->nk * c->Np * c->Np * c->elem();
+  const int64_t A = c->gcache_pairs;
+  const int64_t idx = (A >= c->nth || tau < A) ? tau : tau - c->nt + 2 * A;
+  return c->Gcache.p + (size_t)idx * slab;
+}
+// whether tau chunk [a, b) lies in the cache (chunks are cached whole)
+bool gchunk_cached(const Ctx* c, int64_t b) {
+  return c->gcache_pairs >= c->nth || b <= c->gcache_pairs;
 }
 
 void eval_pi_device(Ctx* c) {
@@ -440,16 +490,17 @@ void eval_pi_device(Ctx* c) {
     int64_t a, b;
     tau_chunk_range(c, i, &a, &b);
     wait_G_chunk(c, i);
-    if (cache) {
-      project_p2a(c, c->G.p + a * gsz, cache + a * slab, b - a);
-      project_p2a(c, c->G.p + (nt - b) * gsz, cache + (nt - b) * slab, b - a);
+    const bool cached = cache && gchunk_cached(c, b);
+    if (cached) {
+      project_p2a(c, c->G.p + a * gsz, gslab(c, a), b - a);
+      project_p2a(c, c->G.p + (nt - b) * gsz, gslab(c, nt - b), b - a);
     }
     for (int64_t it = a; it < b; ++it) {
       const unsigned char* gp = c->Gp.p;
       const unsigned char* gn = c->Gn.p;
-      if (cache) {
-        gp = cache + it * slab;
-        gn = cache + (nt - it - 1) * slab;
+      if (cached) {
+        gp = gslab(c, it);
+        gn = gslab(c, nt - it - 1);
       } else {
         project_p2a(c, c->G.p + it * gsz, c->Gp.p);
         project_p2a(c, c->G.p + (nt - it - 1) * gsz, c->Gn.p);
@@ -1400,14 +1451,15 @@ void sigma_device(Ctx* c, double* host_out) {
   for (int64_t i = 0; i < n_tau_chunks(c); ++i) {
     int64_t a, b;
     tau_chunk_range(c, i, &a, &b);
-    if (!cache) wait_G_chunk(c, i);
+    const bool cached = cache && gchunk_cached(c, b);
+    if (!cached) wait_G_chunk(c, i);
     for (int64_t it = a; it < b; ++it) {
       const bool minus = it < nt / 2;  // thc_gw.icc:59-61 writes Sigma(nt-1-it) for it < nt/2
       unsigned char* gp = c->Gp.p;
       unsigned char* gn = minus ? c->Gn.p : nullptr;
-      if (cache) {
-        gp = cache + it * slab;
-        gn = minus ? cache + (nt - it - 1) * slab : nullptr;
+      if (cached) {
+        gp = gslab(c, it);
+        gn = minus ? gslab(c, nt - it - 1) : nullptr;
       } else {
         project_p2a(c, c->G.p + it * gsz, gp);
         if (minus) project_p2a(c, c->G.p + (nt - it - 1) * gsz, gn);
@@ -1422,15 +1474,15 @@ void sigma_device(Ctx* c, double* host_out) {
           cq::launch_sigma_fused<float>((float2*)gp, (float2*)gn, (float2*)WR, (float2*)gp,
                                         (float2*)gn, ncol, c->g, c->st);
       }
-      if (!cache) {
+      if (!cached) {
         project_a2p(c, gp, c->Sig.p + it * gsz);
         if (minus) project_a2p(c, gn, c->Sig.p + (nt - it - 1) * gsz);
       }
     }
-    if (cache) {
+    if (cached) {
       // for odd nt the middle slice is in both ranges (same values written twice)
-      project_a2p(c, cache + a * slab, c->Sig.p + a * gsz, b - a);
-      project_a2p(c, cache + (nt - b) * slab, c->Sig.p + (nt - b) * gsz, b - a);
+      project_a2p(c, gslab(c, a), c->Sig.p + a * gsz, b - a);
+      project_a2p(c, gslab(c, nt - b), c->Sig.p + (nt - b) * gsz, b - a);
     }
     if (pipe_out) {
       const size_t bytes = (size_t)(b - a) * gsz * sizeof(double2);
@@ -1792,8 +1844,44 @@ int coqui_b200_kernel_stats(const coqui_b200_ctx* c, char* names, int name_len, 
       std::strncpy(names + (size_t)k * name_len, p.first.c_str(), name_len - 1);
       names[(size_t)k * name_len + name_len - 1] = 0;
     }
-    if (ms) ms[k] = p.second.first;
-    if (launches) launches[k] = p.second.second;
+    if (ms) ms[k] = std::get<0>(p.second);
+    if (launches) launches[k] = std::get<1>(p.second);
+    ++k;
+  }
+  return k;
+}
+
+int coqui_b200_set_gcache_limit(coqui_b200_ctx* c, int64_t bytes) {
+  return guarded(c, [&] {
+    CQ_REQUIRE(bytes >= -1, COQUI_B200_EINVAL, "cache limit must be -1, 0 or a byte count");
+    CQ_CHECK_CUDA(cudaStreamSynchronize(c->st));
+    // captured iteration graphs hold the cache's address
+    if (c->gexec) {
+      cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+    }
+    if (c->rexec) {
+      cudaGraphExecDestroy(c->rexec);
+      c->rexec = nullptr;
+    }
+    c->gcache_limit = bytes;
+    c->Gcache.release();
+    c->gcache_valid = false;
+    c->gcache_pairs = 0;
+  });
+}
+
+int coqui_b200_kernel_units(const coqui_b200_ctx* c, char* names, int name_len, int64_t* units,
+                            int n) {
+  if (!c) return COQUI_B200_EINVAL;
+  int k = 0;
+  for (const auto& p : c->prof.acc) {
+    if (k >= n) break;
+    if (names && name_len > 0) {
+      std::strncpy(names + (size_t)k * name_len, p.first.c_str(), name_len - 1);
+      names[(size_t)k * name_len + name_len - 1] = 0;
+    }
+    if (units) units[k] = std::get<2>(p.second);
     ++k;
   }
   return k;

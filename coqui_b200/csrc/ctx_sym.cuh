@@ -249,8 +249,8 @@ void sym_sigma(Ctx* c, double* host_out) {
       const int64_t itg = minus ? nt - it - 1 : it;
       if (minus && itg == nth - 1) continue;  // odd nt: the middle slice once (thc_gw.icc:297)
       const unsigned char* g = c->Gp.p;
-      if (cache)
-        g = cache + itg * slab;
+      if (cache && gcached(c, itg))
+        g = gslab(c, itg);
       else
         project_p2a(c, c->G.p + itg * nk * bb, c->Gp.p);
       const unsigned char* W = S.PWi.p + (size_t)it * nqi * pp * es;
@@ -264,7 +264,7 @@ void sym_sigma(Ctx* c, double* host_out) {
                                        nrow, nk, nqi, pp, factor, (float2*)S.Sq.p, c->st);
       }
       {
-        cq::Prof::Scope sc(&c->prof, "proj_a2p");
+        cq::Prof::Scope sc(&c->prof, "proj_a2p", nrow);
         if (fp64)
           a2p_with(c, S.Xs.p, nrow, (const double2*)S.Sq.p, S.Sab.p);
         else

@@ -198,19 +198,40 @@ int cholesky_lower_batched(double2* A, int64_t Np, int64_t nbatch, cudaStream_t 
   return 0;
 }
 
+namespace {
+// The mixed form with the tensor-core inverse keeps M, the inverse levels' scratch and E in
+// the chunk's own Pi(iW) slices (dead once P1 = L^H Pi is formed; W overwrites them last).
+bool m_in_pi(int64_t Np, bool mixed, bool want_w) { return mixed && want_w && Np > kInvGroup; }
+
+// scratch bytes per problem: T1 (es), M (es, unless in Pi), A (c128), Y (c128; the mixed
+// form's W operands)
+size_t dyson_bytes_per_problem(int64_t Np, bool mixed, bool want_w) {
+  const size_t NN = (size_t)Np * Np, es = mixed ? sizeof(float2) : sizeof(double2);
+  return NN * (es + (m_in_pi(Np, mixed, want_w) ? 0 : es) + sizeof(double2) +
+               (mixed && want_w ? sizeof(double2) : 0)) +
+         64;
+}
+constexpr double kScratchShare = 0.6;  // of the free device memory, per chunk
+}  // namespace
+
+size_t dyson_reserve_bytes(int64_t Np, int64_t nprob, bool mixed) {
+  const int64_t n = std::min<int64_t>(nprob, 2 * chol_wave_size());
+  return (size_t)((double)(dyson_bytes_per_problem(Np, mixed, true) * (size_t)n + 1024) /
+                  kScratchShare);
+}
+
 void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t s,
                std::vector<double>* logdet, std::vector<double2>* trace) {
   const int64_t Np = a.Np, NN = Np * Np, nq = a.nq, nw = a.nw;
   const size_t es = a.mixed ? sizeof(float2) : sizeof(double2);
-  // per problem: T1 (es), M (es), A (c128), Y (c128; the mixed form's W operands)
-  const size_t per = NN * (es + es + sizeof(double2) + (a.mixed && a.want_w ? sizeof(double2) : 0)) +
-                     64;
+  const bool mpi = m_in_pi(Np, a.mixed, a.want_w);
+  const size_t per = dyson_bytes_per_problem(Np, a.mixed, a.want_w);
   // Chunks of the flattened (w, q) problem list (per-q operands addressed periodically), as
   // many problems per chunk as ~60% of the free device memory allows, so the factorisation
   // kernel sees whole waves of problems (one CTA per problem)
   size_t fr = 0, tot = 0;
   CQ_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
-  size_t budget = std::max(scratch.n, (size_t)(0.6 * (double)(fr + scratch.n)));
+  size_t budget = std::max(scratch.n, (size_t)(kScratchShare * (double)(fr + scratch.n)));
   // while a graph is captured the scratch keeps its size (no device allocation or free inside
   // the capture) when it holds at least one problem
   if (a.keep_scratch && scratch.n >= per + 1024) budget = scratch.n - 1024;
@@ -230,7 +251,7 @@ void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t 
     return p;
   };
   unsigned char* T1 = carve(nbq * NN * es);
-  unsigned char* Mb = carve(nbq * NN * es);
+  unsigned char* Mb0 = mpi ? nullptr : carve(nbq * NN * es);
   double2* A = (double2*)carve(nbq * NN * sizeof(double2));
   double2* Y = a.mixed && a.want_w ? (double2*)carve(nbq * NN * sizeof(double2)) : nullptr;
   CQ_REQUIRE(a.info && a.logdet && a.trace, COQUI_B200_EINVAL, "dyson_run: result arrays missing");
@@ -243,6 +264,7 @@ void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t 
     const int64_t nb = std::min(nbq, nprob - p0);
     const int64_t q0 = p0 % nq;
     unsigned char* Pi = a.PW + (size_t)p0 * NN * es;
+    unsigned char* Mb = mpi ? Pi : Mb0;
     const float2* Lc = a.Lc;  // mixed form: complex64 factors, addressed periodically in q
     const float2* LHc = a.LHc;
     // M = L^H (Pi L)

@@ -95,6 +95,10 @@ struct DysonArgs {
   bool defer_check = false;
 };
 
+// Free device memory (bytes, beside the scratch it already holds) with which dyson_run
+// forms chunks of two whole waves of the factorisation (or all nprob problems) for the W step.
+size_t dyson_reserve_bytes(int64_t Np, int64_t nprob, bool mixed);
+
 // Runs every (iW, q) problem; fills logdet / trace (indexed n * nq + q) if want_e.
 void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t s,
                std::vector<double>* logdet, std::vector<double2>* trace);

@@ -326,11 +326,22 @@ COQUI_B200_API int coqui_b200_dyson_w(coqui_b200_ctx* ctx, const double* Pi_wqPQ
 COQUI_B200_API int coqui_b200_last_timings(const coqui_b200_ctx* ctx, char* names, int name_len, double* ms,
                             int n);
 
+/* Device memory of the projected-G cache that carries G_PQ(tau) from the polarizability to
+   the self-energy of the same G: -1 (default) at most half the free memory at its first use,
+   0 none, else at most `bytes` (and half the free memory).  Slices outside the cache are
+   projected again for the self-energy; results are the same.  Releases the current cache. */
+COQUI_B200_API int coqui_b200_set_gcache_limit(coqui_b200_ctx* ctx, int64_t bytes);
+
 /* Per-kernel CUDA-event timing (recorded on the context's stream around every launch
    group) while profiling is on; set_profiling resets the accumulators. */
 COQUI_B200_API int coqui_b200_set_profiling(coqui_b200_ctx* ctx, int on);
 COQUI_B200_API int coqui_b200_kernel_stats(const coqui_b200_ctx* ctx, char* names, int name_len,
                                            double* ms, int64_t* launches, int n);
+/* Work units of the same groups, in the same order: the (tau, k) problems of the primary <->
+   auxiliary projections ("proj_p2a", "proj_a2p"; a G(tau) projected again for the self-energy
+   counts again), 0 for groups that do not count theirs. */
+COQUI_B200_API int coqui_b200_kernel_units(const coqui_b200_ctx* ctx, char* names, int name_len,
+                                           int64_t* units, int n);
 
 /* Tile-shape autotuner of the tensor-core GEMMs (process-wide, on by default; the environment
    variable COQUI_B200_AUTOTUNE=0 starts with it off): the first product of each shape class

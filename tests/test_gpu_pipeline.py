@@ -171,3 +171,33 @@ def test_rpa_energy_graph_matches_direct_launches(case):
     c.gw_iteration(None, want_sigma=False)
     assert abs(c.rpa_energy(None) - e0) < 1e-12
     c.close()
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_partial_projection_cache(case, mode, tol):
+    """The projected-G cache holding every slice, only the first tau chunk (slices [0, 4) and
+    [nt - 4, nt)), or nothing: the self-energy is the same, and the counted projections are the
+    polarizability's 2 nth per k plus the slices the self-energy projects again."""
+    s, ft = case["s"], case["ft"]
+    c = make_ctx(case, mode)
+    G = np.ascontiguousarray(case["G"])
+    nt, nk = ft.nt_f, s.nk
+    nth = (nt + 1) // 2
+    chunk = min(nth, max(4, -(-256 // nk)))
+    slab = nk * s.Np ** 2 * (16 if mode == capi.FP64 else 8)
+    res = {}
+    for name, limit, again in (("all", -1, 0), ("one_chunk", 2 * chunk * slab, nt - 2 * chunk),
+                               ("none", 0, nt)):
+        c.set_gcache_limit(limit)
+        c.set_profiling(True)
+        S, _ = c.gw_iteration(G)
+        units = c.kernel_units()
+        c.set_profiling(False)
+        res[name] = S
+        assert units["proj_p2a"] == (2 * nth + again) * nk, name
+    assert maxabs(res["all"], case["Sigma"]) < tol
+    assert maxabs(res["one_chunk"], res["all"]) < 1e-12
+    assert maxabs(res["none"], res["all"]) < 1e-12
+    c.set_gcache_limit(-1)
+    with pytest.raises(capi.CoquiB200Error):
+        c.set_gcache_limit(-2)
