@@ -351,12 +351,14 @@ def measure_fp64_peak(device):
             # cap as they do inside a GW iteration (the denominator for kernels timed there)
             reps = max(8, int(2.5e3 / best))
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
-                torch.matmul(a, b, out=c)
-            e1.record()
-            e1.synchronize()
+            with Clocks(device) as clk:
+                e0.record()
+                for _ in range(reps):
+                    torch.matmul(a, b, out=c)
+                e1.record()
+                e1.synchronize()
             out["zgemm_sustained_tflops"] = fl * n ** 3 * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
+            out["sustained_sm_mhz"] = clk.summary().get("sm_mhz")
         del a, b, c
     torch.cuda.empty_cache()
     out["tflops"] = max(out["dgemm_tflops"], out["zgemm_tflops"])
@@ -632,6 +634,13 @@ def run_ours(args, rank, world, local):
                     "traffic_source": tsrc, "avg_launch_ms": per_ms,
                     "peak_source": "measured in this run (" + ("sustained" if fp64_sus else
                                    "burst") + "): " + fp64_peak["how"]}
+            # the FP64 pipe's rate scales with the SM clock: the same peak at the clock the
+            # timed iterations ran at (power-capped by their tensor-core phases), as context
+            it_mhz, pk_mhz = clk.summary().get("sm_mhz"), fp64_peak.get("sustained_sm_mhz")
+            if it_mhz and pk_mhz:
+                roof["peak_at_iteration_clock"] = pk * it_mhz / pk_mhz
+                roof["frac_at_iteration_clock"] = g["achieved_TFLOPs"] / roof["peak_at_iteration_clock"]
+                roof["clocks_mhz"] = {"iteration": it_mhz, "peak_measurement": pk_mhz}
         else:
             roof = {"kernel": name, "bound": "tensor", "achieved": g["achieved_TFLOPs"],
                     "peak": bf16, "unit": "TFLOP/s", "frac": g["achieved_TFLOPs"] / bf16,

@@ -1028,7 +1028,7 @@ __global__ void __launch_bounds__(128) k_ir_transform_real(cplx_t<R>* __restrict
 // M (n_out, n_in) FP64 is staged into shared memory as FP32, rows padded to MAXT entries and
 // the row count to a multiple of 4 with zeros, so that one float4 read feeds 8 FMAs.
 template <int MAXT>
-__global__ void __launch_bounds__(256) k_ir_transform_f32(float2* __restrict__ buf, int64_t ncol,
+__global__ void __launch_bounds__(128) k_ir_transform_f32(float2* __restrict__ buf, int64_t ncol,
                                                           int n_in, int n_out,
                                                           const double* __restrict__ M) {
   static_assert(MAXT % 4 == 0, "MAXT must be a multiple of 4");
@@ -1075,8 +1075,10 @@ template <int MAXT>
 static void launch_ir_f32(float2* buf, int64_t ncol, int n_in, int n_out, const double* M,
                           cudaStream_t s) {
   const size_t smem = (size_t)((n_out + 3) / 4) * 4 * MAXT * sizeof(float);
+  // 128-thread blocks: five resident per SM at 96 registers (two of 256 threads) overlap one
+  // block's loads with another's arithmetic (5.19 against 4.94 TB/s for 31 -> 31 points)
   set_smem((const void*)k_ir_transform_f32<MAXT>, smem);
-  k_ir_transform_f32<MAXT><<<grid_for(ncol, 256, 148 * 16), 256, smem, s>>>(buf, ncol, n_in, n_out, M);
+  k_ir_transform_f32<MAXT><<<grid_for(ncol, 128, 148 * 32), 128, smem, s>>>(buf, ncol, n_in, n_out, M);
   CQ_LAUNCHED();
 }
 
