@@ -50,7 +50,9 @@ int rows_aligned(const void* X, bool split, int64_t ld, int64_t sX) {
 
 constexpr int kBM = 128;
 constexpr int kBKR = 32;  // real K per stage (128 bytes of fp32)
-// BNC complex columns per tile; NP producer threads (warps 0..NP/32-1 stage operands, then
+// tcgen05.alloc takes a power of two of at least 32 columns
+constexpr int pow2_at_least(int x) { return x <= 32 ? 32 : 2 * pow2_at_least((x + 1) / 2); }
+// BNC complex columns per tile (32, 64, 96 or 128); NP producer threads (warps 0..NP/32-1 stage operands, then
 // drain the accumulator; warp NP/32 allocates TMEM and issues MMAs); ST pipeline stages.
 // Long-K products use (NP = 256, ST = 2); short-K ones (K <= 64) use (NP = 128, ST = 1), whose
 // smaller footprint lets several CTAs share an SM so one tile's epilogue overlaps another's
@@ -66,7 +68,7 @@ template <int BNC, int NP, int ST> struct TileCfg {
   static constexpr int B_PLANE = NR * 128;             // bytes of one B plane
   static constexpr int STAGE = 2 * A_PLANE + 2 * B_PLANE;
   static constexpr int SMEM = ST * STAGE + 1024 /*align*/ + 256 /*barriers*/;
-  static constexpr int TMEM_COLS = NR;                 // 64, 128 or 256
+  static constexpr int TMEM_COLS = pow2_at_least(NR);  // 64, 128 or 256 (192 -> 256)
   static constexpr int A_CHUNKS = kBM * 8 / NP;        // A chunks per producer thread
   static constexpr int B_CHUNKS = BNC * 8 / NP;        // B chunks per producer thread
   // kind::tf32 dense, F32 accumulate, K-major A and B, M = 128, N = NR
@@ -635,7 +637,8 @@ template <int BNC, int NP, int ST> struct PCfg {
   static constexpr int THREADS = NP + 32 + 128;
   static constexpr int EPI_PITCH = 36;       // floats per row of a warp's 32 x 32 buffer
   static constexpr int EPI_BYTES = 4 * 32 * EPI_PITCH * 4;
-  static constexpr int TMEM_COLS = 2 * Base::NR;  // two accumulators
+  static constexpr int ACC_STRIDE = pow2_at_least(Base::NR);  // columns between accumulators
+  static constexpr int TMEM_COLS = 2 * ACC_STRIDE;              // two accumulators
   static constexpr int SMEM_USED = ST * Base::STAGE + EPI_BYTES + 1024 /*align*/ + 256 /*barriers*/;
   // at least 120 KB, so that one CTA occupies an SM (two CTAs' TMEM accumulators could exceed
   // the SM's 512 columns, and a CTA waiting in tcgen05.alloc for a persistent neighbour would
@@ -819,7 +822,7 @@ __global__ void __maxnreg__((PCfg<BNC, NP, ST>::MAXREG))
         const int b = (int)(u & 1);
         if (!mbar_wait(smem_u32(&acc_empty[b]), (uint32_t)((u >> 1) & 1) ^ 1u)) { ok = false; break; }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t acc_t = tmem + (uint32_t)(b * Cfg::NR);
+        const uint32_t acc_t = tmem + (uint32_t)(b * PC::ACC_STRIDE);
         for (int it = 0; it < tk.nkb; ++it, ++g) {
           const int s = (int)(g % kStages);
           const uint32_t ph = (uint32_t)(g / kStages) & 1u;
@@ -863,7 +866,7 @@ __global__ void __maxnreg__((PCfg<BNC, NP, ST>::MAXREG))
         if (!mbar_wait(smem_u32(&acc_full[b]), (uint32_t)((u >> 1) & 1))) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       }
-      const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * Cfg::NR);
+      const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * PC::ACC_STRIDE);
 #pragma unroll 1
       for (int j = 0; j < Cfg::NR / 32; ++j) {
         uint32_t v[32];
@@ -985,10 +988,11 @@ void launch_tc(const TcParams& p, int64_t batch, cudaStream_t s) {
 }
 
 // Tile configurations: (BNC, producer threads, stages), 0-5 with one tile per CTA
-// (k_tc_cgemm) and 6-11 the same tiles in the persistent kernel.  Every configuration forms
-// the same products in the same K order, so the results are identical and only the speed
-// differs.
-constexpr int kNumCfg = 12;
+// (k_tc_cgemm) and 6-11 the same tiles in the persistent kernel; 12-15 the 96-column tile
+// (UMMA N = 192: products with N = nb = 96 in one column tile, each A block staged once) in
+// both forms.  Every configuration forms the same products in the same K order, so the
+// results are identical and only the speed differs.
+constexpr int kNumCfg = 16;
 
 template <bool A64, bool B64>
 void launch_cfg(int cfg, const TcParams& p, int64_t batch, cudaStream_t s) {
@@ -999,6 +1003,10 @@ void launch_cfg(int cfg, const TcParams& p, int64_t batch, cudaStream_t s) {
     case 9: return launch_tc_persistent<32, 256, 2, A64, B64>(p, batch, s);
     case 10: return launch_tc_persistent<64, 256, 2, A64, B64>(p, batch, s);
     case 11: return launch_tc_persistent<128, 256, 2, A64, B64>(p, batch, s);
+    case 12: return launch_tc<96, 128, 1, A64, B64>(p, batch, s);
+    case 13: return launch_tc<96, 256, 2, A64, B64>(p, batch, s);
+    case 14: return launch_tc_persistent<96, 128, 1, A64, B64>(p, batch, s);
+    case 15: return launch_tc_persistent<96, 256, 2, A64, B64>(p, batch, s);
     default: break;
   }
   switch (cfg) {
@@ -1014,6 +1022,7 @@ void launch_cfg(int cfg, const TcParams& p, int64_t batch, cudaStream_t s) {
 // Default choice: short K gets one stage and four producer warps (several CTAs per SM), long
 // K two stages and eight producer warps; the tile width follows N.
 int heuristic_cfg(const TcParams& p) {
+  if (p.N > 64 && p.N <= 96) return p.K <= 64 ? 12 : 13;  // one 96-column tile
   const int w = p.N >= 128 ? 2 : (p.N > 32 ? 1 : 0);
   return (p.K <= 64 ? 0 : 3) + w;
 }

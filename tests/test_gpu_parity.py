@@ -229,9 +229,9 @@ def test_errors_are_codes_not_aborts(base):
 
 
 def test_every_tile_configuration_gives_identical_results(base):
-    """Four or eight producer warps, one or two stages, 32 to 128 columns: each configuration
-    forms the same products in the same K order, so a whole GW iteration agrees bit for bit
-    whichever configuration every GEMM is pinned to."""
+    """Four or eight producer warps, one or two stages, 32, 64, 96 or 128 columns, one tile per
+    CTA or persistent: each configuration forms the same products in the same K order, so a
+    whole GW iteration agrees bit for bit whichever configuration every GEMM is pinned to."""
     c = base.ctx(capi.MIXED)
     ref = None
     try:
