@@ -81,6 +81,29 @@ def test_ibz_pi_w_sigma_rpa(kind, grid, mode, tol):
 
 
 @pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
+def test_ibz_sigma_with_partial_projection_cache(mode, tol):
+    """The IBZ self-energy reads the projected-G cache slice by slice. With every slice, with
+    the first tau chunk only (16 of 24 tau pairs on 16 k-points) and with none cached, it gives
+    the same Sigma."""
+    b = case("swap", (4, 4, 1))
+    c = b.ctx(mode)
+    G = b.d["G_ibz"]
+    nk, Np, nt = b.sym["nk"], b.d["X"].shape[2], b.ft.nt_f
+    nth = (nt + 1) // 2
+    chunk = min(nth, max(4, -(-256 // nk)))
+    assert chunk < nth  # more than one tau chunk, so one chunk is a partial cache
+    slab = nk * Np * Np * (16 if mode == capi.FP64 else 8)
+    res = []
+    for limit in (-1, 2 * chunk * slab, 0):
+        c.set_gcache_limit(limit)
+        S, _ = c.gw_iteration(G)
+        res.append(S)
+    assert maxabs(res[0], b.Sigma) < tol
+    assert maxabs(res[1], res[0]) < 1e-12
+    assert maxabs(res[2], res[0]) < 1e-12
+
+
+@pytest.mark.parametrize("mode,tol", MODES, ids=MODE_IDS)
 def test_time_reversal_ibz_sigma_is_the_full_bz_sigma(mode, tol):
     # with time reversal the IBZ path reproduces the full-BZ path of the same context at the
     # IBZ k-points (and the RPA energy); back on the full-BZ path after set_symmetry(None)
