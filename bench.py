@@ -211,9 +211,10 @@ def algorithmic_work(w, s, ft):
         "sigma_fused": ("hbm", 5 * nk * ncol * 8, None),
         "dft_w": ("hbm", 2 * nth * nk * ncol * 8, None),
         "ir_transform": ("hbm", (nth + nwh) * nk * ncol * 8, None),
-        # M = L^H Pi L: P1 = L^H Pi (L^H triangular, Np^3 / 2) and the lower triangle of
-        # L^H P1^H (Np^3 / 6) complex multiply-adds
-        "dyson_M_gemm": ("tensor", None, (0.5 + 1 / 6) * 8 * n3 * P),
+        # M = L^H Pi L: the part of P1 = L^H Pi on and above the diagonal (Np^3 / 3; the
+        # lower triangle of M reads no other) and the lower triangle of L^H P1^H (Np^3 / 6)
+        # complex multiply-adds
+        "dyson_M_gemm": ("tensor", None, (1 / 3 + 1 / 6) * 8 * n3 * P),
         # lower triangles of F = D^H D (1/6), T = L E (1/3) and W = T L^H (1/6)
         "dyson_W_gemm": ("tensor", None, (1 / 6 + 1 / 3 + 1 / 6) * 8 * n3 * P),
         # FP64 Cholesky (Np^3 / 6 complex multiply-adds) + inverse of the 128 x 128 diagonal

@@ -173,6 +173,7 @@ void batch_gw(Batch* b) {
     const int64_t Np = b->Np[m], NN = Np * Np;
     cq::TcStructure s1;
     s1.a_upper = true;
+    s1.upper_zero = true;  // M's lower triangle reads P1 on and above the diagonal only
     p1.push_back(group(b->LHs.p + b->offL[m], false, false, Np, 0, b->PW.p + b->offPQ[m], false, true,
                        Np, cols, b->T1.p + b->offD[m], Np, NN, Np, Np, Np, nwh, s1));
     cq::TcStructure s2;  // M = L^H (P1)^H, P1 = L^H Pi (Pi Hermitian)

@@ -272,8 +272,12 @@ void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t 
       Prof::Scope sc(a.prof, "dyson_M_gemm");
       if (a.mixed) {
         // P1 = L^H Pi  (Pi Hermitian: B(k, n) = Pi[k][n] = conj(Pi[n][k]))
+        // Only P1's tiles on and above the diagonal are needed: the lower triangle of M reads
+        // Q = P1^H at (a, j) with a >= i >= j.  The others are written as zeros, which only
+        // meet the zeros of L^H in the next product (Np^3 / 3 products instead of Np^3 / 2).
         TcStructure s1;
         s1.a_upper = true;  // L^H upper triangular
+        s1.upper_zero = true;
         s1.a_mod = nq;
         s1.a_q0 = q0;
         tc_cgemm_nt(LHc, false, false, Np, NN, Pi, false, true, Np, NN, (float2*)T1, Np, NN, Np,
@@ -295,6 +299,7 @@ void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t 
         z1.lda = Np;
         z1.sA = NN;
         z1.a_upper = true;
+        z1.upper_zero = true;  // as in the mixed form: P1's upper tiles are the ones M reads
         z1.a_mod = nq;
         z1.a_q0 = q0;
         z1.B = (const double2*)Pi;
@@ -306,6 +311,7 @@ void dyson_run(const DysonArgs& a, DevBuf<unsigned char>& scratch, cudaStream_t 
         z1.batch = nb;
         zgemm(z1, s);
         ZgemmArgs z2 = z1;
+        z2.upper_zero = false;
         z2.opB = 'C';
         z2.B = (const double2*)T1;
         z2.C = (double2*)Mb;

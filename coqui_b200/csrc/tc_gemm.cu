@@ -91,6 +91,7 @@ struct TcParams {
   int a64, b64;  // element type is complex128
   int conj_a, conj_b;
   int a_upper, a_lower, b_lower, b_upper, lower_only;
+  int upper_zero;        // tiles strictly below the diagonal: zeros, no products
   int a_ident, b_ident;  // operand + identity (complex64 operands only)
   // every row of the operand starts 16-byte aligned at even K (vector loads allowed)
   int a_al, b_al;
@@ -418,6 +419,7 @@ __device__ __forceinline__ void tc_tile(const TcParams& p, int64_t bz, int64_t m
   if (p.b_lower) kb_lo = max(kb_lo, (int)(n0 / 16));
   if (p.a_lower) kb_hi = min(kb_hi, (int)((m0 + kBM - 1) / 16) + 1);
   if (p.b_upper) kb_hi = min(kb_hi, (int)((n0 + BNC - 1) / 16) + 1);
+  if (p.upper_zero && m0 > n0 + BNC - 1) kb_hi = kb_lo;  // written as zeros
   const int nkb = max(kb_hi - kb_lo, 0);
 
   if (threadIdx.x == 0) {
@@ -665,6 +667,7 @@ __device__ __forceinline__ TileK tile_k(const TcParams& p, int64_t m0, int64_t n
   if (p.b_lower) kb_lo = max(kb_lo, (int)(n0 / 16));
   if (p.a_lower) kb_hi = min(kb_hi, (int)((m0 + kBM - 1) / 16) + 1);
   if (p.b_upper) kb_hi = min(kb_hi, (int)((n0 + bnc - 1) / 16) + 1);
+  if (p.upper_zero && m0 > n0 + bnc - 1) kb_hi = kb_lo;  // written as zeros
   t.kb_lo = kb_lo;
   t.nkb = max(kb_hi - kb_lo, 0);
   return t;
@@ -1053,7 +1056,7 @@ void dispatch_n(const TcParams& p, int64_t batch, cudaStream_t s) {
   int64_t bb = 1;
   while (bb < batch) bb <<= 1;  // batch class: next power of two
   const std::vector<int64_t> key = {p.M, p.N, p.K, bb, A64, B64, p.conj_a, p.conj_b, p.a_upper,
-                                    p.a_lower, p.b_lower, p.b_upper, p.lower_only};
+                                    p.a_lower, p.b_lower, p.b_upper, p.lower_only, p.upper_zero};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(key);
@@ -1115,6 +1118,7 @@ void tc_cgemm_nt(const void* A, bool a_split, bool conj_a, int64_t lda, int64_t 
   p.b_lower = st.b_lower;
   p.b_upper = st.b_upper;
   p.lower_only = st.lower_only;
+  p.upper_zero = st.upper_zero;
   CQ_REQUIRE(!(st.a_ident && a_c128) && !(st.b_ident && b_c128), COQUI_B200_EINVAL,
              "tc_cgemm: identity shift needs a complex64 operand");
   p.a_ident = st.a_ident;
@@ -1329,6 +1333,7 @@ TcParams make_params(const TcGroup& g) {
   p.b_lower = g.st.b_lower;
   p.b_upper = g.st.b_upper;
   p.lower_only = g.st.lower_only;
+  p.upper_zero = g.st.upper_zero;
   p.a_ident = g.st.a_ident;
   p.b_ident = g.st.b_ident;
   p.a_al = rows_aligned(g.A, g.a_split, g.lda, g.sA);

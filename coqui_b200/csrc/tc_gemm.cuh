@@ -57,6 +57,9 @@ void to_c64(const double2* in, float2* out, int64_t rows, int64_t cols, int64_t 
 // the operand's own diagonal (m == k for A, n == k for B); complex64 operands only.
 struct TcStructure {
   bool a_upper = false, a_lower = false, b_lower = false, b_upper = false, lower_only = false;
+  // tiles strictly below the diagonal are written as zeros without products (their entries
+  // are not needed, and a later product may still read them)
+  bool upper_zero = false;
   bool a_ident = false, b_ident = false;
   int64_t a_mod = 0, a_q0 = 0, b_mod = 0, b_q0 = 0;
 };

@@ -34,7 +34,7 @@ struct ZP {
   const double2* const* Bp;
   double2* const* Cp;
   int64_t b0;
-  int a_upper, a_lower, b_lower, b_upper, lower_only;
+  int a_upper, a_lower, b_lower, b_upper, lower_only, upper_zero;
   int64_t a_mod, a_q0, b_mod, b_q0;
 };
 
@@ -92,7 +92,8 @@ __global__ void __launch_bounds__(NT, 2) k_zgemm(const __grid_constant__ ZP p) {
   if (p.a_lower) khi = min(khi, m0 + TM);
   if (p.b_upper) khi = min(khi, n0 + TN);
   klo = klo / TK * TK;
-  const int ns = khi > klo ? (int)((khi - klo + TK - 1) / TK) : 0;
+  const bool zero_tile = p.upper_zero && m0 > n0 + TN - 1;  // written as zeros
+  const int ns = (khi > klo && !zero_tile) ? (int)((khi - klo + TK - 1) / TK) : 0;
 
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31, g = l >> 2, q = l & 3;
   const int wm = w / WN, wn = w % WN;
@@ -222,6 +223,7 @@ void zgemm(const ZgemmArgs& a, cudaStream_t s) {
   p.b_lower = a.b_lower;
   p.b_upper = a.b_upper;
   p.lower_only = a.lower_only;
+  p.upper_zero = a.upper_zero;
   p.a_mod = a.a_mod;
   p.a_q0 = a.a_q0;
   p.b_mod = a.b_mod;

@@ -28,6 +28,8 @@ struct ZgemmArgs {
   // structure: op(A) upper (k >= m) / lower (k <= m) triangular, op(B) lower (k >= n) /
   // upper (k <= n) triangular; lower_only: only tiles on or below the diagonal are formed
   bool a_upper = false, a_lower = false, b_lower = false, b_upper = false, lower_only = false;
+  // upper_zero: tiles strictly below the diagonal are written as zeros without products
+  bool upper_zero = false;
   // periodic batch index of A / B (0 = off): problem b uses operand (q0 + b) % mod, for
   // per-q operands of problems ordered (frequency, q)
   int64_t a_mod = 0, a_q0 = 0, b_mod = 0, b_q0 = 0;
