@@ -160,6 +160,44 @@ def test_bench_cpu_sample_counts_and_scaling():
     assert abs(total - sum(parts.values())) < 1e-9 * total
 
 
+def test_bench_group_rates_count_projection_problems():
+    """Kernel-group rates: the projections count flops per (tau, k) problem the library
+    reports (a G(tau) projected again for the self-energy counts again); per-iteration and
+    per-launch amounts are unchanged; groups without an amount get no rate."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    from coqui_b200.iaft import IAFT
+    from coqui_b200.synthetic import make_system
+
+    s = make_system(2, 8, 4, 32, seed=3)
+    ft = IAFT(1000.0, 10.0, "low")
+    work = bench.algorithmic_work(None, s, ft)
+    per_problem = bench.gemm_flops_c(s.Np, s.nb, s.nb) + bench.gemm_flops_c(s.Np, s.Np, s.nb)
+    assert work["proj_p2a"][3] == per_problem
+    steps, problems = 2, 3 * s.nk
+    stats = {"proj_p2a": (4.0, 6), "pi_fused": (2.0, 4), "dyson_M_gemm": (1.0, 2),
+             "other": (1.0, 2)}
+    g = bench.group_rates(stats, steps, work, 6000.0, 1600.0, 30.0, 29.0,
+                          units={"proj_p2a": problems * steps})
+    assert g["proj_p2a"]["units_per_step"] == problems
+    tflops = per_problem * problems / (2.0e-3) / 1e12
+    assert abs(g["proj_p2a"]["achieved_TFLOPs"] - tflops) < 1e-9 * tflops
+    # per launch group (bytes) and per iteration (flops)
+    gbps = work["pi_fused"][1] * 2 / (1.0e-3) / 1e9
+    assert abs(g["pi_fused"]["achieved_GBps"] - gbps) < 1e-9 * gbps
+    mf = work["dyson_M_gemm"][2] / (0.5e-3) / 1e12
+    assert abs(g["dyson_M_gemm"]["achieved_TFLOPs"] - mf) < 1e-9 * mf
+    # the M products count the part of P1 on and above the diagonal: Np^3 / 3 + Np^3 / 6
+    P = s.nk * ft.nw_half
+    assert abs(work["dyson_M_gemm"][2] - 0.5 * 8 * float(s.Np) ** 3 * P) < 1e-6 * work["dyson_M_gemm"][2]
+    assert "achieved_TFLOPs" not in g["other"] and "achieved_GBps" not in g["other"]
+    # without reported units the projection group has no rate rather than a guessed one
+    g0 = bench.group_rates(stats, steps, work, 6000.0, 1600.0, 30.0)
+    assert "achieved_TFLOPs" not in g0["proj_p2a"]
+
+
 def test_truncated_ir_table_is_an_error(tmp_path, monkeypatch):
     """A damaged IR table is refused when it is loaded, before any device work."""
     import shutil
