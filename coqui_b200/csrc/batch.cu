@@ -68,6 +68,8 @@ using cq::DevBuf;
 struct coqui_b200_batch {
   int dev = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;  // the one-CTA factorisations beside the tiled ones
+  cudaEvent_t fork = nullptr, join = nullptr;
   std::string err;
   int64_t nmol = 0, nt = 0, nth = 0, nwb = 0, nwh = 0, nmax = 0;
   std::vector<int64_t> nb, Np;
@@ -83,7 +85,8 @@ struct coqui_b200_batch {
   DevBuf<float2> T1, Mb, Zb, Zl;
   DevBuf<double2> Ab;
   DevBuf<int64_t> dofG, dnb;
-  DevBuf<unsigned char> gtab, ctab, htab;
+  DevBuf<unsigned char> gtab, ctab, ctab2, htab;
+  std::vector<int64_t> chol_perm;  // factorisation list position -> (molecule, iW) problem
   DevBuf<int> info;
   DevBuf<double> ld;
   DevBuf<double2> tr;
@@ -107,10 +110,12 @@ template <typename F> int bguarded(Batch* b, F&& f) {
     return COQUI_B200_OK;
   } catch (const cq::Error& e) {
     b->err = e.what();
+    if (b->st2) (void)cudaStreamSynchronize(b->st2);
     if (b->st) (void)cudaStreamSynchronize(b->st);
     return e.code;
   } catch (const std::exception& e) {
     b->err = e.what();
+    if (b->st2) (void)cudaStreamSynchronize(b->st2);
     if (b->st) (void)cudaStreamSynchronize(b->st);
     return COQUI_B200_EINVAL;
   }
@@ -202,10 +207,51 @@ void batch_gw(Batch* b) {
   // later level needs it, Zc = -C off the groups (in T1), S in Mb.
   std::vector<int64_t> sizes;
   for (const auto& c : cp) sizes.push_back(c.n);
-  if (cq::chol_prefer_tiled(sizes))  // the largest molecules spread over many CTAs each
-    cq::launch_chol_tiled(cp, b->ctab, b->ld.p, b->tr.p, b->info.p, s);
-  else
+  b->chol_perm.resize(nprob);
+  for (int64_t i = 0; i < nprob; ++i) b->chol_perm[i] = i;
+  if (cq::chol_prefer_tiled(sizes)) {
+    // The largest molecules spread over many CTAs each (the tiled form, on this stream).
+    // A molecule whose problems one CTA finishes within the time the tiled form needs for the
+    // larger ones (n^3 x wave <= the larger molecules' sum of n^3) runs one CTA per problem on
+    // the second stream at the same time, in the SMs that the tiled form's late block columns
+    // (only the largest problems left) leave idle.  Same results either way.
+    std::vector<int64_t> order(b->nmol);
+    for (int64_t m = 0; m < b->nmol; ++m) order[m] = m;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t x, int64_t y) { return b->Np[x] > b->Np[y]; });
+    const double wave = (double)cq::chol_wave_size();
+    auto cube = [&](int64_t m) { return (double)b->Np[m] * (double)b->Np[m] * (double)b->Np[m]; };
+    double large = 0;
+    for (int64_t m = 0; m < b->nmol; ++m) large += (double)nwh * cube(m);
+    int64_t nlarge = b->nmol;
+    while (nlarge > 1) {
+      const int64_t m = order[nlarge - 1];
+      if (cube(m) * wave > large - (double)nwh * cube(m)) break;
+      large -= (double)nwh * cube(m);
+      --nlarge;
+    }
+    std::vector<cq::CholProblem> big, small;
+    int64_t pos = 0;
+    for (int64_t i = 0; i < b->nmol; ++i) {
+      const int64_t m = order[i];
+      for (int64_t w = 0; w < nwh; ++w) {
+        (i < nlarge ? big : small).push_back(cp[m * nwh + w]);
+        b->chol_perm[pos++] = m * nwh + w;
+      }
+    }
+    const int64_t nb0 = (int64_t)big.size();
+    if (!small.empty()) {
+      CQ_CHECK_CUDA(cudaEventRecord(b->fork, s));
+      CQ_CHECK_CUDA(cudaStreamWaitEvent(b->st2, b->fork, 0));
+      cq::launch_chol_inv_grouped(small, b->ctab2, b->ld.p + nb0, b->tr.p + nb0,
+                                  b->info.p + nb0, b->st2, true);
+      CQ_CHECK_CUDA(cudaEventRecord(b->join, b->st2));
+    }
+    cq::launch_chol_tiled(big, b->ctab, b->ld.p, b->tr.p, b->info.p, s);
+    if (!small.empty()) CQ_CHECK_CUDA(cudaStreamWaitEvent(s, b->join, 0));
+  } else {
     cq::launch_chol_inv_grouped(cp, b->ctab, b->ld.p, b->tr.p, b->info.p, s, true);
+  }
   for (int64_t m = 0; m < b->nmol; ++m)
     cq::launch_chol_split(b->Ab.p + b->offD[m], b->Zb.p + b->offD[m], b->Zl.p + b->offD[m],
                           b->T1.p + b->offD[m], b->Np[m], nwh, s);
@@ -308,7 +354,8 @@ void batch_gw(Batch* b) {
   CQ_CHECK_CUDA(cudaStreamSynchronize(s));
   for (int64_t i = 0; i < nprob; ++i)
     CQ_REQUIRE(info[i] == 0, COQUI_B200_ENOTHPD,
-               "I - L^H Pi L is not positive definite (problem " + std::to_string(i) + ")");
+               "I - L^H Pi L is not positive definite (problem " +
+                   std::to_string(b->chol_perm[i]) + ")");
 }
 
 }  // namespace
@@ -325,7 +372,14 @@ int coqui_b200_batch_create(coqui_b200_batch** out, int64_t nmol, const int64_t*
   if (!b) return COQUI_B200_ENOMEM;
   b->dev = device;
   int rc = bguarded(b, [&] {
-    CQ_CHECK_CUDA(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+    // the main stream (the tiled factorisation's phases among its work) takes precedence over
+    // the one-CTA factorisations that fill the SMs beside them
+    int prio_least = 0, prio_greatest = 0;
+    CQ_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+    CQ_CHECK_CUDA(cudaStreamCreateWithPriority(&b->st, cudaStreamNonBlocking, prio_greatest));
+    CQ_CHECK_CUDA(cudaStreamCreateWithPriority(&b->st2, cudaStreamNonBlocking, prio_least));
+    CQ_CHECK_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    CQ_CHECK_CUDA(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming));
     CQ_CHECK_CUDA(cudaEventCreate(&b->ev0));
     CQ_CHECK_CUDA(cudaEventCreate(&b->ev1));
     b->nmol = nmol;
@@ -386,12 +440,16 @@ int coqui_b200_batch_create(coqui_b200_batch** out, int64_t nmol, const int64_t*
 void coqui_b200_batch_destroy(coqui_b200_batch* b) {
   if (!b) return;
   cudaSetDevice(b->dev);
+  if (b->st2) cudaStreamSynchronize(b->st2);
   if (b->st) cudaStreamSynchronize(b->st);
-  cudaStream_t st = b->st;
+  cudaStream_t st = b->st, st2 = b->st2;
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->join) cudaEventDestroy(b->join);
   delete b;
   if (st) cudaStreamDestroy(st);
+  if (st2) cudaStreamDestroy(st2);
 }
 
 double coqui_b200_batch_last_ms(const coqui_b200_batch* b) { return b ? b->last_ms : 0.0; }
