@@ -91,14 +91,19 @@ struct TiledRuns {
 constexpr int kTiledG = (int)(kInvGroup / b32::CB);  // blocks per diagonal inverse group
 
 // work items of one launch: kind 0 diagonal block j (one per problem), 1 panel blocks below
-// it, 2 trailing blocks (i, k) with j < k <= i, 3 inverse columns (all columns that have a
-// block below them in their group; j is not used)
+// it, 2 trailing blocks (i, k) with j + 2 <= k <= i, updated by block columns j and j + 1
+// together, 3 inverse columns (all columns that have a block below them in their group; j is
+// not used), 4 the blocks (i, j + 1), i > j, of block column j + 1 updated by column j.
+// Columns are taken in pairs: diagonal j, panel j, column j + 1 by j, diagonal j + 1, panel
+// j + 1, then the trailing blocks by both; the products and their order are those of one
+// column at a time, and the trailing matrix is read and written once per pair.
 __host__ __device__ inline int64_t tiled_items(int kind, int64_t nblk, int j) {
   const int64_t m = nblk - j - 1;
   switch (kind) {
     case 0: return nblk > j ? 1 : 0;
     case 1: return m > 0 ? m : 0;
-    case 2: return m > 0 ? m * (m + 1) / 2 : 0;
+    case 2: return m - 1 > 0 ? (m - 1) * m / 2 : 0;
+    case 4: return m > 0 ? m : 0;
     default: return nblk - (nblk + kTiledG - 1) / kTiledG;
   }
 }
@@ -132,7 +137,9 @@ __global__ void __launch_bounds__(b32::CT, b32::MINB)
     while ((a + 1) * (a + 2) / 2 <= local) ++a;
     while (a * (a + 1) / 2 > local) --a;
     const int64_t b = local - a * (a + 1) / 2;
-    b32::tiled_update(M, A, n, j, j + 1 + (int)a, j + 1 + (int)b);
+    b32::tiled_update2(M, A, n, j, j + 2 + (int)a, j + 2 + (int)b);
+  } else if (kind == 4) {
+    b32::tiled_update(M, A, n, j, j + 1 + (int)local, j + 1);
   } else {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* S0 = reinterpret_cast<double2*>(smem_raw);
@@ -197,8 +204,16 @@ void run_tiled(const CholProblem* t, const TiledRuns& R, int64_t np, double* log
     count_launch();
     CQ_CHECK_CUDA(cudaGetLastError());
   };
-  for (int j = 0; j < maxblk; ++j)
-    for (int kind = 0; kind < 3; ++kind) go(kind, j);
+  for (int j = 0; j < maxblk; j += 2) {
+    go(0, j);
+    go(1, j);
+    if (j + 1 < maxblk) {
+      go(4, j);
+      go(0, j + 1);
+      go(1, j + 1);
+      go(2, j);
+    }
+  }
   go(3, 0);
 }
 

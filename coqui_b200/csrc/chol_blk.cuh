@@ -445,6 +445,38 @@ __device__ void tiled_update(const float2* M, double2* A, int64_t n, int j, int 
     }
 }
 
+// tiled_update for the two block columns j and j + 1 at once (j + 1 < nblk): the same two
+// rank-CB updates in the same order, with the block held in FP64 registers in between rather
+// than stored and reloaded, so the trailing matrix is read and written once per two columns.
+__device__ void tiled_update2(const float2* M, double2* A, int64_t n, int j, int ib, int kb) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* S0 = reinterpret_cast<double2*>(smem_raw);
+  double2* S1 = S0 + CB * PITCH;
+  const int64_t j0 = (int64_t)j * CB, j1 = j0 + CB, i0 = (int64_t)ib * CB, k0 = (int64_t)kb * CB;
+  const int jb0 = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
+  const int jb1 = (int)(CB < (n - j1) ? (int64_t)CB : (n - j1));
+  const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
+  const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
+  load_blk(S0, A, n, i0, j0, rb, jb0);
+  load_blk(S1, A, n, k0, j0, kbsz, jb0);
+  double2 acc[AR][AC];
+  acc_init(acc, A, M, j == 0, n, i0, k0, rb, kbsz, ib > kb);
+  __syncthreads();
+  mma_tile_sub(S0, S1, jb0, acc);
+  __syncthreads();  // every warp is done with column j's blocks
+  load_blk(S0, A, n, i0, j1, rb, jb1);
+  load_blk(S1, A, n, k0, j1, kbsz, jb1);
+  __syncthreads();
+  mma_tile_sub(S0, S1, jb1, acc);
+#pragma unroll
+  for (int i = 0; i < AR; ++i)
+#pragma unroll
+    for (int jj = 0; jj < AC; ++jj) {
+      const int r = acc_row(i, jj), c = acc_col(i, jj);
+      if (r < rb && c < kbsz && (ib > kb || c <= r)) A[(i0 + r) * n + k0 + c] = acc[i][jj];
+    }
+}
+
 // inv_group: the inverse is formed within diagonal groups of inv_group blocks only (the
 // whole matrix when inv_group >= nblk); the tensor-core levels fill in the rest.
 // One problem: M, A (n x n), results at logdet/trace/info[0].
