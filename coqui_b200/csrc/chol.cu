@@ -90,32 +90,43 @@ struct TiledRuns {
 };
 constexpr int kTiledG = (int)(kInvGroup / b32::CB);  // blocks per diagonal inverse group
 
+// Block columns are taken in groups of kTiledCols: for each column of a group, its blocks are
+// updated by the group's earlier columns, then its diagonal block and panel are factored; then
+// the trailing blocks get the whole group's updates in one pass.  The products and their
+// order are those of one column at a time; the trailing matrix is read and written once per
+// group.
+constexpr int kTiledCols = 8;
+
 // work items of one launch: kind 0 diagonal block j (one per problem), 1 panel blocks below
-// it, 2 trailing blocks (i, k) with j + 2 <= k <= i, updated by block columns j and j + 1
-// together, 3 inverse columns (all columns that have a block below them in their group; j is
-// not used), 4 the blocks (i, j + 1), i > j, of block column j + 1 updated by column j.
-// Columns are taken in pairs: diagonal j, panel j, column j + 1 by j, diagonal j + 1, panel
-// j + 1, then the trailing blocks by both; the products and their order are those of one
-// column at a time, and the trailing matrix is read and written once per pair.
-__host__ __device__ inline int64_t tiled_items(int kind, int64_t nblk, int j) {
+// it, 2 trailing blocks (i, k) with j + cols <= k <= i, updated by the block columns j ..
+// j + cols - 1, 3 inverse columns (all columns that have a block below them in their group;
+// j is not used), 4 the blocks (i, j + cols), i >= j + cols, of block column j + cols updated
+// by the columns j .. j + cols - 1.
+__host__ __device__ inline int64_t tiled_items(int kind, int64_t nblk, int j, int cols) {
   const int64_t m = nblk - j - 1;
   switch (kind) {
     case 0: return nblk > j ? 1 : 0;
     case 1: return m > 0 ? m : 0;
-    case 2: return m - 1 > 0 ? (m - 1) * m / 2 : 0;
-    case 4: return m > 0 ? m : 0;
+    case 2: {
+      const int64_t t = nblk - j - cols;
+      return t > 0 ? t * (t + 1) / 2 : 0;
+    }
+    case 4: {
+      const int64_t t = nblk - j - cols;
+      return t > 0 ? t : 0;
+    }
     default: return nblk - (nblk + kTiledG - 1) / kTiledG;
   }
 }
 
 __global__ void __launch_bounds__(b32::CT, b32::MINB)
     k_chol_tiled(const CholProblem* __restrict__ probs, const __grid_constant__ TiledRuns R, int kind,
-                 int j, double* __restrict__ logdet, int* __restrict__ info) {
+                 int j, int cols, double* __restrict__ logdet, int* __restrict__ info) {
   int64_t idx = blockIdx.x, local = 0, nblk = 0;
   int p = -1;
   for (int r = 0; r < R.nrun; ++r) {
     const int64_t nb = (R.n[r] + b32::CB - 1) / b32::CB;
-    const int64_t per = tiled_items(kind, nb, j), tot = per * R.count[r];
+    const int64_t per = tiled_items(kind, nb, j, cols), tot = per * R.count[r];
     if (idx < tot) {
       p = R.first[r] + (int)(idx / per);
       local = idx % per;
@@ -137,9 +148,9 @@ __global__ void __launch_bounds__(b32::CT, b32::MINB)
     while ((a + 1) * (a + 2) / 2 <= local) ++a;
     while (a * (a + 1) / 2 > local) --a;
     const int64_t b = local - a * (a + 1) / 2;
-    b32::tiled_update2(M, A, n, j, j + 2 + (int)a, j + 2 + (int)b);
+    b32::tiled_update_cols(M, A, n, j, cols, j + cols + (int)a, j + cols + (int)b);
   } else if (kind == 4) {
-    b32::tiled_update(M, A, n, j, j + 1 + (int)local, j + 1);
+    b32::tiled_update_cols(M, A, n, j, cols, j + cols + (int)local, j + cols);
   } else {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* S0 = reinterpret_cast<double2*>(smem_raw);
@@ -194,27 +205,26 @@ void run_tiled(const CholProblem* t, const TiledRuns& R, int64_t np, double* log
   }
   int64_t maxblk = 0;
   for (int r = 0; r < R.nrun; ++r) maxblk = std::max<int64_t>(maxblk, (R.n[r] + b32::CB - 1) / b32::CB);
-  auto go = [&](int kind, int j) {
+  auto go = [&](int kind, int j, int cols) {
     int64_t grid = 0;
     for (int r = 0; r < R.nrun; ++r)
-      grid += tiled_items(kind, (R.n[r] + b32::CB - 1) / b32::CB, j) * R.count[r];
+      grid += tiled_items(kind, (R.n[r] + b32::CB - 1) / b32::CB, j, cols) * R.count[r];
     if (grid == 0) return;
     CQ_REQUIRE(grid <= 2147483647, COQUI_B200_EINVAL, "tiled Cholesky: too many blocks");
-    k_chol_tiled<<<(unsigned)grid, b32::CT, smem, s>>>(t, R, kind, j, logdet, info);
+    k_chol_tiled<<<(unsigned)grid, b32::CT, smem, s>>>(t, R, kind, j, cols, logdet, info);
     count_launch();
     CQ_CHECK_CUDA(cudaGetLastError());
   };
-  for (int j = 0; j < maxblk; j += 2) {
-    go(0, j);
-    go(1, j);
-    if (j + 1 < maxblk) {
-      go(4, j);
-      go(0, j + 1);
-      go(1, j + 1);
-      go(2, j);
+  for (int j = 0; j < maxblk; j += kTiledCols) {
+    const int g = (int)std::min<int64_t>(kTiledCols, maxblk - j);
+    for (int c = 0; c < g; ++c) {
+      if (c > 0) go(4, j, c);  // column j + c by the group's columns j .. j + c - 1
+      go(0, j + c, 0);
+      go(1, j + c, 0);
     }
+    go(2, j, g);  // the trailing blocks by the whole group
   }
-  go(3, 0);
+  go(3, 0, 0);
 }
 
 // Form of the one-CTA factorisation, COQUI_B200_CHOL_ORDER: "pair" (default: four warps,

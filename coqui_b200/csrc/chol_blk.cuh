@@ -445,29 +445,28 @@ __device__ void tiled_update(const float2* M, double2* A, int64_t n, int j, int 
     }
 }
 
-// tiled_update for the two block columns j and j + 1 at once (j + 1 < nblk): the same two
-// rank-CB updates in the same order, with the block held in FP64 registers in between rather
-// than stored and reloaded, so the trailing matrix is read and written once per two columns.
-__device__ void tiled_update2(const float2* M, double2* A, int64_t n, int j, int ib, int kb) {
+// tiled_update for the block columns j .. j + cols - 1 at once: the same rank-CB updates in
+// the same order, with the block held in FP64 registers in between rather than stored and
+// reloaded, so the block is read and written once for all of them.
+__device__ void tiled_update_cols(const float2* M, double2* A, int64_t n, int j, int cols, int ib,
+                                  int kb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* S0 = reinterpret_cast<double2*>(smem_raw);
   double2* S1 = S0 + CB * PITCH;
-  const int64_t j0 = (int64_t)j * CB, j1 = j0 + CB, i0 = (int64_t)ib * CB, k0 = (int64_t)kb * CB;
-  const int jb0 = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
-  const int jb1 = (int)(CB < (n - j1) ? (int64_t)CB : (n - j1));
+  const int64_t i0 = (int64_t)ib * CB, k0 = (int64_t)kb * CB;
   const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
   const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
-  load_blk(S0, A, n, i0, j0, rb, jb0);
-  load_blk(S1, A, n, k0, j0, kbsz, jb0);
   double2 acc[AR][AC];
   acc_init(acc, A, M, j == 0, n, i0, k0, rb, kbsz, ib > kb);
-  __syncthreads();
-  mma_tile_sub(S0, S1, jb0, acc);
-  __syncthreads();  // every warp is done with column j's blocks
-  load_blk(S0, A, n, i0, j1, rb, jb1);
-  load_blk(S1, A, n, k0, j1, kbsz, jb1);
-  __syncthreads();
-  mma_tile_sub(S0, S1, jb1, acc);
+  for (int c = 0; c < cols; ++c) {
+    const int64_t jc = (int64_t)(j + c) * CB;
+    const int jb = (int)(CB < (n - jc) ? (int64_t)CB : (n - jc));
+    if (c > 0) __syncthreads();  // every warp is done with the previous column's blocks
+    load_blk(S0, A, n, i0, jc, rb, jb);
+    load_blk(S1, A, n, k0, jc, kbsz, jb);
+    __syncthreads();
+    mma_tile_sub(S0, S1, jb, acc);
+  }
 #pragma unroll
   for (int i = 0; i < AR; ++i)
 #pragma unroll
