@@ -421,33 +421,10 @@ __device__ void tiled_panel(const float2* M, double2* A, int64_t n, int j, int i
     }
 }
 
-// trailing block (i, k), j < k <= i: A_ik -= L_ij L_kj^H (lower triangle only when i == k)
-__device__ void tiled_update(const float2* M, double2* A, int64_t n, int j, int ib, int kb) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* S0 = reinterpret_cast<double2*>(smem_raw);
-  double2* S1 = S0 + CB * PITCH;
-  const int64_t j0 = (int64_t)j * CB, i0 = (int64_t)ib * CB, k0 = (int64_t)kb * CB;
-  const int jb = (int)(CB < (n - j0) ? (int64_t)CB : (n - j0));
-  const int rb = (int)(CB < (n - i0) ? (int64_t)CB : (n - i0));
-  const int kbsz = (int)(CB < (n - k0) ? (int64_t)CB : (n - k0));
-  load_blk(S0, A, n, i0, j0, rb, jb);
-  load_blk(S1, A, n, k0, j0, kbsz, jb);
-  double2 acc[AR][AC];
-  acc_init(acc, A, M, j == 0, n, i0, k0, rb, kbsz, ib > kb);
-  __syncthreads();
-  mma_tile_sub(S0, S1, jb, acc);
-#pragma unroll
-  for (int i = 0; i < AR; ++i)
-#pragma unroll
-    for (int jj = 0; jj < AC; ++jj) {
-      const int r = acc_row(i, jj), c = acc_col(i, jj);
-      if (r < rb && c < kbsz && (ib > kb || c <= r)) A[(i0 + r) * n + k0 + c] = acc[i][jj];
-    }
-}
-
-// tiled_update for the block columns j .. j + cols - 1 at once: the same rank-CB updates in
-// the same order, with the block held in FP64 registers in between rather than stored and
-// reloaded, so the block is read and written once for all of them.
+// Trailing update of block (ib, kb) by the block columns j .. j + cols - 1 (lower triangle
+// only when ib == kb): A_ik -= sum_c L_ic L_kc^H, the rank-CB products one column at a time,
+// with the block held in FP64 registers in between rather than stored and reloaded, so the
+// block is read and written once for all of them.
 __device__ void tiled_update_cols(const float2* M, double2* A, int64_t n, int j, int cols, int ib,
                                   int kb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
