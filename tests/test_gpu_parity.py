@@ -130,6 +130,8 @@ def test_rpa_energy(base, mode, tol):
     (3, 8, 4, 36, 1e4),           # 27 k-points (3-point DFT lines)
     ((2, 1, 6), 8, 4, 24, 1e4),   # 6-point lines (Good-Thomas 2 x 3) on the inner edge
     (6, 4, 2, 16, 1e4),           # 216 k-points: the compile-time cubic edge 6
+    (3, 8, 4, 27, 1e4),           # register-plane kernels, 32-column tiles: 729 columns (odd, ragged last tile)
+    (6, 4, 2, 18, 1e4),           # register-plane kernels, 16-column tiles: 324 columns (ragged last tile)
     ((2, 8, 2), 6, 3, 20, 1e4),   # 8-point lines (radix 2) on the middle edge
     ((1, 5, 7), 6, 3, 20, 1e4),   # 5- and 7-point lines (plain sums)
 ])
